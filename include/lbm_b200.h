@@ -1,0 +1,228 @@
+/*
+ * lbm_b200.h -- C ABI of the B200 (sm_100a) Inamuro two-phase D3Q15 droplet
+ * time step.
+ *
+ * The reference (UniBoy222/LBM) exposes this path only as the C++ class
+ * InamuroCUDA (GPU/InamuroCUDA.hpp:16-248) built on a CPU-side Inamuro object
+ * (GPU/Inamuro.hpp:11-140).  This header is the flat boundary under the C++
+ * drop-in classes of lbm_b200/csrc/inamuro_cuda.hpp: plain pointers and sizes,
+ * integer status codes, no exceptions and no C++ or torch types.  Each entry
+ * point names the reference interface it replaces.
+ *
+ * Field layout (host and device): a field is lx*ly*lz doubles, x fastest,
+ * cell = (z*ly + y)*lx + x.  The "ghosted" variants use the reference's device
+ * layout with one z ghost plane on each side: lx*ly*(lz+2) doubles,
+ * ((z+1)*ly + y)*lx + x (GPU/InamuroCUDA.cu:1438, 1675-1696).
+ *
+ * A handle owns its device buffers and one CUDA stream; it is used by one host
+ * thread at a time.  Every call is synchronous with respect to the host unless
+ * stated otherwise.
+ */
+#ifndef LBM_B200_H
+#define LBM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM_B200_ABI_VERSION 1
+
+typedef enum {
+    LBM_OK = 0,
+    LBM_ERR_CUDA = 1,            /* CUDA runtime error (reference: CUDA_CHECK -> runtime_error, .cu:12-18) */
+    LBM_ERR_NONFINITE = 2,       /* NaN/Inf in source, gauge or residual (reference .cu:1888-2125 throws) */
+    LBM_ERR_POISSON_BUDGET = 3,  /* sweep cap reached without convergence */
+    LBM_ERR_BAD_ARG = 4,         /* invalid argument (reference: std::invalid_argument) */
+    LBM_ERR_OOM = 5,             /* device allocation failed */
+    LBM_ERR_IO = 6,              /* params file missing or unreadable */
+    LBM_ERR_NO_DEVICE = 7,       /* no CUDA device or not sm_100 */
+    LBM_ERR_OVERFLOW = 8         /* counter overflow (reference .cu:21-45) */
+} lbm_status;
+
+typedef enum {
+    LBM_PRECISION_FP64 = 0,      /* plain FP64, reference operation order: the drop-in */
+    LBM_PRECISION_MIXED = 1      /* FP32 populations as deviations + FP64 reductions */
+} lbm_precision;
+
+typedef enum {
+    LBM_FIELD_PHI = 0, LBM_FIELD_RHO = 1, LBM_FIELD_U = 2,
+    LBM_FIELD_V = 3, LBM_FIELD_W = 4, LBM_FIELD_P = 5
+} lbm_field;
+
+/* params.in contents (CPU/Inamuro.cpp:38-53 positional lines, GPU/Inamuro.cpp:56-103
+ * key=value init tokens; struct of GPU/Inamuro.hpp:36-76). */
+typedef struct {
+    int lx, ly, lz;              /* line 1 */
+    int period;                  /* line 2 (read, unused by the step) */
+    int t_max;                   /* line 3 */
+    int nwri;                    /* line 4 */
+    double rho_L, rho_G;         /* line 5 */
+    double tauf, taug;           /* line 6 */
+    double mu_L, mu_G;           /* line 7 */
+    double k_f, k_g;             /* line 8 */
+    double T;                    /* line 9 */
+    double a;                    /* line 10 */
+    double b;                    /* line 11 */
+    double fei_max, fei_min;     /* line 12 */
+    double fei_L, fei_G;         /* line 13 */
+    double DD;                   /* line 14 */
+    /* GPU-tree initial-condition tokens (defaults of GPU/Inamuro.hpp:56-64) */
+    int init_single_droplet;     /* init_mode=single_droplet (else two_droplets) */
+    int init_tanh;               /* init_profile=tanh (else sharp) */
+    double init_velocity;
+    double interface_width;
+    double init_center_x, init_center_y, init_center_z;
+    double init_separation;
+    double init_offset_x;
+} lbm_params;
+
+/* Poisson stopping rule (InamuroCUDA::setPoissonConvergence /
+ * setPoissonIterationLimit / setUsePoissonDualResidual, GPU/InamuroCUDA.hpp:83-86). */
+typedef struct {
+    int check_interval;          /* sweeps between checks; reference contract 100 */
+    double tolerance;            /* relative-change (and dual) tolerance; contract 1e-3 */
+    int dual_residual;           /* 1: also require the kinetic fixed-point residual < tol */
+    uint64_t max_sweeps;         /* 0 = unbounded (contract); else the iteration limit */
+    int fail_on_limit;           /* 0: at the limit stop and finish the step unconverged, as
+                                    the reference's poisson_iteration_limit does (.cu:2336-2339);
+                                    1: return LBM_ERR_POISSON_BUDGET instead */
+} lbm_poisson_cfg;
+
+/* Per-step diagnostics (InamuroCUDA::PoissonStepDiagnostics, GPU/InamuroCUDA.hpp:19-43,
+ * plus the step's mass and device time). */
+typedef struct {
+    uint64_t iterations;
+    double relative_error;
+    double pressure_l1_delta;
+    double pressure_l1_norm;
+    double fixed_point_h_l1;
+    double fixed_point_h_scale;
+    double fixed_point_h_relative;
+    double fixed_point_p_l1;
+    double fixed_point_p_scale;
+    double fixed_point_p_relative;
+    double fixed_point_relative;
+    double source_mean;              /* -mean(div)/3, as the reference reports it */
+    double source_abs_mean;
+    double projected_source_mean;
+    double pressure_gauge_target;
+    double pressure_gauge_max_shift;
+    double mass;                     /* sum of phi over the box after the step */
+    int fixed_point_evaluated;
+    int pressure_converged;
+    int fixed_point_converged;
+    int dual_residual_enabled;
+    int converged;
+    int reserved;
+    double device_ms;                /* device time of the step (CUDA events) */
+} lbm_step_stats;
+
+/* Accumulated device time per kernel class since the last reset (CUDA events
+ * on the handle's stream; replaces printPerformanceMetrics' per-phase timers,
+ * GPU/InamuroCUDA.cu:2377-2437). */
+typedef struct {
+    double collide_ms;       /* fused stencils + collide + stream of f, g */
+    double moments_ms;       /* pull + bounce + phi, rho, u* */
+    double prep_ms;          /* source projection + gauge target */
+    double poisson_ms;       /* all Poisson segments (sweeps + checks) */
+    double correct_ms;       /* velocity correction */
+    uint64_t steps;
+    uint64_t sweeps;         /* Poisson sweeps summed over steps */
+    uint64_t sweep_kernels;  /* sweep-kernel launches (incl. the extra one per check) */
+} lbm_timing;
+
+typedef struct lbm_handle lbm_handle;
+
+/* ---- params and initial condition (host only, no GPU needed) ---- */
+
+/* Reference defaults (GPU/Inamuro.hpp:36-76, box 48x96x128). */
+void lbm_params_default(lbm_params* out);
+
+/* Parses params.in: 14 positional lines (CPU/Inamuro.cpp:38-53), then both the
+ * whitespace-token init keys (GPU/Inamuro.cpp:56-103) and the line-wise
+ * key=value output keys (ignored here; CPU/InamuroSolver.cpp:143-218).
+ * Replaces Inamuro::Parameters::Parameters(const std::string&). */
+lbm_status lbm_params_load(const char* path, lbm_params* out);
+
+/* Droplet initial condition of Inamuro::initializeDroplets (GPU/Inamuro.cpp:491-566)
+ * written into physical-layout host fields (each lx*ly*lz doubles): phi, rho,
+ * u, v, w, p.  Replaces Inamuro::initializeArrays + initializeDroplets. */
+lbm_status lbm_init_droplets(const lbm_params* prm, double* phi, double* rho,
+                             double* u, double* v, double* w, double* p);
+
+/* ---- solver handle ---- */
+
+/* Allocates the device state for one box on `device` (replaces the
+ * InamuroCUDA(const Inamuro&) constructor's allocateDeviceMemory,
+ * GPU/InamuroCUDA.cu:1429-1461, 1536-1607).  Fields start at the background
+ * state; load them with lbm_load_fields*.  Poisson config starts at the
+ * reference contract {100, 1e-3, dual=0, unbounded}. */
+lbm_status lbm_create(const lbm_params* prm, lbm_precision precision, int device,
+                      lbm_handle** out);
+void lbm_destroy(lbm_handle* h);
+
+/* Host -> device upload of the macro fields; resets the step counter so the
+ * next step is a "first step" (f, g set to equilibrium).  p may be NULL (zero).
+ * Replaces InamuroCUDA::initFromCPU (GPU/InamuroCUDA.cu:1628-1673). */
+lbm_status lbm_load_fields(lbm_handle* h, const double* phi, const double* rho,
+                           const double* u, const double* v, const double* w,
+                           const double* p);
+/* Same with ghosted (lx*ly*(lz+2)) arrays; the ghost planes are kept and given
+ * back unchanged by lbm_download_ghosted, as the reference does. */
+lbm_status lbm_load_fields_ghosted(lbm_handle* h, const double* phi, const double* rho,
+                                   const double* u, const double* v, const double* w,
+                                   const double* p);
+/* Device -> device upload (pointers to device memory on the handle's device). */
+lbm_status lbm_load_fields_device(lbm_handle* h, const double* phi, const double* rho,
+                                  const double* u, const double* v, const double* w,
+                                  const double* p);
+
+/* InamuroCUDA::setPoissonConvergence / setPoissonIterationLimit /
+ * setUsePoissonDualResidual (GPU/InamuroCUDA.cu:2573-2608). */
+lbm_status lbm_set_poisson(lbm_handle* h, const lbm_poisson_cfg* cfg);
+lbm_status lbm_get_poisson(const lbm_handle* h, lbm_poisson_cfg* cfg);
+
+/* Advances n_steps time steps (InamuroCUDA::performTimeStepGPU,
+ * GPU/InamuroCUDA.cu:2372-2442).  `stats` (may be NULL) receives n_steps
+ * entries.  On error the state is left as of the failing step. */
+lbm_status lbm_step(lbm_handle* h, int n_steps, lbm_step_stats* stats);
+
+/* Like lbm_step, but every step runs exactly sweeps[i] Poisson sweeps (a
+ * multiple of the check interval); checks, gauges and p_prev updates still run
+ * at every check.  Used to compare two precisions on identical sweep counts. */
+lbm_status lbm_step_replay(lbm_handle* h, int n_steps, const uint64_t* sweeps,
+                           lbm_step_stats* stats);
+
+/* Device -> host download of one field (physical layout). */
+lbm_status lbm_download(lbm_handle* h, lbm_field which, double* host);
+/* Ghosted layout, ghost planes as loaded (InamuroCUDA::downloadFieldsToCPU,
+ * GPU/InamuroCUDA.cu:1675-1701). */
+lbm_status lbm_download_ghosted(lbm_handle* h, lbm_field which, double* host_ghosted);
+/* h populations in the reference's AoS layout cell*15+q, 15*lx*ly*lz doubles
+ * (InamuroCUDA::downloadHH, GPU/InamuroCUDA.cu:1703-1707).  Between steps
+ * h = E_q p, as after update_hh. */
+lbm_status lbm_download_h(lbm_handle* h, double* host);
+/* Device pointer of a field (physical layout, FP64 handles only, valid until
+ * the next call on the handle).  For device-resident consumers. */
+lbm_status lbm_field_device_ptr(lbm_handle* h, lbm_field which, const double** dev);
+
+/* InamuroCUDA::synchronize (GPU/InamuroCUDA.cu:1709-1712). */
+lbm_status lbm_synchronize(lbm_handle* h);
+
+lbm_status lbm_get_timing(const lbm_handle* h, lbm_timing* out);
+lbm_status lbm_reset_timing(lbm_handle* h);
+/* Enables per-kernel-class CUDA-event timing (default on). */
+lbm_status lbm_set_timing(lbm_handle* h, int enabled);
+
+/* Text of the last error on this handle ("" if none); valid until the next call. */
+const char* lbm_last_error(const lbm_handle* h);
+const char* lbm_status_string(lbm_status s);
+int lbm_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LBM_B200_H */

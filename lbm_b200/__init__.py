@@ -1,0 +1,341 @@
+"""lbm_b200 -- B200 (sm_100a) Inamuro two-phase D3Q15 droplet step.
+
+Python view of the C ABI in include/lbm_b200.h (ctypes over the in-tree
+liblbm_b200.so).  The class `InamuroCUDA` mirrors the reference's C++ class of
+the same name (GPU/InamuroCUDA.hpp:16-91): construct from parameters and
+initial fields, `perform_time_step_gpu()`, `download_fields()`,
+`download_hh()`, `synchronize()`, `last_poisson_diagnostics`, and the Poisson
+convergence setters.  Failures raise `LBMError` (the reference throws
+std::runtime_error / std::invalid_argument).
+
+There is no CPU fallback: without the CUDA library or an sm_100 GPU every
+solver call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblbm_b200.so")
+HEADER_PATH = os.path.join(os.path.dirname(HERE), "include", "lbm_b200.h")
+
+FIELDS = ("phi", "rho", "u", "v", "w", "p")
+FIELD_ID = {k: i for i, k in enumerate(FIELDS)}
+
+STATUS = {0: "LBM_OK", 1: "LBM_ERR_CUDA", 2: "LBM_ERR_NONFINITE", 3: "LBM_ERR_POISSON_BUDGET",
+          4: "LBM_ERR_BAD_ARG", 5: "LBM_ERR_OOM", 6: "LBM_ERR_IO", 7: "LBM_ERR_NO_DEVICE",
+          8: "LBM_ERR_OVERFLOW"}
+
+
+class Params(C.Structure):
+    """lbm_params: the params.in contents (GPU/Inamuro.hpp:36-76)."""
+    _fields_ = [("lx", C.c_int), ("ly", C.c_int), ("lz", C.c_int), ("period", C.c_int),
+                ("t_max", C.c_int), ("nwri", C.c_int)] + \
+        [(k, C.c_double) for k in ("rho_L", "rho_G", "tauf", "taug", "mu_L", "mu_G", "k_f", "k_g",
+                                    "T", "a", "b", "fei_max", "fei_min", "fei_L", "fei_G", "DD")] + \
+        [("init_single_droplet", C.c_int), ("init_tanh", C.c_int)] + \
+        [(k, C.c_double) for k in ("init_velocity", "interface_width", "init_center_x",
+                                    "init_center_y", "init_center_z", "init_separation",
+                                    "init_offset_x")]
+
+    @property
+    def shape(self):
+        return (self.lx, self.ly, self.lz)
+
+    def as_dict(self) -> Dict[str, float]:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class PoissonCfg(C.Structure):
+    _fields_ = [("check_interval", C.c_int), ("tolerance", C.c_double), ("dual_residual", C.c_int),
+                ("max_sweeps", C.c_uint64), ("fail_on_limit", C.c_int)]
+
+
+class StepStats(C.Structure):
+    """lbm_step_stats: InamuroCUDA::PoissonStepDiagnostics + mass + device time."""
+    _fields_ = [("iterations", C.c_uint64)] + \
+        [(k, C.c_double) for k in (
+            "relative_error", "pressure_l1_delta", "pressure_l1_norm",
+            "fixed_point_h_l1", "fixed_point_h_scale", "fixed_point_h_relative",
+            "fixed_point_p_l1", "fixed_point_p_scale", "fixed_point_p_relative",
+            "fixed_point_relative", "source_mean", "source_abs_mean", "projected_source_mean",
+            "pressure_gauge_target", "pressure_gauge_max_shift", "mass")] + \
+        [(k, C.c_int) for k in ("fixed_point_evaluated", "pressure_converged",
+                                 "fixed_point_converged", "dual_residual_enabled", "converged",
+                                 "reserved")] + [("device_ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Timing(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("collide_ms", "moments_ms", "prep_ms", "poisson_ms",
+                                           "correct_ms")] + \
+        [(k, C.c_uint64) for k in ("steps", "sweeps", "sweep_kernels")]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class LBMError(RuntimeError):
+    def __init__(self, status: int, message: str = ""):
+        name = STATUS.get(status, str(status))
+        super().__init__(f"{name}: {message}" if message else name)
+        self.status = status
+        self.name = name
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads liblbm_b200.so (raises if it was not built: no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise LBMError(7, f"CUDA library missing at {path}; run lbm_b200.build.build()")
+    L = C.CDLL(path)
+    dp = C.POINTER(C.c_double)
+    H = C.c_void_p
+    L.lbm_params_default.argtypes = [C.POINTER(Params)]
+    L.lbm_params_default.restype = None
+    L.lbm_params_load.argtypes = [C.c_char_p, C.POINTER(Params)]
+    L.lbm_init_droplets.argtypes = [C.POINTER(Params)] + [dp] * 6
+    L.lbm_create.argtypes = [C.POINTER(Params), C.c_int, C.c_int, C.POINTER(H)]
+    L.lbm_destroy.argtypes = [H]
+    L.lbm_destroy.restype = None
+    for name in ("lbm_load_fields", "lbm_load_fields_ghosted", "lbm_load_fields_device"):
+        getattr(L, name).argtypes = [H] + [C.c_void_p] * 6
+    L.lbm_set_poisson.argtypes = [H, C.POINTER(PoissonCfg)]
+    L.lbm_get_poisson.argtypes = [H, C.POINTER(PoissonCfg)]
+    L.lbm_step.argtypes = [H, C.c_int, C.POINTER(StepStats)]
+    L.lbm_step_replay.argtypes = [H, C.c_int, C.POINTER(C.c_uint64), C.POINTER(StepStats)]
+    L.lbm_download.argtypes = [H, C.c_int, dp]
+    L.lbm_download_ghosted.argtypes = [H, C.c_int, dp]
+    L.lbm_download_h.argtypes = [H, dp]
+    L.lbm_field_device_ptr.argtypes = [H, C.c_int, C.POINTER(C.c_void_p)]
+    L.lbm_synchronize.argtypes = [H]
+    L.lbm_get_timing.argtypes = [H, C.POINTER(Timing)]
+    L.lbm_reset_timing.argtypes = [H]
+    L.lbm_set_timing.argtypes = [H, C.c_int]
+    L.lbm_last_error.argtypes = [H]
+    L.lbm_last_error.restype = C.c_char_p
+    L.lbm_status_string.argtypes = [C.c_int]
+    L.lbm_status_string.restype = C.c_char_p
+    L.lbm_abi_version.restype = C.c_int
+    _lib = L
+    return L
+
+
+def header_functions(path: str = HEADER_PATH) -> List[str]:
+    """Names of the functions declared in include/lbm_b200.h."""
+    text = open(path).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(lbm_[a-z0-9_]+)\s*\(", text)))
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def params_default() -> Params:
+    p = Params()
+    load_library().lbm_params_default(C.byref(p))
+    return p
+
+
+def params_load(path: str) -> Params:
+    """Parses a params.in file (Inamuro::Parameters(const std::string&))."""
+    p = Params()
+    st = load_library().lbm_params_load(str(path).encode(), C.byref(p))
+    if st != 0:
+        raise LBMError(st, f"cannot parse {path}")
+    return p
+
+
+def make_params(**kw) -> Params:
+    p = params_default()
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+def init_droplets(p: Params) -> Dict[str, np.ndarray]:
+    """Inamuro::initializeDroplets (GPU/Inamuro.cpp:491-566) on the host.
+    Returns phi, rho, u, v, w, p of shape (lz, ly, lx)."""
+    shape = (p.lz, p.ly, p.lx)
+    out = {k: np.empty(shape) for k in FIELDS}
+    st = load_library().lbm_init_droplets(C.byref(p), *[_dp(out[k]) for k in FIELDS])
+    if st != 0:
+        raise LBMError(st, "init_droplets")
+    return out
+
+
+PRECISION = {"fp64": 0, "mixed": 1}
+
+
+class InamuroCUDA:
+    """One box on one GPU (GPU/InamuroCUDA.hpp:16-91)."""
+
+    def __init__(self, params: Params, fields: Optional[Dict[str, np.ndarray]] = None,
+                 precision: str = "fp64", device: int = 0):
+        self._lib = load_library()
+        self.params = params
+        self.shape = (params.lz, params.ly, params.lx)
+        self.precision = precision
+        h = C.c_void_p()
+        st = self._lib.lbm_create(C.byref(params), PRECISION[precision], device, C.byref(h))
+        if st != 0:
+            raise LBMError(st, "lbm_create")
+        self._h = h
+        self.last_poisson_diagnostics: Dict[str, float] = {}
+        if fields is not None:
+            self.load_fields(fields)
+
+    # -- errors ----------------------------------------------------------
+    def _check(self, st: int, what: str):
+        if st != 0:
+            msg = self._lib.lbm_last_error(self._h)
+            raise LBMError(st, f"{what}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.lbm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- state transfer ---------------------------------------------------
+    def _arrs(self, fields, ghosted=False):
+        shape = (self.shape[0] + 2,) + self.shape[1:] if ghosted else self.shape
+        out = []
+        for k in FIELDS:
+            a = fields.get(k)
+            if a is None:
+                out.append(None)
+                continue
+            a = np.ascontiguousarray(a, dtype=np.float64).reshape(shape)
+            out.append(a)
+        return out
+
+    def load_fields(self, fields: Dict[str, np.ndarray]):
+        """InamuroCUDA::initFromCPU: uploads phi, rho, u, v, w (and p)."""
+        arrs = self._arrs(fields)
+        self._keep = arrs
+        ptrs = [None if a is None else a.ctypes.data for a in arrs]
+        self._check(self._lib.lbm_load_fields(self._h, *ptrs), "load_fields")
+
+    def load_fields_ghosted(self, fields: Dict[str, np.ndarray]):
+        arrs = self._arrs(fields, ghosted=True)
+        self._check(self._lib.lbm_load_fields_ghosted(self._h, *[a.ctypes.data for a in arrs]),
+                    "load_fields_ghosted")
+
+    def load_fields_device(self, ptrs: Sequence[int]):
+        """Device pointers (ints) of phi, rho, u, v, w, p on this handle's GPU."""
+        self._check(self._lib.lbm_load_fields_device(self._h, *ptrs), "load_fields_device")
+
+    def download(self, name: str, out: Optional[np.ndarray] = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.shape)
+        self._check(self._lib.lbm_download(self._h, FIELD_ID[name], _dp(out)), "download")
+        return out
+
+    def download_fields(self) -> Dict[str, np.ndarray]:
+        """InamuroCUDA::downloadFieldsToCPU (physical layout)."""
+        return {k: self.download(k) for k in FIELDS}
+
+    def download_ghosted(self, name: str) -> np.ndarray:
+        out = np.empty((self.shape[0] + 2,) + self.shape[1:])
+        self._check(self._lib.lbm_download_ghosted(self._h, FIELD_ID[name], _dp(out)), "download_ghosted")
+        return out
+
+    def download_hh(self) -> np.ndarray:
+        """InamuroCUDA::downloadHH: AoS cell*15+q."""
+        out = np.empty(15 * int(np.prod(self.shape)))
+        self._check(self._lib.lbm_download_h(self._h, _dp(out)), "download_hh")
+        return out
+
+    def device_ptr(self, name: str) -> int:
+        p = C.c_void_p()
+        self._check(self._lib.lbm_field_device_ptr(self._h, FIELD_ID[name], C.byref(p)), "device_ptr")
+        return p.value
+
+    def synchronize(self):
+        self._check(self._lib.lbm_synchronize(self._h), "synchronize")
+
+    # -- Poisson configuration --------------------------------------------
+    def set_poisson(self, check_interval: int = 100, tolerance: float = 1e-3, dual: bool = False,
+                    max_sweeps: int = 0, fail_on_limit: bool = False):
+        cfg = PoissonCfg(check_interval, tolerance, int(dual), max_sweeps, int(fail_on_limit))
+        self._check(self._lib.lbm_set_poisson(self._h, C.byref(cfg)), "set_poisson")
+
+    # reference setter names (GPU/InamuroCUDA.hpp:83-86)
+    def set_poisson_convergence(self, check_interval: int, tolerance: float):
+        cfg = self.poisson_config()
+        self.set_poisson(check_interval, tolerance, cfg["dual_residual"], cfg["max_sweeps"],
+                         cfg["fail_on_limit"])
+
+    def set_use_poisson_dual_residual(self, enabled: bool):
+        cfg = self.poisson_config()
+        self.set_poisson(cfg["check_interval"], cfg["tolerance"], enabled, cfg["max_sweeps"],
+                         cfg["fail_on_limit"])
+
+    def set_poisson_iteration_limit(self, max_iterations: int):
+        cfg = self.poisson_config()
+        self.set_poisson(cfg["check_interval"], cfg["tolerance"], cfg["dual_residual"],
+                         max_iterations, cfg["fail_on_limit"])
+
+    def poisson_config(self) -> Dict[str, float]:
+        cfg = PoissonCfg()
+        self._check(self._lib.lbm_get_poisson(self._h, C.byref(cfg)), "get_poisson")
+        return {k: getattr(cfg, k) for k, _ in cfg._fields_}
+
+    # -- stepping ---------------------------------------------------------
+    def step(self, n: int = 1) -> List[Dict[str, float]]:
+        stats = (StepStats * max(n, 1))()
+        self._check(self._lib.lbm_step(self._h, n, stats), "step")
+        out = [s.as_dict() for s in stats[:n]]
+        if out:
+            self.last_poisson_diagnostics = out[-1]
+        return out
+
+    def perform_time_step_gpu(self) -> Dict[str, float]:
+        """InamuroCUDA::performTimeStepGPU."""
+        return self.step(1)[0]
+
+    def step_replay(self, sweeps: Sequence[int]) -> List[Dict[str, float]]:
+        n = len(sweeps)
+        arr = (C.c_uint64 * n)(*sweeps)
+        stats = (StepStats * max(n, 1))()
+        self._check(self._lib.lbm_step_replay(self._h, n, arr, stats), "step_replay")
+        return [s.as_dict() for s in stats[:n]]
+
+    # -- timing -----------------------------------------------------------
+    def timing(self) -> Dict[str, float]:
+        t = Timing()
+        self._check(self._lib.lbm_get_timing(self._h, C.byref(t)), "timing")
+        return t.as_dict()
+
+    def reset_timing(self):
+        self._check(self._lib.lbm_reset_timing(self._h), "reset_timing")
+
+    def set_timing(self, enabled: bool):
+        self._check(self._lib.lbm_set_timing(self._h, int(enabled)), "set_timing")

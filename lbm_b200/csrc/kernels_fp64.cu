@@ -1,0 +1,661 @@
+// kernels_fp64.cu -- plain FP64 kernels of the Inamuro D3Q15 step (the
+// drop-in precision).
+//
+// Compiled with -fmad=false: every expression keeps the reference's operand
+// order and rounding (no FMA contraction), so per-cell arithmetic is that of
+// the reference CPU build; only sin() (CUDA vs libm) and the order of global
+// sums differ.
+//
+// Storage between kernels is the POST-COLLISION population (stream-collide
+// form): each kernel pulls x - c_q from the previous kernel's output, applies
+// the x slip overwrite in registers, uses the populations and writes its own
+// collision result at the cell itself.  Pull reads and aligned writes are
+// both coalesced along x; no population is read twice in one kernel.
+//
+// Kernel <-> reference map
+//   collide        gradientKernel x5 + laplacianKernel x4 + collisionKernel +
+//                  streamKernel x2 + slipBounceBackKernel x2 of the NEXT pull
+//                  (GPU/InamuroCUDA.cu:203-451, 462-493, 1399-1425);
+//                  CPU/Inamuro.cpp:134-250
+//   moments        macroKernel (.cu:136-192); CPU/Inamuro.cpp:294-346
+//   prep           sourceStatsBlockKernel + projectSourceMeanKernel +
+//                  pressureSumBlockKernel (.cu:627-714); CPU/Inamuro.cpp:652-668
+//   poisson_init   updateHHKernel + first collisionPressureKernel (.cu:503-537,
+//                  1377-1396); CPU/Inamuro.cpp:755-778, 825-840
+//   sweep          streamKernel + slipBounceBackKernel + computePressureKernel
+//                  of sweep k and collisionPressureKernel of sweep k+1
+//   sweep_check_a  sweep k's stream + bounce + getp at a check, plus sum(p)
+//   sweep_check_b  applyPressureGaugeKernel + pressureErrorBlockKernel + the
+//                  R_p terms of fixedPointResidualBlockKernel + collision of
+//                  sweep k+1 (.cu:716-730, 1062-1171, 1977-2159)
+//   sweep_check_c  the shadow map F = BS[C(h,p)] compared with h (R_h terms)
+//                  fused with sweep k+1's stream/bounce/sum and k+2's collision
+//   correct        correctVelocityKernel (.cu:1330-1371); CPU/Inamuro.cpp:794-823
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#include "lbm_solver.cuh"
+
+namespace lbm {
+namespace {
+
+__device__ __forceinline__ bool tile_coords(const Geom& g, int& x, int& y, int& z)
+{
+    x = blockIdx.x * blockDim.x + threadIdx.x;
+    y = blockIdx.y * blockDim.y + threadIdx.y;
+    z = blockIdx.z;
+    return x < g.lx && y < g.ly;
+}
+
+// x slip overwrite of pulled populations (CPU/Inamuro.cpp:589-623).
+template <class T>
+__device__ __forceinline__ void bounce_regs(T (&v)[Q], const Geom& g, int x)
+{
+    if (g.periodic_x) return;
+    if (x == 0) {
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            if constexpr (bounce_left(q) != q) v[q] = v[bounce_left(q)];
+        });
+    }
+    if (x == g.lx - 1) {
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            if constexpr (bounce_right(q) != q) v[q] = v[bounce_right(q)];
+        });
+    }
+}
+
+template <class T>
+__device__ __forceinline__ void pull_regs(T (&v)[Q], const T* __restrict__ src, const Geom& g,
+                                          int x, int y, int z)
+{
+    const Wrap w(g, x, y, z);
+    static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        v[q] = __ldg(src + (long long)q * g.n + pull_src<q>(g, w, x, y, z));
+    });
+}
+
+// firstord + (optionally) secondord of one field at one cell:
+// CPU/Inamuro.hpp:213-314.  Accumulation order k = 1..14 as in the reference.
+template <bool kLap>
+__device__ __forceinline__ void stencil(const double* __restrict__ f, const Geom& g, const Mirror& m,
+                                        int x, int y, int z, long long c,
+                                        double& gx, double& gy, double& gz, double& lap)
+{
+    double ax = 0.0, ay = 0.0, az = 0.0, al = 0.0;
+    static_for<1, Q>([&](auto kc) {
+        constexpr int k = decltype(kc)::value;
+        const double val = __ldg(f + stencil_nb<k>(g, m, x, y, z));
+        ax = acc_signed<cx(k)>(ax, val);
+        ay = acc_signed<cy(k)>(ay, val);
+        az = acc_signed<cz(k)>(az, val);
+        if constexpr (kLap) al = al + val;
+    });
+    gx = ax / 10.0;
+    gy = ay / 10.0;
+    gz = az / 10.0;
+    if constexpr (kLap) lap = (al - 14.0 * __ldg(f + c)) / 5.0;
+}
+
+// Fused collide (+ the pull of the previous collision's output).
+template <bool kFirst>
+__global__ void __launch_bounds__(256)
+collide_kernel(Geom g, Phys P, const double* __restrict__ fin, double* __restrict__ fout,
+               const double* __restrict__ gin, double* __restrict__ gout,
+               const double* __restrict__ phi, const double* __restrict__ rho,
+               const double* __restrict__ u, const double* __restrict__ v,
+               const double* __restrict__ w, double* __restrict__ dux,
+               double* __restrict__ dvy, double* __restrict__ dwz, double* __restrict__ part,
+               long long nblocks)
+{
+    int x, y, z;
+    const bool active = tile_coords(g, x, y, z);
+    double red[3] = {0.0, 0.0, 0.0};
+    if (active) {
+        const long long c = cell_of(g, x, y, z);
+        const Mirror m(g, x, y, z);
+        double u_x, u_y, u_z, v_x, v_y, v_z, w_x, w_y, w_z;
+        double r_x, r_y, r_z, f_x, f_y, f_z;
+        double u_lap, v_lap, w_lap, f_lap, unused;
+        stencil<true>(u, g, m, x, y, z, c, u_x, u_y, u_z, u_lap);
+        stencil<true>(v, g, m, x, y, z, c, v_x, v_y, v_z, v_lap);
+        stencil<true>(w, g, m, x, y, z, c, w_x, w_y, w_z, w_lap);
+        stencil<false>(rho, g, m, x, y, z, c, r_x, r_y, r_z, unused);
+        stencil<true>(phi, g, m, x, y, z, c, f_x, f_y, f_z, f_lap);
+        (void)unused;
+        dux[c] = u_x;
+        dvy[c] = v_y;
+        dwz[c] = w_z;
+        const double div = u_x + v_y + w_z;
+        if (isfinite(div)) {
+            red[0] = div;
+            red[1] = fabs(div);
+        } else {
+            red[2] = 1.0;
+        }
+
+        const double lrho = __ldg(rho + c), fei = __ldg(phi + c);
+        const double uu = __ldg(u + c), vv = __ldg(v + c), ww = __ldg(w + c);
+        const double mu = (lrho - P.rho_G) * P.mu_slope + P.mu_G;
+        const double sum_fei = f_x * f_x + f_y * f_y + f_z * f_z;
+        const double sum_rho = r_x * r_x + r_y * r_y + r_z * r_z;
+        const double usq = uu * uu + vv * vv + ww * ww;
+        const double p0 = fei * P.T / (1.0 - P.b * fei) - P.a * fei * fei;
+        const double chem = p0 - P.k_f * fei * f_lap - P.k_f * sum_fei / 6.0;
+
+        // ---- f: order parameter ----
+        double fv[Q];
+        if constexpr (!kFirst) {
+            pull_regs(fv, fin, g, x, y, z);
+            bounce_regs(fv, g, x);
+        }
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            constexpr double E = wE(q), F = wF(q);
+            const double un = dotq<q>(uu, vv, ww);
+            const double fe = dotq<q>(f_x, f_y, f_z);
+            double Gfei = 4.5 * (fe * fe);
+            if constexpr (csq(q) == 1) Gfei = Gfei - 1.5 * sum_fei;
+            if constexpr (csq(q) == 3) Gfei = Gfei - 1.5 * sum_fei * 3.0;
+            double fequ;
+            if constexpr (q == 0) {
+                fequ = fei + F * chem;
+            } else {
+                fequ = F * chem + 3.0 * E * fei * un + E * P.k_f * Gfei;
+            }
+            double out;
+            if constexpr (kFirst) {
+                out = fequ;
+            } else {
+                const double d = fv[q] - fequ;
+                out = fv[q] - (P.tauf_pow2 ? d * P.inv_tauf : d / P.tauf);
+            }
+            fout[(long long)q * g.n + c] = out;
+        });
+
+        // ---- g: predicted velocity ----
+        double gv[Q];
+        if constexpr (!kFirst) {
+            pull_regs(gv, gin, g, x, y, z);
+            bounce_regs(gv, g, x);
+        }
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            constexpr double E = wE(q), F = wF(q);
+            constexpr int X = cx(q), Y = cy(q), Z = cz(q);
+            const double un = dotq<q>(uu, vv, ww);
+            double gequ;
+            if constexpr (q == 0) {
+                // un = 0, grad terms vanish: E*(1 - 1.5 usq) - (2/3 F k_g / rho) sum_rho
+                const double velPart = 1.0 - 1.5 * usq;
+                gequ = E * velPart - 2.0 / 3.0 * F * P.k_g / lrho * sum_rho;
+            } else {
+                // c_a c_b (d_b u_a) summed in the reference's 9-term order
+                double S = 0.0;
+                bool started = false;
+                auto addt = [&](int coef, double val) {
+                    if (coef == 0) return;
+                    if (!started) { S = coef > 0 ? val : -val; started = true; }
+                    else S = coef > 0 ? S + val : S - val;
+                };
+                addt(X * X, u_x); addt(X * Y, u_y); addt(X * Z, u_z);
+                addt(Y * X, v_x); addt(Y * Y, v_y); addt(Y * Z, v_z);
+                addt(Z * X, w_x); addt(Z * Y, w_y); addt(Z * Z, w_z);
+                const double velPart = 1.0 + 3.0 * un - 1.5 * usq + 4.5 * un * un + P.visc * S;
+                const double re = dotq<q>(r_x, r_y, r_z);
+                double Grho = 4.5 * (re * re);
+                if constexpr (csq(q) == 1) Grho = Grho - 1.5 * sum_rho;
+                if constexpr (csq(q) == 3) Grho = Grho - 1.5 * sum_rho * 3.0;
+                gequ = E * velPart + E * P.k_g / lrho * Grho - 2.0 / 3.0 * F * P.k_g / lrho * sum_rho;
+            }
+            double out;
+            if constexpr (kFirst) {
+                out = gequ;
+            } else {
+                const double d = gv[q] - gequ;
+                out = gv[q] - (P.taug_pow2 ? d * P.inv_taug : d / P.taug);
+                if constexpr (q != 0) {
+                    const double lapdot = dotq<q>(u_lap, v_lap, w_lap);
+                    out = out + 3.0 * E / lrho * mu * lapdot;
+                }
+            }
+            gout[(long long)q * g.n + c] = out;
+        });
+    }
+    block_sum_store<3>(red, part, nblocks, block_linear());
+}
+
+__global__ void __launch_bounds__(256)
+moments_kernel(Geom g, Phys P, const double* __restrict__ f, const double* __restrict__ gp,
+               double* __restrict__ phi, double* __restrict__ rho, double* __restrict__ u,
+               double* __restrict__ v, double* __restrict__ w, double* __restrict__ part,
+               long long nblocks)
+{
+    int x, y, z;
+    const bool active = tile_coords(g, x, y, z);
+    double red[1] = {0.0};
+    if (active) {
+        const long long c = cell_of(g, x, y, z);
+        double fv[Q];
+        pull_regs(fv, f, g, x, y, z);
+        bounce_regs(fv, g, x);
+        double fei = 0.0;
+        static_for<0, Q>([&](auto qc) { fei = fei + fv[decltype(qc)::value]; });
+        double density;
+        if (fei <= P.fei_G) {
+            density = P.rho_G;
+        } else if (fei >= P.fei_L) {
+            density = P.rho_L;
+        } else {
+            const double arg = (fei - P.fei_avg) / P.dfei * CUDART_PI;
+            density = P.half_drho * (sin(arg) + 1.0) + P.rho_G;
+        }
+        double gv[Q];
+        pull_regs(gv, gp, g, x, y, z);
+        bounce_regs(gv, g, x);
+        double uu = 0.0, vv = 0.0, ww = 0.0;
+        static_for<1, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            uu = acc_signed<cx(q)>(uu, gv[q]);
+            vv = acc_signed<cy(q)>(vv, gv[q]);
+            ww = acc_signed<cz(q)>(ww, gv[q]);
+        });
+        phi[c] = fei;
+        rho[c] = density;
+        u[c] = uu;
+        v[c] = vv;
+        w[c] = ww;
+        red[0] = fei;
+    }
+    block_sum_store<1>(red, part, nblocks, block_linear());
+}
+
+__global__ void __launch_bounds__(256)
+prep_kernel(Geom g, const DevState* __restrict__ ds, const double* __restrict__ dux,
+            const double* __restrict__ dvy, const double* __restrict__ dwz,
+            const double* __restrict__ p, double* __restrict__ s, double* __restrict__ part,
+            long long nblocks)
+{
+    int x, y, z;
+    const bool active = tile_coords(g, x, y, z);
+    double red[3] = {0.0, 0.0, 0.0};
+    if (active) {
+        const long long c = cell_of(g, x, y, z);
+        const double m = ds->div_mean;
+        // u_x -= mean (CPU/Inamuro.cpp:665-668), then u_x + v_y + w_z.
+        const double sv = (dux[c] - m) + dvy[c] + dwz[c];
+        s[c] = sv;
+        if (isfinite(sv)) red[0] = sv; else red[1] = 1.0;
+        red[2] = p[c];
+    }
+    block_sum_store<3>(red, part, nblocks, block_linear());
+}
+
+__global__ void __launch_bounds__(256)
+poisson_init_kernel(Geom g, int h_loaded, const double* __restrict__ hload,
+                    double* __restrict__ hout, const double* __restrict__ p,
+                    const double* __restrict__ rho, const double* __restrict__ s)
+{
+    int x, y, z;
+    if (!tile_coords(g, x, y, z)) return;
+    const long long c = cell_of(g, x, y, z);
+    const double pv = p[c];
+    const double tauh = 1.0 / rho[c] + 0.5;
+    const double sv = s[c];
+    static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        constexpr double E = wE(q);
+        // h = p * E_q after update_hh (CPU/Inamuro.cpp:835), or the loaded h.
+        const double h0 = h_loaded ? hload[(long long)q * g.n + c] : pv * E;
+        const double hequ = E * pv;
+        hout[(long long)q * g.n + c] = h0 - (h0 - hequ) / tauh - (E / 3.0) * sv;
+    });
+}
+
+__device__ __forceinline__ void collide_h_store(const double (&hv)[Q], double pv, double tauh,
+                                                double sv, double* __restrict__ hout,
+                                                long long n, long long c)
+{
+    static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        constexpr double E = wE(q);
+        const double hequ = E * pv;
+        hout[(long long)q * n + c] = hv[q] - (hv[q] - hequ) / tauh - (E / 3.0) * sv;
+    });
+}
+
+__device__ __forceinline__ double sum_q(const double (&hv)[Q])
+{
+    double acc = 0.0;
+    static_for<0, Q>([&](auto qc) { acc = acc + hv[decltype(qc)::value]; });
+    return acc;
+}
+
+__global__ void __launch_bounds__(256)
+sweep_kernel(Geom g, const double* __restrict__ hin, double* __restrict__ hout,
+             const double* __restrict__ rho, const double* __restrict__ s)
+{
+    int x, y, z;
+    if (!tile_coords(g, x, y, z)) return;
+    const long long c = cell_of(g, x, y, z);
+    double hv[Q];
+    pull_regs(hv, hin, g, x, y, z);
+    bounce_regs(hv, g, x);
+    const double pv = sum_q(hv);
+    const double tauh = 1.0 / __ldg(rho + c) + 0.5;
+    collide_h_store(hv, pv, tauh, __ldg(s + c), hout, g.n, c);
+}
+
+__global__ void __launch_bounds__(256)
+sweep_check_a_kernel(Geom g, const double* __restrict__ hin, double* __restrict__ hout,
+                     double* __restrict__ p_chk, double* __restrict__ part, long long nblocks)
+{
+    int x, y, z;
+    const bool active = tile_coords(g, x, y, z);
+    double red[1] = {0.0};
+    if (active) {
+        const long long c = cell_of(g, x, y, z);
+        double hv[Q];
+        pull_regs(hv, hin, g, x, y, z);
+        bounce_regs(hv, g, x);
+        const double pv = sum_q(hv);
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            hout[(long long)q * g.n + c] = hv[q];
+        });
+        p_chk[c] = pv;
+        red[0] = pv;
+    }
+    block_sum_store<1>(red, part, nblocks, block_linear());
+}
+
+template <bool kDual>
+__global__ void __launch_bounds__(256)
+sweep_check_b_kernel(Geom g, double* __restrict__ h, double* __restrict__ hc,
+                     const double* __restrict__ p_chk, double* __restrict__ p_prev,
+                     double* __restrict__ p, const double* __restrict__ rho,
+                     const double* __restrict__ s, const DevState* __restrict__ ds,
+                     double* __restrict__ part, long long nblocks)
+{
+    int x, y, z;
+    const bool active = tile_coords(g, x, y, z);
+    double red[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (active) {
+        const long long c = cell_of(g, x, y, z);
+        const double shift = ds->sigma;
+        const double tgt = ds->target;
+        double hv[Q];
+        // Gauge (CPU/Inamuro.cpp:699-705): p -= shift, h_q -= E_q shift.
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            hv[q] = h[(long long)q * g.n + c] - wE(q) * shift;
+        });
+        const double pv = p_chk[c] - shift;
+        if constexpr (kDual) {
+            static_for<0, Q>([&](auto qc) {
+                constexpr int q = decltype(qc)::value;
+                hc[(long long)q * g.n + c] = hv[q];
+            });
+            const double hsum = sum_q(hv);
+            red[2] = fabs(pv - hsum);
+            red[3] = fabs(pv - tgt);
+            red[4] = fabs(hsum - tgt);
+        }
+        // Relative change (CPU/Inamuro.cpp:726-753).
+        red[0] = fabs(pv - p_prev[c]);
+        red[1] = fabs(pv);
+        p_prev[c] = pv;
+        p[c] = pv;
+        const double tauh = 1.0 / __ldg(rho + c) + 0.5;
+        collide_h_store(hv, pv, tauh, __ldg(s + c), h, g.n, c);
+    }
+    block_sum_store<5>(red, part, nblocks, block_linear());
+}
+
+__global__ void __launch_bounds__(256)
+sweep_check_c_kernel(Geom g, const double* __restrict__ hin, double* __restrict__ hout,
+                     const double* __restrict__ hc, const double* __restrict__ rho,
+                     const double* __restrict__ s, const DevState* __restrict__ ds,
+                     double* __restrict__ part, long long nblocks)
+{
+    int x, y, z;
+    const bool active = tile_coords(g, x, y, z);
+    double red[3] = {0.0, 0.0, 0.0};
+    if (active) {
+        const long long c = cell_of(g, x, y, z);
+        const double tgt = ds->target;
+        double hv[Q];
+        pull_regs(hv, hin, g, x, y, z);
+        bounce_regs(hv, g, x);
+        // hv is F(h, p) = BS[C(h, p)] for the gauged h of the check
+        // (GPU/InamuroCUDA.cu:1997-2009); compare with that h.
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            const double hval = hc[(long long)q * g.n + c];
+            const double ge = wE(q) * tgt;
+            red[0] += fabs(hval - hv[q]);
+            red[1] += fabs(hval - ge);
+            red[2] += fabs(hv[q] - ge);
+        });
+        const double pv = sum_q(hv);
+        const double tauh = 1.0 / __ldg(rho + c) + 0.5;
+        collide_h_store(hv, pv, tauh, __ldg(s + c), hout, g.n, c);
+    }
+    block_sum_store<3>(red, part, nblocks, block_linear());
+}
+
+__global__ void __launch_bounds__(256)
+correct_kernel(Geom g, double* __restrict__ u, double* __restrict__ v, double* __restrict__ w,
+               const double* __restrict__ p, const double* __restrict__ rho)
+{
+    int x, y, z;
+    if (!tile_coords(g, x, y, z)) return;
+    const Mirror m(g, x, y, z);
+    const long long c = cell_of(g, x, y, z);
+    const double inv_2rho = 1.0 / (2.0 * rho[c]);
+    u[c] -= (p[cell_of(g, m.xp, y, z)] - p[cell_of(g, m.xm, y, z)]) * inv_2rho;
+    v[c] -= (p[cell_of(g, x, m.yp, z)] - p[cell_of(g, x, m.ym, z)]) * inv_2rho;
+    w[c] -= (p[cell_of(g, x, y, m.zp)] - p[cell_of(g, x, y, m.zm)]) * inv_2rho;
+}
+
+// ---- finalisation --------------------------------------------------------
+
+__device__ __forceinline__ double relative(double num, double den)
+{
+    if (den > 0.0) return num / den;
+    return num == 0.0 ? 0.0 : CUDART_INF;
+}
+
+// Sums `terms` columns of a [terms][nblocks] partials array in a fixed order:
+// thread t adds blocks t, t+1024, ... sequentially, then a fixed tree.
+template <int T>
+__device__ void reduce_partials(const double* __restrict__ part, long long nblocks, double (&out)[T])
+{
+    __shared__ double sm[1024];
+    for (int t = 0; t < T; ++t) {
+        double acc = 0.0;
+        for (long long i = threadIdx.x; i < nblocks; i += blockDim.x) acc += part[t * nblocks + i];
+        sm[threadIdx.x] = acc;
+        __syncthreads();
+        for (int stride = blockDim.x / 2; stride > 0; stride >>= 1) {
+            if (threadIdx.x < stride) sm[threadIdx.x] += sm[threadIdx.x + stride];
+            __syncthreads();
+        }
+        out[t] = sm[0];
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ void set_error(DevState* ds, int site)
+{
+    if (ds->error == 0) {
+        ds->error = 2;  // LBM_ERR_NONFINITE
+        ds->error_site = site;
+    }
+}
+
+__global__ void __launch_bounds__(1024)
+finalize_kernel(int kind, DevState* __restrict__ ds, const double* __restrict__ part,
+                long long nblocks, const double* __restrict__ part2, long long nblocks2,
+                const double* __restrict__ part3, long long nblocks3)
+{
+    const double n = ds->n_cells;
+    if (kind == FIN_SOURCE) {
+        double r[3];
+        reduce_partials<3>(part, nblocks, r);
+        if (threadIdx.x == 0) {
+            ds->div_sum = r[0];
+            ds->div_abs_sum = r[1];
+            ds->div_mean = r[0] / n;
+            if (r[2] != 0.0 || !isfinite(r[0]) || !isfinite(r[1])) set_error(ds, SITE_SOURCE);
+        }
+    } else if (kind == FIN_PREP) {
+        double r[3];
+        reduce_partials<3>(part, nblocks, r);
+        if (threadIdx.x == 0) {
+            ds->proj_sum = r[0];
+            if (r[1] != 0.0 || !isfinite(r[0])) set_error(ds, SITE_PROJECTED);
+            ds->target = r[2] / n;
+            if (!isfinite(r[2])) set_error(ds, SITE_GAUGE_TARGET);
+            ds->max_shift = 0.0;
+            ds->iterations = 0;
+            ds->converged = 0;
+        }
+    } else if (kind == FIN_SIGMA) {
+        double r[1];
+        reduce_partials<1>(part, nblocks, r);
+        if (threadIdx.x == 0) {
+            const double shift = r[0] / n - ds->target;
+            if (!isfinite(shift)) set_error(ds, SITE_GAUGE_SHIFT);
+            ds->sigma = shift;
+            if (fabs(shift) > ds->max_shift) ds->max_shift = fabs(shift);
+        }
+    } else if (kind == FIN_CHECK) {
+        double rb[5];
+        reduce_partials<5>(part, nblocks, rb);
+        double rc[3] = {0.0, 0.0, 0.0};
+        if (ds->dual) reduce_partials<3>(part2, nblocks2, rc);
+        if (threadIdx.x == 0) {
+            bool fp_ok = true;
+            if (ds->dual) {
+                const double t[6] = {rc[0], rc[1], rc[2], rb[2], rb[3], rb[4]};
+                for (int i = 0; i < 6; ++i) {
+                    ds->fp_terms[i] = t[i];
+                    if (!isfinite(t[i])) set_error(ds, SITE_FIXED_POINT);
+                }
+                ds->fp_h_scale = fmax(t[1], t[2]);
+                ds->fp_h_rel = relative(t[0], ds->fp_h_scale);
+                ds->fp_p_scale = fmax(t[4], t[5]);
+                ds->fp_p_rel = relative(t[3], ds->fp_p_scale);
+                ds->fp_rel = fmax(ds->fp_h_rel, ds->fp_p_rel);
+                if (!isfinite(ds->fp_rel)) set_error(ds, SITE_FIXED_POINT);
+                ds->fp_evaluated = 1;
+                ds->fp_converged = ds->fp_rel < ds->tolerance;
+                fp_ok = ds->fp_converged;
+            }
+            ds->l1_delta = rb[0];
+            ds->l1_norm = rb[1];
+            if (!isfinite(rb[0]) || !isfinite(rb[1])) set_error(ds, SITE_RESIDUAL);
+            ds->rel = relative(rb[0], rb[1]);
+            if (!isfinite(ds->rel)) set_error(ds, SITE_RESIDUAL);
+            ds->pressure_converged = ds->rel < ds->tolerance;
+            ds->converged = ds->pressure_converged && fp_ok;
+            ds->iterations += (unsigned long long)ds->check_interval;
+        }
+    } else if (kind == FIN_MASS) {
+        double r[1];
+        reduce_partials<1>(part, nblocks, r);
+        if (threadIdx.x == 0) ds->mass = r[0];
+    }
+    (void)part3;
+    (void)nblocks3;
+}
+
+}  // namespace
+
+namespace fp64 {
+
+void collide(cudaStream_t st, const Launch& L, const Geom& g, const Phys& P, bool first,
+             const double* fin, double* fout, const double* gin, double* gout,
+             const double* phi, const double* rho, const double* u, const double* v,
+             const double* w, double* dux, double* dvy, double* dwz, double* part)
+{
+    if (first)
+        collide_kernel<true><<<L.grid, L.block, 0, st>>>(g, P, fin, fout, gin, gout, phi, rho, u, v,
+                                                         w, dux, dvy, dwz, part, L.nblocks);
+    else
+        collide_kernel<false><<<L.grid, L.block, 0, st>>>(g, P, fin, fout, gin, gout, phi, rho, u, v,
+                                                          w, dux, dvy, dwz, part, L.nblocks);
+}
+
+void moments(cudaStream_t st, const Launch& L, const Geom& g, const Phys& P, const double* f,
+             const double* gpop, double* phi, double* rho, double* u, double* v, double* w,
+             double* part_mass)
+{
+    moments_kernel<<<L.grid, L.block, 0, st>>>(g, P, f, gpop, phi, rho, u, v, w, part_mass,
+                                               L.nblocks);
+}
+
+void prep(cudaStream_t st, const Launch& L, const Geom& g, const DevState* ds, const double* dux,
+          const double* dvy, const double* dwz, const double* p, double* s, double* part)
+{
+    prep_kernel<<<L.grid, L.block, 0, st>>>(g, ds, dux, dvy, dwz, p, s, part, L.nblocks);
+}
+
+void poisson_init(cudaStream_t st, const Launch& L, const Geom& g, bool h_loaded,
+                  const double* hload, double* hout, const double* p, const double* rho,
+                  const double* s)
+{
+    poisson_init_kernel<<<L.grid, L.block, 0, st>>>(g, h_loaded ? 1 : 0, hload, hout, p, rho, s);
+}
+
+void sweep(cudaStream_t st, const Launch& L, const Geom& g, const double* hin, double* hout,
+           const double* rho, const double* s)
+{
+    sweep_kernel<<<L.grid, L.block, 0, st>>>(g, hin, hout, rho, s);
+}
+
+void sweep_check_a(cudaStream_t st, const Launch& L, const Geom& g, const double* hin,
+                   double* hout, double* p_chk, double* part)
+{
+    sweep_check_a_kernel<<<L.grid, L.block, 0, st>>>(g, hin, hout, p_chk, part, L.nblocks);
+}
+
+void sweep_check_b(cudaStream_t st, const Launch& L, const Geom& g, bool dual, double* h,
+                   double* hc, const double* p_chk, double* p_prev, double* p, const double* rho,
+                   const double* s, const DevState* ds, double* part)
+{
+    if (dual)
+        sweep_check_b_kernel<true><<<L.grid, L.block, 0, st>>>(g, h, hc, p_chk, p_prev, p, rho, s,
+                                                               ds, part, L.nblocks);
+    else
+        sweep_check_b_kernel<false><<<L.grid, L.block, 0, st>>>(g, h, hc, p_chk, p_prev, p, rho, s,
+                                                                ds, part, L.nblocks);
+}
+
+void sweep_check_c(cudaStream_t st, const Launch& L, const Geom& g, const double* hin,
+                   double* hout, const double* hc, const double* rho, const double* s,
+                   const DevState* ds, double* part)
+{
+    sweep_check_c_kernel<<<L.grid, L.block, 0, st>>>(g, hin, hout, hc, rho, s, ds, part,
+                                                     L.nblocks);
+}
+
+void correct(cudaStream_t st, const Launch& L, const Geom& g, double* u, double* v, double* w,
+             const double* p, const double* rho)
+{
+    correct_kernel<<<L.grid, L.block, 0, st>>>(g, u, v, w, p, rho);
+}
+
+}  // namespace fp64
+
+void finalize(cudaStream_t st, FinKind kind, DevState* ds, const double* part, long long nblocks,
+              const double* part2, long long nblocks2, const double* part3, long long nblocks3)
+{
+    finalize_kernel<<<1, 1024, 0, st>>>(static_cast<int>(kind), ds, part, nblocks, part2, nblocks2,
+                                        part3, nblocks3);
+}
+
+}  // namespace lbm

@@ -1,0 +1,748 @@
+// lbm_capi.cu -- the C ABI (include/lbm_b200.h): device buffers, the step
+// sequence and the Poisson loop control of one box.
+//
+// Step sequence (InamuroCUDA::performTimeStepGPU, GPU/InamuroCUDA.cu:2372-2442;
+// Inamuro::performTimeStep, CPU/Inamuro.cpp:347-363):
+//   collide   fused stencils + collide of f, g (pulling the previous step's
+//             post-collision populations) -> f*, g*, u_x, v_y, w_z, sum(div)
+//   moments   pull f*, g* + x slip -> phi, rho, u*, sum(phi)
+//   prep      source projection s = (u_x - mean) + v_y + w_z, sum(p)
+//   Poisson   h* = C(h0, p); then segments of check_interval sweeps, each a
+//             captured CUDA graph ending in the device-side convergence test
+//             and one 200-byte device->host copy of the solver state
+//   correct   u -= grad p / (2 rho)
+//
+// All scalars that the reference brings to the host between kernels (source
+// mean, gauge target, gauge shift, residual norms) are reduced and used on the
+// device; the host reads the state once per segment to decide whether to
+// launch the next one.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/lbm_b200.h"
+#include "lbm_solver.cuh"
+#include "lbm_mixed.cuh"
+
+using namespace lbm;
+
+namespace {
+
+struct SegKey {
+    int start_parity, n_normal, dual;
+    bool operator<(const SegKey& o) const
+    {
+        if (start_parity != o.start_parity) return start_parity < o.start_parity;
+        if (n_normal != o.n_normal) return n_normal < o.n_normal;
+        return dual < o.dual;
+    }
+};
+
+}  // namespace
+
+struct lbm_handle {
+    lbm_params prm{};
+    Geom geom{};
+    Phys phys{};
+    lbm_precision precision = LBM_PRECISION_FP64;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    Launch L{};
+    Fp64Buffers b{};
+    MixedBuffers mb{};
+    bool dual_allocated = false;
+    int fcur = 0;           // f/g buffer holding the current post-collision state
+    bool first_step = true;
+    bool h_loaded = true;   // h0 of the next solve comes from h[1] (a load), not E p
+    lbm_poisson_cfg pcfg{100, 1.0e-3, 0, 0, 0};
+    DevState* ds = nullptr;
+    DevState* ds_host = nullptr;    // pinned
+    std::map<SegKey, cudaGraphExec_t> graphs;
+    std::vector<double> ghost;      // 6 fields x 2 planes x lx*ly
+    std::string err;
+    bool timing = true;
+    cudaEvent_t ev[6]{};
+    lbm_timing acc{};
+    uint64_t steps_done = 0;
+};
+
+namespace {
+
+lbm_status fail(lbm_handle* h, lbm_status s, const std::string& msg)
+{
+    if (h) h->err = msg;
+    return s;
+}
+
+#define LBM_CUDA(h, call)                                                                     \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail((h), e_ == cudaErrorMemoryAllocation ? LBM_ERR_OOM : LBM_ERR_CUDA,    \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                  \
+    } while (0)
+
+bool is_pow2(double t)
+{
+    if (!(t > 0.0) || !std::isfinite(t)) return false;
+    int e = 0;
+    return std::frexp(t, &e) == 0.5;
+}
+
+Phys make_phys(const lbm_params& p)
+{
+    Phys P{};
+    P.rho_L = p.rho_L;
+    P.rho_G = p.rho_G;
+    P.mu_G = p.mu_G;
+    P.mu_slope = (p.mu_L - p.mu_G) / (p.rho_L - p.rho_G);
+    P.tauf = p.tauf;
+    P.taug = p.taug;
+    P.k_f = p.k_f;
+    P.k_g = p.k_g;
+    P.T = p.T;
+    P.a = p.a;
+    P.b = p.b;
+    P.fei_L = p.fei_L;
+    P.fei_G = p.fei_G;
+    P.fei_avg = (p.fei_L + p.fei_G) / 2.0;
+    P.dfei = p.fei_L - p.fei_G;
+    P.half_drho = (p.rho_L - p.rho_G) / 2.0;
+    P.visc = 1.5 * (p.taug - 0.5) * 2.0;
+    P.tauf_pow2 = is_pow2(p.tauf);
+    P.taug_pow2 = is_pow2(p.taug);
+    P.inv_tauf = 1.0 / p.tauf;
+    P.inv_taug = 1.0 / p.taug;
+    return P;
+}
+
+int pick_bx(int lx)
+{
+    if (const char* e = std::getenv("LBM_TILE_BX")) {
+        const int v = std::atoi(e);
+        if (v == 16 || v == 32 || v == 64 || v == 128) return v;
+    }
+    if (lx % 32 == 0 || lx > 48) return 32;
+    return 16;
+}
+
+void free_all(lbm_handle* h)
+{
+    for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
+    h->graphs.clear();
+    double** ptrs[] = {&h->b.f[0], &h->b.f[1], &h->b.g[0], &h->b.g[1], &h->b.h[0], &h->b.h[1],
+                       &h->b.hc, &h->b.phi, &h->b.rho, &h->b.u, &h->b.v, &h->b.w, &h->b.p,
+                       &h->b.p_prev, &h->b.p_chk, &h->b.dux, &h->b.dvy, &h->b.dwz, &h->b.s,
+                       &h->b.part_src, &h->b.part_prep, &h->b.part_a, &h->b.part_b,
+                       &h->b.part_c, &h->b.part_mass};
+    for (double** p : ptrs) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
+    mixed_free(h->mb);
+    if (h->ds) cudaFree(h->ds);
+    if (h->ds_host) cudaFreeHost(h->ds_host);
+    h->ds = nullptr;
+    h->ds_host = nullptr;
+    for (auto& e : h->ev)
+        if (e) cudaEventDestroy(e);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    h->stream = nullptr;
+}
+
+lbm_status alloc_fp64(lbm_handle* h)
+{
+    const size_t n = static_cast<size_t>(h->geom.n);
+    const size_t pop = 15 * n * sizeof(double);
+    const size_t fld = n * sizeof(double);
+    for (int i = 0; i < 2; ++i) {
+        LBM_CUDA(h, cudaMalloc(&h->b.f[i], pop));
+        LBM_CUDA(h, cudaMalloc(&h->b.g[i], pop));
+        LBM_CUDA(h, cudaMalloc(&h->b.h[i], pop));
+    }
+    double** flds[] = {&h->b.phi, &h->b.rho, &h->b.u, &h->b.v, &h->b.w, &h->b.p, &h->b.p_prev,
+                       &h->b.p_chk, &h->b.dux, &h->b.dvy, &h->b.dwz, &h->b.s};
+    for (double** p : flds) {
+        LBM_CUDA(h, cudaMalloc(p, fld));
+        LBM_CUDA(h, cudaMemset(*p, 0, fld));
+    }
+    const size_t nb = static_cast<size_t>(h->L.nblocks) * sizeof(double);
+    LBM_CUDA(h, cudaMalloc(&h->b.part_src, 3 * nb));
+    LBM_CUDA(h, cudaMalloc(&h->b.part_prep, 3 * nb));
+    LBM_CUDA(h, cudaMalloc(&h->b.part_a, 1 * nb));
+    LBM_CUDA(h, cudaMalloc(&h->b.part_b, 5 * nb));
+    LBM_CUDA(h, cudaMalloc(&h->b.part_c, 3 * nb));
+    LBM_CUDA(h, cudaMalloc(&h->b.part_mass, 1 * nb));
+    LBM_CUDA(h, cudaMemset(h->b.part_c, 0, 3 * nb));
+    return LBM_OK;
+}
+
+lbm_status ensure_dual_buffer(lbm_handle* h)
+{
+    if (h->dual_allocated) return LBM_OK;
+    const size_t pop = 15 * static_cast<size_t>(h->geom.n) * sizeof(double);
+    if (h->precision == LBM_PRECISION_FP64) {
+        LBM_CUDA(h, cudaMalloc(&h->b.hc, pop));
+    } else {
+        const lbm_status st = mixed_alloc_dual(h->mb, h->geom);
+        if (st != LBM_OK) return fail(h, st, "cannot allocate the dual-residual buffer");
+    }
+    h->dual_allocated = true;
+    return LBM_OK;
+}
+
+void upload_state_config(lbm_handle* h)
+{
+    h->ds_host->check_interval = h->pcfg.check_interval;
+    h->ds_host->tolerance = h->pcfg.tolerance;
+    h->ds_host->dual = h->pcfg.dual_residual;
+    h->ds_host->n_cells = static_cast<double>(h->geom.lx) * h->geom.ly * h->geom.lz;
+}
+
+// Captures one Poisson segment as a CUDA graph: n_normal plain sweeps, the
+// check pair (A: stream/bounce/sum at the check sweep, B: gauge + relative
+// change + R_p terms + collision of the next sweep), in dual mode the shadow
+// sweep C (R_h terms), the convergence test, and the state copy to the host.
+lbm_status build_segment(lbm_handle* h, const SegKey& key, cudaGraphExec_t* out)
+{
+    cudaStream_t st = h->stream;
+    LBM_CUDA(h, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int cur = key.start_parity;
+    const Geom& g = h->geom;
+    const Launch& L = h->L;
+    if (h->precision == LBM_PRECISION_FP64) {
+        Fp64Buffers& b = h->b;
+        for (int i = 0; i < key.n_normal; ++i) {
+            fp64::sweep(st, L, g, b.h[cur], b.h[1 - cur], b.rho, b.s);
+            cur = 1 - cur;
+        }
+        fp64::sweep_check_a(st, L, g, b.h[cur], b.h[1 - cur], b.p_chk, b.part_a);
+        cur = 1 - cur;
+        finalize(st, FIN_SIGMA, h->ds, b.part_a, L.nblocks, nullptr, 0, nullptr, 0);
+        fp64::sweep_check_b(st, L, g, key.dual != 0, b.h[cur], b.hc, b.p_chk, b.p_prev, b.p, b.rho,
+                            b.s, h->ds, b.part_b);
+        if (key.dual) {
+            fp64::sweep_check_c(st, L, g, b.h[cur], b.h[1 - cur], b.hc, b.rho, b.s, h->ds, b.part_c);
+            cur = 1 - cur;
+        }
+        finalize(st, FIN_CHECK, h->ds, b.part_b, L.nblocks, b.part_c, L.nblocks, nullptr, 0);
+    } else {
+        cur = mixed_segment(st, h->mb, L, g, key.start_parity, key.n_normal, key.dual != 0, h->ds);
+    }
+    cudaMemcpyAsync(h->ds_host, h->ds, sizeof(DevState), cudaMemcpyDeviceToHost, st);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st, &graph);
+    if (e != cudaSuccess) return fail(h, LBM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(out, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(h, LBM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    (void)cur;
+    return LBM_OK;
+}
+
+int segment_parity_change(int n_normal, int dual)
+{
+    return (n_normal + 1 + (dual ? 1 : 0)) & 1;
+}
+
+lbm_status get_segment(lbm_handle* h, const SegKey& key, cudaGraphExec_t* out)
+{
+    auto it = h->graphs.find(key);
+    if (it != h->graphs.end()) {
+        *out = it->second;
+        return LBM_OK;
+    }
+    cudaGraphExec_t ex = nullptr;
+    const lbm_status st = build_segment(h, key, &ex);
+    if (st != LBM_OK) return st;
+    h->graphs[key] = ex;
+    *out = ex;
+    return LBM_OK;
+}
+
+const char* site_text(int site)
+{
+    switch (site) {
+    case SITE_SOURCE: return "Poisson source contains NaN/Inf";
+    case SITE_PROJECTED: return "projected Poisson source contains NaN/Inf";
+    case SITE_GAUGE_TARGET: return "pressure mean is NaN/Inf";
+    case SITE_GAUGE_SHIFT: return "pressure gauge shift is NaN/Inf";
+    case SITE_FIXED_POINT: return "kinetic fixed-point residual contains NaN/Inf";
+    case SITE_RESIDUAL: return "Poisson pressure/residual contains NaN/Inf";
+    default: return "non-finite value";
+    }
+}
+
+void fill_stats(const lbm_handle* h, const DevState& d, lbm_step_stats* s)
+{
+    std::memset(s, 0, sizeof(*s));
+    s->iterations = d.iterations;
+    s->relative_error = d.rel;
+    s->pressure_l1_delta = d.l1_delta;
+    s->pressure_l1_norm = d.l1_norm;
+    const double nan = std::nan("");
+    const bool fp = d.fp_evaluated != 0;
+    s->fixed_point_h_l1 = fp ? d.fp_terms[0] : nan;
+    s->fixed_point_h_scale = fp ? d.fp_h_scale : nan;
+    s->fixed_point_h_relative = fp ? d.fp_h_rel : nan;
+    s->fixed_point_p_l1 = fp ? d.fp_terms[3] : nan;
+    s->fixed_point_p_scale = fp ? d.fp_p_scale : nan;
+    s->fixed_point_p_relative = fp ? d.fp_p_rel : nan;
+    s->fixed_point_relative = fp ? d.fp_rel : nan;
+    // GPU/InamuroCUDA.cu:1892-1893, 1920
+    s->source_mean = -d.div_mean / 3.0;
+    s->source_abs_mean = d.div_abs_sum / (3.0 * d.n_cells);
+    s->projected_source_mean = -d.proj_sum / (3.0 * d.n_cells);
+    s->pressure_gauge_target = d.target;
+    s->pressure_gauge_max_shift = d.max_shift;
+    s->mass = d.mass;
+    s->fixed_point_evaluated = d.fp_evaluated;
+    s->pressure_converged = d.pressure_converged;
+    s->fixed_point_converged = d.fp_converged;
+    s->dual_residual_enabled = h->pcfg.dual_residual;
+    s->converged = d.converged;
+}
+
+// One time step.  replay > 0 forces that many sweeps.
+lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
+{
+    cudaStream_t st = h->stream;
+    const Geom& g = h->geom;
+    const Launch& L = h->L;
+    const int ci = h->pcfg.check_interval;
+    const int dual = h->pcfg.dual_residual;
+    if (dual) {
+        const lbm_status s = ensure_dual_buffer(h);
+        if (s != LBM_OK) return s;
+    }
+    if (h->timing) LBM_CUDA(h, cudaEventRecord(h->ev[0], st));
+    // Reset per-solve flags, keep config.
+    DevState& dh = *h->ds_host;
+    std::memset(&dh, 0, sizeof(DevState));
+    upload_state_config(h);
+    LBM_CUDA(h, cudaMemcpyAsync(h->ds, h->ds_host, sizeof(DevState), cudaMemcpyHostToDevice, st));
+
+    int hcur = 0;
+    if (h->precision == LBM_PRECISION_FP64) {
+        Fp64Buffers& b = h->b;
+        const int fin = h->fcur, fout = 1 - h->fcur;
+        fp64::collide(st, L, g, h->phys, h->first_step, b.f[fin], b.f[fout], b.g[fin], b.g[fout],
+                      b.phi, b.rho, b.u, b.v, b.w, b.dux, b.dvy, b.dwz, b.part_src);
+        h->fcur = fout;
+        if (h->timing) LBM_CUDA(h, cudaEventRecord(h->ev[1], st));
+        fp64::moments(st, L, g, h->phys, b.f[fout], b.g[fout], b.phi, b.rho, b.u, b.v, b.w,
+                      b.part_mass);
+        if (h->timing) LBM_CUDA(h, cudaEventRecord(h->ev[2], st));
+        finalize(st, FIN_SOURCE, h->ds, b.part_src, L.nblocks, nullptr, 0, nullptr, 0);
+        finalize(st, FIN_MASS, h->ds, b.part_mass, L.nblocks, nullptr, 0, nullptr, 0);
+        fp64::prep(st, L, g, h->ds, b.dux, b.dvy, b.dwz, b.p, b.s, b.part_prep);
+        finalize(st, FIN_PREP, h->ds, b.part_prep, L.nblocks, nullptr, 0, nullptr, 0);
+        fp64::poisson_init(st, L, g, h->h_loaded, b.h[1], b.h[0], b.p, b.rho, b.s);
+    } else {
+        const lbm_status s2 = mixed_prologue(st, h->mb, L, g, h->phys, h->first_step, h->fcur,
+                                             h->h_loaded, h->ds, h->timing ? h->ev : nullptr);
+        if (s2 != LBM_OK) return fail(h, s2, "mixed prologue launch failed");
+        h->fcur = 1 - h->fcur;
+    }
+    LBM_CUDA(h, cudaGetLastError());
+    h->first_step = false;
+    h->h_loaded = false;
+    if (h->timing) LBM_CUDA(h, cudaEventRecord(h->ev[3], st));
+
+    // Poisson segments.
+    uint64_t iters = 0;
+    bool first_seg = true;
+    uint64_t kernels = 0;
+    for (;;) {
+        const int n_normal = dual ? (first_seg ? ci - 1 : ci - 2) : ci - 1;
+        SegKey key{hcur, n_normal, dual};
+        cudaGraphExec_t ex = nullptr;
+        const lbm_status gs = get_segment(h, key, &ex);
+        if (gs != LBM_OK) return gs;
+        LBM_CUDA(h, cudaGraphLaunch(ex, st));
+        LBM_CUDA(h, cudaStreamSynchronize(st));
+        hcur ^= segment_parity_change(n_normal, dual);
+        kernels += static_cast<uint64_t>(n_normal) + 2 + (dual ? 1 : 0);
+        first_seg = false;
+        if (dh.error) {
+            return fail(h, static_cast<lbm_status>(dh.error), site_text(dh.error_site));
+        }
+        if (iters > UINT64_MAX - static_cast<uint64_t>(ci))
+            return fail(h, LBM_ERR_OVERFLOW, "Poisson iteration counter overflow");
+        iters += static_cast<uint64_t>(ci);
+        if (replay) {
+            if (iters >= replay) break;
+        } else if (dh.converged) {
+            break;
+        }
+        if (h->pcfg.max_sweeps && iters >= h->pcfg.max_sweeps) {
+            if (h->pcfg.fail_on_limit)
+                return fail(h, LBM_ERR_POISSON_BUDGET, "Poisson sweep limit reached without convergence");
+            break;
+        }
+    }
+    if (h->timing) LBM_CUDA(h, cudaEventRecord(h->ev[4], st));
+    if (h->precision == LBM_PRECISION_FP64) {
+        fp64::correct(st, L, g, h->b.u, h->b.v, h->b.w, h->b.p, h->b.rho);
+    } else {
+        mixed_correct(st, h->mb, L, g);
+    }
+    LBM_CUDA(h, cudaGetLastError());
+    if (h->timing) LBM_CUDA(h, cudaEventRecord(h->ev[5], st));
+    LBM_CUDA(h, cudaStreamSynchronize(st));
+    double dev_ms = 0.0;
+    if (h->timing) {
+        float t[5];
+        for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&t[i], h->ev[i], h->ev[i + 1]);
+        h->acc.collide_ms += t[0];
+        h->acc.moments_ms += t[1];
+        h->acc.prep_ms += t[2];
+        h->acc.poisson_ms += t[3];
+        h->acc.correct_ms += t[4];
+        dev_ms = double(t[0]) + t[1] + t[2] + t[3] + t[4];
+    }
+    h->acc.steps += 1;
+    h->acc.sweeps += iters;
+    h->acc.sweep_kernels += kernels;
+    h->steps_done += 1;
+    if (stats) {
+        fill_stats(h, dh, stats);
+        stats->iterations = iters;
+        stats->device_ms = dev_ms;
+    }
+    return LBM_OK;
+}
+
+lbm_status check_handle(const lbm_handle* h)
+{
+    return h ? LBM_OK : LBM_ERR_BAD_ARG;
+}
+
+const double* field_ptr(const lbm_handle* h, lbm_field which)
+{
+    switch (which) {
+    case LBM_FIELD_PHI: return h->b.phi;
+    case LBM_FIELD_RHO: return h->b.rho;
+    case LBM_FIELD_U: return h->b.u;
+    case LBM_FIELD_V: return h->b.v;
+    case LBM_FIELD_W: return h->b.w;
+    case LBM_FIELD_P: return h->b.p;
+    }
+    return nullptr;
+}
+
+lbm_status load_common(lbm_handle* h, const double* const src[6], cudaMemcpyKind kind)
+{
+    const size_t bytes = static_cast<size_t>(h->geom.n) * sizeof(double);
+    cudaStream_t st = h->stream;
+    if (h->precision == LBM_PRECISION_FP64) {
+        double* dst[6] = {h->b.phi, h->b.rho, h->b.u, h->b.v, h->b.w, h->b.p};
+        for (int i = 0; i < 6; ++i) {
+            if (src[i]) LBM_CUDA(h, cudaMemcpyAsync(dst[i], src[i], bytes, kind, st));
+            else LBM_CUDA(h, cudaMemsetAsync(dst[i], 0, bytes, st));
+        }
+        LBM_CUDA(h, cudaMemsetAsync(h->b.p_prev, 0, bytes, st));
+        // h0 of the first solve: the CPU object's h, all zero after initializeArrays.
+        LBM_CUDA(h, cudaMemsetAsync(h->b.h[1], 0, 15 * bytes, st));
+    } else {
+        const lbm_status s = mixed_load(st, h->mb, h->geom, h->phys, src, kind);
+        if (s != LBM_OK) return fail(h, s, "mixed load failed");
+    }
+    LBM_CUDA(h, cudaStreamSynchronize(st));
+    h->first_step = true;
+    h->h_loaded = true;
+    h->fcur = 0;
+    return LBM_OK;
+}
+
+void default_ghosts(lbm_handle* h)
+{
+    // Ghost planes of a fresh CPU Inamuro: rho_G, fei_min, 0 (CPU/Inamuro.cpp:518-524).
+    const size_t plane = static_cast<size_t>(h->geom.lx) * h->geom.ly;
+    h->ghost.assign(6 * 2 * plane, 0.0);
+    std::fill(h->ghost.begin(), h->ghost.begin() + 2 * plane, h->prm.fei_min);          // phi
+    std::fill(h->ghost.begin() + 2 * plane, h->ghost.begin() + 4 * plane, h->prm.rho_G);  // rho
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_abi_version(void) { return LBM_B200_ABI_VERSION; }
+
+const char* lbm_status_string(lbm_status s)
+{
+    switch (s) {
+    case LBM_OK: return "ok";
+    case LBM_ERR_CUDA: return "CUDA error";
+    case LBM_ERR_NONFINITE: return "non-finite value";
+    case LBM_ERR_POISSON_BUDGET: return "Poisson sweep limit reached";
+    case LBM_ERR_BAD_ARG: return "bad argument";
+    case LBM_ERR_OOM: return "out of device memory";
+    case LBM_ERR_IO: return "I/O error";
+    case LBM_ERR_NO_DEVICE: return "no sm_100 CUDA device";
+    case LBM_ERR_OVERFLOW: return "counter overflow";
+    }
+    return "unknown status";
+}
+
+const char* lbm_last_error(const lbm_handle* h) { return h ? h->err.c_str() : ""; }
+
+lbm_status lbm_create(const lbm_params* prm, lbm_precision precision, int device, lbm_handle** out)
+{
+    if (!prm || !out) return LBM_ERR_BAD_ARG;
+    *out = nullptr;
+    if (prm->lx < 2 || prm->ly < 1 || prm->lz < 1 || prm->lz > 65535) return LBM_ERR_BAD_ARG;
+    if (!(prm->rho_L != prm->rho_G) || !(prm->tauf > 0.0) || !(prm->taug > 0.0)) return LBM_ERR_BAD_ARG;
+    if (precision != LBM_PRECISION_FP64 && precision != LBM_PRECISION_MIXED) return LBM_ERR_BAD_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return LBM_ERR_NO_DEVICE;
+    }
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) return LBM_ERR_NO_DEVICE;
+    if (cudaSetDevice(device) != cudaSuccess) return LBM_ERR_NO_DEVICE;
+
+    lbm_handle* h = new lbm_handle();
+    h->prm = *prm;
+    h->precision = precision;
+    h->device = device;
+    h->geom.lx = prm->lx;
+    h->geom.ly = prm->ly;
+    h->geom.lz = prm->lz;
+    h->geom.periodic_x = 0;
+    h->geom.n = static_cast<long long>(prm->lx) * prm->ly * prm->lz;
+    h->phys = make_phys(*prm);
+    const int bx = pick_bx(prm->lx);
+    h->L = make_launch(prm->lx, prm->ly, prm->lz, bx, 256 / bx);
+    lbm_status st = LBM_OK;
+    auto bail = [&](lbm_status s) {
+        free_all(h);
+        delete h;
+        return s;
+    };
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(LBM_ERR_CUDA);
+    for (auto& e : h->ev)
+        if (cudaEventCreate(&e) != cudaSuccess) return bail(LBM_ERR_CUDA);
+    if (cudaMalloc(&h->ds, sizeof(DevState)) != cudaSuccess) return bail(LBM_ERR_OOM);
+    if (cudaMallocHost(&h->ds_host, sizeof(DevState)) != cudaSuccess) return bail(LBM_ERR_OOM);
+    std::memset(h->ds_host, 0, sizeof(DevState));
+    if (precision == LBM_PRECISION_FP64) st = alloc_fp64(h);
+    else st = mixed_alloc(h->mb, h->geom, h->L);
+    if (st != LBM_OK) return bail(st);
+    default_ghosts(h);
+    // Background state until the caller loads fields.
+    const size_t n = static_cast<size_t>(h->geom.n);
+    std::vector<double> phi(n), rho(n), z(n, 0.0);
+    std::fill(phi.begin(), phi.end(), prm->fei_min);
+    std::fill(rho.begin(), rho.end(), prm->rho_G);
+    const double* src[6] = {phi.data(), rho.data(), z.data(), z.data(), z.data(), z.data()};
+    st = load_common(h, src, cudaMemcpyHostToDevice);
+    if (st != LBM_OK) return bail(st);
+    *out = h;
+    return LBM_OK;
+}
+
+void lbm_destroy(lbm_handle* h)
+{
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_all(h);
+    delete h;
+}
+
+lbm_status lbm_load_fields(lbm_handle* h, const double* phi, const double* rho, const double* u,
+                           const double* v, const double* w, const double* p)
+{
+    if (check_handle(h) != LBM_OK || !phi || !rho || !u || !v || !w) return fail(h, LBM_ERR_BAD_ARG, "null field");
+    cudaSetDevice(h->device);
+    const double* src[6] = {phi, rho, u, v, w, p};
+    default_ghosts(h);
+    return load_common(h, src, cudaMemcpyHostToDevice);
+}
+
+lbm_status lbm_load_fields_device(lbm_handle* h, const double* phi, const double* rho,
+                                  const double* u, const double* v, const double* w, const double* p)
+{
+    if (check_handle(h) != LBM_OK || !phi || !rho || !u || !v || !w) return fail(h, LBM_ERR_BAD_ARG, "null field");
+    cudaSetDevice(h->device);
+    const double* src[6] = {phi, rho, u, v, w, p};
+    return load_common(h, src, cudaMemcpyDeviceToDevice);
+}
+
+lbm_status lbm_load_fields_ghosted(lbm_handle* h, const double* phi, const double* rho,
+                                   const double* u, const double* v, const double* w,
+                                   const double* p)
+{
+    if (check_handle(h) != LBM_OK || !phi || !rho || !u || !v || !w || !p) return fail(h, LBM_ERR_BAD_ARG, "null field");
+    cudaSetDevice(h->device);
+    const size_t plane = static_cast<size_t>(h->geom.lx) * h->geom.ly;
+    const size_t n = static_cast<size_t>(h->geom.n);
+    const double* gsrc[6] = {phi, rho, u, v, w, p};
+    std::vector<double> phys(6 * n);
+    h->ghost.assign(6 * 2 * plane, 0.0);
+    for (int f = 0; f < 6; ++f) {
+        std::memcpy(phys.data() + f * n, gsrc[f] + plane, n * sizeof(double));
+        std::memcpy(h->ghost.data() + (2 * f) * plane, gsrc[f], plane * sizeof(double));
+        std::memcpy(h->ghost.data() + (2 * f + 1) * plane, gsrc[f] + (h->geom.lz + 1) * plane,
+                    plane * sizeof(double));
+    }
+    const double* src[6] = {phys.data(), phys.data() + n, phys.data() + 2 * n,
+                            phys.data() + 3 * n, phys.data() + 4 * n, phys.data() + 5 * n};
+    return load_common(h, src, cudaMemcpyHostToDevice);
+}
+
+lbm_status lbm_set_poisson(lbm_handle* h, const lbm_poisson_cfg* cfg)
+{
+    if (check_handle(h) != LBM_OK || !cfg) return fail(h, LBM_ERR_BAD_ARG, "null config");
+    // Same validation as InamuroCUDA::setPoissonConvergence / setPoissonIterationLimit
+    // (GPU/InamuroCUDA.cu:2582-2608); the dual test needs >= 2 sweeps per segment.
+    if (cfg->check_interval <= 0) return fail(h, LBM_ERR_BAD_ARG, "poisson check interval must be positive");
+    if (cfg->dual_residual && cfg->check_interval < 2)
+        return fail(h, LBM_ERR_BAD_ARG, "dual residual needs a check interval of at least 2");
+    if (!(cfg->tolerance > 0.0)) return fail(h, LBM_ERR_BAD_ARG, "poisson tolerance must be positive");
+    if (cfg->max_sweeps != 0 && cfg->max_sweeps % static_cast<uint64_t>(cfg->check_interval) != 0)
+        return fail(h, LBM_ERR_BAD_ARG, "Poisson iteration limit must be a multiple of check interval");
+    if (cfg->check_interval != h->pcfg.check_interval || cfg->dual_residual != h->pcfg.dual_residual) {
+        for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
+        h->graphs.clear();
+    }
+    h->pcfg = *cfg;
+    h->pcfg.dual_residual = cfg->dual_residual ? 1 : 0;
+    return LBM_OK;
+}
+
+lbm_status lbm_get_poisson(const lbm_handle* h, lbm_poisson_cfg* cfg)
+{
+    if (!h || !cfg) return LBM_ERR_BAD_ARG;
+    *cfg = h->pcfg;
+    return LBM_OK;
+}
+
+lbm_status lbm_step(lbm_handle* h, int n_steps, lbm_step_stats* stats)
+{
+    if (check_handle(h) != LBM_OK || n_steps < 0) return fail(h, LBM_ERR_BAD_ARG, "bad step count");
+    cudaSetDevice(h->device);
+    for (int i = 0; i < n_steps; ++i) {
+        const lbm_status s = step_once(h, 0, stats ? stats + i : nullptr);
+        if (s != LBM_OK) return s;
+    }
+    return LBM_OK;
+}
+
+lbm_status lbm_step_replay(lbm_handle* h, int n_steps, const uint64_t* sweeps, lbm_step_stats* stats)
+{
+    if (check_handle(h) != LBM_OK || n_steps < 0 || !sweeps) return fail(h, LBM_ERR_BAD_ARG, "bad replay");
+    cudaSetDevice(h->device);
+    for (int i = 0; i < n_steps; ++i) {
+        if (sweeps[i] == 0 || sweeps[i] % static_cast<uint64_t>(h->pcfg.check_interval) != 0)
+            return fail(h, LBM_ERR_BAD_ARG, "replay sweeps must be a positive multiple of the check interval");
+        const lbm_status s = step_once(h, sweeps[i], stats ? stats + i : nullptr);
+        if (s != LBM_OK) return s;
+    }
+    return LBM_OK;
+}
+
+lbm_status lbm_download(lbm_handle* h, lbm_field which, double* host)
+{
+    if (check_handle(h) != LBM_OK || !host || which < LBM_FIELD_PHI || which > LBM_FIELD_P)
+        return fail(h, LBM_ERR_BAD_ARG, "bad download");
+    cudaSetDevice(h->device);
+    const size_t bytes = static_cast<size_t>(h->geom.n) * sizeof(double);
+    if (h->precision == LBM_PRECISION_FP64) {
+        LBM_CUDA(h, cudaMemcpyAsync(host, field_ptr(h, which), bytes, cudaMemcpyDeviceToHost, h->stream));
+    } else {
+        const lbm_status s = mixed_download(h->stream, h->mb, h->geom, static_cast<int>(which), host);
+        if (s != LBM_OK) return fail(h, s, "mixed download failed");
+    }
+    LBM_CUDA(h, cudaStreamSynchronize(h->stream));
+    return LBM_OK;
+}
+
+lbm_status lbm_download_ghosted(lbm_handle* h, lbm_field which, double* host)
+{
+    if (check_handle(h) != LBM_OK || !host) return fail(h, LBM_ERR_BAD_ARG, "bad download");
+    const size_t plane = static_cast<size_t>(h->geom.lx) * h->geom.ly;
+    const lbm_status s = lbm_download(h, which, host + plane);
+    if (s != LBM_OK) return s;
+    const int f = static_cast<int>(which);
+    std::memcpy(host, h->ghost.data() + (2 * f) * plane, plane * sizeof(double));
+    std::memcpy(host + (h->geom.lz + 1) * plane, h->ghost.data() + (2 * f + 1) * plane,
+                plane * sizeof(double));
+    return LBM_OK;
+}
+
+lbm_status lbm_download_h(lbm_handle* h, double* host)
+{
+    if (check_handle(h) != LBM_OK || !host) return fail(h, LBM_ERR_BAD_ARG, "bad download");
+    cudaSetDevice(h->device);
+    const size_t n = static_cast<size_t>(h->geom.n);
+    if (h->h_loaded && h->precision == LBM_PRECISION_FP64) {
+        std::vector<double> soa(15 * n);
+        LBM_CUDA(h, cudaMemcpyAsync(soa.data(), h->b.h[1], 15 * n * sizeof(double),
+                                    cudaMemcpyDeviceToHost, h->stream));
+        LBM_CUDA(h, cudaStreamSynchronize(h->stream));
+        for (size_t c = 0; c < n; ++c)
+            for (int q = 0; q < 15; ++q) host[c * 15 + q] = soa[q * n + c];
+        return LBM_OK;
+    }
+    if (h->h_loaded) {
+        std::fill(host, host + 15 * n, 0.0);
+        return LBM_OK;
+    }
+    // After update_hh: h_q = p * E_q (CPU/Inamuro.cpp:825-840).
+    std::vector<double> p(n);
+    const lbm_status s = lbm_download(h, LBM_FIELD_P, p.data());
+    if (s != LBM_OK) return s;
+    for (size_t c = 0; c < n; ++c)
+        for (int q = 0; q < 15; ++q) host[c * 15 + q] = p[c] * wE(q);
+    return LBM_OK;
+}
+
+lbm_status lbm_field_device_ptr(lbm_handle* h, lbm_field which, const double** dev)
+{
+    if (check_handle(h) != LBM_OK || !dev || which < LBM_FIELD_PHI || which > LBM_FIELD_P)
+        return fail(h, LBM_ERR_BAD_ARG, "bad field");
+    if (h->precision != LBM_PRECISION_FP64) return fail(h, LBM_ERR_BAD_ARG, "device pointers are FP64-only");
+    *dev = field_ptr(h, which);
+    return LBM_OK;
+}
+
+lbm_status lbm_synchronize(lbm_handle* h)
+{
+    if (check_handle(h) != LBM_OK) return LBM_ERR_BAD_ARG;
+    cudaSetDevice(h->device);
+    LBM_CUDA(h, cudaStreamSynchronize(h->stream));
+    return LBM_OK;
+}
+
+lbm_status lbm_get_timing(const lbm_handle* h, lbm_timing* out)
+{
+    if (!h || !out) return LBM_ERR_BAD_ARG;
+    *out = h->acc;
+    return LBM_OK;
+}
+
+lbm_status lbm_reset_timing(lbm_handle* h)
+{
+    if (!h) return LBM_ERR_BAD_ARG;
+    h->acc = lbm_timing{};
+    return LBM_OK;
+}
+
+lbm_status lbm_set_timing(lbm_handle* h, int enabled)
+{
+    if (!h) return LBM_ERR_BAD_ARG;
+    h->timing = enabled != 0;
+    return LBM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,45 @@
+// lbm_mixed.cuh -- the mixed-precision box: FP32 populations stored as
+// deviations from rest-state values, FP32 stencils, FP64 reductions,
+// convergence test and pressure accumulation (kernels_mixed.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "../../include/lbm_b200.h"
+#include "lbm_solver.cuh"
+
+namespace lbm {
+
+struct MixedBuffers {
+    float* f[2] = {nullptr, nullptr};
+    float* g[2] = {nullptr, nullptr};
+    float* h[2] = {nullptr, nullptr};
+    float* hc = nullptr;
+    float *phi = nullptr, *rho = nullptr, *u = nullptr, *v = nullptr, *w = nullptr;
+    float* s = nullptr;
+    double *p = nullptr, *p_prev = nullptr, *p_chk = nullptr;
+    float *dux = nullptr, *dvy = nullptr, *dwz = nullptr;
+    double *part_src = nullptr, *part_prep = nullptr, *part_a = nullptr, *part_b = nullptr,
+           *part_c = nullptr, *part_mass = nullptr;
+    double* scratch = nullptr;   // FP64 staging for loads/downloads (n doubles)
+    bool allocated = false;
+};
+
+lbm_status mixed_alloc(MixedBuffers& mb, const Geom& g, const Launch& L);
+lbm_status mixed_alloc_dual(MixedBuffers& mb, const Geom& g);
+void mixed_free(MixedBuffers& mb);
+lbm_status mixed_load(cudaStream_t st, MixedBuffers& mb, const Geom& g, const Phys& P,
+                      const double* const src[6], cudaMemcpyKind kind);
+lbm_status mixed_download(cudaStream_t st, MixedBuffers& mb, const Geom& g, int which, double* host);
+// Launches collide, moments, source prep and the Poisson initial collision.
+// ev (may be null) receives events 1 and 2 after collide and moments.
+lbm_status mixed_prologue(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom& g,
+                          const Phys& P, bool first, int fcur, bool h_loaded, DevState* ds,
+                          cudaEvent_t* ev);
+// Enqueues one Poisson segment (captured into a graph by the caller); returns
+// the parity of the h buffer that holds the state afterwards.
+int mixed_segment(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom& g,
+                  int start_parity, int n_normal, bool dual, DevState* ds);
+void mixed_correct(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom& g);
+
+}  // namespace lbm

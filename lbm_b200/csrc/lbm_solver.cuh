@@ -1,0 +1,129 @@
+// lbm_solver.cuh -- structures shared by the host orchestration (lbm_capi.cu)
+// and the kernels (kernels_fp64.cu, kernels_mixed.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "lbm_device.cuh"
+
+namespace lbm {
+
+// Physical constants of one box, with the derived constants the reference
+// computes at run time folded here in the same IEEE operations.
+struct Phys {
+    double rho_L, rho_G;
+    double mu_G;
+    double mu_slope;      // (mu_L - mu_G) / (rho_L - rho_G)      CPU/Inamuro.cpp:137
+    double tauf, taug;
+    double k_f, k_g;
+    double T, a, b;
+    double fei_L, fei_G;
+    double fei_avg;       // (fei_L + fei_G) / 2.0                CPU/Inamuro.cpp:296
+    double dfei;          // fei_L - fei_G
+    double half_drho;     // (rho_L - rho_G) / 2.0                CPU/Inamuro.cpp:326
+    double visc;          // 1.5 * (taug - 0.5) * 2.0             CPU/Inamuro.cpp:217
+    double inv_tauf, inv_taug;
+    int tauf_pow2, taug_pow2;   // 1: tau is a power of two, x/tau == x*(1/tau) exactly
+};
+
+// Device-resident solver state: the scalars the reference computes on the
+// host between kernel launches (GPU/InamuroCUDA.cu:1868-2159) live here, so a
+// whole Poisson segment runs without a host round trip.
+struct DevState {
+    // source projection and gauge (per step)
+    double div_sum, div_abs_sum, div_mean;
+    double proj_sum;
+    double target;              // pressure gauge target (mean p at solve start)
+    // last check
+    double sigma;               // gauge shift
+    double max_shift;
+    double l1_delta, l1_norm, rel;
+    double fp_terms[6];
+    double fp_h_scale, fp_h_rel, fp_p_scale, fp_p_rel, fp_rel;
+    double mass;
+    unsigned long long iterations;   // sweeps counted up to the last check
+    int converged, pressure_converged, fp_converged, fp_evaluated;
+    int error;                  // lbm_status code, 0 = ok
+    int error_site;             // which check raised it
+    int check_interval;
+    int dual;
+    double tolerance;
+    double n_cells;             // (double)lx * ly * lz
+};
+
+enum ErrorSite {
+    SITE_NONE = 0,
+    SITE_SOURCE = 1,        // "Poisson source contains NaN/Inf"
+    SITE_PROJECTED = 2,     // "projected Poisson source contains NaN/Inf"
+    SITE_GAUGE_TARGET = 3,  // "pressure mean is NaN/Inf"
+    SITE_GAUGE_SHIFT = 4,   // "pressure gauge shift is NaN/Inf"
+    SITE_FIXED_POINT = 5,   // "kinetic fixed-point residual contains NaN/Inf"
+    SITE_RESIDUAL = 6       // "Poisson pressure/residual contains NaN/Inf"
+};
+
+// Launch shape: 2-D tiles of (bx, by) cells in an xy plane, one grid z-slice
+// per lattice plane.
+struct Launch {
+    dim3 grid, block;
+    long long nblocks;
+};
+
+inline Launch make_launch(int lx, int ly, int lz, int bx, int by)
+{
+    Launch L;
+    L.block = dim3(bx, by, 1);
+    L.grid = dim3((lx + bx - 1) / bx, (ly + by - 1) / by, lz);
+    L.nblocks = (long long)L.grid.x * L.grid.y * L.grid.z;
+    return L;
+}
+
+// Buffers of one FP64 box.  Populations are q-major SoA: a[q*n + cell].
+struct Fp64Buffers {
+    double* f[2];       // post-collision f* ping-pong
+    double* g[2];
+    double* h[2];       // post-collision h* ping-pong (and h0 after a load)
+    double* hc;         // gauged h at a check (dual residual only)
+    double *phi, *rho, *u, *v, *w;
+    double *p, *p_prev, *p_chk;
+    double *dux, *dvy, *dwz, *s;
+    double *part_src, *part_prep, *part_a, *part_b, *part_c, *part_mass;
+};
+
+// Kernel launchers (kernels_fp64.cu).
+namespace fp64 {
+void collide(cudaStream_t st, const Launch& L, const Geom& g, const Phys& P, bool first,
+             const double* fin, double* fout, const double* gin, double* gout,
+             const double* phi, const double* rho, const double* u, const double* v,
+             const double* w, double* dux, double* dvy, double* dwz, double* part);
+void moments(cudaStream_t st, const Launch& L, const Geom& g, const Phys& P,
+             const double* f, const double* gpop, double* phi, double* rho, double* u,
+             double* v, double* w, double* part_mass);
+void prep(cudaStream_t st, const Launch& L, const Geom& g, const DevState* ds,
+          const double* dux, const double* dvy, const double* dwz, const double* p,
+          double* s, double* part);
+void poisson_init(cudaStream_t st, const Launch& L, const Geom& g, bool h_loaded,
+                  const double* hload, double* hout, const double* p, const double* rho,
+                  const double* s);
+void sweep(cudaStream_t st, const Launch& L, const Geom& g, const double* hin, double* hout,
+           const double* rho, const double* s);
+void sweep_check_a(cudaStream_t st, const Launch& L, const Geom& g, const double* hin,
+                   double* hout, double* p_chk, double* part);
+void sweep_check_b(cudaStream_t st, const Launch& L, const Geom& g, bool dual, double* h,
+                   double* hc, const double* p_chk, double* p_prev, double* p,
+                   const double* rho, const double* s, const DevState* ds, double* part);
+void sweep_check_c(cudaStream_t st, const Launch& L, const Geom& g, const double* hin,
+                   double* hout, const double* hc, const double* rho, const double* s,
+                   const DevState* ds, double* part);
+void correct(cudaStream_t st, const Launch& L, const Geom& g, double* u, double* v, double* w,
+             const double* p, const double* rho);
+}  // namespace fp64
+
+// Finalisation kernels (kernels_fp64.cu): reduce block partials in a fixed
+// order and update DevState.
+enum FinKind { FIN_SOURCE = 0, FIN_PREP = 1, FIN_SIGMA = 2, FIN_CHECK = 3, FIN_MASS = 4 };
+void finalize(cudaStream_t st, FinKind kind, DevState* ds, const double* part,
+              long long nblocks, const double* part2, long long nblocks2,
+              const double* part3, long long nblocks3);
+
+}  // namespace lbm

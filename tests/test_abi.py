@@ -1,0 +1,60 @@
+"""The C ABI library loads and exports every function include/lbm_b200.h
+declares (no GPU needed; no compute calls)."""
+import ctypes
+import os
+import subprocess
+
+import lbm_b200 as L
+
+
+def test_library_exports_every_declared_symbol():
+    lib = L.load_library()
+    names = L.header_functions()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_nm_lists_exports_as_c_symbols():
+    out = subprocess.run(["nm", "-D", "--defined-only", L.LIB_PATH], capture_output=True,
+                         text=True, check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    for n in L.header_functions():
+        assert n in exported, n
+
+
+def test_status_strings_and_version():
+    lib = L.load_library()
+    assert lib.lbm_abi_version() == 1
+    for s in range(9):
+        assert lib.lbm_status_string(s)
+
+
+def test_struct_sizes_match_header():
+    # lbm_params: 6 ints + 16 doubles + 2 ints + 7 doubles (natural alignment)
+    assert ctypes.sizeof(L.Params) == 6 * 4 + 16 * 8 + 2 * 4 + 7 * 8
+    assert ctypes.sizeof(L.PoissonCfg) == 40
+    assert ctypes.sizeof(L.StepStats) == 8 + 16 * 8 + 6 * 4 + 8
+    assert ctypes.sizeof(L.Timing) == 5 * 8 + 3 * 8
+
+
+def test_create_without_gpu_fails_loudly():
+    """On a machine without an sm_100 GPU the solver refuses to start (no CPU fallback)."""
+    import torch
+    if torch.cuda.is_available():
+        return
+    p = L.make_params(lx=8, ly=8, lz=8)
+    try:
+        L.InamuroCUDA(p)
+    except L.LBMError as e:
+        assert e.status == 7
+    else:
+        raise AssertionError("expected LBM_ERR_NO_DEVICE")
+
+
+def test_header_compiles_as_c():
+    src = "#include \"lbm_b200.h\"\nint main(void){lbm_params p; lbm_params_default(&p); return p.lx != 48;}\n"
+    inc = os.path.join(os.path.dirname(L.HEADER_PATH))
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-fsyntax-only", "-I", inc, "-x", "c", "-"],
+                       input=src, text=True, capture_output=True)
+    assert r.returncode == 0, r.stderr
