@@ -1,0 +1,411 @@
+"""Benchmark of the Inamuro two-phase D3Q15 droplet step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+                    [--impl ours|reference]
+
+Workload (the head-on binary droplet collision): 256^3 box, two spheres R = 32
+whose centres are 96 cells apart, approaching at +-0.02 (lattice units),
+rho_L/rho_G = 100, a = 1, b = 6.7, T = 0.035, kappa_f = 0.06, kappa_g = 6e-6,
+tau_f = tau_g = 1, mu = 0.1 rho (nu = 0.1 in both phases), tanh interface with
+W = 4 (interface_width = 2), seeded uniform noise of amplitude 1e-4 on phi.
+The collision runs along z: x carries the reference's slip walls.  The Poisson
+stop is the contract shared by every reference entry point (check every 100
+sweeps, relative pressure change below 1e-3; WHILE_BASELINE.md); --dual adds
+the GPU production switch's kinetic fixed-point residual.  Inputs are synthetic;
+the box (about 14 GB of FP64 state) is far larger than L2, so no flush is
+needed between timed steps.
+
+A step is one full time step including its Poisson solve.  The metric is
+MLUPS with Poisson sweeps counted: cells * (steps + sweeps) / time / 1e6.
+
+--impl reference times the reference's own CPU solver (oracle/_ref, built from
+the unmodified reference sources) on the host cores with a bounded sample of
+the same 256^3 workload: one non-Poisson step part plus a few kinetic sweeps,
+extrapolated to the sweeps-per-step of the GPU run.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MLUPS (Poisson sweeps counted) of the Inamuro D3Q15 droplet step"
+UNIT = "MLUPS"
+N_SIDE = 256
+# Algorithmic bytes per cell of one kinetic Poisson sweep (FP64: 30 pops +
+# rho, s, p_in, p_out; mixed: FP32 pops).
+SWEEP_BYTES = {"fp64": 272.0, "mixed": 144.0}
+# Mean sweeps per step of this workload (measured on B200 with this bench);
+# the CPU sample is extrapolated to it when no GPU run preceded it.
+DEFAULT_SWEEPS_PER_STEP = 1000.0
+
+
+def workload_params(n=N_SIDE):
+    import lbm_b200 as L
+    return L.make_params(lx=n, ly=n, lz=n, rho_L=100.0, rho_G=1.0, mu_L=10.0, mu_G=0.1, tauf=1.0,
+                         taug=1.0, k_f=0.06, k_g=6e-6, T=0.035, a=1.0, b=6.7, DD=64.0,
+                         init_single_droplet=0, init_tanh=1, interface_width=2.0,
+                         init_velocity=0.02, init_center_x=n / 2.0, init_separation=48.0)
+
+
+def workload_fields(p, seed=1234):
+    import lbm_b200 as L
+    f = L.init_droplets(p)
+    rng = np.random.default_rng(seed)
+    f["phi"] = f["phi"] + rng.uniform(-1e-4, 1e-4, size=f["phi"].shape)
+    return f
+
+
+def config_dict(n, precision, dual=False):
+    return {"workload": f"head-on binary droplet collision {n}^3, 2 x R=32 drops 96 apart, "
+                        f"+-0.02, rho_L/rho_G=100",
+            "box": [n, n, n], "cells": n ** 3, "precision": precision,
+            "poisson": {"check_interval": 100, "tolerance": 1e-3, "dual_residual": dual},
+            "l2": "inputs larger than L2 (14 GB FP64 state vs 126 MB L2)",
+            "parallelism": "replicas (one box per GPU)"}
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """Samples nvidia-smi clocks/throttle reasons in the background."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) < 9:
+                continue
+            for name, val in zip(names, r[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------- CPU sample
+def reference_cpu_samples(n, sample_sweeps=1, reps=1):
+    """Runs the reference CPU solver (oracle/_ref/ref_cpu_harness, built from
+    the unmodified reference sources) on the n^3 workload: `reps` times one
+    non-Poisson step part + `sample_sweeps` kinetic sweeps.  Returns
+    ([(seconds_nonpoisson, seconds_per_sweep), ...], cells, wall_s) or raises."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_cpu_harness")
+    if not os.path.exists(exe):
+        raise FileNotFoundError("reference harness not built (oracle/_ref missing)")
+    import lbm_b200 as L
+    p = workload_params(n)
+    f = workload_fields(p)
+    with tempfile.TemporaryDirectory() as tmp:
+        pf = os.path.join(tmp, "params.in")
+        with open(pf, "w") as fh:
+            fh.write(f"{n} {n} {n}\n1\n20\n20\n{p.rho_L!r} {p.rho_G!r}\n{p.tauf!r} {p.taug!r}\n"
+                     f"{p.mu_L!r} {p.mu_G!r}\n{p.k_f!r} {p.k_g!r}\n{p.T!r}\n{p.a!r}\n{p.b!r}\n"
+                     f"{p.fei_max!r} {p.fei_min!r}\n{p.fei_L!r} {p.fei_G!r}\n{p.DD!r}\n")
+        ib = os.path.join(tmp, "init.bin")
+        np.concatenate([f[k].ravel() for k in L.FIELDS]).tofile(ib)
+        del f
+        t0 = time.perf_counter()
+        r = subprocess.run([exe, "--params", pf, "--sample-sweeps", str(sample_sweeps), "--out", tmp,
+                            "--init", ib, "--sample-reps", str(reps)], capture_output=True, text=True)
+        wall = time.perf_counter() - t0
+        if r.returncode != 0:
+            raise RuntimeError(f"reference harness failed: {r.stderr[-300:]}")
+        cells, reps_out = None, []
+        for line in open(os.path.join(tmp, "sample.txt")):
+            parts = line.split()
+            if parts[0] == "cells":
+                cells = float(parts[1])
+            elif parts[0] == "rep":
+                reps_out.append((float(parts[2]) / 1e3, float(parts[3]) / 1e3 / max(sample_sweeps, 1)))
+    return reps_out, cells, wall
+
+
+def cpu_value(cells, t_np, t_sw, sweeps_per_step):
+    """MLUPS (sweeps counted) of a step with `sweeps_per_step` sweeps."""
+    return cells * (1.0 + sweeps_per_step) / (t_np + sweeps_per_step * t_sw) / 1e6
+
+
+def cpu_baseline_entry(n, reps_out, cells, wall, sweeps_per_step, sample_sweeps, value=None):
+    t_np = statistics.median(r[0] for r in reps_out)
+    t_sw = statistics.median(r[1] for r in reps_out)
+    v = cpu_value(cells, t_np, t_sw, sweeps_per_step) if value is None else value
+    sample = (f"reference CPU solver (CPU/Inamuro.cpp, g++ -O3, single-threaded) on the {n}^3 "
+              f"workload, {len(reps_out)} rep(s) of 1 non-Poisson step part ({t_np:.2f} s) + "
+              f"{sample_sweeps} kinetic sweep(s) ({t_sw:.2f} s each), extrapolated to "
+              f"{sweeps_per_step:.0f} sweeps/step; harness wall {wall:.1f} s incl. setup")
+    return {"value": v, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample,
+            "seconds_per_sweep": t_sw, "seconds_nonpoisson": t_np}
+
+
+# ---------------------------------------------------------------- helpers
+def dist_setup(gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        backend = os.environ.get("LBM_BENCH_BACKEND", "nccl")
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def dist_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_sum(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def read_traffic(precision):
+    """DRAM bytes per sweep launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"sweep_{precision}_256.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_launch_256:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- arms
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    n = args.size
+    try:
+        reps_out, cells, wall = reference_cpu_samples(n, args.sample_sweeps, args.warmup + args.steps)
+    except Exception as e:  # harness missing or failed: report, do not crash the driver
+        print(json.dumps({"impl": "reference", "unavailable": str(e)[:200]}))
+        return 0
+    timed = reps_out[args.warmup:] or reps_out
+    vals = [cpu_value(cells, t_np, t_sw, args.sweeps_per_step) for t_np, t_sw in timed]
+    value = statistics.median(vals)
+    step_s = statistics.median(t_np + args.sweeps_per_step * t_sw for t_np, t_sw in timed)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_dict(n, "fp64"), "impl": "reference",
+            "cpu_baseline": cpu_baseline_entry(n, timed, cells, wall, args.sweeps_per_step,
+                                               args.sample_sweeps, value=value),
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    world, rank, local = dist_setup(args.gpus)
+    import lbm_b200 as L
+    n = args.size
+    p = workload_params(n)
+    f = workload_fields(p, seed=1234 + rank)
+    dual = args.dual
+    g = L.InamuroCUDA(p, f, precision=args.precision, device=local)
+    g.set_poisson(check_interval=100, tolerance=1e-3, dual=dual, max_sweeps=args.max_sweeps)
+    # warm-up steps (also the first, equilibrium-initialised step)
+    for _ in range(args.warmup):
+        g.step(1)
+    g.synchronize()
+    barrier(world)
+    g.reset_timing()
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0 = time.perf_counter()
+    stats = g.step(args.steps)
+    g.synchronize()
+    wall = time.perf_counter() - t0
+    barrier(world)
+    clk = clocks.stop()
+    tm = g.timing()
+    dev_s = sum(s["device_ms"] for s in stats) / 1e3
+    sweeps = sum(s["iterations"] for s in stats)
+    units = float(p.lx * p.ly * p.lz) * (args.steps + sweeps)
+    t_max = dist_max(dev_s, world)
+    units_all = dist_sum(units, world)
+    value = units_all / t_max / 1e6
+    launches = int(dist_sum(tm["kernel_launches"], world))
+
+    # roofline of the dominant kernel (the kinetic sweep)
+    sweep_ms = tm["poisson_ms"] / max(tm["sweep_kernels"], 1)
+    bytes_per_launch = SWEEP_BYTES[args.precision] * p.lx * p.ly * p.lz
+    achieved = bytes_per_launch / (sweep_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = read_traffic(args.precision)
+
+    # end to end through the public API with host buffers: upload the initial
+    # fields from pinned host memory, run K steps, download all six fields
+    # after every step.
+    e2e = None
+    if not args.no_e2e:
+        import torch
+        pinned = {k: torch.from_numpy(np.ascontiguousarray(f[k])).pin_memory() for k in L.FIELDS}
+        outs = {k: torch.empty(f[k].shape, dtype=torch.float64).pin_memory() for k in L.FIELDS}
+        h2d = 6 * p.lx * p.ly * p.lz * 8
+        g.synchronize()
+        barrier(world)
+        t0 = time.perf_counter()
+        g.load_fields({k: pinned[k].numpy() for k in L.FIELDS})
+        e_sweeps = 0
+        for _ in range(args.steps):
+            st = g.step(1)[0]
+            e_sweeps += st["iterations"]
+            for k in L.FIELDS:
+                g.download(k, outs[k].numpy())
+        g.synchronize()
+        e_wall = time.perf_counter() - t0
+        barrier(world)
+        e_units = float(p.lx * p.ly * p.lz) * (args.steps + e_sweeps)
+        e_value = dist_sum(e_units, world) / dist_max(e_wall, world) / 1e6
+        e2e = {"value": e_value, "unit": UNIT, "h2d_bytes_per_step": h2d // args.steps,
+               "d2h_bytes_per_step": h2d, "steps": args.steps, "sweeps": e_sweeps,
+               "note": "fresh run from the host initial condition: one H2D upload of the six "
+                       "fields (amortised per step) + K steps + D2H of all six fields after each "
+                       "step, host wall clock"}
+    g.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            reps_out, cells, cwall = reference_cpu_samples(n, args.sample_sweeps, 1)
+            cpu = cpu_baseline_entry(n, reps_out, cells, cwall, sweeps / max(args.steps, 1),
+                                     args.sample_sweeps)
+        except Exception as e:
+            cpu = {"value": None, "unavailable": str(e)[:200]}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+                "data": "synthetic (seeded droplet initial condition, random noise 1e-4 on phi)",
+                "config": config_dict(n, args.precision, dual),
+                "sweeps_per_step": sweeps / args.steps,
+                "converged_steps": int(sum(s["converged"] for s in stats)),
+                "mlups_reference_definition": float(p.lx * p.ly * p.lz) * args.steps * world / t_max / 1e6,
+                "gpu_launches": launches,
+                "clocks": clk,
+                "roofline": {"bound": "hbm", "kernel": f"sweep ({args.precision})",
+                             "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "peak_kind": peak_kind,
+                             "traffic": traffic, "bytes_per_cell": SWEEP_BYTES[args.precision],
+                             "avg_launch_ms": sweep_ms},
+                "phase_ms_per_step": {k: tm[k] / max(tm["steps"], 1) for k in
+                                      ("collide_ms", "moments_ms", "prep_ms", "poisson_ms", "correct_ms")},
+                "wall_s": wall,
+                "e2e": e2e, "cpu_baseline": cpu}
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64")
+    ap.add_argument("--size", type=int, default=N_SIDE)
+    ap.add_argument("--dual", action="store_true",
+                    help="also require the kinetic fixed-point residual (GPU production switch)")
+    ap.add_argument("--max-sweeps", type=int, default=500000,
+                    help="per-step sweep cap (a multiple of 100); reported if reached")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--sample-sweeps", type=int, default=1)
+    ap.add_argument("--sweeps-per-step", type=float, default=DEFAULT_SWEEPS_PER_STEP)
+    args = ap.parse_args(argv)
+    if args.warmup < 0 or args.steps < 1:
+        ap.error("steps >= 1, warmup >= 0")
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

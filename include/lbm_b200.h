@@ -132,6 +132,7 @@ typedef struct {
     uint64_t steps;
     uint64_t sweeps;         /* Poisson sweeps summed over steps */
     uint64_t sweep_kernels;  /* sweep-kernel launches (incl. the extra one per check) */
+    uint64_t kernel_launches;/* all kernels launched by the library (graph nodes included) */
 } lbm_timing;
 
 typedef struct lbm_handle lbm_handle;

@@ -359,6 +359,8 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
     uint64_t iters = 0;
     bool first_seg = true;
     uint64_t kernels = 0;
+    // collide, moments, 2 finalize, prep, finalize, poisson_init (+ correct below)
+    uint64_t launches = 7;
     for (;;) {
         const int n_normal = dual ? (first_seg ? ci - 1 : ci - 2) : ci - 1;
         SegKey key{hcur, n_normal, dual};
@@ -369,6 +371,7 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
         LBM_CUDA(h, cudaStreamSynchronize(st));
         hcur ^= segment_parity_change(n_normal, dual);
         kernels += static_cast<uint64_t>(n_normal) + 2 + (dual ? 1 : 0);
+        launches += static_cast<uint64_t>(n_normal) + 4 + (dual ? 1 : 0);
         first_seg = false;
         if (dh.error) {
             return fail(h, static_cast<lbm_status>(dh.error), site_text(dh.error_site));
@@ -410,6 +413,7 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
     h->acc.steps += 1;
     h->acc.sweeps += iters;
     h->acc.sweep_kernels += kernels;
+    h->acc.kernel_launches += launches + 1;
     h->steps_done += 1;
     if (stats) {
         fill_stats(h, dh, stats);

@@ -14,10 +14,11 @@
 //           Writes DIR/init.bin, DIR/step%04d.bin (phi rho u v w p, N doubles
 //           each, x fastest, no ghost layers) and DIR/summary.txt
 //           ("step sweeps ms" per line).
-//   sample: --params F --sample-sweeps K --out DIR [--init FIELDS.bin]
-//           Times one non-Poisson step part (collision, stream, bounce,
-//           moments) and K kinetic Poisson sweeps (collision_p, stream,
-//           bounce, getp) on the box of F; writes DIR/sample.txt.
+//   sample: --params F --sample-sweeps K --out DIR [--init FIELDS.bin] [--sample-reps R]
+//           R times (default 1): times one non-Poisson step part (collision,
+//           stream, bounce, moments) and K kinetic Poisson sweeps
+//           (collision_p, stream, bounce, getp) on the box of F; writes
+//           DIR/sample.txt ("cells N", then "rep i nonpoisson_ms sweeps_ms").
 #include <chrono>
 #include <cstdint>
 #include <cstdio>
@@ -130,6 +131,7 @@ int main(int argc, char** argv)
     std::string params, out, init;
     int steps = 0;
     long sample_sweeps = -1;
+    int sample_reps = 1;
     bool dump_h = false;
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
@@ -142,6 +144,7 @@ int main(int argc, char** argv)
         else if (a == "--out") out = val();
         else if (a == "--init") init = val();
         else if (a == "--sample-sweeps") sample_sweeps = std::stol(val());
+        else if (a == "--sample-reps") sample_reps = std::stoi(val());
         else if (a == "--dump-h") dump_h = true;
         else {
             std::cerr << "unknown argument " << a << "\n";
@@ -157,17 +160,20 @@ int main(int argc, char** argv)
         if (!init.empty()) h.loadFields(readRaw(init, 6 * h.cells()));
         using clk = std::chrono::steady_clock;
         if (sample_sweeps >= 0) {
-            const auto t0 = clk::now();
-            h.nonPoissonPart();
-            const auto t1 = clk::now();
-            for (long k = 0; k < sample_sweeps; ++k) h.sweep();
-            const auto t2 = clk::now();
             std::ofstream s(out + "/sample.txt");
             s.precision(17);
-            s << "cells " << h.cells() << "\n"
-              << "nonpoisson_ms " << std::chrono::duration<double, std::milli>(t1 - t0).count() << "\n"
-              << "sweeps " << sample_sweeps << "\n"
-              << "sweeps_ms " << std::chrono::duration<double, std::milli>(t2 - t1).count() << "\n";
+            s << "cells " << h.cells() << "\n";
+            for (int r = 0; r < sample_reps; ++r) {
+                const auto t0 = clk::now();
+                h.nonPoissonPart();
+                const auto t1 = clk::now();
+                for (long k = 0; k < sample_sweeps; ++k) h.sweep();
+                const auto t2 = clk::now();
+                s << "rep " << r << " "
+                  << std::chrono::duration<double, std::milli>(t1 - t0).count() << " "
+                  << std::chrono::duration<double, std::milli>(t2 - t1).count() << "\n";
+                s.flush();
+            }
             return 0;
         }
         h.dumpFields(out + "/init.bin");
