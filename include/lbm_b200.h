@@ -135,6 +135,18 @@ typedef struct {
     uint64_t kernel_launches;/* all kernels launched by the library (graph nodes included) */
 } lbm_timing;
 
+/* Statistics of one field over the box (Inamuro::FieldStatistics,
+ * CPU/Inamuro.hpp:91-99, filled as collectDiagnostics does,
+ * CPU/Inamuro.cpp:412-507, 1050-1092): NaN and +-Inf values are counted and
+ * left out; min, max, mean and abs_max are over the finite values (NaN when
+ * there are none).  sum is the sum of the finite values (the mass for phi). */
+typedef struct {
+    double min, max, mean, abs_max;
+    uint64_t nan_count, inf_count;
+    double sum;
+    uint64_t valid_count;
+} lbm_field_stats;
+
 typedef struct lbm_handle lbm_handle;
 
 /* ---- params and initial condition (host only, no GPU needed) ---- */
@@ -209,6 +221,12 @@ lbm_status lbm_download_h(lbm_handle* h, double* host);
 /* Device pointer of a field (physical layout, FP64 handles only, valid until
  * the next call on the handle).  For device-resident consumers. */
 lbm_status lbm_field_device_ptr(lbm_handle* h, lbm_field which, const double** dev);
+
+/* Device reduction of one field's statistics (Inamuro::collectDiagnostics /
+ * updateFieldStatistics / finalizeFieldStatistics, CPU/Inamuro.cpp:412-507,
+ * 1050-1092; the reference computes them on the host after a download).
+ * Fixed-order reduction: repeated calls give identical results. */
+lbm_status lbm_field_statistics(lbm_handle* h, lbm_field which, lbm_field_stats* out);
 
 /* InamuroCUDA::synchronize (GPU/InamuroCUDA.cu:1709-1712). */
 lbm_status lbm_synchronize(lbm_handle* h);

@@ -82,6 +82,16 @@ class Timing(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class FieldStats(C.Structure):
+    """lbm_field_stats: Inamuro::FieldStatistics (CPU/Inamuro.hpp:91-99) + sum."""
+    _fields_ = [(k, C.c_double) for k in ("min", "max", "mean", "abs_max")] + \
+        [("nan_count", C.c_uint64), ("inf_count", C.c_uint64), ("sum", C.c_double),
+         ("valid_count", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class LBMError(RuntimeError):
     def __init__(self, status: int, message: str = ""):
         name = STATUS.get(status, str(status))
@@ -121,6 +131,7 @@ def load_library(path: str = LIB_PATH):
     L.lbm_download_h.argtypes = [H, dp]
     L.lbm_field_device_ptr.argtypes = [H, C.c_int, C.POINTER(C.c_void_p)]
     L.lbm_synchronize.argtypes = [H]
+    L.lbm_field_statistics.argtypes = [H, C.c_int, C.POINTER(FieldStats)]
     L.lbm_get_timing.argtypes = [H, C.POINTER(Timing)]
     L.lbm_reset_timing.argtypes = [H]
     L.lbm_set_timing.argtypes = [H, C.c_int]
@@ -280,6 +291,13 @@ class InamuroCUDA:
 
     def synchronize(self):
         self._check(self._lib.lbm_synchronize(self._h), "synchronize")
+
+    def field_statistics(self, name: str) -> Dict[str, float]:
+        """Device-side Inamuro::collectDiagnostics statistics of one field."""
+        st = FieldStats()
+        self._check(self._lib.lbm_field_statistics(self._h, FIELD_ID[name], C.byref(st)),
+                    "field_statistics")
+        return st.as_dict()
 
     # -- Poisson configuration --------------------------------------------
     def set_poisson(self, check_interval: int = 100, tolerance: float = 1e-3, dual: bool = False,

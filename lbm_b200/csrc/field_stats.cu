@@ -1,0 +1,134 @@
+// field_stats.cu -- device reduction of the per-field statistics of the
+// reference's collectDiagnostics (CPU/Inamuro.cpp:412-507) and
+// updateFieldStatistics / finalizeFieldStatistics (:1050-1092).
+//
+// Two passes, both in a fixed order (results are run-to-run identical):
+//   stats_partial_kernel  block b reduces cells [4096 b, 4096 (b+1)): each of
+//                         its 256 threads visits 16 cells (stride 256, so
+//                         every warp load is coalesced), then a fixed
+//                         shuffle/shared-memory tree
+//   stats_final_kernel    one block folds the per-block partials
+// The partials live in caller-provided global scratch (7 doubles per block).
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#include "../../include/lbm_b200.h"
+#include "field_stats.cuh"
+
+namespace lbm {
+namespace {
+
+enum { T_SUM = 0, T_CNT, T_NAN, T_INF, T_MIN, T_MAX, T_AMAX };
+
+template <class T>
+__global__ void __launch_bounds__(256)
+stats_partial_kernel(const T* __restrict__ f, long long n, double* __restrict__ part, long long nblocks)
+{
+    double v[kStatsTerms] = {0.0, 0.0, 0.0, 0.0, CUDART_INF, -CUDART_INF, 0.0};
+    const long long base = (long long)blockIdx.x * kStatsCellsPerBlock + threadIdx.x;
+#pragma unroll 4
+    for (int k = 0; k < kStatsCellsPerBlock / 256; ++k) {
+        const long long i = base + 256LL * k;
+        if (i < n) {
+            const double x = static_cast<double>(f[i]);
+            if (isnan(x)) {
+                v[T_NAN] += 1.0;
+            } else if (isinf(x)) {
+                v[T_INF] += 1.0;
+            } else {
+                v[T_SUM] += x;
+                v[T_CNT] += 1.0;
+                v[T_MIN] = fmin(v[T_MIN], x);
+                v[T_MAX] = fmax(v[T_MAX], x);
+                v[T_AMAX] = fmax(v[T_AMAX], fabs(x));
+            }
+        }
+    }
+    __shared__ double red[8][kStatsTerms];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int t = 0; t < kStatsTerms; ++t) {
+        double s = v[t];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double other = __shfl_xor_sync(0xffffffffu, s, o);
+            s = (t == T_MIN) ? fmin(s, other) : (t >= T_MAX) ? fmax(s, other) : s + other;
+        }
+        if (lane == 0) red[warp][t] = s;
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int t = 0; t < kStatsTerms; ++t) {
+            const double ident = (t == T_MIN) ? CUDART_INF : (t == T_MAX) ? -CUDART_INF : 0.0;
+            double s = lane < 8 ? red[lane][t] : ident;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double other = __shfl_xor_sync(0xffffffffu, s, o);
+                s = (t == T_MIN) ? fmin(s, other) : (t >= T_MAX) ? fmax(s, other) : s + other;
+            }
+            if (lane == 0) part[(long long)t * nblocks + blockIdx.x] = s;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(1024)
+stats_final_kernel(const double* __restrict__ part, long long nblocks, lbm_field_stats* __restrict__ out)
+{
+    __shared__ double sm[1024];
+    double r[kStatsTerms];
+    for (int t = 0; t < kStatsTerms; ++t) {
+        const double ident = (t == T_MIN) ? CUDART_INF : (t == T_MAX) ? -CUDART_INF : 0.0;
+        double acc = ident;
+        for (long long i = threadIdx.x; i < nblocks; i += blockDim.x) {
+            const double x = part[(long long)t * nblocks + i];
+            acc = (t == T_MIN) ? fmin(acc, x) : (t >= T_MAX) ? fmax(acc, x) : acc + x;
+        }
+        sm[threadIdx.x] = acc;
+        __syncthreads();
+        for (int stride = blockDim.x / 2; stride > 0; stride >>= 1) {
+            if (threadIdx.x < stride) {
+                const double a = sm[threadIdx.x], b = sm[threadIdx.x + stride];
+                sm[threadIdx.x] = (t == T_MIN) ? fmin(a, b) : (t >= T_MAX) ? fmax(a, b) : a + b;
+            }
+            __syncthreads();
+        }
+        r[t] = sm[0];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        lbm_field_stats s;
+        const unsigned long long valid = static_cast<unsigned long long>(r[T_CNT]);
+        s.valid_count = valid;
+        s.nan_count = static_cast<unsigned long long>(r[T_NAN]);
+        s.inf_count = static_cast<unsigned long long>(r[T_INF]);
+        s.sum = r[T_SUM];
+        if (valid == 0) {
+            s.min = s.max = s.mean = s.abs_max = CUDART_NAN;
+        } else {
+            s.min = r[T_MIN];
+            s.max = r[T_MAX];
+            s.abs_max = r[T_AMAX];
+            s.mean = r[T_SUM] / static_cast<double>(valid);
+        }
+        *out = s;
+    }
+}
+
+}  // namespace
+
+template <class T>
+cudaError_t field_stats(cudaStream_t st, const T* f, long long n, double* partials,
+                        lbm_field_stats* dev_out)
+{
+    const long long nb = stats_blocks(n);
+    if (nb <= 0 || nb > 0x7fffffffLL) return cudaErrorInvalidValue;
+    stats_partial_kernel<T><<<static_cast<unsigned>(nb), 256, 0, st>>>(f, n, partials, nb);
+    stats_final_kernel<<<1, 1024, 0, st>>>(partials, nb, dev_out);
+    return cudaGetLastError();
+}
+
+template cudaError_t field_stats<double>(cudaStream_t, const double*, long long, double*, lbm_field_stats*);
+template cudaError_t field_stats<float>(cudaStream_t, const float*, long long, double*, lbm_field_stats*);
+
+}  // namespace lbm

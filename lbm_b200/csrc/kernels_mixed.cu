@@ -24,5 +24,6 @@ int mixed_segment(cudaStream_t, MixedBuffers&, const Launch&, const Geom&, int s
     return start_parity;
 }
 void mixed_correct(cudaStream_t, MixedBuffers&, const Launch&, const Geom&) {}
+const void* mixed_field_ptr(const MixedBuffers&, int) { return nullptr; }
 
 }  // namespace lbm

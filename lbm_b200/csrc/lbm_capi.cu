@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "../../include/lbm_b200.h"
+#include "field_stats.cuh"
 #include "lbm_solver.cuh"
 #include "lbm_mixed.cuh"
 
@@ -70,6 +71,8 @@ struct lbm_handle {
     cudaEvent_t ev[6]{};
     lbm_timing acc{};
     uint64_t steps_done = 0;
+    double* stats_part = nullptr;        // field-statistics partials
+    lbm_field_stats* stats_dev = nullptr;
 };
 
 namespace {
@@ -146,6 +149,10 @@ void free_all(lbm_handle* h)
         *p = nullptr;
     }
     mixed_free(h->mb);
+    if (h->stats_part) cudaFree(h->stats_part);
+    if (h->stats_dev) cudaFree(h->stats_dev);
+    h->stats_part = nullptr;
+    h->stats_dev = nullptr;
     if (h->ds) cudaFree(h->ds);
     if (h->ds_host) cudaFreeHost(h->ds_host);
     h->ds = nullptr;
@@ -537,6 +544,9 @@ lbm_status lbm_create(const lbm_params* prm, lbm_precision precision, int device
         if (cudaEventCreate(&e) != cudaSuccess) return bail(LBM_ERR_CUDA);
     if (cudaMalloc(&h->ds, sizeof(DevState)) != cudaSuccess) return bail(LBM_ERR_OOM);
     if (cudaMallocHost(&h->ds_host, sizeof(DevState)) != cudaSuccess) return bail(LBM_ERR_OOM);
+    if (cudaMalloc(&h->stats_part, sizeof(double) * kStatsTerms * stats_blocks(h->geom.n)) != cudaSuccess ||
+        cudaMalloc(&h->stats_dev, sizeof(lbm_field_stats)) != cudaSuccess)
+        return bail(LBM_ERR_OOM);
     std::memset(h->ds_host, 0, sizeof(DevState));
     if (precision == LBM_PRECISION_FP64) st = alloc_fp64(h);
     else st = mixed_alloc(h->mb, h->geom, h->L);
@@ -717,6 +727,26 @@ lbm_status lbm_field_device_ptr(lbm_handle* h, lbm_field which, const double** d
         return fail(h, LBM_ERR_BAD_ARG, "bad field");
     if (h->precision != LBM_PRECISION_FP64) return fail(h, LBM_ERR_BAD_ARG, "device pointers are FP64-only");
     *dev = field_ptr(h, which);
+    return LBM_OK;
+}
+
+lbm_status lbm_field_statistics(lbm_handle* h, lbm_field which, lbm_field_stats* out)
+{
+    if (check_handle(h) != LBM_OK || !out || which < LBM_FIELD_PHI || which > LBM_FIELD_P)
+        return fail(h, LBM_ERR_BAD_ARG, "bad field statistics request");
+    cudaSetDevice(h->device);
+    cudaError_t e;
+    if (h->precision == LBM_PRECISION_FP64) {
+        e = field_stats<double>(h->stream, field_ptr(h, which), h->geom.n, h->stats_part, h->stats_dev);
+    } else {
+        const void* f = mixed_field_ptr(h->mb, static_cast<int>(which));
+        e = (which == LBM_FIELD_P)
+                ? field_stats<double>(h->stream, static_cast<const double*>(f), h->geom.n, h->stats_part, h->stats_dev)
+                : field_stats<float>(h->stream, static_cast<const float*>(f), h->geom.n, h->stats_part, h->stats_dev);
+    }
+    if (e != cudaSuccess) return fail(h, LBM_ERR_CUDA, std::string("field statistics: ") + cudaGetErrorString(e));
+    LBM_CUDA(h, cudaMemcpyAsync(out, h->stats_dev, sizeof(lbm_field_stats), cudaMemcpyDeviceToHost, h->stream));
+    LBM_CUDA(h, cudaStreamSynchronize(h->stream));
     return LBM_OK;
 }
 

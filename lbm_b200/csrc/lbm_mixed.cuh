@@ -41,5 +41,7 @@ lbm_status mixed_prologue(cudaStream_t st, MixedBuffers& mb, const Launch& L, co
 int mixed_segment(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom& g,
                   int start_parity, int n_normal, bool dual, DevState* ds);
 void mixed_correct(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom& g);
+// Device pointer of a field: float for phi..w, double for p.
+const void* mixed_field_ptr(const MixedBuffers& mb, int which);
 
 }  // namespace lbm
