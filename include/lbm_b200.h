@@ -228,6 +228,34 @@ lbm_status lbm_field_device_ptr(lbm_handle* h, lbm_field which, const double** d
  * Fixed-order reduction: repeated calls give identical results. */
 lbm_status lbm_field_statistics(lbm_handle* h, lbm_field which, lbm_field_stats* out);
 
+/* Largest field lbm_field_statistics_noalloc accepts: 8192 partial blocks of
+ * 4096 cells each, the capacity of its static device scratch (8192 x 7 doubles,
+ * 458,752 bytes, plus one result record; every GPU that loads the library keeps
+ * that much reserved until the process exits). */
+#define LBM_NOALLOC_MAX_CELLS 33554432ULL
+
+/* Same statistics as lbm_field_statistics for a caller-owned device field of
+ * n_cells doubles, without allocating anything.  It has no counterpart in the
+ * reference.  It is for callers that must not allocate device memory: a host
+ * application that hands the GPU's memory to its own pool at start-up (an
+ * extra cudaMalloc would fail or fragment that pool), a time-critical loop
+ * that cannot afford cudaMalloc/cudaFree (they may synchronize the whole
+ * device), or a plugin that is given device pointers but no allocator.
+ *   - field: device pointer on the calling thread's current device;
+ *     stream: a cudaStream_t (NULL = the legacy default stream); the call
+ *     returns after the result has been copied into *out.
+ *   - The scratch is a static array inside the library, shared by every call
+ *     on a device and keeping the last call's contents; nothing in it needs to
+ *     start at zero (each block writes its own slot before the final pass reads
+ *     it).  Calls whose GPU work overlaps (other threads or streams) race on
+ *     it: serialise them.
+ *   - The first call on each device looks up the array's device address with
+ *     that device current; make that first call before any stream capture.
+ *   - Returns LBM_ERR_BAD_ARG for a null pointer, n_cells == 0 or
+ *     n_cells > LBM_NOALLOC_MAX_CELLS, LBM_ERR_CUDA on a CUDA failure. */
+lbm_status lbm_field_statistics_noalloc(const double* field, uint64_t n_cells, void* stream,
+                                        lbm_field_stats* out);
+
 /* InamuroCUDA::synchronize (GPU/InamuroCUDA.cu:1709-1712). */
 lbm_status lbm_synchronize(lbm_handle* h);
 

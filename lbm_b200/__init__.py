@@ -132,6 +132,8 @@ def load_library(path: str = LIB_PATH):
     L.lbm_field_device_ptr.argtypes = [H, C.c_int, C.POINTER(C.c_void_p)]
     L.lbm_synchronize.argtypes = [H]
     L.lbm_field_statistics.argtypes = [H, C.c_int, C.POINTER(FieldStats)]
+    L.lbm_field_statistics_noalloc.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p,
+                                               C.POINTER(FieldStats)]
     L.lbm_get_timing.argtypes = [H, C.POINTER(Timing)]
     L.lbm_reset_timing.argtypes = [H]
     L.lbm_set_timing.argtypes = [H, C.c_int]
@@ -188,6 +190,26 @@ def init_droplets(p: Params) -> Dict[str, np.ndarray]:
     if st != 0:
         raise LBMError(st, "init_droplets")
     return out
+
+
+NOALLOC_MAX_CELLS = 33554432  # LBM_NOALLOC_MAX_CELLS
+
+
+def field_statistics_noalloc(dev_ptr: int, n_cells: int, stream: Optional[int] = None) -> Dict[str, float]:
+    """lbm_field_statistics_noalloc: statistics of a caller-owned device field
+    (doubles on the current device) computed without any device allocation.
+    For callers that must not allocate (pre-reserved memory pools, loops where
+    cudaMalloc's device-wide synchronisation is not allowed, plugins without an
+    allocator).  The library's static scratch is shared by all calls on a
+    device, so calls must not overlap on the GPU; the first call on a device
+    should come before any stream capture."""
+    if n_cells > NOALLOC_MAX_CELLS:
+        raise LBMError(4, f"{n_cells} cells exceed the no-alloc maximum of {NOALLOC_MAX_CELLS}")
+    st = FieldStats()
+    code = load_library().lbm_field_statistics_noalloc(dev_ptr, n_cells, stream, C.byref(st))
+    if code != 0:
+        raise LBMError(code, "field_statistics_noalloc")
+    return st.as_dict()
 
 
 PRECISION = {"fp64": 0, "mixed": 1}

@@ -12,6 +12,8 @@
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
+#include <mutex>
+
 #include "../../include/lbm_b200.h"
 #include "field_stats.cuh"
 
@@ -132,3 +134,57 @@ template cudaError_t field_stats<double>(cudaStream_t, const double*, long long,
 template cudaError_t field_stats<float>(cudaStream_t, const float*, long long, double*, lbm_field_stats*);
 
 }  // namespace lbm
+
+// ---- lbm_field_statistics_noalloc ----------------------------------------
+// The same two passes with their scratch in a statically sized device array,
+// for callers that cannot allocate device memory (include/lbm_b200.h).
+namespace {
+
+constexpr long long kNoAllocMaxBlocks = 8192;   // x 4096 cells = LBM_NOALLOC_MAX_CELLS
+static_assert(kNoAllocMaxBlocks * lbm::kStatsCellsPerBlock == (long long)LBM_NOALLOC_MAX_CELLS,
+              "header limit and scratch capacity disagree");
+
+struct NoAllocScratch {
+    double partials[lbm::kStatsTerms * kNoAllocMaxBlocks];
+    lbm_field_stats result;
+};
+
+// One instance per device that loads the library, reserved until exit.
+static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+// In host code `g_noalloc_scratch` names a host-side shadow, not device memory:
+// its device address is looked up once per device (with that device current)
+// and cached here.
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+NoAllocScratch* g_noalloc_addr[kMaxDevices] = {};
+
+}  // namespace
+
+extern "C" lbm_status lbm_field_statistics_noalloc(const double* field, uint64_t n_cells, void* stream,
+                                                   lbm_field_stats* out)
+{
+    if (!field || !out || n_cells == 0 || n_cells > LBM_NOALLOC_MAX_CELLS) return LBM_ERR_BAD_ARG;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return LBM_ERR_CUDA;
+    NoAllocScratch* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_addr[dev]) {
+            void* addr = nullptr;
+            if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || !addr)
+                return LBM_ERR_CUDA;
+            g_noalloc_addr[dev] = static_cast<NoAllocScratch*>(addr);
+        }
+        scratch = g_noalloc_addr[dev];
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (lbm::field_stats<double>(st, field, static_cast<long long>(n_cells), scratch->partials,
+                                 &scratch->result) != cudaSuccess)
+        return LBM_ERR_CUDA;
+    if (cudaMemcpyAsync(out, &scratch->result, sizeof(lbm_field_stats), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return LBM_ERR_CUDA;
+    return LBM_OK;
+}
