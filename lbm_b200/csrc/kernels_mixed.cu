@@ -1,29 +1,608 @@
-// kernels_mixed.cu -- mixed-precision box (placeholder until the FP32
-// kernels land): every entry reports that the precision is unavailable.
+// kernels_mixed.cu -- mixed-precision box: FP32 populations and macro fields,
+// FP64 pressure accumulation, reductions and convergence test.
+//
+// Storage (all q-major SoA like the FP64 box):
+//   f*  FP32, deviation from the gas rest-state equilibrium
+//       f_rest,q = H_q phi_G + F_q p0(phi_G)      (sum_q f_rest,q = phi_G)
+//   g*  FP32, deviation from its rest weight g_rest,q = E_q
+//   h*  FP32 (its rest state E_q p_target is ~0: the gauge keeps mean p fixed)
+//   phi, rho, u, v, w, div, s, omega_h  FP32;  p, p_prev, p_chk  FP64
+// Equilibria and BGK are evaluated directly in deviation form (the rest
+// values cancel exactly in f - (f - f_eq)/tau), so FP32 keeps its mantissa
+// for the part that moves.  phi = phi_G + sum f_dev and p = sum h are
+// accumulated in FP64; all block reductions are FP64.
+//
+// The kernel sequence and the Poisson segment structure (A/B/C check kernels)
+// are those of kernels_fp64.cu; see there for the reference map.
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
 #include "lbm_mixed.cuh"
 
 namespace lbm {
+namespace {
 
-lbm_status mixed_alloc(MixedBuffers&, const Geom&, const Launch&) { return LBM_ERR_BAD_ARG; }
-lbm_status mixed_alloc_dual(MixedBuffers&, const Geom&) { return LBM_ERR_BAD_ARG; }
-void mixed_free(MixedBuffers&) {}
-lbm_status mixed_load(cudaStream_t, MixedBuffers&, const Geom&, const Phys&, const double* const[6],
-                      cudaMemcpyKind)
+__device__ __forceinline__ bool tile_coords(const Geom& g, int& x, int& y, int& z)
 {
-    return LBM_ERR_BAD_ARG;
+    x = blockIdx.x * blockDim.x + threadIdx.x;
+    y = blockIdx.y * blockDim.y + threadIdx.y;
+    z = blockIdx.z;
+    return x < g.lx && y < g.ly;
 }
-lbm_status mixed_download(cudaStream_t, MixedBuffers&, const Geom&, int, double*) { return LBM_ERR_BAD_ARG; }
-lbm_status mixed_prologue(cudaStream_t, MixedBuffers&, const Launch&, const Geom&, const Phys&, bool,
-                          int, bool, DevState*, cudaEvent_t*)
+
+template <class T>
+__device__ __forceinline__ void bounce_regs(T (&v)[Q], const Geom& g, int x)
 {
-    return LBM_ERR_BAD_ARG;
+    if (g.periodic_x) return;
+    if (x == 0) {
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            if constexpr (bounce_left(q) != q) v[q] = v[bounce_left(q)];
+        });
+    }
+    if (x == g.lx - 1) {
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            if constexpr (bounce_right(q) != q) v[q] = v[bounce_right(q)];
+        });
+    }
 }
-int mixed_segment(cudaStream_t, MixedBuffers&, const Launch&, const Geom&, int start_parity, int,
-                  bool, DevState*)
+
+__device__ __forceinline__ void pull_regs(float (&v)[Q], const float* __restrict__ src, const Geom& g,
+                                          int x, int y, int z)
 {
-    return start_parity;
+    const Wrap w(g, x, y, z);
+    static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        v[q] = __ldg(src + (long long)q * g.n + pull_src<q>(g, w, x, y, z));
+    });
 }
-void mixed_correct(cudaStream_t, MixedBuffers&, const Launch&, const Geom&) {}
-const void* mixed_field_ptr(const MixedBuffers&, int) { return nullptr; }
+
+template <bool kLap>
+__device__ __forceinline__ void stencil(const float* __restrict__ f, const Geom& g, const Mirror& m,
+                                        int x, int y, int z, long long c,
+                                        float& gx, float& gy, float& gz, float& lap)
+{
+    float ax = 0.f, ay = 0.f, az = 0.f, al = 0.f;
+    static_for<1, Q>([&](auto kc) {
+        constexpr int k = decltype(kc)::value;
+        const float val = __ldg(f + stencil_nb<k>(g, m, x, y, z));
+        ax = acc_signed<cx(k)>(ax, val);
+        ay = acc_signed<cy(k)>(ay, val);
+        az = acc_signed<cz(k)>(az, val);
+        if constexpr (kLap) al += val;
+    });
+    gx = ax * 0.1f;
+    gy = ay * 0.1f;
+    gz = az * 0.1f;
+    if constexpr (kLap) lap = (al - 14.f * __ldg(f + c)) * 0.2f;
+}
+
+struct MixPhys {
+    float rho_G, mu_G, mu_slope, inv_tauf, inv_taug, k_f, k_g, T, a, b, visc;
+    float fei_G, p0_G;          // gas rest state of f
+};
+
+template <bool kFirst>
+__global__ void __launch_bounds__(256)
+collide_kernel(Geom g, MixPhys P, const float* __restrict__ fin, float* __restrict__ fout,
+               const float* __restrict__ gin, float* __restrict__ gout,
+               const float* __restrict__ phi, const float* __restrict__ rho,
+               const float* __restrict__ u, const float* __restrict__ v,
+               const float* __restrict__ w, float* __restrict__ div_out,
+               double* __restrict__ part, long long nblocks)
+{
+    int x, y, z;
+    const bool active = tile_coords(g, x, y, z);
+    double red[3] = {0.0, 0.0, 0.0};
+    if (active) {
+        const long long c = cell_of(g, x, y, z);
+        const Mirror m(g, x, y, z);
+        float u_x, u_y, u_z, v_x, v_y, v_z, w_x, w_y, w_z, r_x, r_y, r_z, f_x, f_y, f_z;
+        float u_lap, v_lap, w_lap, f_lap, unused;
+        stencil<true>(u, g, m, x, y, z, c, u_x, u_y, u_z, u_lap);
+        stencil<true>(v, g, m, x, y, z, c, v_x, v_y, v_z, v_lap);
+        stencil<true>(w, g, m, x, y, z, c, w_x, w_y, w_z, w_lap);
+        stencil<false>(rho, g, m, x, y, z, c, r_x, r_y, r_z, unused);
+        stencil<true>(phi, g, m, x, y, z, c, f_x, f_y, f_z, f_lap);
+        (void)unused;
+        const float div = u_x + v_y + w_z;
+        div_out[c] = div;
+        if (isfinite(div)) {
+            red[0] = div;
+            red[1] = fabs((double)div);
+        } else {
+            red[2] = 1.0;
+        }
+        const float lrho = __ldg(rho + c), fei = __ldg(phi + c);
+        const float uu = __ldg(u + c), vv = __ldg(v + c), ww = __ldg(w + c);
+        const float inv_rho = 1.f / lrho;
+        const float mu = (lrho - P.rho_G) * P.mu_slope + P.mu_G;
+        const float sum_fei = f_x * f_x + f_y * f_y + f_z * f_z;
+        const float sum_rho = r_x * r_x + r_y * r_y + r_z * r_z;
+        const float usq = uu * uu + vv * vv + ww * ww;
+        const float p0 = fei * P.T / (1.f - P.b * fei) - P.a * fei * fei;
+        const float chem_dev = (p0 - P.p0_G) - P.k_f * fei * f_lap - P.k_f * sum_fei * (1.f / 6.f);
+        const float dphi = fei - P.fei_G;
+        const float kg_rho = P.k_g * inv_rho;
+
+        float fv[Q];
+        if constexpr (!kFirst) {
+            pull_regs(fv, fin, g, x, y, z);
+            bounce_regs(fv, g, x);
+        }
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            constexpr float E = float(wE(q)), F = float(wF(q));
+            const float un = dotq<q>(uu, vv, ww);
+            const float fe = dotq<q>(f_x, f_y, f_z);
+            float feq;   // f_eq - f_rest
+            if constexpr (q == 0) {
+                feq = dphi + F * chem_dev;
+            } else {
+                const float Gfei = 4.5f * fe * fe - 1.5f * float(csq(q)) * sum_fei;
+                feq = F * chem_dev + 3.f * E * fei * un + E * P.k_f * Gfei;
+            }
+            if constexpr (kFirst) fout[(long long)q * g.n + c] = feq;
+            else fout[(long long)q * g.n + c] = fv[q] - (fv[q] - feq) * P.inv_tauf;
+        });
+
+        float gv[Q];
+        if constexpr (!kFirst) {
+            pull_regs(gv, gin, g, x, y, z);
+            bounce_regs(gv, g, x);
+        }
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            constexpr float E = float(wE(q)), F = float(wF(q));
+            constexpr int X = cx(q), Y = cy(q), Z = cz(q);
+            const float un = dotq<q>(uu, vv, ww);
+            float geq;   // g_eq - E_q
+            if constexpr (q == 0) {
+                geq = -1.5f * E * usq - (2.f / 3.f) * F * kg_rho * sum_rho;
+            } else {
+                const float S = float(X * X) * u_x + float(X * Y) * u_y + float(X * Z) * u_z +
+                                float(Y * X) * v_x + float(Y * Y) * v_y + float(Y * Z) * v_z +
+                                float(Z * X) * w_x + float(Z * Y) * w_y + float(Z * Z) * w_z;
+                const float re = dotq<q>(r_x, r_y, r_z);
+                const float Grho = 4.5f * re * re - 1.5f * float(csq(q)) * sum_rho;
+                geq = E * (3.f * un - 1.5f * usq + 4.5f * un * un + P.visc * S) + E * kg_rho * Grho -
+                      (2.f / 3.f) * F * kg_rho * sum_rho;
+            }
+            float out;
+            if constexpr (kFirst) {
+                out = geq;
+            } else {
+                out = gv[q] - (gv[q] - geq) * P.inv_taug;
+                if constexpr (q != 0) out += 3.f * E * inv_rho * mu * dotq<q>(u_lap, v_lap, w_lap);
+            }
+            gout[(long long)q * g.n + c] = out;
+        });
+    }
+    block_sum_store<3>(red, part, nblocks, block_linear());
+}
+
+__global__ void __launch_bounds__(256)
+moments_kernel(Geom g, double fei_G, double fei_L, double rho_G, double rho_L, double fei_avg,
+               double dfei, double half_drho, const float* __restrict__ f,
+               const float* __restrict__ gp, float* __restrict__ phi, float* __restrict__ rho,
+               float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
+               double* __restrict__ part, long long nblocks)
+{
+    int x, y, z;
+    const bool active = tile_coords(g, x, y, z);
+    double red[1] = {0.0};
+    if (active) {
+        const long long c = cell_of(g, x, y, z);
+        float fv[Q];
+        pull_regs(fv, f, g, x, y, z);
+        bounce_regs(fv, g, x);
+        double dev = 0.0;
+        static_for<0, Q>([&](auto qc) { dev += (double)fv[decltype(qc)::value]; });
+        const double fei = fei_G + dev;
+        double density;
+        if (fei <= fei_G) density = rho_G;
+        else if (fei >= fei_L) density = rho_L;
+        else density = half_drho * (sin((fei - fei_avg) / dfei * CUDART_PI) + 1.0) + rho_G;
+        float gv[Q];
+        pull_regs(gv, gp, g, x, y, z);
+        bounce_regs(gv, g, x);
+        float uu = 0.f, vv = 0.f, ww = 0.f;
+        static_for<1, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            uu = acc_signed<cx(q)>(uu, gv[q]);
+            vv = acc_signed<cy(q)>(vv, gv[q]);
+            ww = acc_signed<cz(q)>(ww, gv[q]);
+        });
+        phi[c] = (float)fei;
+        rho[c] = (float)density;
+        u[c] = uu;
+        v[c] = vv;
+        w[c] = ww;
+        red[0] = fei;
+    }
+    block_sum_store<1>(red, part, nblocks, block_linear());
+}
+
+// s = div - mean(div); omega_h = 1 / (1/rho + 1/2); sum(p) for the gauge target.
+__global__ void __launch_bounds__(256)
+prep_kernel(Geom g, const DevState* __restrict__ ds, const float* __restrict__ div,
+            const float* __restrict__ rho, const double* __restrict__ p, float* __restrict__ s,
+            float* __restrict__ omega, double* __restrict__ part, long long nblocks)
+{
+    int x, y, z;
+    const bool active = tile_coords(g, x, y, z);
+    double red[3] = {0.0, 0.0, 0.0};
+    if (active) {
+        const long long c = cell_of(g, x, y, z);
+        const float sv = (float)((double)div[c] - ds->div_mean);
+        s[c] = sv;
+        omega[c] = 1.f / (1.f / rho[c] + 0.5f);
+        if (isfinite(sv)) red[0] = sv; else red[1] = 1.0;
+        red[2] = p[c];
+    }
+    block_sum_store<3>(red, part, nblocks, block_linear());
+}
+
+__device__ __forceinline__ void collide_h_store(const float (&hv)[Q], double pv, float om, float sv,
+                                                float* __restrict__ hout, long long n, long long c)
+{
+    const float p32 = (float)pv;
+    static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        constexpr float E = float(wE(q));
+        hout[(long long)q * n + c] = hv[q] - (hv[q] - E * p32) * om - (E * (1.f / 3.f)) * sv;
+    });
+}
+
+__device__ __forceinline__ double sum_q(const float (&hv)[Q])
+{
+    double acc = 0.0;
+    static_for<0, Q>([&](auto qc) { acc += (double)hv[decltype(qc)::value]; });
+    return acc;
+}
+
+__global__ void __launch_bounds__(256)
+poisson_init_kernel(Geom g, int h_loaded, const float* __restrict__ hload, float* __restrict__ hout,
+                    const double* __restrict__ p, const float* __restrict__ omega,
+                    const float* __restrict__ s)
+{
+    int x, y, z;
+    if (!tile_coords(g, x, y, z)) return;
+    const long long c = cell_of(g, x, y, z);
+    const double pv = p[c];
+    float hv[Q];
+    static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        hv[q] = h_loaded ? hload[(long long)q * g.n + c] : (float)(pv * wE(q));
+    });
+    collide_h_store(hv, pv, omega[c], s[c], hout, g.n, c);
+}
+
+__global__ void __launch_bounds__(256)
+sweep_kernel(Geom g, const float* __restrict__ hin, float* __restrict__ hout,
+             const float* __restrict__ omega, const float* __restrict__ s)
+{
+    int x, y, z;
+    if (!tile_coords(g, x, y, z)) return;
+    const long long c = cell_of(g, x, y, z);
+    float hv[Q];
+    pull_regs(hv, hin, g, x, y, z);
+    bounce_regs(hv, g, x);
+    collide_h_store(hv, sum_q(hv), __ldg(omega + c), __ldg(s + c), hout, g.n, c);
+}
+
+__global__ void __launch_bounds__(256)
+sweep_check_a_kernel(Geom g, const float* __restrict__ hin, float* __restrict__ hout,
+                     double* __restrict__ p_chk, double* __restrict__ part, long long nblocks)
+{
+    int x, y, z;
+    const bool active = tile_coords(g, x, y, z);
+    double red[1] = {0.0};
+    if (active) {
+        const long long c = cell_of(g, x, y, z);
+        float hv[Q];
+        pull_regs(hv, hin, g, x, y, z);
+        bounce_regs(hv, g, x);
+        const double pv = sum_q(hv);
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            hout[(long long)q * g.n + c] = hv[q];
+        });
+        p_chk[c] = pv;
+        red[0] = pv;
+    }
+    block_sum_store<1>(red, part, nblocks, block_linear());
+}
+
+template <bool kDual>
+__global__ void __launch_bounds__(256)
+sweep_check_b_kernel(Geom g, float* __restrict__ h, float* __restrict__ hc,
+                     const double* __restrict__ p_chk, double* __restrict__ p_prev,
+                     double* __restrict__ p, const float* __restrict__ omega,
+                     const float* __restrict__ s, const DevState* __restrict__ ds,
+                     double* __restrict__ part, long long nblocks)
+{
+    int x, y, z;
+    const bool active = tile_coords(g, x, y, z);
+    double red[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (active) {
+        const long long c = cell_of(g, x, y, z);
+        const double shift = ds->sigma;
+        const double tgt = ds->target;
+        float hv[Q];
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            hv[q] = (float)((double)h[(long long)q * g.n + c] - wE(q) * shift);
+        });
+        const double pv = p_chk[c] - shift;
+        if constexpr (kDual) {
+            static_for<0, Q>([&](auto qc) {
+                constexpr int q = decltype(qc)::value;
+                hc[(long long)q * g.n + c] = hv[q];
+            });
+            const double hsum = sum_q(hv);
+            red[2] = fabs(pv - hsum);
+            red[3] = fabs(pv - tgt);
+            red[4] = fabs(hsum - tgt);
+        }
+        red[0] = fabs(pv - p_prev[c]);
+        red[1] = fabs(pv);
+        p_prev[c] = pv;
+        p[c] = pv;
+        collide_h_store(hv, pv, __ldg(omega + c), __ldg(s + c), h, g.n, c);
+    }
+    block_sum_store<5>(red, part, nblocks, block_linear());
+}
+
+__global__ void __launch_bounds__(256)
+sweep_check_c_kernel(Geom g, const float* __restrict__ hin, float* __restrict__ hout,
+                     const float* __restrict__ hc, const float* __restrict__ omega,
+                     const float* __restrict__ s, const DevState* __restrict__ ds,
+                     double* __restrict__ part, long long nblocks)
+{
+    int x, y, z;
+    const bool active = tile_coords(g, x, y, z);
+    double red[3] = {0.0, 0.0, 0.0};
+    if (active) {
+        const long long c = cell_of(g, x, y, z);
+        const double tgt = ds->target;
+        float hv[Q];
+        pull_regs(hv, hin, g, x, y, z);
+        bounce_regs(hv, g, x);
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            const double hval = hc[(long long)q * g.n + c];
+            const double ge = wE(q) * tgt;
+            red[0] += fabs(hval - (double)hv[q]);
+            red[1] += fabs(hval - ge);
+            red[2] += fabs((double)hv[q] - ge);
+        });
+        collide_h_store(hv, sum_q(hv), __ldg(omega + c), __ldg(s + c), hout, g.n, c);
+    }
+    block_sum_store<3>(red, part, nblocks, block_linear());
+}
+
+__global__ void __launch_bounds__(256)
+correct_kernel(Geom g, float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
+               const double* __restrict__ p, const float* __restrict__ rho)
+{
+    int x, y, z;
+    if (!tile_coords(g, x, y, z)) return;
+    const Mirror m(g, x, y, z);
+    const long long c = cell_of(g, x, y, z);
+    const double inv_2rho = 1.0 / (2.0 * (double)rho[c]);
+    u[c] = (float)((double)u[c] - (p[cell_of(g, m.xp, y, z)] - p[cell_of(g, m.xm, y, z)]) * inv_2rho);
+    v[c] = (float)((double)v[c] - (p[cell_of(g, x, m.yp, z)] - p[cell_of(g, x, m.ym, z)]) * inv_2rho);
+    w[c] = (float)((double)w[c] - (p[cell_of(g, x, y, m.zp)] - p[cell_of(g, x, y, m.zm)]) * inv_2rho);
+}
+
+__global__ void to_float_kernel(const double* __restrict__ src, float* __restrict__ dst, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        dst[i] = (float)src[i];
+}
+
+__global__ void to_double_kernel(const float* __restrict__ src, double* __restrict__ dst, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        dst[i] = (double)src[i];
+}
+
+MixPhys mix_phys(const Phys& P)
+{
+    MixPhys M;
+    M.rho_G = (float)P.rho_G;
+    M.mu_G = (float)P.mu_G;
+    M.mu_slope = (float)P.mu_slope;
+    M.inv_tauf = (float)(1.0 / P.tauf);
+    M.inv_taug = (float)(1.0 / P.taug);
+    M.k_f = (float)P.k_f;
+    M.k_g = (float)P.k_g;
+    M.T = (float)P.T;
+    M.a = (float)P.a;
+    M.b = (float)P.b;
+    M.visc = (float)P.visc;
+    M.fei_G = (float)P.fei_G;
+    const double fg = P.fei_G;
+    M.p0_G = (float)(fg * P.T / (1.0 - P.b * fg) - P.a * fg * fg);
+    return M;
+}
+
+float* field_f(MixedBuffers& mb, int which)
+{
+    switch (which) {
+    case 0: return mb.phi;
+    case 1: return mb.rho;
+    case 2: return mb.u;
+    case 3: return mb.v;
+    case 4: return mb.w;
+    }
+    return nullptr;
+}
+
+}  // namespace
+
+lbm_status mixed_alloc(MixedBuffers& mb, const Geom& g, const Launch& L)
+{
+    const size_t n = static_cast<size_t>(g.n);
+    auto okf = [&](float** p, size_t count) { return cudaMalloc(p, count * sizeof(float)) == cudaSuccess; };
+    auto okd = [&](double** p, size_t count) { return cudaMalloc(p, count * sizeof(double)) == cudaSuccess; };
+    bool ok = true;
+    for (int i = 0; i < 2; ++i) ok = ok && okf(&mb.f[i], 15 * n) && okf(&mb.g[i], 15 * n) && okf(&mb.h[i], 15 * n);
+    ok = ok && okf(&mb.phi, n) && okf(&mb.rho, n) && okf(&mb.u, n) && okf(&mb.v, n) && okf(&mb.w, n) &&
+         okf(&mb.s, n) && okf(&mb.dux, n) && okf(&mb.dvy, n);
+    ok = ok && okd(&mb.p, n) && okd(&mb.p_prev, n) && okd(&mb.p_chk, n) && okd(&mb.scratch, n);
+    const size_t nb = static_cast<size_t>(L.nblocks);
+    ok = ok && okd(&mb.part_src, 3 * nb) && okd(&mb.part_prep, 3 * nb) && okd(&mb.part_a, nb) &&
+         okd(&mb.part_b, 5 * nb) && okd(&mb.part_c, 3 * nb) && okd(&mb.part_mass, nb);
+    if (!ok) {
+        mixed_free(mb);
+        return LBM_ERR_OOM;
+    }
+    cudaMemset(mb.part_c, 0, 3 * nb * sizeof(double));
+    mb.dwz = nullptr;
+    mb.allocated = true;
+    return LBM_OK;
+}
+
+lbm_status mixed_alloc_dual(MixedBuffers& mb, const Geom& g)
+{
+    if (mb.hc) return LBM_OK;
+    if (cudaMalloc(&mb.hc, 15 * static_cast<size_t>(g.n) * sizeof(float)) != cudaSuccess) return LBM_ERR_OOM;
+    return LBM_OK;
+}
+
+void mixed_free(MixedBuffers& mb)
+{
+    float** fl[] = {&mb.f[0], &mb.f[1], &mb.g[0], &mb.g[1], &mb.h[0], &mb.h[1], &mb.hc, &mb.phi, &mb.rho,
+                    &mb.u, &mb.v, &mb.w, &mb.s, &mb.dux, &mb.dvy, &mb.dwz};
+    for (float** p : fl) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
+    double** db[] = {&mb.p, &mb.p_prev, &mb.p_chk, &mb.scratch, &mb.part_src, &mb.part_prep, &mb.part_a,
+                     &mb.part_b, &mb.part_c, &mb.part_mass};
+    for (double** p : db) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
+    mb.allocated = false;
+}
+
+lbm_status mixed_load(cudaStream_t st, MixedBuffers& mb, const Geom& g, const Phys&,
+                      const double* const src[6], cudaMemcpyKind kind)
+{
+    const size_t n = static_cast<size_t>(g.n);
+    const int blocks = 1184;
+    for (int i = 0; i < 5; ++i) {
+        float* dst = field_f(mb, i);
+        if (src[i]) {
+            if (cudaMemcpyAsync(mb.scratch, src[i], n * sizeof(double), kind, st) != cudaSuccess) return LBM_ERR_CUDA;
+            to_float_kernel<<<blocks, 256, 0, st>>>(mb.scratch, dst, g.n);
+        } else if (cudaMemsetAsync(dst, 0, n * sizeof(float), st) != cudaSuccess) {
+            return LBM_ERR_CUDA;
+        }
+    }
+    if (src[5]) {
+        if (cudaMemcpyAsync(mb.p, src[5], n * sizeof(double), kind, st) != cudaSuccess) return LBM_ERR_CUDA;
+    } else if (cudaMemsetAsync(mb.p, 0, n * sizeof(double), st) != cudaSuccess) {
+        return LBM_ERR_CUDA;
+    }
+    if (cudaMemsetAsync(mb.p_prev, 0, n * sizeof(double), st) != cudaSuccess) return LBM_ERR_CUDA;
+    if (cudaMemsetAsync(mb.h[1], 0, 15 * n * sizeof(float), st) != cudaSuccess) return LBM_ERR_CUDA;
+    return cudaGetLastError() == cudaSuccess ? LBM_OK : LBM_ERR_CUDA;
+}
+
+lbm_status mixed_download(cudaStream_t st, MixedBuffers& mb, const Geom& g, int which, double* host)
+{
+    const size_t n = static_cast<size_t>(g.n);
+    if (which == 5) {
+        return cudaMemcpyAsync(host, mb.p, n * sizeof(double), cudaMemcpyDeviceToHost, st) == cudaSuccess
+                   ? LBM_OK : LBM_ERR_CUDA;
+    }
+    float* src = field_f(mb, which);
+    if (!src) return LBM_ERR_BAD_ARG;
+    to_double_kernel<<<1184, 256, 0, st>>>(src, mb.scratch, g.n);
+    if (cudaMemcpyAsync(host, mb.scratch, n * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return LBM_ERR_CUDA;
+    return cudaGetLastError() == cudaSuccess ? LBM_OK : LBM_ERR_CUDA;
+}
+
+lbm_status mixed_prologue(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom& g,
+                          const Phys& P, bool first, int fcur, bool h_loaded, DevState* ds,
+                          cudaEvent_t* ev)
+{
+    const MixPhys M = mix_phys(P);
+    const int fin = fcur, fout = 1 - fcur;
+    float* div = mb.dux;      // div = u_x + v_y + w_z
+    float* omega = mb.dvy;    // 1 / tau_h
+    if (first)
+        collide_kernel<true><<<L.grid, L.block, 0, st>>>(g, M, mb.f[fin], mb.f[fout], mb.g[fin], mb.g[fout],
+                                                         mb.phi, mb.rho, mb.u, mb.v, mb.w, div,
+                                                         mb.part_src, L.nblocks);
+    else
+        collide_kernel<false><<<L.grid, L.block, 0, st>>>(g, M, mb.f[fin], mb.f[fout], mb.g[fin], mb.g[fout],
+                                                          mb.phi, mb.rho, mb.u, mb.v, mb.w, div,
+                                                          mb.part_src, L.nblocks);
+    if (ev) cudaEventRecord(ev[1], st);
+    moments_kernel<<<L.grid, L.block, 0, st>>>(g, P.fei_G, P.fei_L, P.rho_G, P.rho_L, P.fei_avg, P.dfei,
+                                               P.half_drho, mb.f[fout], mb.g[fout], mb.phi, mb.rho, mb.u,
+                                               mb.v, mb.w, mb.part_mass, L.nblocks);
+    if (ev) cudaEventRecord(ev[2], st);
+    finalize(st, FIN_SOURCE, ds, mb.part_src, L.nblocks, nullptr, 0, nullptr, 0);
+    finalize(st, FIN_MASS, ds, mb.part_mass, L.nblocks, nullptr, 0, nullptr, 0);
+    prep_kernel<<<L.grid, L.block, 0, st>>>(g, ds, div, mb.rho, mb.p, mb.s, omega, mb.part_prep, L.nblocks);
+    finalize(st, FIN_PREP, ds, mb.part_prep, L.nblocks, nullptr, 0, nullptr, 0);
+    poisson_init_kernel<<<L.grid, L.block, 0, st>>>(g, h_loaded ? 1 : 0, mb.h[1], mb.h[0], mb.p, omega, mb.s);
+    return cudaGetLastError() == cudaSuccess ? LBM_OK : LBM_ERR_CUDA;
+}
+
+int mixed_segment(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom& g, int start_parity,
+                  int n_normal, bool dual, DevState* ds)
+{
+    const float* omega = mb.dvy;
+    int cur = start_parity;
+    for (int i = 0; i < n_normal; ++i) {
+        sweep_kernel<<<L.grid, L.block, 0, st>>>(g, mb.h[cur], mb.h[1 - cur], omega, mb.s);
+        cur = 1 - cur;
+    }
+    sweep_check_a_kernel<<<L.grid, L.block, 0, st>>>(g, mb.h[cur], mb.h[1 - cur], mb.p_chk, mb.part_a, L.nblocks);
+    cur = 1 - cur;
+    finalize(st, FIN_SIGMA, ds, mb.part_a, L.nblocks, nullptr, 0, nullptr, 0);
+    if (dual)
+        sweep_check_b_kernel<true><<<L.grid, L.block, 0, st>>>(g, mb.h[cur], mb.hc, mb.p_chk, mb.p_prev, mb.p,
+                                                               omega, mb.s, ds, mb.part_b, L.nblocks);
+    else
+        sweep_check_b_kernel<false><<<L.grid, L.block, 0, st>>>(g, mb.h[cur], mb.hc, mb.p_chk, mb.p_prev, mb.p,
+                                                                omega, mb.s, ds, mb.part_b, L.nblocks);
+    if (dual) {
+        sweep_check_c_kernel<<<L.grid, L.block, 0, st>>>(g, mb.h[cur], mb.h[1 - cur], mb.hc, omega, mb.s, ds,
+                                                         mb.part_c, L.nblocks);
+        cur = 1 - cur;
+    }
+    finalize(st, FIN_CHECK, ds, mb.part_b, L.nblocks, mb.part_c, L.nblocks, nullptr, 0);
+    return cur;
+}
+
+void mixed_correct(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom& g)
+{
+    correct_kernel<<<L.grid, L.block, 0, st>>>(g, mb.u, mb.v, mb.w, mb.p, mb.rho);
+}
+
+const void* mixed_field_ptr(const MixedBuffers& mb, int which)
+{
+    switch (which) {
+    case 0: return mb.phi;
+    case 1: return mb.rho;
+    case 2: return mb.u;
+    case 3: return mb.v;
+    case 4: return mb.w;
+    case 5: return mb.p;
+    }
+    return nullptr;
+}
 
 }  // namespace lbm

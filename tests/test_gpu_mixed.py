@@ -1,0 +1,88 @@
+"""Mixed precision (FP32 populations as rest-state deviations, FP64 pressure
+accumulation, reductions and exit test) against the FP64 oracle.
+
+Tolerance: 1e-5 norm-wise relative error in phi, rho, u, v, w after each step
+when both run the same sweep counts (replay of the oracle's counts; a
+relative-change exit can stop one check earlier or later, a 1e-3 effect on
+p).  p is held to 1e-4 (it is a small, zero-mean field)."""
+import numpy as np
+import pytest
+
+import lbm_b200 as L
+from oracle import pyoracle
+from tests.helpers import fixture, fields_dict, laplace_case, oracle_params, params_from_text, rel_err
+
+pytestmark = pytest.mark.gpu
+TOL = {"phi": 1e-5, "rho": 1e-5, "u": 1e-5, "v": 1e-5, "w": 1e-5, "p": 1e-4}
+CAP = 60000
+
+
+def mixed_vs_oracle(p, f, steps, dual=False):
+    o = pyoracle.Oracle(p.shape, oracle_params(p), f, dual=dual, max_sweeps=CAP)
+    g = L.InamuroCUDA(p, f, precision="mixed")
+    g.set_poisson(dual=dual, max_sweeps=CAP, fail_on_limit=True)
+    errs = []
+    for _ in range(steps):
+        info = o.step()
+        st = g.step_replay([int(info["sweeps"])])[0]
+        assert st["iterations"] == info["sweeps"]
+        gf, of = g.download_fields(), o.fields()
+        errs.append({k: rel_err(gf[k], of[k]) for k in L.FIELDS})
+        assert abs(st["mass"] - info["mass"]) <= 1e-6 * abs(info["mass"])
+    g.close()
+    return errs
+
+
+@pytest.mark.parametrize("name", ["step_single_tanh", "step_two_sharp", "step_example_16x32x32"])
+def test_mixed_matches_fp64_oracle(name):
+    fx = fixture(name)
+    p = params_from_text(fx["params_text"])
+    for s, e in enumerate(mixed_vs_oracle(p, fields_dict(fx["init"]), len(fx["sweeps"]))):
+        for k, v in e.items():
+            assert v <= TOL[k], f"step {s + 1} {k}: {v:.3e}"
+
+
+def test_mixed_laplace_32():
+    fx = fixture("step_laplace_32")
+    p = params_from_text(fx["params_text"])
+    for s, e in enumerate(mixed_vs_oracle(p, fields_dict(fx["init"]), 2)):
+        for k, v in e.items():
+            assert v <= TOL[k], f"step {s + 1} {k}: {v:.3e}"
+
+
+def test_mixed_dual_residual_runs():
+    fx = fixture("step_two_sharp")
+    p = params_from_text(fx["params_text"])
+    errs = mixed_vs_oracle(p, fields_dict(fx["init"]), 2, dual=True)
+    for k, v in errs[-1].items():
+        assert v <= TOL[k], (k, v)
+
+
+def test_mixed_natural_exit_close_to_fp64():
+    """Without replay the mixed run picks its own exits; sweep counts agree to
+    within one check interval and phi, u stay within 1e-4."""
+    p, f = laplace_case((24, 20, 16), DD=8.0, noise=1e-4)
+    f["w"] = 0.01 * np.sin(2 * np.pi * np.arange(16) / 16)[:, None, None] * np.ones_like(f["w"])
+    a = L.InamuroCUDA(p, f, precision="mixed")
+    b = L.InamuroCUDA(p, f, precision="fp64")
+    for g in (a, b):
+        g.set_poisson(max_sweeps=CAP, fail_on_limit=True)
+    for _ in range(3):
+        sa, sb = a.step(1)[0], b.step(1)[0]
+        assert abs(int(sa["iterations"]) - int(sb["iterations"])) <= 100
+    fa, fb = a.download_fields(), b.download_fields()
+    for k in ("phi", "u", "v", "w"):
+        assert rel_err(fa[k], fb[k]) <= 1e-4, k
+
+
+def test_mixed_field_statistics_and_ghosts():
+    p, f = laplace_case((16, 12, 10), DD=6.0)
+    g = L.InamuroCUDA(p, f, precision="mixed")
+    g.set_poisson(max_sweeps=CAP, fail_on_limit=True)
+    g.step(1)
+    phi = g.download("phi")
+    st = g.field_statistics("phi")
+    assert st["valid_count"] == phi.size
+    assert abs(st["sum"] - phi.sum()) <= 1e-9 * np.abs(phi).sum()
+    gh = g.download_ghosted("rho")
+    assert np.all(gh[0] == p.rho_G) and np.all(gh[-1] == p.rho_G)
