@@ -1,0 +1,389 @@
+// InamuroCUDA.hpp -- drop-in replacement of the reference's GPU class
+// (GPU/InamuroCUDA.hpp:16-248 + GPU/InamuroCUDA.cu of UniBoy222/LBM) over the
+// B200 C ABI (lbm_b200.h, liblbm_b200.so).
+//
+// Same class name, constructor and public methods, so the reference's
+// unchanged GPU/main.cpp and GPU/Inamuro.{hpp,cpp} build against it: put this
+// directory before the reference's GPU directory on the include path, link
+// liblbm_b200.so instead of compiling InamuroCUDA.cu.  The reference's
+// `friend class InamuroCUDA` (GPU/Inamuro.hpp:13) gives this class the same
+// access to the CPU object's fields as the original.
+//
+// Header-only; errors are thrown like the reference throws: std::runtime_error
+// for CUDA failures and non-finite values, std::invalid_argument for bad
+// settings, std::overflow_error for counter overflow.
+//
+// Precision: FP64 with the reference's per-cell operation order (the
+// default), or the mixed FP32/FP64 mode through the second constructor.
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <limits>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "Inamuro.hpp"
+#include "lbm_b200.h"
+
+class InamuroCUDA
+{
+public:
+    struct PoissonStepDiagnostics
+    {
+        std::uint64_t iterations = 0;
+        double relative_error = 0.0;
+        double pressure_l1_delta = 0.0;
+        double pressure_l1_norm = 0.0;
+        double fixed_point_h_l1 = 0.0;
+        double fixed_point_h_scale = 0.0;
+        double fixed_point_h_relative = 0.0;
+        double fixed_point_p_l1 = 0.0;
+        double fixed_point_p_scale = 0.0;
+        double fixed_point_p_relative = 0.0;
+        double fixed_point_relative = 0.0;
+        double source_mean = 0.0;
+        double source_abs_mean = 0.0;
+        double projected_source_mean = 0.0;
+        double pressure_gauge_target = 0.0;
+        double pressure_gauge_max_shift = 0.0;
+        bool fixed_point_evaluated = false;
+        bool pressure_converged = false;
+        bool fixed_point_converged = false;
+        bool dual_residual_enabled = false;
+        bool converged = false;
+        int fallback_count = 0;
+    };
+
+    explicit InamuroCUDA(const Inamuro& cpuSolver) : InamuroCUDA(cpuSolver, LBM_PRECISION_FP64) {}
+
+    InamuroCUDA(const Inamuro& cpuSolver, lbm_precision precision)
+    {
+        int nx = 0, ny = 0, nz = 0;
+        cpuSolver.getGridSize(nx, ny, nz);
+        lx_ = nx;
+        ly_ = ny;
+        lz_ = nz;
+        lbm_params prm;
+        lbm_params_default(&prm);
+        prm.lx = nx;
+        prm.ly = ny;
+        prm.lz = nz;
+        const auto& P = cpuSolver.params;   // friend access, as the reference does (.cu:1444-1456)
+        prm.rho_L = P.rho_L;
+        prm.rho_G = P.rho_G;
+        prm.mu_L = P.mu_L;
+        prm.mu_G = P.mu_G;
+        prm.tauf = P.tauf;
+        prm.taug = P.taug;
+        prm.k_f = P.k_f;
+        prm.k_g = P.k_g;
+        prm.T = P.T;
+        prm.a = P.a;
+        prm.b = P.b;
+        prm.fei_L = P.fei_L;
+        prm.fei_G = P.fei_G;
+        prm.fei_max = P.fei_max;
+        prm.fei_min = P.fei_min;
+        prm.DD = P.DD;
+        check(lbm_create(&prm, precision, 0, &h_), "InamuroCUDA: device set-up");
+        // initFromCPU (.cu:1628-1673): the ghosted macro fields of the CPU object.
+        std::vector<double> buf[6];
+        const std::vector<std::vector<std::vector<double>>>* src[6] = {
+            &cpuSolver.fei, &cpuSolver.rho, &cpuSolver.u, &cpuSolver.v, &cpuSolver.w, &cpuSolver.p};
+        for (int f = 0; f < 6; ++f) {
+            buf[f].resize(static_cast<std::size_t>(lx_) * ly_ * (lz_ + 2));
+            for (int z = 0; z < lz_ + 2; ++z)
+                for (int y = 0; y < ly_; ++y)
+                    for (int x = 0; x < lx_; ++x)
+                        buf[f][(static_cast<std::size_t>(z) * ly_ + y) * lx_ + x] = (*src[f])[x][y][z];
+        }
+        check(lbm_load_fields_ghosted(h_, buf[0].data(), buf[1].data(), buf[2].data(), buf[3].data(),
+                                      buf[4].data(), buf[5].data()),
+              "InamuroCUDA: upload");
+        lbm_set_check_callback(h_, &InamuroCUDA::onCheck, this);
+        applyPoissonConfig();
+    }
+
+    InamuroCUDA(const InamuroCUDA&) = delete;
+    InamuroCUDA& operator=(const InamuroCUDA&) = delete;
+    InamuroCUDA(InamuroCUDA&& o) noexcept { *this = std::move(o); }
+    InamuroCUDA& operator=(InamuroCUDA&& o) noexcept
+    {
+        if (this != &o) {
+            release();
+            h_ = o.h_;
+            o.h_ = nullptr;
+            lx_ = o.lx_; ly_ = o.ly_; lz_ = o.lz_;
+            check_interval_ = o.check_interval_;
+            tolerance_ = o.tolerance_;
+            iteration_limit_ = o.iteration_limit_;
+            dual_ = o.dual_;
+            shadow_ = o.shadow_;
+            diag_ = o.diag_;
+            csv_path_ = o.csv_path_;
+            if (h_) lbm_set_check_callback(h_, &InamuroCUDA::onCheck, this);
+        }
+        return *this;
+    }
+
+    ~InamuroCUDA() { release(); }
+
+    // One time step (performTimeStepGPU, GPU/InamuroCUDA.cu:2372-2442).
+    void performTimeStepGPU()
+    {
+        lbm_step_stats st{};
+        const lbm_status s = lbm_step(h_, 1, &st);
+        if (s == LBM_ERR_BAD_ARG) throw std::invalid_argument(lbm_last_error(h_));
+        if (s == LBM_ERR_OVERFLOW) throw std::overflow_error(lbm_last_error(h_));
+        if (s != LBM_OK) throw std::runtime_error(lbm_last_error(h_));
+        diag_.iterations = st.iterations;
+        diag_.relative_error = st.relative_error;
+        diag_.pressure_l1_delta = st.pressure_l1_delta;
+        diag_.pressure_l1_norm = st.pressure_l1_norm;
+        diag_.fixed_point_h_l1 = st.fixed_point_h_l1;
+        diag_.fixed_point_h_scale = st.fixed_point_h_scale;
+        diag_.fixed_point_h_relative = st.fixed_point_h_relative;
+        diag_.fixed_point_p_l1 = st.fixed_point_p_l1;
+        diag_.fixed_point_p_scale = st.fixed_point_p_scale;
+        diag_.fixed_point_p_relative = st.fixed_point_p_relative;
+        diag_.fixed_point_relative = st.fixed_point_relative;
+        diag_.source_mean = st.source_mean;
+        diag_.source_abs_mean = st.source_abs_mean;
+        diag_.projected_source_mean = st.projected_source_mean;
+        diag_.pressure_gauge_target = st.pressure_gauge_target;
+        diag_.pressure_gauge_max_shift = st.pressure_gauge_max_shift;
+        diag_.fixed_point_evaluated = st.fixed_point_evaluated != 0;
+        diag_.pressure_converged = st.pressure_converged != 0;
+        diag_.fixed_point_converged = st.fixed_point_converged != 0;
+        diag_.dual_residual_enabled = st.dual_residual_enabled != 0;
+        diag_.converged = st.converged != 0;
+        diag_.fallback_count = st.converged ? 0 : 1;
+    }
+
+    // downloadFieldsToCPU (.cu:1675-1701): rho, phi, u, v, w, p with ghosts.
+    void downloadFieldsToCPU(Inamuro& cpuSolver) const
+    {
+        std::vector<double> buf(static_cast<std::size_t>(lx_) * ly_ * (lz_ + 2));
+        std::vector<std::vector<std::vector<double>>>* dst[6] = {
+            &cpuSolver.fei, &cpuSolver.rho, &cpuSolver.u, &cpuSolver.v, &cpuSolver.w, &cpuSolver.p};
+        for (int f = 0; f < 6; ++f) {
+            check(lbm_download_ghosted(h_, static_cast<lbm_field>(f), buf.data()), "downloadFieldsToCPU");
+            for (int z = 0; z < lz_ + 2; ++z)
+                for (int y = 0; y < ly_; ++y)
+                    for (int x = 0; x < lx_; ++x)
+                        (*dst[f])[x][y][z] = buf[(static_cast<std::size_t>(z) * ly_ + y) * lx_ + x];
+        }
+    }
+
+    void downloadHH(std::vector<double>& hh) const
+    {
+        hh.resize(static_cast<std::size_t>(lx_) * ly_ * lz_ * 15);
+        check(lbm_download_h(h_, hh.data()), "downloadHH");
+    }
+
+    void synchronize() const { check(lbm_synchronize(h_), "synchronize"); }
+
+    const PoissonStepDiagnostics& getLastPoissonDiagnostics() const { return diag_; }
+
+    // ---- settings (GPU/InamuroCUDA.hpp:67-88) ----
+    // The reference's non-production Poisson accelerators are not part of this
+    // build; enabling one is rejected, disabling is accepted.
+    void setUseFusedPoisson(bool e) { rejectAccelerator(e, "fused Poisson"); }
+    void setUseOnePassPoisson(bool e) { rejectAccelerator(e, "one-pass Poisson"); }
+    void setUseScalarPoisson(bool e) { rejectAccelerator(e, "scalar Poisson"); }
+    void setUseSourceAwareHHInit(bool e) { rejectAccelerator(e, "source-aware hh init"); }
+    void setUsePoissonAndersonM1(bool e) { rejectAccelerator(e, "Anderson-m1"); }
+    void setUsePoissonTwoGridCorrection(bool e) { rejectAccelerator(e, "two-grid correction"); }
+    void setUseFusedBoundaryPressure(bool e) { rejectAccelerator(e, "fused boundary+pressure"); }
+    void setUsePoissonSpatialDiagnostics(bool e) { rejectAccelerator(e, "spatial diagnostics"); }
+    // Every Poisson segment already runs as a captured CUDA graph.
+    void setUsePoissonGraph(bool) {}
+    // Per-phase device timing is always collected.
+    void setEnablePoissonDetailTiming(bool) {}
+    // Reductions are always fixed-order (deterministic).
+    void setUsePoissonDeterministicReductions(bool) {}
+    void setScalarPoissonSourceScale(double) {}
+    void setSourceAwareHHScale(double) {}
+    void setPressureRelaxScale(double scale)
+    {
+        if (!(scale > 0.0)) throw std::invalid_argument("pressure relaxation scale must be positive");
+        if (scale != 1.0) throw std::invalid_argument("only unit pressure relaxation is supported");
+    }
+    void setPoissonFixedPointRelax(double omega)
+    {
+        if (!(omega > 0.0)) throw std::invalid_argument("Poisson fixed-point relaxation must be positive");
+        if (omega != 1.0) throw std::invalid_argument("only unit fixed-point relaxation is supported");
+    }
+    void setPoissonAndersonBetaMax(double v)
+    {
+        if (!(v >= 0.0)) throw std::invalid_argument("Poisson Anderson beta max must be non-negative");
+    }
+    void setPoissonTwoGridStrength(double v)
+    {
+        if (!(v >= 0.0)) throw std::invalid_argument("Poisson two-grid strength must be non-negative");
+    }
+    void setEnablePoissonFixedPointShadow(bool e)
+    {
+        shadow_ = e;
+        applyPoissonConfig();
+    }
+    void setUsePoissonDualResidual(bool e)
+    {
+        dual_ = e;
+        if (e) shadow_ = true;
+        applyPoissonConfig();
+    }
+    void setPoissonConvergence(int check_interval, double tolerance)
+    {
+        if (check_interval <= 0) throw std::invalid_argument("poisson check interval must be positive");
+        if (!(tolerance > 0.0)) throw std::invalid_argument("poisson tolerance must be positive");
+        if (iteration_limit_ != 0 && iteration_limit_ % static_cast<std::uint64_t>(check_interval) != 0)
+            throw std::invalid_argument("Poisson iteration limit must be a multiple of check interval");
+        check_interval_ = check_interval;
+        tolerance_ = tolerance;
+        applyPoissonConfig();
+    }
+    void setPoissonIterationLimit(std::uint64_t max_iterations)
+    {
+        if (max_iterations != 0 && max_iterations % static_cast<std::uint64_t>(check_interval_) != 0)
+            throw std::invalid_argument("Poisson iteration limit must be a multiple of check interval");
+        iteration_limit_ = max_iterations;
+        applyPoissonConfig();
+    }
+    // Per-check CSV, same header and columns as GPU/InamuroCUDA.cu:2610-2682.
+    void setPoissonDiagnosticsPath(const std::string& path)
+    {
+        csv_path_ = path;
+        if (path.empty()) return;
+        std::ofstream out(path);
+        if (!out) throw std::runtime_error("failed to open Poisson diagnostics CSV: " + path);
+        out << "step,iteration,pressure_l1_delta,pressure_l1_norm,relative_error,"
+            << "fixed_point_h_l1,fixed_point_h_scale,fixed_point_h_relative,"
+            << "fixed_point_p_l1,fixed_point_p_scale,fixed_point_p_relative,"
+            << "fixed_point_relative,fixed_point_evaluated,pressure_converged,fixed_point_converged,"
+            << "dual_residual_enabled,converged,block_low_frequency_fraction,"
+            << "block_size,block_count\n";
+    }
+
+    void printPerformanceMetrics() const
+    {
+        lbm_timing t{};
+        lbm_get_timing(h_, &t);
+        if (t.steps == 0) {
+            std::cout << "No performance data collected yet." << std::endl;
+            return;
+        }
+        const double sites = static_cast<double>(lx_) * ly_ * lz_;
+        const double n = static_cast<double>(t.steps);
+        const double total = t.collide_ms + t.moments_ms + t.prep_ms + t.poisson_ms + t.correct_ms;
+        std::cout << "\n========== GPU Performance Metrics (B200 sm_100a) ==========" << std::endl;
+        std::cout << "Total time steps: " << t.steps << std::endl;
+        std::cout << "Poisson convergence: check_interval=" << check_interval_ << ", tolerance=" << tolerance_
+                  << ", dual-residual exit=" << (dual_ ? "enabled" : "disabled")
+                  << ", fixed-point shadow=" << (shadow_ ? "enabled" : "disabled") << std::endl;
+        std::cout << "poisson_iteration_limit=" << iteration_limit_
+                  << (iteration_limit_ == 0 ? " (unbounded)" : "") << std::endl;
+        std::cout << "\nAverage device time per step (ms):" << std::endl;
+        std::cout << "  Collide+stream: " << t.collide_ms / n << std::endl;
+        std::cout << "  Macro:          " << t.moments_ms / n << std::endl;
+        std::cout << "  Source prep:    " << t.prep_ms / n << std::endl;
+        std::cout << "  Poisson:        " << t.poisson_ms / n << std::endl;
+        std::cout << "  Correction:     " << t.correct_ms / n << std::endl;
+        std::cout << "  Poisson iters:  " << static_cast<double>(t.sweeps) / n << std::endl;
+        std::cout << "  Total per step: " << total / n << std::endl;
+        std::cout << "  MLUPS:          " << sites / (total / n * 1000.0) << std::endl;
+        std::cout << "  MLUPS (sweeps counted): " << sites * (n + static_cast<double>(t.sweeps)) / (total * 1000.0)
+                  << std::endl;
+        std::cout << "=============================================================\n" << std::endl;
+    }
+
+    void printRooflineSummary() const
+    {
+        lbm_timing t{};
+        lbm_get_timing(h_, &t);
+        const double cells = static_cast<double>(lx_) * ly_ * lz_;
+        std::cout << "\n========== Roofline (measured) ==========" << std::endl;
+        std::cout << "Grid cells: " << cells << std::endl;
+        if (t.sweep_kernels > 0) {
+            const double ms = t.poisson_ms / static_cast<double>(t.sweep_kernels);
+            std::cout << std::fixed << std::setprecision(2)
+                      << "Kinetic sweep: " << ms * 1e3 << " us/launch, "
+                      << 272.0 * cells / (ms * 1e-3) / 1e9 << " GB/s at 272 B/cell (FP64 model)" << std::endl;
+        }
+        std::cout << "=========================================\n" << std::endl;
+    }
+
+    void resetPerformanceMetrics() { lbm_reset_timing(h_); }
+
+private:
+    lbm_handle* h_ = nullptr;
+    int lx_ = 0, ly_ = 0, lz_ = 0;
+    int check_interval_ = 100;
+    double tolerance_ = 1.0e-3;
+    std::uint64_t iteration_limit_ = 0;
+    bool dual_ = false;
+    bool shadow_ = false;
+    PoissonStepDiagnostics diag_;
+    std::string csv_path_;
+
+    void release()
+    {
+        if (h_) lbm_destroy(h_);
+        h_ = nullptr;
+    }
+
+    void check(lbm_status s, const char* what) const
+    {
+        if (s == LBM_OK) return;
+        const std::string msg = std::string(what) + ": " + lbm_status_string(s) + " " +
+                                (h_ ? lbm_last_error(h_) : "");
+        if (s == LBM_ERR_BAD_ARG) throw std::invalid_argument(msg);
+        if (s == LBM_ERR_OVERFLOW) throw std::overflow_error(msg);
+        throw std::runtime_error(msg);
+    }
+
+    static void rejectAccelerator(bool enabled, const char* name)
+    {
+        if (enabled)
+            throw std::invalid_argument(std::string(name) +
+                                        ": the reference's non-production Poisson accelerators are not part "
+                                        "of this build (split Poisson only)");
+    }
+
+    void applyPoissonConfig()
+    {
+        if (!h_) return;
+        lbm_poisson_cfg cfg{};
+        cfg.check_interval = check_interval_;
+        cfg.tolerance = tolerance_;
+        cfg.dual_residual = dual_ ? 1 : (shadow_ ? 2 : 0);
+        cfg.max_sweeps = iteration_limit_;
+        cfg.fail_on_limit = 0;
+        check(lbm_set_poisson(h_, &cfg), "Poisson configuration");
+    }
+
+    static void onCheck(void* user, const lbm_check_record* r)
+    {
+        const InamuroCUDA* self = static_cast<const InamuroCUDA*>(user);
+        if (self->csv_path_.empty()) return;
+        std::ofstream out(self->csv_path_, std::ios::app);
+        if (!out) return;
+        out << r->step << ',' << r->iteration << ',' << std::setprecision(17) << r->pressure_l1_delta << ','
+            << r->pressure_l1_norm << ',' << r->relative_error << ',';
+        const double opt[7] = {r->fixed_point_h_l1, r->fixed_point_h_scale, r->fixed_point_h_relative,
+                               r->fixed_point_p_l1, r->fixed_point_p_scale, r->fixed_point_p_relative,
+                               r->fixed_point_relative};
+        for (double v : opt) {
+            if (std::isfinite(v)) out << v;
+            out << ',';
+        }
+        out << r->fixed_point_evaluated << ',' << r->pressure_converged << ',' << r->fixed_point_converged << ','
+            << r->dual_residual_enabled << ',' << r->converged << ",,0,0\n";
+    }
+};

@@ -84,7 +84,10 @@ typedef struct {
 typedef struct {
     int check_interval;          /* sweeps between checks; reference contract 100 */
     double tolerance;            /* relative-change (and dual) tolerance; contract 1e-3 */
-    int dual_residual;           /* 1: also require the kinetic fixed-point residual < tol */
+    int dual_residual;           /* 0: relative change only; 1: also require the kinetic
+                                    fixed-point residual < tol (--poisson-dual-residual);
+                                    2: evaluate and report it without changing the exit
+                                    (--poisson-fixed-point-shadow) */
     uint64_t max_sweeps;         /* 0 = unbounded (contract); else the iteration limit */
     int fail_on_limit;           /* 0: at the limit stop and finish the step unconverged, as
                                     the reference's poisson_iteration_limit does (.cu:2336-2339);
@@ -146,6 +149,27 @@ typedef struct {
     double sum;
     uint64_t valid_count;
 } lbm_field_stats;
+
+/* One Poisson convergence check (the row InamuroCUDA::writePoissonDiagnostic
+ * appends to the diagnostics CSV, GPU/InamuroCUDA.cu:2634-2682). */
+typedef struct {
+    uint64_t step;                   /* 1-based time step of the handle */
+    uint64_t iteration;              /* sweep count at the check */
+    double pressure_l1_delta;
+    double pressure_l1_norm;
+    double relative_error;
+    double fixed_point_h_l1, fixed_point_h_scale, fixed_point_h_relative;
+    double fixed_point_p_l1, fixed_point_p_scale, fixed_point_p_relative;
+    double fixed_point_relative;     /* NaN when not evaluated */
+    int fixed_point_evaluated;
+    int pressure_converged;
+    int fixed_point_converged;
+    int dual_residual_enabled;
+    int converged;
+    int reserved;
+} lbm_check_record;
+
+typedef void (*lbm_check_callback)(void* user, const lbm_check_record* record);
 
 typedef struct lbm_handle lbm_handle;
 
@@ -209,6 +233,11 @@ lbm_status lbm_step(lbm_handle* h, int n_steps, lbm_step_stats* stats);
 lbm_status lbm_step_replay(lbm_handle* h, int n_steps, const uint64_t* sweeps,
                            lbm_step_stats* stats);
 
+/* Calls cb(user, record) on the host after every Poisson convergence check
+ * (NULL cb disables).  Replaces InamuroCUDA::setPoissonDiagnosticsPath's
+ * per-check CSV rows (GPU/InamuroCUDA.cu:2610-2682): the caller formats them. */
+lbm_status lbm_set_check_callback(lbm_handle* h, lbm_check_callback cb, void* user);
+
 /* Device -> host download of one field (physical layout). */
 lbm_status lbm_download(lbm_handle* h, lbm_field which, double* host);
 /* Ghosted layout, ghost planes as loaded (InamuroCUDA::downloadFieldsToCPU,
@@ -264,7 +293,8 @@ lbm_status lbm_reset_timing(lbm_handle* h);
 /* Enables per-kernel-class CUDA-event timing (default on). */
 lbm_status lbm_set_timing(lbm_handle* h, int enabled);
 
-/* Text of the last error on this handle ("" if none); valid until the next call. */
+/* Text of the last error on this handle ("" if none); valid until the next call.
+ * With h == NULL: why the calling thread's last lbm_create failed. */
 const char* lbm_last_error(const lbm_handle* h);
 const char* lbm_status_string(lbm_status s);
 int lbm_abi_version(void);

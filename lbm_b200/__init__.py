@@ -227,7 +227,8 @@ class InamuroCUDA:
         h = C.c_void_p()
         st = self._lib.lbm_create(C.byref(params), PRECISION[precision], device, C.byref(h))
         if st != 0:
-            raise LBMError(st, "lbm_create")
+            why = self._lib.lbm_last_error(None)
+            raise LBMError(st, "lbm_create: " + (why.decode() if why else ""))
         self._h = h
         self.last_poisson_diagnostics: Dict[str, float] = {}
         if fields is not None:

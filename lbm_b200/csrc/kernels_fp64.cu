@@ -348,6 +348,69 @@ sweep_kernel(Geom g, const double* __restrict__ hin, double* __restrict__ hout,
     collide_h_store(hv, pv, tauh, __ldg(s + c), hout, g.n, c);
 }
 
+// Two sweeps in one pass (temporal blocking; same scheme as the mixed box).
+// A CTA owns a TX x TY xy tile and a run of `zlen` planes; marching in z it
+// computes sweep k on the tile plus a one-cell halo (wrapped coordinates,
+// pulled from global memory) into a ring of three shared-memory planes, then
+// sweep k+1 on the tile from that ring.  Every cell's arithmetic is
+// collide_h_store's expression, so (without FMA contraction in this file) the
+// result is bitwise that of two sweep_kernel launches.  lx % TX == 0 and
+// ly % TY == 0 are required (checked by the launcher).
+constexpr int F2_TX = 32, F2_TY = 4;
+constexpr int F2_RX = F2_TX + 2, F2_RY = F2_TY + 2, F2_RC = F2_RX * F2_RY;
+constexpr int F2_SMEM = 3 * Q * F2_RC * (int)sizeof(double);
+
+__global__ void __launch_bounds__(F2_TX * F2_TY)
+sweep2_kernel(Geom g, int zlen, const double* __restrict__ hin, double* __restrict__ hout,
+              const double* __restrict__ rho, const double* __restrict__ s)
+{
+    extern __shared__ double ring2[];   // [3][Q][F2_RC]
+    const int tid = threadIdx.x + F2_TX * threadIdx.y;
+    const int x0 = blockIdx.x * F2_TX, y0 = blockIdx.y * F2_TY;
+    const int z0 = blockIdx.z * zlen;
+    const int z1 = min(z0 + zlen, g.lz);
+
+    auto first_sweep = [&](int zz) {
+        const int zw = (zz % g.lz + g.lz) % g.lz;
+        double* slot = ring2 + ((zz % 3 + 3) % 3) * (Q * F2_RC);
+        for (int r = tid; r < F2_RC; r += F2_TX * F2_TY) {
+            const int rx = r % F2_RX, ry = r / F2_RX;
+            const int xw = (x0 - 1 + rx + g.lx) % g.lx;
+            const int yw = (y0 - 1 + ry + g.ly) % g.ly;
+            double hv[Q];
+            pull_regs(hv, hin, g, xw, yw, zw);
+            bounce_regs(hv, g, xw);
+            const long long c = cell_of(g, xw, yw, zw);
+            const double pv = sum_q(hv);
+            const double tauh = 1.0 / __ldg(rho + c) + 0.5;
+            // collide_h_store into the ring (n = F2_RC, cell = r)
+            collide_h_store(hv, pv, tauh, __ldg(s + c), slot, F2_RC, r);
+        }
+    };
+
+    first_sweep(z0 - 1);
+    first_sweep(z0);
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int x = x0 + tx, y = y0 + ty;
+    for (int z = z0; z < z1; ++z) {
+        first_sweep(z + 1);
+        __syncthreads();
+        double hv[Q];
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            const int zs = z - cz(q);
+            const double* slot = ring2 + ((zs % 3 + 3) % 3) * (Q * F2_RC);
+            hv[q] = slot[q * F2_RC + (ty + 1 - cy(q)) * F2_RX + (tx + 1 - cx(q))];
+        });
+        bounce_regs(hv, g, x);
+        const long long c = cell_of(g, x, y, z);
+        const double pv = sum_q(hv);
+        const double tauh = 1.0 / __ldg(rho + c) + 0.5;
+        collide_h_store(hv, pv, tauh, __ldg(s + c), hout, g.n, c);
+        __syncthreads();
+    }
+}
+
 __global__ void __launch_bounds__(256)
 sweep_check_a_kernel(Geom g, const double* __restrict__ hin, double* __restrict__ hout,
                      double* __restrict__ p_chk, double* __restrict__ part, long long nblocks)
@@ -553,7 +616,8 @@ finalize_kernel(int kind, DevState* __restrict__ ds, const double* __restrict__ 
                 if (!isfinite(ds->fp_rel)) set_error(ds, SITE_FIXED_POINT);
                 ds->fp_evaluated = 1;
                 ds->fp_converged = ds->fp_rel < ds->tolerance;
-                fp_ok = ds->fp_converged;
+                // dual == 2 is the shadow mode: reported, not part of the exit
+                fp_ok = (ds->dual == 1) ? ds->fp_converged : true;
             }
             ds->l1_delta = rb[0];
             ds->l1_norm = rb[1];
@@ -615,6 +679,21 @@ void sweep(cudaStream_t st, const Launch& L, const Geom& g, const double* hin, d
            const double* rho, const double* s)
 {
     sweep_kernel<<<L.grid, L.block, 0, st>>>(g, hin, hout, rho, s);
+}
+
+int sweep2_prepare(const Geom& g)
+{
+    if (g.lx % F2_TX != 0 || g.ly % F2_TY != 0 || g.lz < 3) return 0;
+    if (cudaFuncSetAttribute(sweep2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, F2_SMEM) != cudaSuccess)
+        return 0;
+    return 1;
+}
+
+void sweep2(cudaStream_t st, const Geom& g, int zlen, const double* hin, double* hout,
+            const double* rho, const double* s)
+{
+    const dim3 grid(g.lx / F2_TX, g.ly / F2_TY, (g.lz + zlen - 1) / zlen);
+    sweep2_kernel<<<grid, dim3(F2_TX, F2_TY), F2_SMEM, st>>>(g, zlen, hin, hout, rho, s);
 }
 
 void sweep_check_a(cudaStream_t st, const Launch& L, const Geom& g, const double* hin,

@@ -17,6 +17,8 @@
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
+#include <cstdlib>
+
 #include "lbm_mixed.cuh"
 
 namespace lbm {
@@ -244,14 +246,21 @@ prep_kernel(Geom g, const DevState* __restrict__ ds, const float* __restrict__ d
     block_sum_store<3>(red, part, nblocks, block_linear());
 }
 
+// Kinetic collision of one population: h - (h - E p) omega - (E/3) s.
+template <int q>
+__device__ __forceinline__ float collide_h(float h, float p32, float om, float sv)
+{
+    constexpr float E = float(wE(q));
+    return h - (h - E * p32) * om - (E * (1.f / 3.f)) * sv;
+}
+
 __device__ __forceinline__ void collide_h_store(const float (&hv)[Q], double pv, float om, float sv,
                                                 float* __restrict__ hout, long long n, long long c)
 {
     const float p32 = (float)pv;
     static_for<0, Q>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
-        constexpr float E = float(wE(q));
-        hout[(long long)q * n + c] = hv[q] - (hv[q] - E * p32) * om - (E * (1.f / 3.f)) * sv;
+        hout[(long long)q * n + c] = collide_h<q>(hv[q], p32, om, sv);
     });
 }
 
@@ -290,6 +299,73 @@ sweep_kernel(Geom g, const float* __restrict__ hin, float* __restrict__ hout,
     pull_regs(hv, hin, g, x, y, z);
     bounce_regs(hv, g, x);
     collide_h_store(hv, sum_q(hv), __ldg(omega + c), __ldg(s + c), hout, g.n, c);
+}
+
+// Two sweeps in one pass (temporal blocking).  A CTA owns an xy tile of
+// TX x TY output cells and a run of `zlen` planes.  Marching in z it computes
+// sweep k on the tile plus a one-cell xy halo (pulling from global memory)
+// into a ring of three shared-memory planes, then sweep k+1 on the tile by
+// pulling from that ring, and writes only the second result.  Halo cells use
+// wrapped coordinates, so the periodic stream and the x slip overwrite are
+// those of two single sweeps, and each cell's arithmetic is the same
+// collide_h as in sweep_kernel.
+// Requires lx % TX == 0 and ly % TY == 0 (the launcher checks).
+constexpr int S2_TX = 32, S2_TY = 8;
+constexpr int S2_RX = S2_TX + 2, S2_RY = S2_TY + 2, S2_RC = S2_RX * S2_RY;
+constexpr int S2_SMEM = 3 * Q * S2_RC * (int)sizeof(float);
+
+__global__ void __launch_bounds__(256)
+sweep2_kernel(Geom g, int zlen, const float* __restrict__ hin, float* __restrict__ hout,
+              const float* __restrict__ omega, const float* __restrict__ s)
+{
+    extern __shared__ float ring[];   // [3][Q][S2_RC]
+    const int tid = threadIdx.x + S2_TX * threadIdx.y;
+    const int x0 = blockIdx.x * S2_TX, y0 = blockIdx.y * S2_TY;
+    const int z0 = blockIdx.z * zlen;
+    const int z1 = min(z0 + zlen, g.lz);
+
+    // sweep k on plane zz (wrapped) for the tile + halo, into ring slot zz mod 3
+    auto first_sweep = [&](int zz) {
+        const int zw = (zz % g.lz + g.lz) % g.lz;
+        float* slot = ring + ((zz % 3 + 3) % 3) * (Q * S2_RC);
+        for (int r = tid; r < S2_RC; r += S2_TX * S2_TY) {
+            const int rx = r % S2_RX, ry = r / S2_RX;
+            const int xw = (x0 - 1 + rx + g.lx) % g.lx;
+            const int yw = (y0 - 1 + ry + g.ly) % g.ly;
+            float hv[Q];
+            pull_regs(hv, hin, g, xw, yw, zw);
+            bounce_regs(hv, g, xw);
+            const long long c = cell_of(g, xw, yw, zw);
+            const double pv = sum_q(hv);
+            const float p32 = (float)pv;
+            const float om = __ldg(omega + c), sv = __ldg(s + c);
+            static_for<0, Q>([&](auto qc) {
+                constexpr int q = decltype(qc)::value;
+                slot[q * S2_RC + r] = collide_h<q>(hv[q], p32, om, sv);
+            });
+        }
+    };
+
+    first_sweep(z0 - 1);
+    first_sweep(z0);
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int x = x0 + tx, y = y0 + ty;
+    for (int z = z0; z < z1; ++z) {
+        first_sweep(z + 1);
+        __syncthreads();
+        // sweep k+1 at (x, y, z): pull from the ring
+        float hv[Q];
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            const int zs = z - cz(q);
+            const float* slot = ring + ((zs % 3 + 3) % 3) * (Q * S2_RC);
+            hv[q] = slot[q * S2_RC + (ty + 1 - cy(q)) * S2_RX + (tx + 1 - cx(q))];
+        });
+        bounce_regs(hv, g, x);
+        const long long c = cell_of(g, x, y, z);
+        collide_h_store(hv, sum_q(hv), __ldg(omega + c), __ldg(s + c), hout, g.n, c);
+        __syncthreads();
+    }
 }
 
 __global__ void __launch_bounds__(256)
@@ -464,6 +540,13 @@ lbm_status mixed_alloc(MixedBuffers& mb, const Geom& g, const Launch& L)
     }
     cudaMemset(mb.part_c, 0, 3 * nb * sizeof(double));
     mb.dwz = nullptr;
+    // Two-sweep temporal blocking where the tile divides the box.
+    mb.fuse_zlen = 0;
+    const char* env = std::getenv("LBM_SWEEP2_ZLEN");
+    const int zlen = env ? std::atoi(env) : 32;
+    if (zlen > 0 && g.lx % S2_TX == 0 && g.ly % S2_TY == 0 && g.lz >= 3 &&
+        cudaFuncSetAttribute(sweep2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, S2_SMEM) == cudaSuccess)
+        mb.fuse_zlen = zlen;
     mb.allocated = true;
     return LBM_OK;
 }
@@ -565,6 +648,15 @@ int mixed_segment(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom
 {
     const float* omega = mb.dvy;
     int cur = start_parity;
+    if (mb.fuse_zlen > 0) {
+        const dim3 grid(g.lx / S2_TX, g.ly / S2_TY, (g.lz + mb.fuse_zlen - 1) / mb.fuse_zlen);
+        for (int i = 0; i + 1 < n_normal; i += 2) {
+            sweep2_kernel<<<grid, dim3(S2_TX, S2_TY), S2_SMEM, st>>>(g, mb.fuse_zlen, mb.h[cur], mb.h[1 - cur],
+                                                                     omega, mb.s);
+            cur = 1 - cur;
+        }
+        n_normal &= 1;
+    }
     for (int i = 0; i < n_normal; ++i) {
         sweep_kernel<<<L.grid, L.block, 0, st>>>(g, mb.h[cur], mb.h[1 - cur], omega, mb.s);
         cur = 1 - cur;

@@ -64,18 +64,24 @@ struct lbm_handle {
     lbm_poisson_cfg pcfg{100, 1.0e-3, 0, 0, 0};
     DevState* ds = nullptr;
     DevState* ds_host = nullptr;    // pinned
-    std::map<SegKey, cudaGraphExec_t> graphs;
+    std::map<SegKey, std::pair<cudaGraphExec_t, int>> graphs;   // graph, end parity
     std::vector<double> ghost;      // 6 fields x 2 planes x lx*ly
     std::string err;
     bool timing = true;
     cudaEvent_t ev[6]{};
     lbm_timing acc{};
     uint64_t steps_done = 0;
+    lbm_check_callback check_cb = nullptr;
+    void* check_user = nullptr;
+    int fuse_zlen = 0;                   // FP64: >0 runs plain sweeps two per launch
     double* stats_part = nullptr;        // field-statistics partials
     lbm_field_stats* stats_dev = nullptr;
 };
 
 namespace {
+
+// Why the calling thread's last lbm_create failed (lbm_last_error(NULL)).
+thread_local std::string g_create_error;
 
 lbm_status fail(lbm_handle* h, lbm_status s, const std::string& msg)
 {
@@ -137,7 +143,7 @@ int pick_bx(int lx)
 
 void free_all(lbm_handle* h)
 {
-    for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
+    for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second.first);
     h->graphs.clear();
     double** ptrs[] = {&h->b.f[0], &h->b.f[1], &h->b.g[0], &h->b.g[1], &h->b.h[0], &h->b.h[1],
                        &h->b.hc, &h->b.phi, &h->b.rho, &h->b.u, &h->b.v, &h->b.w, &h->b.p,
@@ -216,7 +222,7 @@ void upload_state_config(lbm_handle* h)
 // check pair (A: stream/bounce/sum at the check sweep, B: gauge + relative
 // change + R_p terms + collision of the next sweep), in dual mode the shadow
 // sweep C (R_h terms), the convergence test, and the state copy to the host.
-lbm_status build_segment(lbm_handle* h, const SegKey& key, cudaGraphExec_t* out)
+lbm_status build_segment(lbm_handle* h, const SegKey& key, cudaGraphExec_t* out, int* end_parity)
 {
     cudaStream_t st = h->stream;
     LBM_CUDA(h, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
@@ -225,7 +231,15 @@ lbm_status build_segment(lbm_handle* h, const SegKey& key, cudaGraphExec_t* out)
     const Launch& L = h->L;
     if (h->precision == LBM_PRECISION_FP64) {
         Fp64Buffers& b = h->b;
-        for (int i = 0; i < key.n_normal; ++i) {
+        int n_single = key.n_normal;
+        if (h->fuse_zlen > 0) {
+            for (int i = 0; i + 1 < key.n_normal; i += 2) {
+                fp64::sweep2(st, g, h->fuse_zlen, b.h[cur], b.h[1 - cur], b.rho, b.s);
+                cur = 1 - cur;
+            }
+            n_single = key.n_normal & 1;
+        }
+        for (int i = 0; i < n_single; ++i) {
             fp64::sweep(st, L, g, b.h[cur], b.h[1 - cur], b.rho, b.s);
             cur = 1 - cur;
         }
@@ -249,26 +263,23 @@ lbm_status build_segment(lbm_handle* h, const SegKey& key, cudaGraphExec_t* out)
     e = cudaGraphInstantiate(out, graph, 0);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) return fail(h, LBM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-    (void)cur;
+    *end_parity = cur;
     return LBM_OK;
 }
 
-int segment_parity_change(int n_normal, int dual)
-{
-    return (n_normal + 1 + (dual ? 1 : 0)) & 1;
-}
-
-lbm_status get_segment(lbm_handle* h, const SegKey& key, cudaGraphExec_t* out)
+// Cached segment graph for `key` and the h buffer parity it ends on.
+lbm_status get_segment(lbm_handle* h, const SegKey& key, cudaGraphExec_t* out, int* end_parity)
 {
     auto it = h->graphs.find(key);
     if (it != h->graphs.end()) {
-        *out = it->second;
+        *out = it->second.first;
+        *end_parity = it->second.second;
         return LBM_OK;
     }
     cudaGraphExec_t ex = nullptr;
-    const lbm_status st = build_segment(h, key, &ex);
+    const lbm_status st = build_segment(h, key, &ex, end_parity);
     if (st != LBM_OK) return st;
-    h->graphs[key] = ex;
+    h->graphs[key] = {ex, *end_parity};
     *out = ex;
     return LBM_OK;
 }
@@ -312,7 +323,7 @@ void fill_stats(const lbm_handle* h, const DevState& d, lbm_step_stats* s)
     s->fixed_point_evaluated = d.fp_evaluated;
     s->pressure_converged = d.pressure_converged;
     s->fixed_point_converged = d.fp_converged;
-    s->dual_residual_enabled = h->pcfg.dual_residual;
+    s->dual_residual_enabled = h->pcfg.dual_residual == 1;
     s->converged = d.converged;
 }
 
@@ -323,7 +334,7 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
     const Geom& g = h->geom;
     const Launch& L = h->L;
     const int ci = h->pcfg.check_interval;
-    const int dual = h->pcfg.dual_residual;
+    const int dual = h->pcfg.dual_residual != 0;   // residual kernels run in exit and shadow mode
     if (dual) {
         const lbm_status s = ensure_dual_buffer(h);
         if (s != LBM_OK) return s;
@@ -372,13 +383,19 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
         const int n_normal = dual ? (first_seg ? ci - 1 : ci - 2) : ci - 1;
         SegKey key{hcur, n_normal, dual};
         cudaGraphExec_t ex = nullptr;
-        const lbm_status gs = get_segment(h, key, &ex);
+        int end_parity = hcur;
+        const lbm_status gs = get_segment(h, key, &ex, &end_parity);
         if (gs != LBM_OK) return gs;
         LBM_CUDA(h, cudaGraphLaunch(ex, st));
         LBM_CUDA(h, cudaStreamSynchronize(st));
-        hcur ^= segment_parity_change(n_normal, dual);
+        hcur = end_parity;
+        // sweep-equivalents executed (plain, A, B, C) and actual launches
+        // (two plain sweeps per launch where the mixed box fuses them)
         kernels += static_cast<uint64_t>(n_normal) + 2 + (dual ? 1 : 0);
-        launches += static_cast<uint64_t>(n_normal) + 4 + (dual ? 1 : 0);
+        const bool fused = h->precision == LBM_PRECISION_MIXED ? h->mb.fuse_zlen > 0 : h->fuse_zlen > 0;
+        const uint64_t plain_launches = fused ? static_cast<uint64_t>(n_normal / 2 + n_normal % 2)
+                                              : static_cast<uint64_t>(n_normal);
+        launches += plain_launches + 4 + (dual ? 1 : 0);
         first_seg = false;
         if (dh.error) {
             return fail(h, static_cast<lbm_status>(dh.error), site_text(dh.error_site));
@@ -386,6 +403,29 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
         if (iters > UINT64_MAX - static_cast<uint64_t>(ci))
             return fail(h, LBM_ERR_OVERFLOW, "Poisson iteration counter overflow");
         iters += static_cast<uint64_t>(ci);
+        if (h->check_cb) {
+            lbm_step_stats tmp;
+            fill_stats(h, dh, &tmp);
+            lbm_check_record rec{};
+            rec.step = h->steps_done + 1;
+            rec.iteration = iters;
+            rec.pressure_l1_delta = tmp.pressure_l1_delta;
+            rec.pressure_l1_norm = tmp.pressure_l1_norm;
+            rec.relative_error = tmp.relative_error;
+            rec.fixed_point_h_l1 = tmp.fixed_point_h_l1;
+            rec.fixed_point_h_scale = tmp.fixed_point_h_scale;
+            rec.fixed_point_h_relative = tmp.fixed_point_h_relative;
+            rec.fixed_point_p_l1 = tmp.fixed_point_p_l1;
+            rec.fixed_point_p_scale = tmp.fixed_point_p_scale;
+            rec.fixed_point_p_relative = tmp.fixed_point_p_relative;
+            rec.fixed_point_relative = tmp.fixed_point_relative;
+            rec.fixed_point_evaluated = tmp.fixed_point_evaluated;
+            rec.pressure_converged = tmp.pressure_converged;
+            rec.fixed_point_converged = tmp.fixed_point_converged;
+            rec.dual_residual_enabled = h->pcfg.dual_residual == 1;
+            rec.converged = tmp.converged;
+            h->check_cb(h->check_user, &rec);
+        }
         if (replay) {
             if (iters >= replay) break;
         } else if (dh.converged) {
@@ -503,7 +543,7 @@ const char* lbm_status_string(lbm_status s)
     return "unknown status";
 }
 
-const char* lbm_last_error(const lbm_handle* h) { return h ? h->err.c_str() : ""; }
+const char* lbm_last_error(const lbm_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
 
 lbm_status lbm_create(const lbm_params* prm, lbm_precision precision, int device, lbm_handle** out)
 {
@@ -513,13 +553,27 @@ lbm_status lbm_create(const lbm_params* prm, lbm_precision precision, int device
     if (!(prm->rho_L != prm->rho_G) || !(prm->tauf > 0.0) || !(prm->taug > 0.0)) return LBM_ERR_BAD_ARG;
     if (precision != LBM_PRECISION_FP64 && precision != LBM_PRECISION_MIXED) return LBM_ERR_BAD_ARG;
     int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || device < 0 || device >= ndev) {
+    const cudaError_t ce = cudaGetDeviceCount(&ndev);
+    if (ce != cudaSuccess || ndev <= 0 || device < 0 || device >= ndev) {
         cudaGetLastError();
+        g_create_error = std::string("no usable CUDA device: cudaGetDeviceCount -> ") + cudaGetErrorString(ce) +
+                         ", " + std::to_string(ndev) + " device(s), requested " + std::to_string(device);
         return LBM_ERR_NO_DEVICE;
     }
     cudaDeviceProp prop{};
-    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) return LBM_ERR_NO_DEVICE;
-    if (cudaSetDevice(device) != cudaSuccess) return LBM_ERR_NO_DEVICE;
+    const cudaError_t pe = cudaGetDeviceProperties(&prop, device);
+    if (pe != cudaSuccess || prop.major != 10) {
+        g_create_error = std::string("device ") + std::to_string(device) + " is not sm_100 (" +
+                         (pe == cudaSuccess ? std::string(prop.name) + ", sm_" + std::to_string(prop.major) +
+                                                  std::to_string(prop.minor)
+                                            : std::string(cudaGetErrorString(pe))) + ")";
+        return LBM_ERR_NO_DEVICE;
+    }
+    const cudaError_t se = cudaSetDevice(device);
+    if (se != cudaSuccess) {
+        g_create_error = std::string("cudaSetDevice: ") + cudaGetErrorString(se);
+        return LBM_ERR_NO_DEVICE;
+    }
 
     lbm_handle* h = new lbm_handle();
     h->prm = *prm;
@@ -551,6 +605,13 @@ lbm_status lbm_create(const lbm_params* prm, lbm_precision precision, int device
     if (precision == LBM_PRECISION_FP64) st = alloc_fp64(h);
     else st = mixed_alloc(h->mb, h->geom, h->L);
     if (st != LBM_OK) return bail(st);
+    if (precision == LBM_PRECISION_FP64) {
+        // Two-sweep temporal blocking where the tile divides the box; the z
+        // run length can be tuned (0 disables) through LBM_SWEEP2_ZLEN.
+        const char* env = std::getenv("LBM_SWEEP2_ZLEN");
+        const int zlen = env ? std::atoi(env) : 32;
+        h->fuse_zlen = (zlen > 0 && fp64::sweep2_prepare(h->geom)) ? zlen : 0;
+    }
     default_ghosts(h);
     // Background state until the caller loads fields.
     const size_t n = static_cast<size_t>(h->geom.n);
@@ -620,17 +681,18 @@ lbm_status lbm_set_poisson(lbm_handle* h, const lbm_poisson_cfg* cfg)
     // Same validation as InamuroCUDA::setPoissonConvergence / setPoissonIterationLimit
     // (GPU/InamuroCUDA.cu:2582-2608); the dual test needs >= 2 sweeps per segment.
     if (cfg->check_interval <= 0) return fail(h, LBM_ERR_BAD_ARG, "poisson check interval must be positive");
+    if (cfg->dual_residual < 0 || cfg->dual_residual > 2)
+        return fail(h, LBM_ERR_BAD_ARG, "dual_residual must be 0, 1 or 2");
     if (cfg->dual_residual && cfg->check_interval < 2)
         return fail(h, LBM_ERR_BAD_ARG, "dual residual needs a check interval of at least 2");
     if (!(cfg->tolerance > 0.0)) return fail(h, LBM_ERR_BAD_ARG, "poisson tolerance must be positive");
     if (cfg->max_sweeps != 0 && cfg->max_sweeps % static_cast<uint64_t>(cfg->check_interval) != 0)
         return fail(h, LBM_ERR_BAD_ARG, "Poisson iteration limit must be a multiple of check interval");
-    if (cfg->check_interval != h->pcfg.check_interval || cfg->dual_residual != h->pcfg.dual_residual) {
-        for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
+    if (cfg->check_interval != h->pcfg.check_interval || (cfg->dual_residual != 0) != (h->pcfg.dual_residual != 0)) {
+        for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second.first);
         h->graphs.clear();
     }
     h->pcfg = *cfg;
-    h->pcfg.dual_residual = cfg->dual_residual ? 1 : 0;
     return LBM_OK;
 }
 
@@ -662,6 +724,14 @@ lbm_status lbm_step_replay(lbm_handle* h, int n_steps, const uint64_t* sweeps, l
         const lbm_status s = step_once(h, sweeps[i], stats ? stats + i : nullptr);
         if (s != LBM_OK) return s;
     }
+    return LBM_OK;
+}
+
+lbm_status lbm_set_check_callback(lbm_handle* h, lbm_check_callback cb, void* user)
+{
+    if (check_handle(h) != LBM_OK) return LBM_ERR_BAD_ARG;
+    h->check_cb = cb;
+    h->check_user = user;
     return LBM_OK;
 }
 

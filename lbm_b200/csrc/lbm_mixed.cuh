@@ -22,6 +22,7 @@ struct MixedBuffers {
     double *part_src = nullptr, *part_prep = nullptr, *part_a = nullptr, *part_b = nullptr,
            *part_c = nullptr, *part_mass = nullptr;
     double* scratch = nullptr;   // FP64 staging for loads/downloads (n doubles)
+    int fuse_zlen = 0;           // >0: plain sweeps run two per pass, z runs of this length
     bool allocated = false;
 };
 
