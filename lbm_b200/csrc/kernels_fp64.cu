@@ -354,59 +354,72 @@ sweep_kernel(Geom g, const double* __restrict__ hin, double* __restrict__ hout,
 // pulled from global memory) into a ring of three shared-memory planes, then
 // sweep k+1 on the tile from that ring.  Every cell's arithmetic is
 // collide_h_store's expression, so (without FMA contraction in this file) the
-// result is bitwise that of two sweep_kernel launches.  lx % TX == 0 and
-// ly % TY == 0 are required (checked by the launcher).
+// result is bitwise that of two sweep_kernel launches.  Each thread owns one
+// halo-region cell for the whole march and keeps the next plane's global
+// pulls in flight while the CTA works through the shared-memory phase.
+// lx % TX == 0 and ly % TY == 0 are required (checked by the launcher).
 constexpr int F2_TX = 32, F2_TY = 4;
 constexpr int F2_RX = F2_TX + 2, F2_RY = F2_TY + 2, F2_RC = F2_RX * F2_RY;
+constexpr int F2_THREADS = (F2_RC + 31) / 32 * 32;   // 224: one thread per region cell
 constexpr int F2_SMEM = 3 * Q * F2_RC * (int)sizeof(double);
 
-__global__ void __launch_bounds__(F2_TX * F2_TY)
+__global__ void __launch_bounds__(F2_THREADS)
 sweep2_kernel(Geom g, int zlen, const double* __restrict__ hin, double* __restrict__ hout,
               const double* __restrict__ rho, const double* __restrict__ s)
 {
     extern __shared__ double ring2[];   // [3][Q][F2_RC]
-    const int tid = threadIdx.x + F2_TX * threadIdx.y;
+    const int t = threadIdx.x;
     const int x0 = blockIdx.x * F2_TX, y0 = blockIdx.y * F2_TY;
     const int z0 = blockIdx.z * zlen;
     const int z1 = min(z0 + zlen, g.lz);
+    const bool owner = t < F2_RC;
+    const int xw = (x0 - 1 + t % F2_RX + g.lx) % g.lx;
+    const int yw = (y0 - 1 + t / F2_RX + g.ly) % g.ly;
 
-    auto first_sweep = [&](int zz) {
+    double a[Q];
+    double a_rho = 1.0, a_s = 0.0;
+    auto prefetch = [&](int zz) {
+        if (!owner) return;
         const int zw = (zz % g.lz + g.lz) % g.lz;
-        double* slot = ring2 + ((zz % 3 + 3) % 3) * (Q * F2_RC);
-        for (int r = tid; r < F2_RC; r += F2_TX * F2_TY) {
-            const int rx = r % F2_RX, ry = r / F2_RX;
-            const int xw = (x0 - 1 + rx + g.lx) % g.lx;
-            const int yw = (y0 - 1 + ry + g.ly) % g.ly;
-            double hv[Q];
-            pull_regs(hv, hin, g, xw, yw, zw);
-            bounce_regs(hv, g, xw);
-            const long long c = cell_of(g, xw, yw, zw);
-            const double pv = sum_q(hv);
-            const double tauh = 1.0 / __ldg(rho + c) + 0.5;
-            // collide_h_store into the ring (n = F2_RC, cell = r)
-            collide_h_store(hv, pv, tauh, __ldg(s + c), slot, F2_RC, r);
-        }
+        pull_regs(a, hin, g, xw, yw, zw);
+        const long long c = cell_of(g, xw, yw, zw);
+        a_rho = __ldg(rho + c);
+        a_s = __ldg(s + c);
+    };
+    auto finish = [&](int zz) {
+        if (!owner) return;
+        bounce_regs(a, g, xw);
+        const double pv = sum_q(a);
+        const double tauh = 1.0 / a_rho + 0.5;
+        // collide_h_store into the ring (n = F2_RC, cell = t)
+        collide_h_store(a, pv, tauh, a_s, ring2 + ((zz % 3 + 3) % 3) * (Q * F2_RC), F2_RC, t);
     };
 
-    first_sweep(z0 - 1);
-    first_sweep(z0);
-    const int tx = threadIdx.x, ty = threadIdx.y;
+    prefetch(z0 - 1);
+    finish(z0 - 1);
+    prefetch(z0);
+    finish(z0);
+    prefetch(z0 + 1);
+    const int tx = t % F2_TX, ty = t / F2_TX;
     const int x = x0 + tx, y = y0 + ty;
     for (int z = z0; z < z1; ++z) {
-        first_sweep(z + 1);
+        finish(z + 1);
+        if (z + 1 < z1) prefetch(z + 2);
         __syncthreads();
-        double hv[Q];
-        static_for<0, Q>([&](auto qc) {
-            constexpr int q = decltype(qc)::value;
-            const int zs = z - cz(q);
-            const double* slot = ring2 + ((zs % 3 + 3) % 3) * (Q * F2_RC);
-            hv[q] = slot[q * F2_RC + (ty + 1 - cy(q)) * F2_RX + (tx + 1 - cx(q))];
-        });
-        bounce_regs(hv, g, x);
-        const long long c = cell_of(g, x, y, z);
-        const double pv = sum_q(hv);
-        const double tauh = 1.0 / __ldg(rho + c) + 0.5;
-        collide_h_store(hv, pv, tauh, __ldg(s + c), hout, g.n, c);
+        if (t < F2_TX * F2_TY) {
+            double hv[Q];
+            static_for<0, Q>([&](auto qc) {
+                constexpr int q = decltype(qc)::value;
+                const int zs = z - cz(q);
+                const double* slot = ring2 + ((zs % 3 + 3) % 3) * (Q * F2_RC);
+                hv[q] = slot[q * F2_RC + (ty + 1 - cy(q)) * F2_RX + (tx + 1 - cx(q))];
+            });
+            bounce_regs(hv, g, x);
+            const long long c = cell_of(g, x, y, z);
+            const double pv = sum_q(hv);
+            const double tauh = 1.0 / __ldg(rho + c) + 0.5;
+            collide_h_store(hv, pv, tauh, __ldg(s + c), hout, g.n, c);
+        }
         __syncthreads();
     }
 }
@@ -693,7 +706,7 @@ void sweep2(cudaStream_t st, const Geom& g, int zlen, const double* hin, double*
             const double* rho, const double* s)
 {
     const dim3 grid(g.lx / F2_TX, g.ly / F2_TY, (g.lz + zlen - 1) / zlen);
-    sweep2_kernel<<<grid, dim3(F2_TX, F2_TY), F2_SMEM, st>>>(g, zlen, hin, hout, rho, s);
+    sweep2_kernel<<<grid, F2_THREADS, F2_SMEM, st>>>(g, zlen, hin, hout, rho, s);
 }
 
 void sweep_check_a(cudaStream_t st, const Launch& L, const Geom& g, const double* hin,

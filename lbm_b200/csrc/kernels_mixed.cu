@@ -309,61 +309,75 @@ sweep_kernel(Geom g, const float* __restrict__ hin, float* __restrict__ hout,
 // wrapped coordinates, so the periodic stream and the x slip overwrite are
 // those of two single sweeps, and each cell's arithmetic is the same
 // collide_h as in sweep_kernel.
+// Each of the CTA's threads owns one cell of the halo region for the whole z
+// march and keeps the global pulls of the NEXT plane in flight (registers)
+// while the CTA works through the shared-memory phase of the current one, so
+// load latency overlaps the ring reads, the second collision and the stores.
 // Requires lx % TX == 0 and ly % TY == 0 (the launcher checks).
 constexpr int S2_TX = 32, S2_TY = 8;
 constexpr int S2_RX = S2_TX + 2, S2_RY = S2_TY + 2, S2_RC = S2_RX * S2_RY;
+constexpr int S2_THREADS = (S2_RC + 31) / 32 * 32;   // 352: one thread per region cell
 constexpr int S2_SMEM = 3 * Q * S2_RC * (int)sizeof(float);
 
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(S2_THREADS, 2)
 sweep2_kernel(Geom g, int zlen, const float* __restrict__ hin, float* __restrict__ hout,
               const float* __restrict__ omega, const float* __restrict__ s)
 {
     extern __shared__ float ring[];   // [3][Q][S2_RC]
-    const int tid = threadIdx.x + S2_TX * threadIdx.y;
+    const int t = threadIdx.x;
     const int x0 = blockIdx.x * S2_TX, y0 = blockIdx.y * S2_TY;
     const int z0 = blockIdx.z * zlen;
     const int z1 = min(z0 + zlen, g.lz);
+    // this thread's halo-region cell (wrapped coordinates)
+    const bool owner = t < S2_RC;
+    const int xw = (x0 - 1 + t % S2_RX + g.lx) % g.lx;
+    const int yw = (y0 - 1 + t / S2_RX + g.ly) % g.ly;
 
-    // sweep k on plane zz (wrapped) for the tile + halo, into ring slot zz mod 3
-    auto first_sweep = [&](int zz) {
+    float a[Q];
+    float a_om = 0.f, a_s = 0.f;
+    auto prefetch = [&](int zz) {        // issue sweep k's pulls for plane zz
+        if (!owner) return;
         const int zw = (zz % g.lz + g.lz) % g.lz;
-        float* slot = ring + ((zz % 3 + 3) % 3) * (Q * S2_RC);
-        for (int r = tid; r < S2_RC; r += S2_TX * S2_TY) {
-            const int rx = r % S2_RX, ry = r / S2_RX;
-            const int xw = (x0 - 1 + rx + g.lx) % g.lx;
-            const int yw = (y0 - 1 + ry + g.ly) % g.ly;
-            float hv[Q];
-            pull_regs(hv, hin, g, xw, yw, zw);
-            bounce_regs(hv, g, xw);
-            const long long c = cell_of(g, xw, yw, zw);
-            const double pv = sum_q(hv);
-            const float p32 = (float)pv;
-            const float om = __ldg(omega + c), sv = __ldg(s + c);
-            static_for<0, Q>([&](auto qc) {
-                constexpr int q = decltype(qc)::value;
-                slot[q * S2_RC + r] = collide_h<q>(hv[q], p32, om, sv);
-            });
-        }
+        pull_regs(a, hin, g, xw, yw, zw);
+        const long long c = cell_of(g, xw, yw, zw);
+        a_om = __ldg(omega + c);
+        a_s = __ldg(s + c);
     };
-
-    first_sweep(z0 - 1);
-    first_sweep(z0);
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int x = x0 + tx, y = y0 + ty;
-    for (int z = z0; z < z1; ++z) {
-        first_sweep(z + 1);
-        __syncthreads();
-        // sweep k+1 at (x, y, z): pull from the ring
-        float hv[Q];
+    auto finish = [&](int zz) {          // complete sweep k on plane zz into its ring slot
+        if (!owner) return;
+        bounce_regs(a, g, xw);
+        const float p32 = (float)sum_q(a);
+        float* slot = ring + ((zz % 3 + 3) % 3) * (Q * S2_RC);
         static_for<0, Q>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
-            const int zs = z - cz(q);
-            const float* slot = ring + ((zs % 3 + 3) % 3) * (Q * S2_RC);
-            hv[q] = slot[q * S2_RC + (ty + 1 - cy(q)) * S2_RX + (tx + 1 - cx(q))];
+            slot[q * S2_RC + t] = collide_h<q>(a[q], p32, a_om, a_s);
         });
-        bounce_regs(hv, g, x);
-        const long long c = cell_of(g, x, y, z);
-        collide_h_store(hv, sum_q(hv), __ldg(omega + c), __ldg(s + c), hout, g.n, c);
+    };
+
+    prefetch(z0 - 1);
+    finish(z0 - 1);
+    prefetch(z0);
+    finish(z0);
+    prefetch(z0 + 1);
+    const int tx = t % S2_TX, ty = t / S2_TX;
+    const int x = x0 + tx, y = y0 + ty;
+    for (int z = z0; z < z1; ++z) {
+        finish(z + 1);
+        if (z + 1 < z1) prefetch(z + 2);
+        __syncthreads();
+        if (t < S2_TX * S2_TY) {
+            // sweep k+1 at (x, y, z): pull from the ring
+            float hv[Q];
+            static_for<0, Q>([&](auto qc) {
+                constexpr int q = decltype(qc)::value;
+                const int zs = z - cz(q);
+                const float* slot = ring + ((zs % 3 + 3) % 3) * (Q * S2_RC);
+                hv[q] = slot[q * S2_RC + (ty + 1 - cy(q)) * S2_RX + (tx + 1 - cx(q))];
+            });
+            bounce_regs(hv, g, x);
+            const long long c = cell_of(g, x, y, z);
+            collide_h_store(hv, sum_q(hv), __ldg(omega + c), __ldg(s + c), hout, g.n, c);
+        }
         __syncthreads();
     }
 }
@@ -651,7 +665,7 @@ int mixed_segment(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom
     if (mb.fuse_zlen > 0) {
         const dim3 grid(g.lx / S2_TX, g.ly / S2_TY, (g.lz + mb.fuse_zlen - 1) / mb.fuse_zlen);
         for (int i = 0; i + 1 < n_normal; i += 2) {
-            sweep2_kernel<<<grid, dim3(S2_TX, S2_TY), S2_SMEM, st>>>(g, mb.fuse_zlen, mb.h[cur], mb.h[1 - cur],
+            sweep2_kernel<<<grid, S2_THREADS, S2_SMEM, st>>>(g, mb.fuse_zlen, mb.h[cur], mb.h[1 - cur],
                                                                      omega, mb.s);
             cur = 1 - cur;
         }

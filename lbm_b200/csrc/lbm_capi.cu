@@ -609,7 +609,7 @@ lbm_status lbm_create(const lbm_params* prm, lbm_precision precision, int device
         // Two-sweep temporal blocking where the tile divides the box; the z
         // run length can be tuned (0 disables) through LBM_SWEEP2_ZLEN.
         const char* env = std::getenv("LBM_SWEEP2_ZLEN");
-        const int zlen = env ? std::atoi(env) : 32;
+        const int zlen = env ? std::atoi(env) : 0;
         h->fuse_zlen = (zlen > 0 && fp64::sweep2_prepare(h->geom)) ? zlen : 0;
     }
     default_ghosts(h);

@@ -251,3 +251,21 @@ def test_full_size_256_translation_and_mirror():
     assert rel_err(c["phi"][1:][::-1], c["phi"][1:]) <= 1e-11
     assert rel_err(-c["w"][1:][::-1], c["w"][1:]) <= 1e-9
     assert np.max(np.abs(c["w"])) > 0.0
+
+
+@pytest.mark.parametrize("zlen", ["32", "7"])
+def test_fp64_two_sweep_pass_is_bitwise(zlen, monkeypatch):
+    """The FP64 temporally blocked pass (two sweeps per launch) keeps every
+    cell's arithmetic, so it reproduces single-sweep launches bit for bit."""
+    p, f = laplace_case((64, 12, 20), DD=8.0, noise=1e-4)
+    f["w"] = 0.01 * np.sin(2 * np.pi * np.arange(20) / 20)[:, None, None] * np.ones_like(f["w"])
+    monkeypatch.setenv("LBM_SWEEP2_ZLEN", "0")
+    a = solver(p, f)
+    monkeypatch.setenv("LBM_SWEEP2_ZLEN", zlen)
+    b = solver(p, f)
+    for _ in range(3):
+        assert a.step(1)[0]["iterations"] == b.step(1)[0]["iterations"]
+    fa, fb = a.download_fields(), b.download_fields()
+    for k in L.FIELDS:
+        assert np.array_equal(fa[k], fb[k]), k
+    assert b.timing()["kernel_launches"] < a.timing()["kernel_launches"]
