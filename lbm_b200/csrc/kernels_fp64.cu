@@ -314,17 +314,19 @@ poisson_init_kernel(Geom g, int h_loaded, const double* __restrict__ hload,
     });
 }
 
+// I: index type (long long in general, int where 15 n < 2^31).
+template <class I>
 __device__ __forceinline__ void collide_h_store(const double (&hv)[Q], double pv, double tauh,
-                                                double sv, double* __restrict__ hout,
-                                                long long n, long long c)
+                                                double sv, double* __restrict__ hout, I n, I c)
 {
     static_for<0, Q>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
         constexpr double E = wE(q);
         const double hequ = E * pv;
-        hout[(long long)q * n + c] = hv[q] - (hv[q] - hequ) / tauh - (E / 3.0) * sv;
+        hout[(I)q * n + c] = hv[q] - (hv[q] - hequ) / tauh - (E / 3.0) * sv;
     });
 }
+
 
 __device__ __forceinline__ double sum_q(const double (&hv)[Q])
 {
@@ -333,56 +335,73 @@ __device__ __forceinline__ double sum_q(const double (&hv)[Q])
     return acc;
 }
 
+// kOff32: 32-bit offsets (the launcher picks it when 15 n < 2^31).
+template <bool kOff32>
 __global__ void __launch_bounds__(256)
 sweep_kernel(Geom g, const double* __restrict__ hin, double* __restrict__ hout,
              const double* __restrict__ rho, const double* __restrict__ s)
 {
     int x, y, z;
     if (!tile_coords(g, x, y, z)) return;
-    const long long c = cell_of(g, x, y, z);
     double hv[Q];
-    pull_regs(hv, hin, g, x, y, z);
-    bounce_regs(hv, g, x);
-    const double pv = sum_q(hv);
-    const double tauh = 1.0 / __ldg(rho + c) + 0.5;
-    collide_h_store(hv, pv, tauh, __ldg(s + c), hout, g.n, c);
+    if constexpr (kOff32) {
+        const int n = (int)g.n;
+        const int c = (z * g.ly + y) * g.lx + x;
+        pull_regs32(hv, hin, n, g, x, y, z);
+        bounce_regs(hv, g, x);
+        const double pv = sum_q(hv);
+        const double tauh = 1.0 / __ldg(rho + c) + 0.5;
+        collide_h_store(hv, pv, tauh, __ldg(s + c), hout, n, c);
+    } else {
+        const long long c = cell_of(g, x, y, z);
+        pull_regs(hv, hin, g, x, y, z);
+        bounce_regs(hv, g, x);
+        const double pv = sum_q(hv);
+        const double tauh = 1.0 / __ldg(rho + c) + 0.5;
+        collide_h_store(hv, pv, tauh, __ldg(s + c), hout, g.n, c);
+    }
 }
 
 // Two sweeps in one pass (temporal blocking; same scheme as the mixed box).
 // A CTA owns a TX x TY xy tile and a run of `zlen` planes; marching in z it
 // computes sweep k on the tile plus a one-cell halo (wrapped coordinates,
-// pulled from global memory) into a ring of three shared-memory planes, then
-// sweep k+1 on the tile from that ring.  Every cell's arithmetic is
+// pulled from global memory) into a ring of shared-memory planes, then sweep
+// k+1 on the tile from that ring.  Every cell's arithmetic is
 // collide_h_store's expression, so (without FMA contraction in this file) the
 // result is bitwise that of two sweep_kernel launches.  Each thread owns one
 // halo-region cell for the whole march and keeps the next plane's global
 // pulls in flight while the CTA works through the shared-memory phase.
-// lx % TX == 0 and ly % TY == 0 are required (checked by the launcher).
+// Four ring slots make one barrier per plane enough (the slot written at
+// iteration z+1 was last read at z-1).  lx % TX == 0, ly % TY == 0 and
+// 15 n < 2^31 are required (checked by the launcher).
 constexpr int F2_TX = 32, F2_TY = 4;
 constexpr int F2_RX = F2_TX + 2, F2_RY = F2_TY + 2, F2_RC = F2_RX * F2_RY;
 constexpr int F2_THREADS = (F2_RC + 31) / 32 * 32;   // 224: one thread per region cell
-constexpr int F2_SMEM = 3 * Q * F2_RC * (int)sizeof(double);
+constexpr int F2_SLOTS = 4;
+constexpr int F2_SMEM = F2_SLOTS * Q * F2_RC * (int)sizeof(double);
 
-__global__ void __launch_bounds__(F2_THREADS)
+__global__ void __launch_bounds__(F2_THREADS, 2)
 sweep2_kernel(Geom g, int zlen, const double* __restrict__ hin, double* __restrict__ hout,
               const double* __restrict__ rho, const double* __restrict__ s)
 {
-    extern __shared__ double ring2[];   // [3][Q][F2_RC]
+    extern __shared__ double ring2[];   // [F2_SLOTS][Q][F2_RC]
     const int t = threadIdx.x;
+    const int n = (int)g.n;
     const int x0 = blockIdx.x * F2_TX, y0 = blockIdx.y * F2_TY;
     const int z0 = blockIdx.z * zlen;
     const int z1 = min(z0 + zlen, g.lz);
     const bool owner = t < F2_RC;
     const int xw = (x0 - 1 + t % F2_RX + g.lx) % g.lx;
     const int yw = (y0 - 1 + t / F2_RX + g.ly) % g.ly;
+    auto slot_of = [&](int zz) { return ring2 + ((zz + F2_SLOTS) & (F2_SLOTS - 1)) * (Q * F2_RC); };
 
     double a[Q];
     double a_rho = 1.0, a_s = 0.0;
     auto prefetch = [&](int zz) {
         if (!owner) return;
-        const int zw = (zz % g.lz + g.lz) % g.lz;
-        pull_regs(a, hin, g, xw, yw, zw);
-        const long long c = cell_of(g, xw, yw, zw);
+        const int zw = zz < 0 ? zz + g.lz : (zz >= g.lz ? zz - g.lz : zz);
+        pull_regs32(a, hin, n, g, xw, yw, zw);
+        const int c = (zw * g.ly + yw) * g.lx + xw;
         a_rho = __ldg(rho + c);
         a_s = __ldg(s + c);
     };
@@ -392,7 +411,7 @@ sweep2_kernel(Geom g, int zlen, const double* __restrict__ hin, double* __restri
         const double pv = sum_q(a);
         const double tauh = 1.0 / a_rho + 0.5;
         // collide_h_store into the ring (n = F2_RC, cell = t)
-        collide_h_store(a, pv, tauh, a_s, ring2 + ((zz % 3 + 3) % 3) * (Q * F2_RC), F2_RC, t);
+        collide_h_store(a, pv, tauh, a_s, slot_of(zz), F2_RC, t);
     };
 
     prefetch(z0 - 1);
@@ -402,25 +421,27 @@ sweep2_kernel(Geom g, int zlen, const double* __restrict__ hin, double* __restri
     prefetch(z0 + 1);
     const int tx = t % F2_TX, ty = t / F2_TX;
     const int x = x0 + tx, y = y0 + ty;
+    const int rc = (ty + 1) * F2_RX + (tx + 1);
     for (int z = z0; z < z1; ++z) {
         finish(z + 1);
         if (z + 1 < z1) prefetch(z + 2);
         __syncthreads();
         if (t < F2_TX * F2_TY) {
+            const double* sm = slot_of(z - 1);
+            const double* s0 = slot_of(z);
+            const double* sp = slot_of(z + 1);
             double hv[Q];
             static_for<0, Q>([&](auto qc) {
                 constexpr int q = decltype(qc)::value;
-                const int zs = z - cz(q);
-                const double* slot = ring2 + ((zs % 3 + 3) % 3) * (Q * F2_RC);
-                hv[q] = slot[q * F2_RC + (ty + 1 - cy(q)) * F2_RX + (tx + 1 - cx(q))];
+                const double* slot = pick_t<-cz(q)>(sm, s0, sp);
+                hv[q] = slot[q * F2_RC + rc - cy(q) * F2_RX - cx(q)];
             });
             bounce_regs(hv, g, x);
-            const long long c = cell_of(g, x, y, z);
+            const int c = (z * g.ly + y) * g.lx + x;
             const double pv = sum_q(hv);
             const double tauh = 1.0 / __ldg(rho + c) + 0.5;
-            collide_h_store(hv, pv, tauh, __ldg(s + c), hout, g.n, c);
+            collide_h_store(hv, pv, tauh, __ldg(s + c), hout, n, c);
         }
-        __syncthreads();
     }
 }
 
@@ -691,12 +712,15 @@ void poisson_init(cudaStream_t st, const Launch& L, const Geom& g, bool h_loaded
 void sweep(cudaStream_t st, const Launch& L, const Geom& g, const double* hin, double* hout,
            const double* rho, const double* s)
 {
-    sweep_kernel<<<L.grid, L.block, 0, st>>>(g, hin, hout, rho, s);
+    if (15 * g.n < 0x7fffffffLL)
+        sweep_kernel<true><<<L.grid, L.block, 0, st>>>(g, hin, hout, rho, s);
+    else
+        sweep_kernel<false><<<L.grid, L.block, 0, st>>>(g, hin, hout, rho, s);
 }
 
 int sweep2_prepare(const Geom& g)
 {
-    if (g.lx % F2_TX != 0 || g.ly % F2_TY != 0 || g.lz < 3) return 0;
+    if (g.lx % F2_TX != 0 || g.ly % F2_TY != 0 || g.lz < 3 || 15 * g.n >= 0x7fffffffLL) return 0;
     if (cudaFuncSetAttribute(sweep2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, F2_SMEM) != cudaSuccess)
         return 0;
     return 1;

@@ -288,9 +288,41 @@ poisson_init_kernel(Geom g, int h_loaded, const float* __restrict__ hload, float
     collide_h_store(hv, pv, omega[c], s[c], hout, g.n, c);
 }
 
+// p = sum_q h in FP32, pairwise (plain sweeps; the check kernels sum in FP64).
+__device__ __forceinline__ float sum_q32(const float (&h)[Q])
+{
+    return (((h[0] + h[1]) + (h[2] + h[3])) + ((h[4] + h[5]) + (h[6] + h[7]))) +
+           (((h[8] + h[9]) + (h[10] + h[11])) + ((h[12] + h[13]) + h[14]));
+}
+
+__device__ __forceinline__ void collide_h_store32(const float (&hv)[Q], float p32, float om, float sv,
+                                                  float* __restrict__ hout, int n, int c)
+{
+    static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        hout[q * n + c] = collide_h<q>(hv[q], p32, om, sv);
+    });
+}
+
+// Plain sweep with 32-bit offsets (the launcher uses it when 15 n < 2^31).
 __global__ void __launch_bounds__(256)
 sweep_kernel(Geom g, const float* __restrict__ hin, float* __restrict__ hout,
              const float* __restrict__ omega, const float* __restrict__ s)
+{
+    int x, y, z;
+    if (!tile_coords(g, x, y, z)) return;
+    const int n = (int)g.n;
+    const int c = (z * g.ly + y) * g.lx + x;
+    float hv[Q];
+    pull_regs32(hv, hin, n, g, x, y, z);
+    bounce_regs(hv, g, x);
+    collide_h_store32(hv, sum_q32(hv), __ldg(omega + c), __ldg(s + c), hout, n, c);
+}
+
+// The same with 64-bit offsets for boxes with 15 n >= 2^31.
+__global__ void __launch_bounds__(256)
+sweep_kernel64(Geom g, const float* __restrict__ hin, float* __restrict__ hout,
+               const float* __restrict__ omega, const float* __restrict__ s)
 {
     int x, y, z;
     if (!tile_coords(g, x, y, z)) return;
@@ -298,33 +330,38 @@ sweep_kernel(Geom g, const float* __restrict__ hin, float* __restrict__ hout,
     float hv[Q];
     pull_regs(hv, hin, g, x, y, z);
     bounce_regs(hv, g, x);
-    collide_h_store(hv, sum_q(hv), __ldg(omega + c), __ldg(s + c), hout, g.n, c);
+    collide_h_store(hv, (double)sum_q32(hv), __ldg(omega + c), __ldg(s + c), hout, g.n, c);
 }
 
 // Two sweeps in one pass (temporal blocking).  A CTA owns an xy tile of
 // TX x TY output cells and a run of `zlen` planes.  Marching in z it computes
 // sweep k on the tile plus a one-cell xy halo (pulling from global memory)
-// into a ring of three shared-memory planes, then sweep k+1 on the tile by
-// pulling from that ring, and writes only the second result.  Halo cells use
-// wrapped coordinates, so the periodic stream and the x slip overwrite are
-// those of two single sweeps, and each cell's arithmetic is the same
-// collide_h as in sweep_kernel.
+// into a ring of shared-memory planes, then sweep k+1 on the tile by pulling
+// from that ring, and writes only the second result.  Halo cells use wrapped
+// coordinates, so the periodic stream and the x slip overwrite are those of
+// two single sweeps, and each cell's arithmetic is sweep_kernel's (collide_h,
+// sum_q32).
 // Each of the CTA's threads owns one cell of the halo region for the whole z
 // march and keeps the global pulls of the NEXT plane in flight (registers)
 // while the CTA works through the shared-memory phase of the current one, so
 // load latency overlaps the ring reads, the second collision and the stores.
-// Requires lx % TX == 0 and ly % TY == 0 (the launcher checks).
+// The ring has four plane slots: the slot written at iteration z+1 was last
+// read at iteration z-1, which every thread has left when it passes the single
+// barrier of iteration z.
+// Requires lx % TX == 0, ly % TY == 0 and 15 n < 2^31 (the launcher checks).
 constexpr int S2_TX = 32, S2_TY = 8;
 constexpr int S2_RX = S2_TX + 2, S2_RY = S2_TY + 2, S2_RC = S2_RX * S2_RY;
 constexpr int S2_THREADS = (S2_RC + 31) / 32 * 32;   // 352: one thread per region cell
-constexpr int S2_SMEM = 3 * Q * S2_RC * (int)sizeof(float);
+constexpr int S2_SLOTS = 4;
+constexpr int S2_SMEM = S2_SLOTS * Q * S2_RC * (int)sizeof(float);
 
 __global__ void __launch_bounds__(S2_THREADS, 2)
 sweep2_kernel(Geom g, int zlen, const float* __restrict__ hin, float* __restrict__ hout,
               const float* __restrict__ omega, const float* __restrict__ s)
 {
-    extern __shared__ float ring[];   // [3][Q][S2_RC]
+    extern __shared__ float ring[];   // [S2_SLOTS][Q][S2_RC]
     const int t = threadIdx.x;
+    const int n = (int)g.n;
     const int x0 = blockIdx.x * S2_TX, y0 = blockIdx.y * S2_TY;
     const int z0 = blockIdx.z * zlen;
     const int z1 = min(z0 + zlen, g.lz);
@@ -332,22 +369,23 @@ sweep2_kernel(Geom g, int zlen, const float* __restrict__ hin, float* __restrict
     const bool owner = t < S2_RC;
     const int xw = (x0 - 1 + t % S2_RX + g.lx) % g.lx;
     const int yw = (y0 - 1 + t / S2_RX + g.ly) % g.ly;
+    auto slot_of = [&](int zz) { return ring + ((zz + S2_SLOTS) & (S2_SLOTS - 1)) * (Q * S2_RC); };
 
     float a[Q];
     float a_om = 0.f, a_s = 0.f;
     auto prefetch = [&](int zz) {        // issue sweep k's pulls for plane zz
         if (!owner) return;
-        const int zw = (zz % g.lz + g.lz) % g.lz;
-        pull_regs(a, hin, g, xw, yw, zw);
-        const long long c = cell_of(g, xw, yw, zw);
+        const int zw = zz < 0 ? zz + g.lz : (zz >= g.lz ? zz - g.lz : zz);
+        pull_regs32(a, hin, n, g, xw, yw, zw);
+        const int c = (zw * g.ly + yw) * g.lx + xw;
         a_om = __ldg(omega + c);
         a_s = __ldg(s + c);
     };
     auto finish = [&](int zz) {          // complete sweep k on plane zz into its ring slot
         if (!owner) return;
         bounce_regs(a, g, xw);
-        const float p32 = (float)sum_q(a);
-        float* slot = ring + ((zz % 3 + 3) % 3) * (Q * S2_RC);
+        const float p32 = sum_q32(a);
+        float* slot = slot_of(zz);
         static_for<0, Q>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
             slot[q * S2_RC + t] = collide_h<q>(a[q], p32, a_om, a_s);
@@ -361,24 +399,26 @@ sweep2_kernel(Geom g, int zlen, const float* __restrict__ hin, float* __restrict
     prefetch(z0 + 1);
     const int tx = t % S2_TX, ty = t / S2_TX;
     const int x = x0 + tx, y = y0 + ty;
+    const int rc = (ty + 1) * S2_RX + (tx + 1);
     for (int z = z0; z < z1; ++z) {
         finish(z + 1);
         if (z + 1 < z1) prefetch(z + 2);
         __syncthreads();
         if (t < S2_TX * S2_TY) {
-            // sweep k+1 at (x, y, z): pull from the ring
+            // sweep k+1 at (x, y, z): pull from the ring (planes z-1, z, z+1)
+            const float* sm = slot_of(z - 1);
+            const float* s0 = slot_of(z);
+            const float* sp = slot_of(z + 1);
             float hv[Q];
             static_for<0, Q>([&](auto qc) {
                 constexpr int q = decltype(qc)::value;
-                const int zs = z - cz(q);
-                const float* slot = ring + ((zs % 3 + 3) % 3) * (Q * S2_RC);
-                hv[q] = slot[q * S2_RC + (ty + 1 - cy(q)) * S2_RX + (tx + 1 - cx(q))];
+                const float* slot = pick_t<-cz(q)>(sm, s0, sp);
+                hv[q] = slot[q * S2_RC + rc - cy(q) * S2_RX - cx(q)];
             });
             bounce_regs(hv, g, x);
-            const long long c = cell_of(g, x, y, z);
-            collide_h_store(hv, sum_q(hv), __ldg(omega + c), __ldg(s + c), hout, g.n, c);
+            const int c = (z * g.ly + y) * g.lx + x;
+            collide_h_store32(hv, sum_q32(hv), __ldg(omega + c), __ldg(s + c), hout, n, c);
         }
-        __syncthreads();
     }
 }
 
@@ -558,7 +598,7 @@ lbm_status mixed_alloc(MixedBuffers& mb, const Geom& g, const Launch& L)
     mb.fuse_zlen = 0;
     const char* env = std::getenv("LBM_SWEEP2_ZLEN");
     const int zlen = env ? std::atoi(env) : 32;
-    if (zlen > 0 && g.lx % S2_TX == 0 && g.ly % S2_TY == 0 && g.lz >= 3 &&
+    if (zlen > 0 && g.lx % S2_TX == 0 && g.ly % S2_TY == 0 && g.lz >= 3 && 15 * g.n < 0x7fffffffLL &&
         cudaFuncSetAttribute(sweep2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, S2_SMEM) == cudaSuccess)
         mb.fuse_zlen = zlen;
     mb.allocated = true;
@@ -671,8 +711,12 @@ int mixed_segment(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom
         }
         n_normal &= 1;
     }
+    const bool off32 = 15 * g.n < 0x7fffffffLL;
     for (int i = 0; i < n_normal; ++i) {
-        sweep_kernel<<<L.grid, L.block, 0, st>>>(g, mb.h[cur], mb.h[1 - cur], omega, mb.s);
+        if (off32)
+            sweep_kernel<<<L.grid, L.block, 0, st>>>(g, mb.h[cur], mb.h[1 - cur], omega, mb.s);
+        else
+            sweep_kernel64<<<L.grid, L.block, 0, st>>>(g, mb.h[cur], mb.h[1 - cur], omega, mb.s);
         cur = 1 - cur;
     }
     sweep_check_a_kernel<<<L.grid, L.block, 0, st>>>(g, mb.h[cur], mb.h[1 - cur], mb.p_chk, mb.part_a, L.nblocks);

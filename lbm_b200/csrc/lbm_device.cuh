@@ -166,6 +166,29 @@ __device__ __forceinline__ long long pull_src(const Geom& g, const Wrap& w, int 
                    pick<-cz(q)>(w.zm, z, w.zp));
 }
 
+template <int D, class T>
+__device__ __forceinline__ T pick_t(T m, T c, T p)
+{
+    if constexpr (D < 0) return m;
+    else if constexpr (D > 0) return p;
+    else return c;
+}
+
+// Pull stream of all 15 populations into (x, y, z) with 32-bit offsets: the
+// caller guarantees 15 * n < 2^31 (the 64-bit form is pull_src + cell_of).
+template <class T>
+__device__ __forceinline__ void pull_regs32(T (&v)[Q], const T* __restrict__ src, int n,
+                                            const Geom& g, int x, int y, int z)
+{
+    const Wrap w(g, x, y, z);
+    static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        const int idx = (pick<-cz(q)>(w.zm, z, w.zp) * g.ly + pick<-cy(q)>(w.ym, y, w.yp)) * g.lx +
+                        pick<-cx(q)>(w.xm, x, w.xp);
+        v[q] = __ldg(src + (q * n + idx));
+    });
+}
+
 // Stencil neighbour x + c_k.
 template <int k>
 __device__ __forceinline__ long long stencil_nb(const Geom& g, const Mirror& m, int x, int y, int z)
