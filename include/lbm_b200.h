@@ -5,7 +5,7 @@
  * The reference (UniBoy222/LBM) exposes this path only as the C++ class
  * InamuroCUDA (GPU/InamuroCUDA.hpp:16-248) built on a CPU-side Inamuro object
  * (GPU/Inamuro.hpp:11-140).  This header is the flat boundary under the C++
- * drop-in classes of lbm_b200/csrc/inamuro_cuda.hpp: plain pointers and sizes,
+ * drop-in class of include/InamuroCUDA.hpp: plain pointers and sizes,
  * integer status codes, no exceptions and no C++ or torch types.  Each entry
  * point names the reference interface it replaces.
  *
@@ -136,6 +136,7 @@ typedef struct {
     uint64_t sweeps;         /* Poisson sweeps summed over steps */
     uint64_t sweep_kernels;  /* sweep-kernel launches (incl. the extra one per check) */
     uint64_t kernel_launches;/* all kernels launched by the library (graph nodes included) */
+    uint64_t fused_sweeps;   /* sweeps run inside two-sweep (temporally blocked) launches */
 } lbm_timing;
 
 /* Statistics of one field over the box (Inamuro::FieldStatistics,

@@ -76,7 +76,7 @@ class StepStats(C.Structure):
 class Timing(C.Structure):
     _fields_ = [(k, C.c_double) for k in ("collide_ms", "moments_ms", "prep_ms", "poisson_ms",
                                            "correct_ms")] + \
-        [(k, C.c_uint64) for k in ("steps", "sweeps", "sweep_kernels", "kernel_launches")]
+        [(k, C.c_uint64) for k in ("steps", "sweeps", "sweep_kernels", "kernel_launches", "fused_sweeps")]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -379,6 +379,7 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
     uint64_t kernels = 0;
     // collide, moments, 2 finalize, prep, finalize, poisson_init (+ correct below)
     uint64_t launches = 7;
+    uint64_t fused_sweeps = 0;
     for (;;) {
         const int n_normal = dual ? (first_seg ? ci - 1 : ci - 2) : ci - 1;
         SegKey key{hcur, n_normal, dual};
@@ -396,6 +397,7 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
         const uint64_t plain_launches = fused ? static_cast<uint64_t>(n_normal / 2 + n_normal % 2)
                                               : static_cast<uint64_t>(n_normal);
         launches += plain_launches + 4 + (dual ? 1 : 0);
+        if (fused) fused_sweeps += static_cast<uint64_t>(n_normal / 2) * 2;
         first_seg = false;
         if (dh.error) {
             return fail(h, static_cast<lbm_status>(dh.error), site_text(dh.error_site));
@@ -461,6 +463,7 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
     h->acc.sweeps += iters;
     h->acc.sweep_kernels += kernels;
     h->acc.kernel_launches += launches + 1;
+    h->acc.fused_sweeps += fused_sweeps;
     h->steps_done += 1;
     if (stats) {
         fill_stats(h, dh, stats);

@@ -35,7 +35,7 @@ def test_struct_sizes_match_header():
     assert ctypes.sizeof(L.Params) == 6 * 4 + 16 * 8 + 2 * 4 + 7 * 8
     assert ctypes.sizeof(L.PoissonCfg) == 40
     assert ctypes.sizeof(L.StepStats) == 8 + 16 * 8 + 6 * 4 + 8
-    assert ctypes.sizeof(L.Timing) == 5 * 8 + 4 * 8
+    assert ctypes.sizeof(L.Timing) == 5 * 8 + 5 * 8
 
 
 def test_create_without_gpu_fails_loudly():
