@@ -10,7 +10,7 @@ tau_f = tau_g = 1, mu = 0.1 rho (nu = 0.1 in both phases), tanh interface with
 W = 4 (interface_width = 2), seeded uniform noise of amplitude 1e-4 on phi.
 The collision runs along z: x carries the reference's slip walls.  The Poisson
 stop is the contract shared by every reference entry point (check every 100
-sweeps, relative pressure change below 1e-3; WHILE_BASELINE.md); --dual adds
+sweeps, relative pressure change below 1e-3; the reference's WHILE_BASELINE.md); --dual adds
 the GPU production switch's kinetic fixed-point residual.  Inputs are synthetic;
 the box (about 14 GB of FP64 state) is far larger than L2, so no flush is
 needed between timed steps.

@@ -192,8 +192,8 @@ public:
     const PoissonStepDiagnostics& getLastPoissonDiagnostics() const { return diag_; }
 
     // ---- settings (GPU/InamuroCUDA.hpp:67-88) ----
-    // The reference's non-production Poisson accelerators are not part of this
-    // build; enabling one is rejected, disabling is accepted.
+    // The reference's non-production Poisson accelerators are not provided by the
+    // library; enabling one is rejected, disabling is accepted.
     void setUseFusedPoisson(bool e) { rejectAccelerator(e, "fused Poisson"); }
     void setUseOnePassPoisson(bool e) { rejectAccelerator(e, "one-pass Poisson"); }
     void setUseScalarPoisson(bool e) { rejectAccelerator(e, "scalar Poisson"); }
@@ -352,8 +352,8 @@ private:
     {
         if (enabled)
             throw std::invalid_argument(std::string(name) +
-                                        ": the reference's non-production Poisson accelerators are not part "
-                                        "of this build (split Poisson only)");
+                                        ": the experimental Poisson accelerators are not provided by "
+                                        "liblbm_b200 (split Poisson only)");
     }
 
     void applyPoissonConfig()

@@ -32,8 +32,11 @@
 //                  fused with sweep k+1's stream/bounce/sum and k+2's collision
 //   correct        correctVelocityKernel (.cu:1330-1371); CPU/Inamuro.cpp:794-823
 #include <cuda_runtime.h>
+
+#include <cstdlib>
 #include <math_constants.h>
 
+#include "collide_zm.cuh"
 #include "lbm_solver.cuh"
 
 namespace lbm {
@@ -99,7 +102,136 @@ __device__ __forceinline__ void stencil(const double* __restrict__ f, const Geom
     if constexpr (kLap) lap = (al - 14.0 * __ldg(f + c)) / 5.0;
 }
 
-// Fused collide (+ the pull of the previous collision's output).
+// Per-cell constants of the FP64 collision (CPU/Inamuro.cpp:134-250, the
+// reference's operand order throughout).
+struct Fp64Cell {
+    double mu, sum_fei, sum_rho, usq, chem;
+};
+
+__device__ __forceinline__ void fp64_cell(const Phys& P, const CellDeriv<double>& d, Fp64Cell& k)
+{
+    k.mu = (d.lrho - P.rho_G) * P.mu_slope + P.mu_G;
+    k.sum_fei = d.f_x * d.f_x + d.f_y * d.f_y + d.f_z * d.f_z;
+    k.sum_rho = d.r_x * d.r_x + d.r_y * d.r_y + d.r_z * d.r_z;
+    k.usq = d.uu * d.uu + d.vv * d.vv + d.ww * d.ww;
+    const double p0 = d.fei * P.T / (1.0 - P.b * d.fei) - P.a * d.fei * d.fei;
+    k.chem = p0 - P.k_f * d.fei * d.f_lap - P.k_f * k.sum_fei / 6.0;
+}
+
+// BGK relaxation x - (x - x_eq)/tau; kPow2: tau is a power of two, so the
+// division is the exact multiplication by 1/tau.  The choice is a kernel-wide
+// branch around the whole loop, so no division is evaluated when it is not used.
+template <bool kPow2>
+__device__ __forceinline__ double bgk(double x, double xeq, double tau, double inv_tau)
+{
+    const double d = x - xeq;
+    return x - (kPow2 ? d * inv_tau : d / tau);
+}
+
+// Post-collision f_q; fin: the pulled, bounced f_q.
+template <int q, bool kFirst, bool kPow2>
+__device__ __forceinline__ double fp64_f_post(const Phys& P, const CellDeriv<double>& d, const Fp64Cell& k,
+                                              double fin)
+{
+    constexpr double E = wE(q), F = wF(q);
+    const double un = dotq<q>(d.uu, d.vv, d.ww);
+    const double fe = dotq<q>(d.f_x, d.f_y, d.f_z);
+    double Gfei = 4.5 * (fe * fe);
+    if constexpr (csq(q) == 1) Gfei = Gfei - 1.5 * k.sum_fei;
+    if constexpr (csq(q) == 3) Gfei = Gfei - 1.5 * k.sum_fei * 3.0;
+    double fequ;
+    if constexpr (q == 0) {
+        fequ = d.fei + F * k.chem;
+    } else {
+        fequ = F * k.chem + 3.0 * E * d.fei * un + E * P.k_f * Gfei;
+    }
+    if constexpr (kFirst) return fequ;
+    else return bgk<kPow2>(fin, fequ, P.tauf, P.inv_tauf);
+}
+
+// Post-collision g_q with the viscous term.
+template <int q, bool kFirst, bool kPow2>
+__device__ __forceinline__ double fp64_g_post(const Phys& P, const CellDeriv<double>& d, const Fp64Cell& k,
+                                              double gin)
+{
+    constexpr double E = wE(q), F = wF(q);
+    const double un = dotq<q>(d.uu, d.vv, d.ww);
+    double gequ;
+    if constexpr (q == 0) {
+        // un = 0, grad terms vanish: E*(1 - 1.5 usq) - (2/3 F k_g / rho) sum_rho
+        const double velPart = 1.0 - 1.5 * k.usq;
+        gequ = E * velPart - 2.0 / 3.0 * F * P.k_g / d.lrho * k.sum_rho;
+    } else {
+        // c_a c_b (d_b u_a) summed in the reference's 9-term order
+        const double S = cc_contract<q>(d);
+        const double velPart = 1.0 + 3.0 * un - 1.5 * k.usq + 4.5 * un * un + P.visc * S;
+        const double re = dotq<q>(d.r_x, d.r_y, d.r_z);
+        double Grho = 4.5 * (re * re);
+        if constexpr (csq(q) == 1) Grho = Grho - 1.5 * k.sum_rho;
+        if constexpr (csq(q) == 3) Grho = Grho - 1.5 * k.sum_rho * 3.0;
+        gequ = E * velPart + E * P.k_g / d.lrho * Grho - 2.0 / 3.0 * F * P.k_g / d.lrho * k.sum_rho;
+    }
+    if constexpr (kFirst) return gequ;
+    double out = bgk<kPow2>(gin, gequ, P.taug, P.inv_taug);
+    if constexpr (q != 0) {
+        const double lapdot = dotq<q>(d.u_lap, d.v_lap, d.w_lap);
+        out = out + 3.0 * E / d.lrho * k.mu * lapdot;
+    }
+    return out;
+}
+
+// div = u_x + v_y + w_z into the source partial sums (sum, sum |.|, non-finite flag).
+__device__ __forceinline__ void fp64_div(const CellDeriv<double>& d, double (&red)[3])
+{
+    const double div = d.u_x + d.v_y + d.w_z;
+    if (isfinite(div)) {
+        red[0] += div;
+        red[1] += fabs(div);
+    } else {
+        red[2] = 1.0;
+    }
+}
+
+// Collision of f and g at cell c from their pulled, bounced populations
+// (unused when kFirst); I: the index type of c and of the q-major stride n.
+template <bool kFirst, bool kPowF, bool kPowG, class I>
+__device__ __forceinline__ void fp64_collide_store(const Phys& P, const CellDeriv<double>& d, const Fp64Cell& k,
+                                                   const double (&fv)[Q], const double (&gv)[Q],
+                                                   double* __restrict__ fout, double* __restrict__ gout,
+                                                   I n, I c)
+{
+    static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        double in = 0.0;
+        if constexpr (!kFirst) in = fv[q];
+        fout[I(q) * n + c] = fp64_f_post<q, kFirst, kPowF>(P, d, k, in);
+    });
+    static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        double in = 0.0;
+        if constexpr (!kFirst) in = gv[q];
+        gout[I(q) * n + c] = fp64_g_post<q, kFirst, kPowG>(P, d, k, in);
+    });
+}
+
+template <bool kFirst, class I>
+__device__ __forceinline__ void fp64_collide_dispatch(const Phys& P, const CellDeriv<double>& d,
+                                                      const Fp64Cell& k, const double (&fv)[Q],
+                                                      const double (&gv)[Q], double* __restrict__ fout,
+                                                      double* __restrict__ gout, I n, I c)
+{
+    if (P.tauf_pow2 && P.taug_pow2)
+        fp64_collide_store<kFirst, true, true>(P, d, k, fv, gv, fout, gout, n, c);
+    else if (P.tauf_pow2)
+        fp64_collide_store<kFirst, true, false>(P, d, k, fv, gv, fout, gout, n, c);
+    else if (P.taug_pow2)
+        fp64_collide_store<kFirst, false, true>(P, d, k, fv, gv, fout, gout, n, c);
+    else
+        fp64_collide_store<kFirst, false, false>(P, d, k, fv, gv, fout, gout, n, c);
+}
+
+// Fused collide (+ the pull of the previous collision's output), one CTA per
+// 2-D tile of one plane, stencil neighbours gathered from global memory.
 template <bool kFirst>
 __global__ void __launch_bounds__(256)
 collide_kernel(Geom g, Phys P, const double* __restrict__ fin, double* __restrict__ fout,
@@ -116,113 +248,92 @@ collide_kernel(Geom g, Phys P, const double* __restrict__ fin, double* __restric
     if (active) {
         const long long c = cell_of(g, x, y, z);
         const Mirror m(g, x, y, z);
-        double u_x, u_y, u_z, v_x, v_y, v_z, w_x, w_y, w_z;
-        double r_x, r_y, r_z, f_x, f_y, f_z;
-        double u_lap, v_lap, w_lap, f_lap, unused;
-        stencil<true>(u, g, m, x, y, z, c, u_x, u_y, u_z, u_lap);
-        stencil<true>(v, g, m, x, y, z, c, v_x, v_y, v_z, v_lap);
-        stencil<true>(w, g, m, x, y, z, c, w_x, w_y, w_z, w_lap);
-        stencil<false>(rho, g, m, x, y, z, c, r_x, r_y, r_z, unused);
-        stencil<true>(phi, g, m, x, y, z, c, f_x, f_y, f_z, f_lap);
+        CellDeriv<double> d;
+        double unused;
+        stencil<true>(u, g, m, x, y, z, c, d.u_x, d.u_y, d.u_z, d.u_lap);
+        stencil<true>(v, g, m, x, y, z, c, d.v_x, d.v_y, d.v_z, d.v_lap);
+        stencil<true>(w, g, m, x, y, z, c, d.w_x, d.w_y, d.w_z, d.w_lap);
+        stencil<false>(rho, g, m, x, y, z, c, d.r_x, d.r_y, d.r_z, unused);
+        stencil<true>(phi, g, m, x, y, z, c, d.f_x, d.f_y, d.f_z, d.f_lap);
         (void)unused;
-        dux[c] = u_x;
-        dvy[c] = v_y;
-        dwz[c] = w_z;
-        const double div = u_x + v_y + w_z;
-        if (isfinite(div)) {
-            red[0] = div;
-            red[1] = fabs(div);
-        } else {
-            red[2] = 1.0;
-        }
-
-        const double lrho = __ldg(rho + c), fei = __ldg(phi + c);
-        const double uu = __ldg(u + c), vv = __ldg(v + c), ww = __ldg(w + c);
-        const double mu = (lrho - P.rho_G) * P.mu_slope + P.mu_G;
-        const double sum_fei = f_x * f_x + f_y * f_y + f_z * f_z;
-        const double sum_rho = r_x * r_x + r_y * r_y + r_z * r_z;
-        const double usq = uu * uu + vv * vv + ww * ww;
-        const double p0 = fei * P.T / (1.0 - P.b * fei) - P.a * fei * fei;
-        const double chem = p0 - P.k_f * fei * f_lap - P.k_f * sum_fei / 6.0;
-
-        // ---- f: order parameter ----
-        double fv[Q];
+        dux[c] = d.u_x;
+        dvy[c] = d.v_y;
+        dwz[c] = d.w_z;
+        fp64_div(d, red);
+        d.lrho = __ldg(rho + c);
+        d.fei = __ldg(phi + c);
+        d.uu = __ldg(u + c);
+        d.vv = __ldg(v + c);
+        d.ww = __ldg(w + c);
+        Fp64Cell k;
+        fp64_cell(P, d, k);
+        double fv[Q], gv[Q];
         if constexpr (!kFirst) {
             pull_regs(fv, fin, g, x, y, z);
             bounce_regs(fv, g, x);
-        }
-        static_for<0, Q>([&](auto qc) {
-            constexpr int q = decltype(qc)::value;
-            constexpr double E = wE(q), F = wF(q);
-            const double un = dotq<q>(uu, vv, ww);
-            const double fe = dotq<q>(f_x, f_y, f_z);
-            double Gfei = 4.5 * (fe * fe);
-            if constexpr (csq(q) == 1) Gfei = Gfei - 1.5 * sum_fei;
-            if constexpr (csq(q) == 3) Gfei = Gfei - 1.5 * sum_fei * 3.0;
-            double fequ;
-            if constexpr (q == 0) {
-                fequ = fei + F * chem;
-            } else {
-                fequ = F * chem + 3.0 * E * fei * un + E * P.k_f * Gfei;
-            }
-            double out;
-            if constexpr (kFirst) {
-                out = fequ;
-            } else {
-                const double d = fv[q] - fequ;
-                out = fv[q] - (P.tauf_pow2 ? d * P.inv_tauf : d / P.tauf);
-            }
-            fout[(long long)q * g.n + c] = out;
-        });
-
-        // ---- g: predicted velocity ----
-        double gv[Q];
-        if constexpr (!kFirst) {
             pull_regs(gv, gin, g, x, y, z);
             bounce_regs(gv, g, x);
         }
-        static_for<0, Q>([&](auto qc) {
-            constexpr int q = decltype(qc)::value;
-            constexpr double E = wE(q), F = wF(q);
-            constexpr int X = cx(q), Y = cy(q), Z = cz(q);
-            const double un = dotq<q>(uu, vv, ww);
-            double gequ;
-            if constexpr (q == 0) {
-                // un = 0, grad terms vanish: E*(1 - 1.5 usq) - (2/3 F k_g / rho) sum_rho
-                const double velPart = 1.0 - 1.5 * usq;
-                gequ = E * velPart - 2.0 / 3.0 * F * P.k_g / lrho * sum_rho;
-            } else {
-                // c_a c_b (d_b u_a) summed in the reference's 9-term order
-                double S = 0.0;
-                bool started = false;
-                auto addt = [&](int coef, double val) {
-                    if (coef == 0) return;
-                    if (!started) { S = coef > 0 ? val : -val; started = true; }
-                    else S = coef > 0 ? S + val : S - val;
-                };
-                addt(X * X, u_x); addt(X * Y, u_y); addt(X * Z, u_z);
-                addt(Y * X, v_x); addt(Y * Y, v_y); addt(Y * Z, v_z);
-                addt(Z * X, w_x); addt(Z * Y, w_y); addt(Z * Z, w_z);
-                const double velPart = 1.0 + 3.0 * un - 1.5 * usq + 4.5 * un * un + P.visc * S;
-                const double re = dotq<q>(r_x, r_y, r_z);
-                double Grho = 4.5 * (re * re);
-                if constexpr (csq(q) == 1) Grho = Grho - 1.5 * sum_rho;
-                if constexpr (csq(q) == 3) Grho = Grho - 1.5 * sum_rho * 3.0;
-                gequ = E * velPart + E * P.k_g / lrho * Grho - 2.0 / 3.0 * F * P.k_g / lrho * sum_rho;
-            }
-            double out;
-            if constexpr (kFirst) {
-                out = gequ;
-            } else {
-                const double d = gv[q] - gequ;
-                out = gv[q] - (P.taug_pow2 ? d * P.inv_taug : d / P.taug);
-                if constexpr (q != 0) {
-                    const double lapdot = dotq<q>(u_lap, v_lap, w_lap);
-                    out = out + 3.0 * E / lrho * mu * lapdot;
-                }
-            }
-            gout[(long long)q * g.n + c] = out;
-        });
+        fp64_collide_dispatch<kFirst>(P, d, k, fv, gv, fout, gout, g.n, c);
+    }
+    block_sum_store<3>(red, part, nblocks, block_linear());
+}
+
+// z-marching collide (collide_zm.cuh): one CTA per 32 x 8 column and run of
+// zlen planes, the macro fields staged through the shared-memory ring, the
+// populations pulled into registers with 32-bit offsets.  Same per-cell
+// arithmetic as collide_kernel (bitwise); the source partial sums are
+// accumulated per thread over its planes.
+template <bool kFirst, int kMinBlocks>
+__global__ void __launch_bounds__(ZM_THREADS, kMinBlocks)
+collide_zm_kernel(Geom g, Phys P, int zlen, const double* __restrict__ fin, double* __restrict__ fout,
+                  const double* __restrict__ gin, double* __restrict__ gout,
+                  const double* __restrict__ phi, const double* __restrict__ rho,
+                  const double* __restrict__ u, const double* __restrict__ v,
+                  const double* __restrict__ w, double* __restrict__ dux,
+                  double* __restrict__ dvy, double* __restrict__ dwz, double* __restrict__ part,
+                  long long nblocks)
+{
+    extern __shared__ __align__(16) unsigned char zm_raw[];
+    const int tid = threadIdx.x;
+    const int tx = tid % ZM_TX, ty = tid / ZM_TX;
+    const int x0 = blockIdx.x * ZM_TX, y0 = blockIdx.y * ZM_TY;
+    const int x = x0 + tx, y = y0 + ty;
+    const int z0 = blockIdx.z * zlen;
+    const int z1 = min(z0 + zlen, g.lz);
+    const int n = static_cast<int>(g.n);
+    const int t = (ty + 1) * ZM_HX + tx + 1;
+    const MacroRing<double> ring(reinterpret_cast<double*>(zm_raw), g, x0, y0, phi, rho, u, v, w, tid);
+    ring.issue(z0 - 1);
+    ring.issue(z0);
+    ring.issue(z0 + 1);
+    double red[3] = {0.0, 0.0, 0.0};
+    for (int z = z0; z < z1; ++z) {
+        // Both population sets are requested before the plane barrier, so
+        // their latency overlaps the wait and the stencil arithmetic.
+        double fv[Q], gv[Q];
+        if constexpr (!kFirst) {
+            pull_regs32(fv, fin, n, g, x, y, z);
+            pull_regs32(gv, gin, n, g, x, y, z);
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        if (z + 2 <= z1) ring.issue(z + 2);
+        const unsigned c = static_cast<unsigned>((z * g.ly + y) * g.lx + x);
+        CellDeriv<double> d;
+        zm_derivs_g(ring, z, t, d);
+        zm_derivs_f(ring, z, t, d);
+        dux[c] = d.u_x;
+        dvy[c] = d.v_y;
+        dwz[c] = d.w_z;
+        fp64_div(d, red);
+        Fp64Cell k;
+        fp64_cell(P, d, k);
+        if constexpr (!kFirst) {
+            bounce_regs(fv, g, x);
+            bounce_regs(gv, g, x);
+        }
+        fp64_collide_dispatch<kFirst>(P, d, k, fv, gv, fout, gout, static_cast<unsigned>(n), c);
     }
     block_sum_store<3>(red, part, nblocks, block_linear());
 }
@@ -675,17 +786,43 @@ finalize_kernel(int kind, DevState* __restrict__ ds, const double* __restrict__ 
 
 namespace fp64 {
 
-void collide(cudaStream_t st, const Launch& L, const Geom& g, const Phys& P, bool first,
-             const double* fin, double* fout, const double* gin, double* gout,
-             const double* phi, const double* rho, const double* u, const double* v,
-             const double* w, double* dux, double* dvy, double* dwz, double* part)
+static int g_zm_minb = 2;
+
+int collide_zm_prepare(const Geom& g)
 {
+    if (!zm_fits(g)) return 0;
+    constexpr int smem = zm_ring_bytes<double>();
+    const void* kerns[] = {(const void*)collide_zm_kernel<true, 1>, (const void*)collide_zm_kernel<false, 1>,
+                           (const void*)collide_zm_kernel<true, 2>, (const void*)collide_zm_kernel<false, 2>};
+    for (const void* k : kerns)
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return 0;
+    const char* env = std::getenv("LBM_COLLIDE_MINB");
+    g_zm_minb = (env && std::atoi(env) == 1) ? 1 : 2;
+    return 1;
+}
+
+long long collide(cudaStream_t st, const Launch& L, const Geom& g, const Phys& P, bool first, int zlen,
+                  const double* fin, double* fout, const double* gin, double* gout,
+                  const double* phi, const double* rho, const double* u, const double* v,
+                  const double* w, double* dux, double* dvy, double* dwz, double* part)
+{
+    if (zlen > 0) {
+        const dim3 grid(g.lx / ZM_TX, g.ly / ZM_TY, (g.lz + zlen - 1) / zlen);
+        const long long nb = static_cast<long long>(grid.x) * grid.y * grid.z;
+        constexpr int smem = zm_ring_bytes<double>();
+        auto kern = g_zm_minb == 1 ? (first ? collide_zm_kernel<true, 1> : collide_zm_kernel<false, 1>)
+                                   : (first ? collide_zm_kernel<true, 2> : collide_zm_kernel<false, 2>);
+        kern<<<grid, ZM_THREADS, smem, st>>>(g, P, zlen, fin, fout, gin, gout, phi, rho, u, v, w, dux, dvy, dwz,
+                                             part, nb);
+        return nb;
+    }
     if (first)
         collide_kernel<true><<<L.grid, L.block, 0, st>>>(g, P, fin, fout, gin, gout, phi, rho, u, v,
                                                          w, dux, dvy, dwz, part, L.nblocks);
     else
         collide_kernel<false><<<L.grid, L.block, 0, st>>>(g, P, fin, fout, gin, gout, phi, rho, u, v,
                                                           w, dux, dvy, dwz, part, L.nblocks);
+    return L.nblocks;
 }
 
 void moments(cudaStream_t st, const Launch& L, const Geom& g, const Phys& P, const double* f,

@@ -19,6 +19,7 @@
 
 #include <cstdlib>
 
+#include "collide_zm.cuh"
 #include "lbm_mixed.cuh"
 
 namespace lbm {
@@ -85,6 +86,88 @@ struct MixPhys {
     float fei_G, p0_G;          // gas rest state of f
 };
 
+// Per-cell constants of the mixed collision (CPU/Inamuro.cpp:134-250 in
+// deviation form: f_rest and E_q cancel in f - (f - f_eq)/tau).
+struct MixCell {
+    float inv_rho, mu, sum_fei, sum_rho, usq, chem_dev, dphi, kg_rho;
+};
+
+// The constants the g collision uses.
+__device__ __forceinline__ void mix_cell_g(const MixPhys& P, const CellDeriv<float>& d, MixCell& k)
+{
+    k.inv_rho = 1.f / d.lrho;
+    k.mu = (d.lrho - P.rho_G) * P.mu_slope + P.mu_G;
+    k.sum_rho = d.r_x * d.r_x + d.r_y * d.r_y + d.r_z * d.r_z;
+    k.usq = d.uu * d.uu + d.vv * d.vv + d.ww * d.ww;
+    k.kg_rho = P.k_g * k.inv_rho;
+}
+
+// The constants the f collision uses.
+__device__ __forceinline__ void mix_cell_f(const MixPhys& P, const CellDeriv<float>& d, MixCell& k)
+{
+    k.sum_fei = d.f_x * d.f_x + d.f_y * d.f_y + d.f_z * d.f_z;
+    const float p0 = d.fei * P.T / (1.f - P.b * d.fei) - P.a * d.fei * d.fei;
+    k.chem_dev = (p0 - P.p0_G) - P.k_f * d.fei * d.f_lap - P.k_f * k.sum_fei * (1.f / 6.f);
+    k.dphi = d.fei - P.fei_G;
+}
+
+// Post-collision f_q (deviation from f_rest,q); fin: the pulled, bounced f_q.
+template <int q, bool kFirst>
+__device__ __forceinline__ float mix_f_post(const MixPhys& P, const CellDeriv<float>& d, const MixCell& k,
+                                            float fin)
+{
+    constexpr float E = float(wE(q)), F = float(wF(q));
+    const float un = dotq<q>(d.uu, d.vv, d.ww);
+    const float fe = dotq<q>(d.f_x, d.f_y, d.f_z);
+    float feq;
+    if constexpr (q == 0) {
+        feq = k.dphi + F * k.chem_dev;
+    } else {
+        const float Gfei = 4.5f * fe * fe - 1.5f * float(csq(q)) * k.sum_fei;
+        feq = F * k.chem_dev + 3.f * E * d.fei * un + E * P.k_f * Gfei;
+    }
+    if constexpr (kFirst) return feq;
+    else return fin - (fin - feq) * P.inv_tauf;
+}
+
+// Post-collision g_q (deviation from E_q) with the viscous term.
+template <int q, bool kFirst>
+__device__ __forceinline__ float mix_g_post(const MixPhys& P, const CellDeriv<float>& d, const MixCell& k,
+                                            float gin)
+{
+    constexpr float E = float(wE(q)), F = float(wF(q));
+    const float un = dotq<q>(d.uu, d.vv, d.ww);
+    float geq;
+    if constexpr (q == 0) {
+        geq = -1.5f * E * k.usq - (2.f / 3.f) * F * k.kg_rho * k.sum_rho;
+    } else {
+        const float S = cc_contract<q>(d);
+        const float re = dotq<q>(d.r_x, d.r_y, d.r_z);
+        const float Grho = 4.5f * re * re - 1.5f * float(csq(q)) * k.sum_rho;
+        geq = E * (3.f * un - 1.5f * k.usq + 4.5f * un * un + P.visc * S) + E * k.kg_rho * Grho -
+              (2.f / 3.f) * F * k.kg_rho * k.sum_rho;
+    }
+    if constexpr (kFirst) return geq;
+    float out = gin - (gin - geq) * P.inv_taug;
+    if constexpr (q != 0) out += 3.f * E * k.inv_rho * k.mu * dotq<q>(d.u_lap, d.v_lap, d.w_lap);
+    return out;
+}
+
+// div = u_x + v_y + w_z into the source partial sums (sum, sum |.|, non-finite flag).
+__device__ __forceinline__ float mix_div(const CellDeriv<float>& d, double (&red)[3])
+{
+    const float div = d.u_x + d.v_y + d.w_z;
+    if (isfinite(div)) {
+        red[0] += div;
+        red[1] += fabs((double)div);
+    } else {
+        red[2] = 1.0;
+    }
+    return div;
+}
+
+// Plane-per-CTA collide for boxes the z-marching frame does not tile: stencil
+// neighbours gathered from global memory, 64-bit indices.
 template <bool kFirst>
 __global__ void __launch_bounds__(256)
 collide_kernel(Geom g, MixPhys P, const float* __restrict__ fin, float* __restrict__ fout,
@@ -100,34 +183,23 @@ collide_kernel(Geom g, MixPhys P, const float* __restrict__ fin, float* __restri
     if (active) {
         const long long c = cell_of(g, x, y, z);
         const Mirror m(g, x, y, z);
-        float u_x, u_y, u_z, v_x, v_y, v_z, w_x, w_y, w_z, r_x, r_y, r_z, f_x, f_y, f_z;
-        float u_lap, v_lap, w_lap, f_lap, unused;
-        stencil<true>(u, g, m, x, y, z, c, u_x, u_y, u_z, u_lap);
-        stencil<true>(v, g, m, x, y, z, c, v_x, v_y, v_z, v_lap);
-        stencil<true>(w, g, m, x, y, z, c, w_x, w_y, w_z, w_lap);
-        stencil<false>(rho, g, m, x, y, z, c, r_x, r_y, r_z, unused);
-        stencil<true>(phi, g, m, x, y, z, c, f_x, f_y, f_z, f_lap);
+        CellDeriv<float> d;
+        float unused;
+        stencil<true>(u, g, m, x, y, z, c, d.u_x, d.u_y, d.u_z, d.u_lap);
+        stencil<true>(v, g, m, x, y, z, c, d.v_x, d.v_y, d.v_z, d.v_lap);
+        stencil<true>(w, g, m, x, y, z, c, d.w_x, d.w_y, d.w_z, d.w_lap);
+        stencil<false>(rho, g, m, x, y, z, c, d.r_x, d.r_y, d.r_z, unused);
+        stencil<true>(phi, g, m, x, y, z, c, d.f_x, d.f_y, d.f_z, d.f_lap);
         (void)unused;
-        const float div = u_x + v_y + w_z;
-        div_out[c] = div;
-        if (isfinite(div)) {
-            red[0] = div;
-            red[1] = fabs((double)div);
-        } else {
-            red[2] = 1.0;
-        }
-        const float lrho = __ldg(rho + c), fei = __ldg(phi + c);
-        const float uu = __ldg(u + c), vv = __ldg(v + c), ww = __ldg(w + c);
-        const float inv_rho = 1.f / lrho;
-        const float mu = (lrho - P.rho_G) * P.mu_slope + P.mu_G;
-        const float sum_fei = f_x * f_x + f_y * f_y + f_z * f_z;
-        const float sum_rho = r_x * r_x + r_y * r_y + r_z * r_z;
-        const float usq = uu * uu + vv * vv + ww * ww;
-        const float p0 = fei * P.T / (1.f - P.b * fei) - P.a * fei * fei;
-        const float chem_dev = (p0 - P.p0_G) - P.k_f * fei * f_lap - P.k_f * sum_fei * (1.f / 6.f);
-        const float dphi = fei - P.fei_G;
-        const float kg_rho = P.k_g * inv_rho;
-
+        d.lrho = __ldg(rho + c);
+        d.fei = __ldg(phi + c);
+        d.uu = __ldg(u + c);
+        d.vv = __ldg(v + c);
+        d.ww = __ldg(w + c);
+        div_out[c] = mix_div(d, red);
+        MixCell k;
+        mix_cell_g(P, d, k);
+        mix_cell_f(P, d, k);
         float fv[Q];
         if constexpr (!kFirst) {
             pull_regs(fv, fin, g, x, y, z);
@@ -135,20 +207,10 @@ collide_kernel(Geom g, MixPhys P, const float* __restrict__ fin, float* __restri
         }
         static_for<0, Q>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
-            constexpr float E = float(wE(q)), F = float(wF(q));
-            const float un = dotq<q>(uu, vv, ww);
-            const float fe = dotq<q>(f_x, f_y, f_z);
-            float feq;   // f_eq - f_rest
-            if constexpr (q == 0) {
-                feq = dphi + F * chem_dev;
-            } else {
-                const float Gfei = 4.5f * fe * fe - 1.5f * float(csq(q)) * sum_fei;
-                feq = F * chem_dev + 3.f * E * fei * un + E * P.k_f * Gfei;
-            }
-            if constexpr (kFirst) fout[(long long)q * g.n + c] = feq;
-            else fout[(long long)q * g.n + c] = fv[q] - (fv[q] - feq) * P.inv_tauf;
+            float in = 0.f;
+            if constexpr (!kFirst) in = fv[q];
+            fout[(long long)q * g.n + c] = mix_f_post<q, kFirst>(P, d, k, in);
         });
-
         float gv[Q];
         if constexpr (!kFirst) {
             pull_regs(gv, gin, g, x, y, z);
@@ -156,29 +218,74 @@ collide_kernel(Geom g, MixPhys P, const float* __restrict__ fin, float* __restri
         }
         static_for<0, Q>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
-            constexpr float E = float(wE(q)), F = float(wF(q));
-            constexpr int X = cx(q), Y = cy(q), Z = cz(q);
-            const float un = dotq<q>(uu, vv, ww);
-            float geq;   // g_eq - E_q
-            if constexpr (q == 0) {
-                geq = -1.5f * E * usq - (2.f / 3.f) * F * kg_rho * sum_rho;
-            } else {
-                const float S = float(X * X) * u_x + float(X * Y) * u_y + float(X * Z) * u_z +
-                                float(Y * X) * v_x + float(Y * Y) * v_y + float(Y * Z) * v_z +
-                                float(Z * X) * w_x + float(Z * Y) * w_y + float(Z * Z) * w_z;
-                const float re = dotq<q>(r_x, r_y, r_z);
-                const float Grho = 4.5f * re * re - 1.5f * float(csq(q)) * sum_rho;
-                geq = E * (3.f * un - 1.5f * usq + 4.5f * un * un + P.visc * S) + E * kg_rho * Grho -
-                      (2.f / 3.f) * F * kg_rho * sum_rho;
-            }
-            float out;
-            if constexpr (kFirst) {
-                out = geq;
-            } else {
-                out = gv[q] - (gv[q] - geq) * P.inv_taug;
-                if constexpr (q != 0) out += 3.f * E * inv_rho * mu * dotq<q>(u_lap, v_lap, w_lap);
-            }
-            gout[(long long)q * g.n + c] = out;
+            float in = 0.f;
+            if constexpr (!kFirst) in = gv[q];
+            gout[(long long)q * g.n + c] = mix_g_post<q, kFirst>(P, d, k, in);
+        });
+    }
+    block_sum_store<3>(red, part, nblocks, block_linear());
+}
+
+// z-marching collide (collide_zm.cuh): one CTA per 32 x 8 column and run of
+// zlen planes, macro fields staged through the shared-memory ring, 32-bit
+// population offsets.  Same per-cell arithmetic as collide_kernel; the
+// source partial sums are accumulated per thread over its planes.
+template <bool kFirst>
+__global__ void __launch_bounds__(ZM_THREADS, 2)
+collide_zm_kernel(Geom g, MixPhys P, int zlen, const float* __restrict__ fin, float* __restrict__ fout,
+                  const float* __restrict__ gin, float* __restrict__ gout,
+                  const float* __restrict__ phi, const float* __restrict__ rho,
+                  const float* __restrict__ u, const float* __restrict__ v,
+                  const float* __restrict__ w, float* __restrict__ div_out,
+                  double* __restrict__ part, long long nblocks)
+{
+    extern __shared__ __align__(16) unsigned char zm_raw[];
+    const int tid = threadIdx.x;
+    const int tx = tid % ZM_TX, ty = tid / ZM_TX;
+    const int x0 = blockIdx.x * ZM_TX, y0 = blockIdx.y * ZM_TY;
+    const int x = x0 + tx, y = y0 + ty;
+    const int z0 = blockIdx.z * zlen;
+    const int z1 = min(z0 + zlen, g.lz);
+    const int n = static_cast<int>(g.n);
+    const int t = (ty + 1) * ZM_HX + tx + 1;
+    const MacroRing<float> ring(reinterpret_cast<float*>(zm_raw), g, x0, y0, phi, rho, u, v, w, tid);
+    ring.issue(z0 - 1);
+    ring.issue(z0);
+    ring.issue(z0 + 1);
+    double red[3] = {0.0, 0.0, 0.0};
+    for (int z = z0; z < z1; ++z) {
+        // Both population sets are requested before the plane barrier, so
+        // their latency overlaps the wait and the stencil arithmetic.
+        float gv[Q], fv[Q];
+        if constexpr (!kFirst) {
+            pull_regs32(gv, gin, n, g, x, y, z);
+            pull_regs32(fv, fin, n, g, x, y, z);
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        if (z + 2 <= z1) ring.issue(z + 2);
+        const unsigned c = static_cast<unsigned>((z * g.ly + y) * g.lx + x);
+        CellDeriv<float> d;
+        MixCell k;
+        // g first: the phi stencil is only live for the f half.
+        zm_derivs_g(ring, z, t, d);
+        div_out[c] = mix_div(d, red);
+        mix_cell_g(P, d, k);
+        if constexpr (!kFirst) bounce_regs(gv, g, x);
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            float in = 0.f;
+            if constexpr (!kFirst) in = gv[q];
+            gout[q * static_cast<unsigned>(n) + c] = mix_g_post<q, kFirst>(P, d, k, in);
+        });
+        zm_derivs_f(ring, z, t, d);
+        mix_cell_f(P, d, k);
+        if constexpr (!kFirst) bounce_regs(fv, g, x);
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            float in = 0.f;
+            if constexpr (!kFirst) in = fv[q];
+            fout[q * static_cast<unsigned>(n) + c] = mix_f_post<q, kFirst>(P, d, k, in);
         });
     }
     block_sum_store<3>(red, part, nblocks, block_linear());
@@ -601,6 +708,10 @@ lbm_status mixed_alloc(MixedBuffers& mb, const Geom& g, const Launch& L)
     if (zlen > 0 && g.lx % S2_TX == 0 && g.ly % S2_TY == 0 && g.lz >= 3 && 15 * g.n < 0x7fffffffLL &&
         cudaFuncSetAttribute(sweep2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, S2_SMEM) == cudaSuccess)
         mb.fuse_zlen = zlen;
+    // z-marching collide where its tile divides the box.
+    const char* cenv = std::getenv("LBM_COLLIDE_ZLEN");
+    const int czlen = cenv ? std::atoi(cenv) : 16;
+    mb.collide_zlen = (czlen > 0 && zm_fits(g)) ? czlen : 0;
     mb.allocated = true;
     return LBM_OK;
 }
@@ -676,20 +787,29 @@ lbm_status mixed_prologue(cudaStream_t st, MixedBuffers& mb, const Launch& L, co
     const int fin = fcur, fout = 1 - fcur;
     float* div = mb.dux;      // div = u_x + v_y + w_z
     float* omega = mb.dvy;    // 1 / tau_h
-    if (first)
+    long long src_blocks = L.nblocks;
+    if (mb.collide_zlen > 0) {
+        const dim3 grid(g.lx / ZM_TX, g.ly / ZM_TY, (g.lz + mb.collide_zlen - 1) / mb.collide_zlen);
+        src_blocks = static_cast<long long>(grid.x) * grid.y * grid.z;
+        constexpr int smem = zm_ring_bytes<float>();
+        auto kern = first ? collide_zm_kernel<true> : collide_zm_kernel<false>;
+        kern<<<grid, ZM_THREADS, smem, st>>>(g, M, mb.collide_zlen, mb.f[fin], mb.f[fout], mb.g[fin], mb.g[fout],
+                                             mb.phi, mb.rho, mb.u, mb.v, mb.w, div, mb.part_src, src_blocks);
+    } else if (first) {
         collide_kernel<true><<<L.grid, L.block, 0, st>>>(g, M, mb.f[fin], mb.f[fout], mb.g[fin], mb.g[fout],
                                                          mb.phi, mb.rho, mb.u, mb.v, mb.w, div,
                                                          mb.part_src, L.nblocks);
-    else
+    } else {
         collide_kernel<false><<<L.grid, L.block, 0, st>>>(g, M, mb.f[fin], mb.f[fout], mb.g[fin], mb.g[fout],
                                                           mb.phi, mb.rho, mb.u, mb.v, mb.w, div,
                                                           mb.part_src, L.nblocks);
+    }
     if (ev) cudaEventRecord(ev[1], st);
     moments_kernel<<<L.grid, L.block, 0, st>>>(g, P.fei_G, P.fei_L, P.rho_G, P.rho_L, P.fei_avg, P.dfei,
                                                P.half_drho, mb.f[fout], mb.g[fout], mb.phi, mb.rho, mb.u,
                                                mb.v, mb.w, mb.part_mass, L.nblocks);
     if (ev) cudaEventRecord(ev[2], st);
-    finalize(st, FIN_SOURCE, ds, mb.part_src, L.nblocks, nullptr, 0, nullptr, 0);
+    finalize(st, FIN_SOURCE, ds, mb.part_src, src_blocks, nullptr, 0, nullptr, 0);
     finalize(st, FIN_MASS, ds, mb.part_mass, L.nblocks, nullptr, 0, nullptr, 0);
     prep_kernel<<<L.grid, L.block, 0, st>>>(g, ds, div, mb.rho, mb.p, mb.s, omega, mb.part_prep, L.nblocks);
     finalize(st, FIN_PREP, ds, mb.part_prep, L.nblocks, nullptr, 0, nullptr, 0);

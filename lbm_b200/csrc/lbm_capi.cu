@@ -74,6 +74,7 @@ struct lbm_handle {
     lbm_check_callback check_cb = nullptr;
     void* check_user = nullptr;
     int fuse_zlen = 0;                   // FP64: >0 runs plain sweeps two per launch
+    int collide_zlen = 0;                // FP64: >0 runs the z-marching collide
     double* stats_part = nullptr;        // field-statistics partials
     lbm_field_stats* stats_dev = nullptr;
 };
@@ -339,25 +340,26 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
         const lbm_status s = ensure_dual_buffer(h);
         if (s != LBM_OK) return s;
     }
-    if (h->timing) LBM_CUDA(h, cudaEventRecord(h->ev[0], st));
     // Reset per-solve flags, keep config.
     DevState& dh = *h->ds_host;
     std::memset(&dh, 0, sizeof(DevState));
     upload_state_config(h);
     LBM_CUDA(h, cudaMemcpyAsync(h->ds, h->ds_host, sizeof(DevState), cudaMemcpyHostToDevice, st));
+    if (h->timing) LBM_CUDA(h, cudaEventRecord(h->ev[0], st));
 
     int hcur = 0;
     if (h->precision == LBM_PRECISION_FP64) {
         Fp64Buffers& b = h->b;
         const int fin = h->fcur, fout = 1 - h->fcur;
-        fp64::collide(st, L, g, h->phys, h->first_step, b.f[fin], b.f[fout], b.g[fin], b.g[fout],
-                      b.phi, b.rho, b.u, b.v, b.w, b.dux, b.dvy, b.dwz, b.part_src);
+        const long long src_blocks =
+            fp64::collide(st, L, g, h->phys, h->first_step, h->collide_zlen, b.f[fin], b.f[fout], b.g[fin],
+                          b.g[fout], b.phi, b.rho, b.u, b.v, b.w, b.dux, b.dvy, b.dwz, b.part_src);
         h->fcur = fout;
         if (h->timing) LBM_CUDA(h, cudaEventRecord(h->ev[1], st));
         fp64::moments(st, L, g, h->phys, b.f[fout], b.g[fout], b.phi, b.rho, b.u, b.v, b.w,
                       b.part_mass);
         if (h->timing) LBM_CUDA(h, cudaEventRecord(h->ev[2], st));
-        finalize(st, FIN_SOURCE, h->ds, b.part_src, L.nblocks, nullptr, 0, nullptr, 0);
+        finalize(st, FIN_SOURCE, h->ds, b.part_src, src_blocks, nullptr, 0, nullptr, 0);
         finalize(st, FIN_MASS, h->ds, b.part_mass, L.nblocks, nullptr, 0, nullptr, 0);
         fp64::prep(st, L, g, h->ds, b.dux, b.dvy, b.dwz, b.p, b.s, b.part_prep);
         finalize(st, FIN_PREP, h->ds, b.part_prep, L.nblocks, nullptr, 0, nullptr, 0);
@@ -614,6 +616,11 @@ lbm_status lbm_create(const lbm_params* prm, lbm_precision precision, int device
         const char* env = std::getenv("LBM_SWEEP2_ZLEN");
         const int zlen = env ? std::atoi(env) : 0;
         h->fuse_zlen = (zlen > 0 && fp64::sweep2_prepare(h->geom)) ? zlen : 0;
+        // z-marching collide where its tile divides the box (LBM_COLLIDE_ZLEN,
+        // 0 disables).
+        const char* cenv = std::getenv("LBM_COLLIDE_ZLEN");
+        const int czlen = cenv ? std::atoi(cenv) : 16;
+        h->collide_zlen = (czlen > 0 && fp64::collide_zm_prepare(h->geom)) ? czlen : 0;
     }
     default_ghosts(h);
     // Background state until the caller loads fields.

@@ -185,7 +185,7 @@ __device__ __forceinline__ void pull_regs32(T (&v)[Q], const T* __restrict__ src
         constexpr int q = decltype(qc)::value;
         const int idx = (pick<-cz(q)>(w.zm, z, w.zp) * g.ly + pick<-cy(q)>(w.ym, y, w.yp)) * g.lx +
                         pick<-cx(q)>(w.xm, x, w.xp);
-        v[q] = __ldg(src + (q * n + idx));
+        v[q] = __ldg(src + static_cast<unsigned>(q * n + idx));
     });
 }
 

@@ -92,10 +92,14 @@ struct Fp64Buffers {
 
 // Kernel launchers (kernels_fp64.cu).
 namespace fp64 {
-void collide(cudaStream_t st, const Launch& L, const Geom& g, const Phys& P, bool first,
-             const double* fin, double* fout, const double* gin, double* gout,
-             const double* phi, const double* rho, const double* u, const double* v,
-             const double* w, double* dux, double* dvy, double* dwz, double* part);
+// Collide: the z-marching form when zlen > 0 (collide_zm_prepare returned 1
+// for the box), else one CTA per plane tile.  Returns the number of source
+// partial-sum blocks written to part.
+int collide_zm_prepare(const Geom& g);
+long long collide(cudaStream_t st, const Launch& L, const Geom& g, const Phys& P, bool first, int zlen,
+                  const double* fin, double* fout, const double* gin, double* gout,
+                  const double* phi, const double* rho, const double* u, const double* v,
+                  const double* w, double* dux, double* dvy, double* dwz, double* part);
 void moments(cudaStream_t st, const Launch& L, const Geom& g, const Phys& P,
              const double* f, const double* gpop, double* phi, double* rho, double* u,
              double* v, double* w, double* part_mass);

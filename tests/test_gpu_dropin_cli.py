@@ -101,4 +101,4 @@ def test_reference_main_production_flags(tmp_path):
     assert rows[-1]["converged"] == "1" and float(rows[-1]["fixed_point_relative"]) < 1e-3
     r = subprocess.run([DROPIN, "--mode", "gpu", "--params", str(pf), "--steps", "1", "--poisson", "onepass"],
                        cwd=tmp_path, capture_output=True, text=True, timeout=120)
-    assert r.returncode == 1 and "not part of this build" in (r.stdout + r.stderr)
+    assert r.returncode == 1 and "not provided by liblbm_b200" in (r.stdout + r.stderr)
