@@ -91,6 +91,10 @@ public:
         prm.fei_max = P.fei_max;
         prm.fei_min = P.fei_min;
         prm.DD = P.DD;
+        if (lbm_abi_version() != LBM_B200_ABI_VERSION)
+            throw std::runtime_error("InamuroCUDA: liblbm_b200 ABI " + std::to_string(lbm_abi_version()) +
+                                     " does not match the header's ABI " +
+                                     std::to_string(LBM_B200_ABI_VERSION) + "; rebuild against the library");
         check(lbm_create(&prm, precision, 0, &h_), "InamuroCUDA: device set-up");
         // initFromCPU (.cu:1628-1673): the ghosted macro fields of the CPU object.
         std::vector<double> buf[6];

@@ -28,7 +28,9 @@
 extern "C" {
 #endif
 
-#define LBM_B200_ABI_VERSION 1
+/* Bumped whenever a struct layout or a signature of this header changes;
+   callers compare it with lbm_abi_version() of the loaded library. */
+#define LBM_B200_ABI_VERSION 2
 
 typedef enum {
     LBM_OK = 0,

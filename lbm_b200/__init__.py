@@ -101,6 +101,8 @@ class LBMError(RuntimeError):
 
 
 _lib = None
+# LBM_B200_ABI_VERSION of include/lbm_b200.h that the structures above mirror.
+ABI_VERSION = 2
 
 
 def load_library(path: str = LIB_PATH):
@@ -142,6 +144,9 @@ def load_library(path: str = LIB_PATH):
     L.lbm_status_string.argtypes = [C.c_int]
     L.lbm_status_string.restype = C.c_char_p
     L.lbm_abi_version.restype = C.c_int
+    if L.lbm_abi_version() != ABI_VERSION:
+        raise LBMError(7, f"{path} has ABI {L.lbm_abi_version()}, these bindings expect {ABI_VERSION}; "
+                          "rebuild with lbm_b200.build.build()")
     _lib = L
     return L
 
