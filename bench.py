@@ -411,6 +411,42 @@ def run_ours(args):
     return 0
 
 
+# Algorithmic bytes per cell of the non-Poisson kernels: collide (K4), moments
+# (K1) and correction (C), FP64 and mixed.
+PHASE_BYTES = {"collide_ms": {"fp64": 528.0, "mixed": 264.0},
+               "moments_ms": {"fp64": 280.0, "mixed": 140.0},
+               "correct_ms": {"fp64": 64.0, "mixed": 36.0}}
+
+
+def run_phase_timing(args):
+    """Per-kernel device times of the step's non-Poisson kernels with a fixed
+    number of sweeps per step (replay), one JSON line per precision: the
+    measurement behind the collide/moments/correction roofline fractions."""
+    import lbm_b200 as L
+    p = workload_params(args.size)
+    f = workload_fields(p)
+    cells = args.size ** 3
+    peak, kind = measured_peaks()
+    for prec in (["fp64", "mixed"] if args.precision == "both" else [args.precision]):
+        s = L.InamuroCUDA(p, f, precision=prec)
+        s.step_replay([args.phase_sweeps] * max(args.warmup, 1))
+        s.reset_timing()
+        s.step_replay([args.phase_sweeps] * args.steps)
+        t = s.timing()
+        n = t["steps"]
+        out = {"mode": "phase-timing", "precision": prec, "box": [args.size] * 3,
+               "sweeps_per_step": args.phase_sweeps, "steps": n, "peak_gbs": peak, "peak_kind": kind}
+        for k, b in PHASE_BYTES.items():
+            ms = t[k] / n
+            out[k] = ms
+            out[k.replace("_ms", "_frac")] = b[prec] * cells / (ms / 1e3) / 1e9 / peak
+        out["prep_ms"] = t["prep_ms"] / n
+        out["sweep_ms"] = t["poisson_ms"] / max(t["sweep_kernels"], 1)
+        print(json.dumps(out), flush=True)
+        s.close()
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -428,9 +464,14 @@ def main(argv=None):
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--sample-sweeps", type=int, default=1)
     ap.add_argument("--sweeps-per-step", type=float, default=DEFAULT_SWEEPS_PER_STEP)
+    ap.add_argument("--phase-timing", action="store_true",
+                    help="time the non-Poisson kernels per step with --phase-sweeps sweeps per step")
+    ap.add_argument("--phase-sweeps", type=int, default=100)
     args = ap.parse_args(argv)
     if args.warmup < 0 or args.steps < 1:
         ap.error("steps >= 1, warmup >= 0")
+    if args.phase_timing:
+        return run_phase_timing(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_ours(args)

@@ -42,6 +42,18 @@
 namespace lbm {
 namespace {
 
+// Tile of a check kernel: planes [blockIdx.z * zrun, +zrun) of one 2-D tile,
+// so the CTA's block reduction and its loads of the device-side scalars are
+// amortised over zrun planes.
+__device__ __forceinline__ bool tile_zrun(const Geom& g, int zrun, int& x, int& y, int& z0, int& z1)
+{
+    x = blockIdx.x * blockDim.x + threadIdx.x;
+    y = blockIdx.y * blockDim.y + threadIdx.y;
+    z0 = blockIdx.z * zrun;
+    z1 = min(z0 + zrun, g.lz);
+    return x < g.lx && y < g.ly;
+}
+
 __device__ __forceinline__ bool tile_coords(const Geom& g, int& x, int& y, int& z)
 {
     x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -557,13 +569,13 @@ sweep2_kernel(Geom g, int zlen, const double* __restrict__ hin, double* __restri
 }
 
 __global__ void __launch_bounds__(256)
-sweep_check_a_kernel(Geom g, const double* __restrict__ hin, double* __restrict__ hout,
+sweep_check_a_kernel(Geom g, int zrun, const double* __restrict__ hin, double* __restrict__ hout,
                      double* __restrict__ p_chk, double* __restrict__ part, long long nblocks)
 {
-    int x, y, z;
-    const bool active = tile_coords(g, x, y, z);
+    int x, y, z0, z1;
+    const bool active = tile_zrun(g, zrun, x, y, z0, z1);
     double red[1] = {0.0};
-    if (active) {
+    for (int z = z0; active && z < z1; ++z) {
         const long long c = cell_of(g, x, y, z);
         double hv[Q];
         pull_regs(hv, hin, g, x, y, z);
@@ -574,31 +586,32 @@ sweep_check_a_kernel(Geom g, const double* __restrict__ hin, double* __restrict_
             hout[(long long)q * g.n + c] = hv[q];
         });
         p_chk[c] = pv;
-        red[0] = pv;
+        red[0] += pv;
     }
     block_sum_store<1>(red, part, nblocks, block_linear());
 }
 
 template <bool kDual>
 __global__ void __launch_bounds__(256)
-sweep_check_b_kernel(Geom g, double* __restrict__ h, double* __restrict__ hc,
+sweep_check_b_kernel(Geom g, int zrun, const double* __restrict__ hin, double* __restrict__ hout,
+                     double* __restrict__ hc,
                      const double* __restrict__ p_chk, double* __restrict__ p_prev,
                      double* __restrict__ p, const double* __restrict__ rho,
                      const double* __restrict__ s, const DevState* __restrict__ ds,
                      double* __restrict__ part, long long nblocks)
 {
-    int x, y, z;
-    const bool active = tile_coords(g, x, y, z);
+    int x, y, z0, z1;
+    const bool active = tile_zrun(g, zrun, x, y, z0, z1);
     double red[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    if (active) {
+    const double shift = ds->sigma;
+    const double tgt = ds->target;
+    for (int z = z0; active && z < z1; ++z) {
         const long long c = cell_of(g, x, y, z);
-        const double shift = ds->sigma;
-        const double tgt = ds->target;
         double hv[Q];
         // Gauge (CPU/Inamuro.cpp:699-705): p -= shift, h_q -= E_q shift.
         static_for<0, Q>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
-            hv[q] = h[(long long)q * g.n + c] - wE(q) * shift;
+            hv[q] = __ldg(hin + (long long)q * g.n + c) - wE(q) * shift;
         });
         const double pv = p_chk[c] - shift;
         if constexpr (kDual) {
@@ -607,33 +620,33 @@ sweep_check_b_kernel(Geom g, double* __restrict__ h, double* __restrict__ hc,
                 hc[(long long)q * g.n + c] = hv[q];
             });
             const double hsum = sum_q(hv);
-            red[2] = fabs(pv - hsum);
-            red[3] = fabs(pv - tgt);
-            red[4] = fabs(hsum - tgt);
+            red[2] += fabs(pv - hsum);
+            red[3] += fabs(pv - tgt);
+            red[4] += fabs(hsum - tgt);
         }
         // Relative change (CPU/Inamuro.cpp:726-753).
-        red[0] = fabs(pv - p_prev[c]);
-        red[1] = fabs(pv);
+        red[0] += fabs(pv - p_prev[c]);
+        red[1] += fabs(pv);
         p_prev[c] = pv;
         p[c] = pv;
         const double tauh = 1.0 / __ldg(rho + c) + 0.5;
-        collide_h_store(hv, pv, tauh, __ldg(s + c), h, g.n, c);
+        collide_h_store(hv, pv, tauh, __ldg(s + c), hout, g.n, c);
     }
     block_sum_store<5>(red, part, nblocks, block_linear());
 }
 
 __global__ void __launch_bounds__(256)
-sweep_check_c_kernel(Geom g, const double* __restrict__ hin, double* __restrict__ hout,
+sweep_check_c_kernel(Geom g, int zrun, const double* __restrict__ hin, double* __restrict__ hout,
                      const double* __restrict__ hc, const double* __restrict__ rho,
                      const double* __restrict__ s, const DevState* __restrict__ ds,
                      double* __restrict__ part, long long nblocks)
 {
-    int x, y, z;
-    const bool active = tile_coords(g, x, y, z);
+    int x, y, z0, z1;
+    const bool active = tile_zrun(g, zrun, x, y, z0, z1);
     double red[3] = {0.0, 0.0, 0.0};
-    if (active) {
+    const double tgt = ds->target;
+    for (int z = z0; active && z < z1; ++z) {
         const long long c = cell_of(g, x, y, z);
-        const double tgt = ds->target;
         double hv[Q];
         pull_regs(hv, hin, g, x, y, z);
         bounce_regs(hv, g, x);
@@ -873,27 +886,27 @@ void sweep2(cudaStream_t st, const Geom& g, int zlen, const double* hin, double*
 void sweep_check_a(cudaStream_t st, const Launch& L, const Geom& g, const double* hin,
                    double* hout, double* p_chk, double* part)
 {
-    sweep_check_a_kernel<<<L.grid, L.block, 0, st>>>(g, hin, hout, p_chk, part, L.nblocks);
+    sweep_check_a_kernel<<<L.cgrid, L.block, 0, st>>>(g, L.zrun, hin, hout, p_chk, part, L.cnblocks);
 }
 
-void sweep_check_b(cudaStream_t st, const Launch& L, const Geom& g, bool dual, double* h,
+void sweep_check_b(cudaStream_t st, const Launch& L, const Geom& g, bool dual, const double* hin, double* hout,
                    double* hc, const double* p_chk, double* p_prev, double* p, const double* rho,
                    const double* s, const DevState* ds, double* part)
 {
     if (dual)
-        sweep_check_b_kernel<true><<<L.grid, L.block, 0, st>>>(g, h, hc, p_chk, p_prev, p, rho, s,
-                                                               ds, part, L.nblocks);
+        sweep_check_b_kernel<true><<<L.cgrid, L.block, 0, st>>>(g, L.zrun, hin, hout, hc, p_chk, p_prev, p, rho,
+                                                                s, ds, part, L.cnblocks);
     else
-        sweep_check_b_kernel<false><<<L.grid, L.block, 0, st>>>(g, h, hc, p_chk, p_prev, p, rho, s,
-                                                                ds, part, L.nblocks);
+        sweep_check_b_kernel<false><<<L.cgrid, L.block, 0, st>>>(g, L.zrun, hin, hout, hc, p_chk, p_prev, p, rho,
+                                                                 s, ds, part, L.cnblocks);
 }
 
 void sweep_check_c(cudaStream_t st, const Launch& L, const Geom& g, const double* hin,
                    double* hout, const double* hc, const double* rho, const double* s,
                    const DevState* ds, double* part)
 {
-    sweep_check_c_kernel<<<L.grid, L.block, 0, st>>>(g, hin, hout, hc, rho, s, ds, part,
-                                                     L.nblocks);
+    sweep_check_c_kernel<<<L.cgrid, L.block, 0, st>>>(g, L.zrun, hin, hout, hc, rho, s, ds, part,
+                                                      L.cnblocks);
 }
 
 void correct(cudaStream_t st, const Launch& L, const Geom& g, double* u, double* v, double* w,

@@ -25,6 +25,18 @@
 namespace lbm {
 namespace {
 
+// Tile of a check kernel: planes [blockIdx.z * zrun, +zrun) of one 2-D tile,
+// so the CTA's block reduction and its loads of the device-side scalars are
+// amortised over zrun planes.
+__device__ __forceinline__ bool tile_zrun(const Geom& g, int zrun, int& x, int& y, int& z0, int& z1)
+{
+    x = blockIdx.x * blockDim.x + threadIdx.x;
+    y = blockIdx.y * blockDim.y + threadIdx.y;
+    z0 = blockIdx.z * zrun;
+    z1 = min(z0 + zrun, g.lz);
+    return x < g.lx && y < g.ly;
+}
+
 __device__ __forceinline__ bool tile_coords(const Geom& g, int& x, int& y, int& z)
 {
     x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -530,13 +542,13 @@ sweep2_kernel(Geom g, int zlen, const float* __restrict__ hin, float* __restrict
 }
 
 __global__ void __launch_bounds__(256)
-sweep_check_a_kernel(Geom g, const float* __restrict__ hin, float* __restrict__ hout,
+sweep_check_a_kernel(Geom g, int zrun, const float* __restrict__ hin, float* __restrict__ hout,
                      double* __restrict__ p_chk, double* __restrict__ part, long long nblocks)
 {
-    int x, y, z;
-    const bool active = tile_coords(g, x, y, z);
+    int x, y, z0, z1;
+    const bool active = tile_zrun(g, zrun, x, y, z0, z1);
     double red[1] = {0.0};
-    if (active) {
+    for (int z = z0; active && z < z1; ++z) {
         const long long c = cell_of(g, x, y, z);
         float hv[Q];
         pull_regs(hv, hin, g, x, y, z);
@@ -547,30 +559,31 @@ sweep_check_a_kernel(Geom g, const float* __restrict__ hin, float* __restrict__ 
             hout[(long long)q * g.n + c] = hv[q];
         });
         p_chk[c] = pv;
-        red[0] = pv;
+        red[0] += pv;
     }
     block_sum_store<1>(red, part, nblocks, block_linear());
 }
 
 template <bool kDual>
 __global__ void __launch_bounds__(256)
-sweep_check_b_kernel(Geom g, float* __restrict__ h, float* __restrict__ hc,
+sweep_check_b_kernel(Geom g, int zrun, const float* __restrict__ hin, float* __restrict__ hout,
+                     float* __restrict__ hc,
                      const double* __restrict__ p_chk, double* __restrict__ p_prev,
                      double* __restrict__ p, const float* __restrict__ omega,
                      const float* __restrict__ s, const DevState* __restrict__ ds,
                      double* __restrict__ part, long long nblocks)
 {
-    int x, y, z;
-    const bool active = tile_coords(g, x, y, z);
+    int x, y, z0, z1;
+    const bool active = tile_zrun(g, zrun, x, y, z0, z1);
     double red[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    if (active) {
+    const double shift = ds->sigma;
+    const double tgt = ds->target;
+    for (int z = z0; active && z < z1; ++z) {
         const long long c = cell_of(g, x, y, z);
-        const double shift = ds->sigma;
-        const double tgt = ds->target;
         float hv[Q];
         static_for<0, Q>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
-            hv[q] = (float)((double)h[(long long)q * g.n + c] - wE(q) * shift);
+            hv[q] = (float)((double)__ldg(hin + (long long)q * g.n + c) - wE(q) * shift);
         });
         const double pv = p_chk[c] - shift;
         if constexpr (kDual) {
@@ -579,31 +592,31 @@ sweep_check_b_kernel(Geom g, float* __restrict__ h, float* __restrict__ hc,
                 hc[(long long)q * g.n + c] = hv[q];
             });
             const double hsum = sum_q(hv);
-            red[2] = fabs(pv - hsum);
-            red[3] = fabs(pv - tgt);
-            red[4] = fabs(hsum - tgt);
+            red[2] += fabs(pv - hsum);
+            red[3] += fabs(pv - tgt);
+            red[4] += fabs(hsum - tgt);
         }
-        red[0] = fabs(pv - p_prev[c]);
-        red[1] = fabs(pv);
+        red[0] += fabs(pv - p_prev[c]);
+        red[1] += fabs(pv);
         p_prev[c] = pv;
         p[c] = pv;
-        collide_h_store(hv, pv, __ldg(omega + c), __ldg(s + c), h, g.n, c);
+        collide_h_store(hv, pv, __ldg(omega + c), __ldg(s + c), hout, g.n, c);
     }
     block_sum_store<5>(red, part, nblocks, block_linear());
 }
 
 __global__ void __launch_bounds__(256)
-sweep_check_c_kernel(Geom g, const float* __restrict__ hin, float* __restrict__ hout,
+sweep_check_c_kernel(Geom g, int zrun, const float* __restrict__ hin, float* __restrict__ hout,
                      const float* __restrict__ hc, const float* __restrict__ omega,
                      const float* __restrict__ s, const DevState* __restrict__ ds,
                      double* __restrict__ part, long long nblocks)
 {
-    int x, y, z;
-    const bool active = tile_coords(g, x, y, z);
+    int x, y, z0, z1;
+    const bool active = tile_zrun(g, zrun, x, y, z0, z1);
     double red[3] = {0.0, 0.0, 0.0};
-    if (active) {
+    const double tgt = ds->target;
+    for (int z = z0; active && z < z1; ++z) {
         const long long c = cell_of(g, x, y, z);
-        const double tgt = ds->target;
         float hv[Q];
         pull_regs(hv, hin, g, x, y, z);
         bounce_regs(hv, g, x);
@@ -839,21 +852,25 @@ int mixed_segment(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom
             sweep_kernel64<<<L.grid, L.block, 0, st>>>(g, mb.h[cur], mb.h[1 - cur], omega, mb.s);
         cur = 1 - cur;
     }
-    sweep_check_a_kernel<<<L.grid, L.block, 0, st>>>(g, mb.h[cur], mb.h[1 - cur], mb.p_chk, mb.part_a, L.nblocks);
+    sweep_check_a_kernel<<<L.cgrid, L.block, 0, st>>>(g, L.zrun, mb.h[cur], mb.h[1 - cur], mb.p_chk, mb.part_a,
+                                                      L.cnblocks);
     cur = 1 - cur;
-    finalize(st, FIN_SIGMA, ds, mb.part_a, L.nblocks, nullptr, 0, nullptr, 0);
+    finalize(st, FIN_SIGMA, ds, mb.part_a, L.cnblocks, nullptr, 0, nullptr, 0);
     if (dual)
-        sweep_check_b_kernel<true><<<L.grid, L.block, 0, st>>>(g, mb.h[cur], mb.hc, mb.p_chk, mb.p_prev, mb.p,
-                                                               omega, mb.s, ds, mb.part_b, L.nblocks);
+        sweep_check_b_kernel<true><<<L.cgrid, L.block, 0, st>>>(g, L.zrun, mb.h[cur], mb.h[1 - cur], mb.hc,
+                                                                mb.p_chk, mb.p_prev, mb.p, omega, mb.s, ds,
+                                                                mb.part_b, L.cnblocks);
     else
-        sweep_check_b_kernel<false><<<L.grid, L.block, 0, st>>>(g, mb.h[cur], mb.hc, mb.p_chk, mb.p_prev, mb.p,
-                                                                omega, mb.s, ds, mb.part_b, L.nblocks);
+        sweep_check_b_kernel<false><<<L.cgrid, L.block, 0, st>>>(g, L.zrun, mb.h[cur], mb.h[1 - cur], mb.hc,
+                                                                 mb.p_chk, mb.p_prev, mb.p, omega, mb.s, ds,
+                                                                 mb.part_b, L.cnblocks);
+    cur = 1 - cur;
     if (dual) {
-        sweep_check_c_kernel<<<L.grid, L.block, 0, st>>>(g, mb.h[cur], mb.h[1 - cur], mb.hc, omega, mb.s, ds,
-                                                         mb.part_c, L.nblocks);
+        sweep_check_c_kernel<<<L.cgrid, L.block, 0, st>>>(g, L.zrun, mb.h[cur], mb.h[1 - cur], mb.hc, omega, mb.s,
+                                                          ds, mb.part_c, L.cnblocks);
         cur = 1 - cur;
     }
-    finalize(st, FIN_CHECK, ds, mb.part_b, L.nblocks, mb.part_c, L.nblocks, nullptr, 0);
+    finalize(st, FIN_CHECK, ds, mb.part_b, L.cnblocks, mb.part_c, L.cnblocks, nullptr, 0);
     return cur;
 }
 

@@ -246,14 +246,15 @@ lbm_status build_segment(lbm_handle* h, const SegKey& key, cudaGraphExec_t* out,
         }
         fp64::sweep_check_a(st, L, g, b.h[cur], b.h[1 - cur], b.p_chk, b.part_a);
         cur = 1 - cur;
-        finalize(st, FIN_SIGMA, h->ds, b.part_a, L.nblocks, nullptr, 0, nullptr, 0);
-        fp64::sweep_check_b(st, L, g, key.dual != 0, b.h[cur], b.hc, b.p_chk, b.p_prev, b.p, b.rho,
-                            b.s, h->ds, b.part_b);
+        finalize(st, FIN_SIGMA, h->ds, b.part_a, L.cnblocks, nullptr, 0, nullptr, 0);
+        fp64::sweep_check_b(st, L, g, key.dual != 0, b.h[cur], b.h[1 - cur], b.hc, b.p_chk, b.p_prev, b.p,
+                            b.rho, b.s, h->ds, b.part_b);
+        cur = 1 - cur;
         if (key.dual) {
             fp64::sweep_check_c(st, L, g, b.h[cur], b.h[1 - cur], b.hc, b.rho, b.s, h->ds, b.part_c);
             cur = 1 - cur;
         }
-        finalize(st, FIN_CHECK, h->ds, b.part_b, L.nblocks, b.part_c, L.nblocks, nullptr, 0);
+        finalize(st, FIN_CHECK, h->ds, b.part_b, L.cnblocks, b.part_c, L.cnblocks, nullptr, 0);
     } else {
         cur = mixed_segment(st, h->mb, L, g, key.start_parity, key.n_normal, key.dual != 0, h->ds);
     }

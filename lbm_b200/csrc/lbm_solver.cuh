@@ -64,9 +64,16 @@ enum ErrorSite {
 
 // Launch shape: 2-D tiles of (bx, by) cells in an xy plane, one grid z-slice
 // per lattice plane.
+// The Poisson check kernels (A, B, C) use the same tiles but let one CTA
+// cover runs of `zrun` planes (cgrid, cnblocks partial sums).
+constexpr int kCheckZrun = 8;
+
 struct Launch {
     dim3 grid, block;
     long long nblocks;
+    dim3 cgrid;
+    long long cnblocks;
+    int zrun;
 };
 
 inline Launch make_launch(int lx, int ly, int lz, int bx, int by)
@@ -75,6 +82,9 @@ inline Launch make_launch(int lx, int ly, int lz, int bx, int by)
     L.block = dim3(bx, by, 1);
     L.grid = dim3((lx + bx - 1) / bx, (ly + by - 1) / by, lz);
     L.nblocks = (long long)L.grid.x * L.grid.y * L.grid.z;
+    L.zrun = kCheckZrun;
+    L.cgrid = dim3(L.grid.x, L.grid.y, (lz + kCheckZrun - 1) / kCheckZrun);
+    L.cnblocks = (long long)L.cgrid.x * L.cgrid.y * L.cgrid.z;
     return L;
 }
 
@@ -118,7 +128,7 @@ void sweep2(cudaStream_t st, const Geom& g, int zlen, const double* hin, double*
             const double* rho, const double* s);
 void sweep_check_a(cudaStream_t st, const Launch& L, const Geom& g, const double* hin,
                    double* hout, double* p_chk, double* part);
-void sweep_check_b(cudaStream_t st, const Launch& L, const Geom& g, bool dual, double* h,
+void sweep_check_b(cudaStream_t st, const Launch& L, const Geom& g, bool dual, const double* hin, double* hout,
                    double* hc, const double* p_chk, double* p_prev, double* p,
                    const double* rho, const double* s, const DevState* ds, double* part);
 void sweep_check_c(cudaStream_t st, const Launch& L, const Geom& g, const double* hin,
