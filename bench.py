@@ -49,6 +49,11 @@ SWEEP_BYTES = {"fp64": 272.0, "mixed": 144.0}
 # What the sweep kernels actually have to move per cell (p is not stored per
 # sweep): FP64 15x8 read + 15x8 write + rho, s; mixed 15x4 + 15x4 + omega, s.
 COMPULSORY_BYTES = {"fp64": 256.0, "mixed": 128.0}
+# Algorithmic bytes per cell of the non-Poisson kernels: collide (K4), moments
+# (K1) and correction (C), FP64 and mixed.
+PHASE_BYTES = {"collide_ms": {"fp64": 528.0, "mixed": 264.0},
+               "moments_ms": {"fp64": 280.0, "mixed": 140.0},
+               "correct_ms": {"fp64": 64.0, "mixed": 36.0}}
 # Mean sweeps per step of this workload (measured on B200 with this bench);
 # the CPU sample is extrapolated to it when no GPU run preceded it.
 DEFAULT_SWEEPS_PER_STEP = 1000.0
@@ -332,6 +337,14 @@ def run_leg(args, precision, world, rank, local, p, f, e2e: bool):
                        "note": "frac uses the per-sweep byte model (one DRAM pass per sweep); "
                                "two-sweep passes beat it, frac_compulsory is against what the "
                                "launches actually have to move"}
+    # the collide+stream kernel (K4: stencils, f and g collision, pull
+    # stream), one launch per step, from the same timed steps
+    col_ms = tm["collide_ms"] / max(tm["steps"], 1)
+    col_bytes = PHASE_BYTES["collide_ms"][precision]
+    leg["roofline_collide"] = {"bound": "hbm", "kernel": f"collide ({precision})",
+                               "achieved": col_bytes * cells / (col_ms / 1e3) / 1e9, "peak": peak,
+                               "unit": "GB/s", "frac": col_bytes * cells / (col_ms / 1e3) / 1e9 / peak,
+                               "bytes_per_cell": col_bytes, "avg_launch_ms": col_ms}
     if e2e:
         # end to end through the public API with host buffers: upload the
         # initial fields from pinned host memory, run K steps, download all six
@@ -361,6 +374,37 @@ def run_leg(args, precision, world, rank, local, p, f, e2e: bool):
                               "each step, host wall clock"}
     g.close()
     return leg
+
+
+def accuracy_probe(n, steps, sweeps):
+    """Mixed against FP64 on the bench workload, outside the timed region: both
+    precisions advance `steps` steps from the same initial fields with the same
+    replayed sweep count per step (so the comparison is not blurred by where
+    each run's 1e-3 exit falls), then the norm-wise relative error
+    max|mixed - fp64| / max|fp64| per field.  The FP64 path matches the FP64
+    oracle to ~1e-15, so these are the errors against the oracle.  Mass drift:
+    max over steps k of |M_k - M_1| / |M_1|, M_k = sum(phi) after step k (the
+    step's FP64 device reduction), for each precision."""
+    import lbm_b200 as L
+    p = workload_params(n)
+    f = workload_fields(p)
+    out = {"box": [n, n, n], "steps": steps, "sweeps_per_step": sweeps}
+    fields, drift = {}, {}
+    for prec in ("fp64", "mixed"):
+        s = L.InamuroCUDA(p, f, precision=prec)
+        d, m1 = 0.0, None
+        for _ in range(steps):
+            st = s.step_replay([sweeps])[0]
+            m1 = st["mass"] if m1 is None else m1
+            d = max(d, abs(st["mass"] - m1) / abs(m1))
+        fields[prec] = s.download_fields()
+        drift[prec] = d
+        s.close()
+    out["rel_err_mixed_vs_fp64"] = {
+        k: float(np.max(np.abs(fields["mixed"][k] - fields["fp64"][k])) /
+                 max(float(np.max(np.abs(fields["fp64"][k]))), 1e-300)) for k in L.FIELDS}
+    out["mass_drift"] = drift
+    return out
 
 
 def run_ours(args):
@@ -404,18 +448,16 @@ def run_ours(args):
             line["mixed"]["stated_error"] = ("<= 1e-5 norm-wise relative error in phi, rho, u, v, w vs the "
                                              "FP64 oracle on equal sweep counts (tests/test_gpu_mixed.py)")
             line["speedup_mixed_vs_fp64"] = m["value"] / head["value"]
+            if world == 1 and not args.no_accuracy:
+                try:
+                    line["mixed"]["accuracy"] = accuracy_probe(n, 3, 1000)
+                except Exception as e:
+                    line["mixed"]["accuracy"] = {"unavailable": str(e)[:200]}
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0
-
-
-# Algorithmic bytes per cell of the non-Poisson kernels: collide (K4), moments
-# (K1) and correction (C), FP64 and mixed.
-PHASE_BYTES = {"collide_ms": {"fp64": 528.0, "mixed": 264.0},
-               "moments_ms": {"fp64": 280.0, "mixed": 140.0},
-               "correct_ms": {"fp64": 64.0, "mixed": 36.0}}
 
 
 def run_phase_timing(args):
@@ -462,6 +504,8 @@ def main(argv=None):
                     help="per-step sweep cap (a multiple of 100); reported if reached")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the mixed-vs-FP64 error and mass-drift probe")
     ap.add_argument("--sample-sweeps", type=int, default=1)
     ap.add_argument("--sweeps-per-step", type=float, default=DEFAULT_SWEEPS_PER_STEP)
     ap.add_argument("--phase-timing", action="store_true",
