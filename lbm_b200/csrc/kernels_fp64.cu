@@ -37,6 +37,7 @@
 #include <math_constants.h>
 
 #include "collide_zm.cuh"
+#include "finalize.cuh"
 #include "lbm_solver.cuh"
 
 namespace lbm {
@@ -681,118 +682,11 @@ correct_kernel(Geom g, double* __restrict__ u, double* __restrict__ v, double* _
     w[c] -= (p[cell_of(g, x, y, m.zp)] - p[cell_of(g, x, y, m.zm)]) * inv_2rho;
 }
 
-// ---- finalisation --------------------------------------------------------
-
-__device__ __forceinline__ double relative(double num, double den)
-{
-    if (den > 0.0) return num / den;
-    return num == 0.0 ? 0.0 : CUDART_INF;
-}
-
-// Sums `terms` columns of a [terms][nblocks] partials array in a fixed order:
-// thread t adds blocks t, t+1024, ... sequentially, then a fixed tree.
-template <int T>
-__device__ void reduce_partials(const double* __restrict__ part, long long nblocks, double (&out)[T])
-{
-    __shared__ double sm[1024];
-    for (int t = 0; t < T; ++t) {
-        double acc = 0.0;
-        for (long long i = threadIdx.x; i < nblocks; i += blockDim.x) acc += part[t * nblocks + i];
-        sm[threadIdx.x] = acc;
-        __syncthreads();
-        for (int stride = blockDim.x / 2; stride > 0; stride >>= 1) {
-            if (threadIdx.x < stride) sm[threadIdx.x] += sm[threadIdx.x + stride];
-            __syncthreads();
-        }
-        out[t] = sm[0];
-        __syncthreads();
-    }
-}
-
-__device__ __forceinline__ void set_error(DevState* ds, int site)
-{
-    if (ds->error == 0) {
-        ds->error = 2;  // LBM_ERR_NONFINITE
-        ds->error_site = site;
-    }
-}
-
 __global__ void __launch_bounds__(1024)
 finalize_kernel(int kind, DevState* __restrict__ ds, const double* __restrict__ part,
-                long long nblocks, const double* __restrict__ part2, long long nblocks2,
-                const double* __restrict__ part3, long long nblocks3)
+                long long nblocks, const double* __restrict__ part2, long long nblocks2)
 {
-    const double n = ds->n_cells;
-    if (kind == FIN_SOURCE) {
-        double r[3];
-        reduce_partials<3>(part, nblocks, r);
-        if (threadIdx.x == 0) {
-            ds->div_sum = r[0];
-            ds->div_abs_sum = r[1];
-            ds->div_mean = r[0] / n;
-            if (r[2] != 0.0 || !isfinite(r[0]) || !isfinite(r[1])) set_error(ds, SITE_SOURCE);
-        }
-    } else if (kind == FIN_PREP) {
-        double r[3];
-        reduce_partials<3>(part, nblocks, r);
-        if (threadIdx.x == 0) {
-            ds->proj_sum = r[0];
-            if (r[1] != 0.0 || !isfinite(r[0])) set_error(ds, SITE_PROJECTED);
-            ds->target = r[2] / n;
-            if (!isfinite(r[2])) set_error(ds, SITE_GAUGE_TARGET);
-            ds->max_shift = 0.0;
-            ds->iterations = 0;
-            ds->converged = 0;
-        }
-    } else if (kind == FIN_SIGMA) {
-        double r[1];
-        reduce_partials<1>(part, nblocks, r);
-        if (threadIdx.x == 0) {
-            const double shift = r[0] / n - ds->target;
-            if (!isfinite(shift)) set_error(ds, SITE_GAUGE_SHIFT);
-            ds->sigma = shift;
-            if (fabs(shift) > ds->max_shift) ds->max_shift = fabs(shift);
-        }
-    } else if (kind == FIN_CHECK) {
-        double rb[5];
-        reduce_partials<5>(part, nblocks, rb);
-        double rc[3] = {0.0, 0.0, 0.0};
-        if (ds->dual) reduce_partials<3>(part2, nblocks2, rc);
-        if (threadIdx.x == 0) {
-            bool fp_ok = true;
-            if (ds->dual) {
-                const double t[6] = {rc[0], rc[1], rc[2], rb[2], rb[3], rb[4]};
-                for (int i = 0; i < 6; ++i) {
-                    ds->fp_terms[i] = t[i];
-                    if (!isfinite(t[i])) set_error(ds, SITE_FIXED_POINT);
-                }
-                ds->fp_h_scale = fmax(t[1], t[2]);
-                ds->fp_h_rel = relative(t[0], ds->fp_h_scale);
-                ds->fp_p_scale = fmax(t[4], t[5]);
-                ds->fp_p_rel = relative(t[3], ds->fp_p_scale);
-                ds->fp_rel = fmax(ds->fp_h_rel, ds->fp_p_rel);
-                if (!isfinite(ds->fp_rel)) set_error(ds, SITE_FIXED_POINT);
-                ds->fp_evaluated = 1;
-                ds->fp_converged = ds->fp_rel < ds->tolerance;
-                // dual == 2 is the shadow mode: reported, not part of the exit
-                fp_ok = (ds->dual == 1) ? ds->fp_converged : true;
-            }
-            ds->l1_delta = rb[0];
-            ds->l1_norm = rb[1];
-            if (!isfinite(rb[0]) || !isfinite(rb[1])) set_error(ds, SITE_RESIDUAL);
-            ds->rel = relative(rb[0], rb[1]);
-            if (!isfinite(ds->rel)) set_error(ds, SITE_RESIDUAL);
-            ds->pressure_converged = ds->rel < ds->tolerance;
-            ds->converged = ds->pressure_converged && fp_ok;
-            ds->iterations += (unsigned long long)ds->check_interval;
-        }
-    } else if (kind == FIN_MASS) {
-        double r[1];
-        reduce_partials<1>(part, nblocks, r);
-        if (threadIdx.x == 0) ds->mass = r[0];
-    }
-    (void)part3;
-    (void)nblocks3;
+    finalize_body(kind, ds, part, nblocks, nblocks, part2, nblocks2, nblocks2);
 }
 
 }  // namespace
@@ -920,8 +814,9 @@ void correct(cudaStream_t st, const Launch& L, const Geom& g, double* u, double*
 void finalize(cudaStream_t st, FinKind kind, DevState* ds, const double* part, long long nblocks,
               const double* part2, long long nblocks2, const double* part3, long long nblocks3)
 {
-    finalize_kernel<<<1, 1024, 0, st>>>(static_cast<int>(kind), ds, part, nblocks, part2, nblocks2,
-                                        part3, nblocks3);
+    finalize_kernel<<<1, 1024, 0, st>>>(static_cast<int>(kind), ds, part, nblocks, part2, nblocks2);
+    (void)part3;
+    (void)nblocks3;
 }
 
 }  // namespace lbm

@@ -21,6 +21,7 @@
 
 #include "collide_zm.cuh"
 #include "lbm_mixed.cuh"
+#include "mixed_cells.cuh"
 
 namespace lbm {
 namespace {
@@ -45,139 +46,6 @@ __device__ __forceinline__ bool tile_coords(const Geom& g, int& x, int& y, int& 
     return x < g.lx && y < g.ly;
 }
 
-template <class T>
-__device__ __forceinline__ void bounce_regs(T (&v)[Q], const Geom& g, int x)
-{
-    if (g.periodic_x) return;
-    if (x == 0) {
-        static_for<0, Q>([&](auto qc) {
-            constexpr int q = decltype(qc)::value;
-            if constexpr (bounce_left(q) != q) v[q] = v[bounce_left(q)];
-        });
-    }
-    if (x == g.lx - 1) {
-        static_for<0, Q>([&](auto qc) {
-            constexpr int q = decltype(qc)::value;
-            if constexpr (bounce_right(q) != q) v[q] = v[bounce_right(q)];
-        });
-    }
-}
-
-__device__ __forceinline__ void pull_regs(float (&v)[Q], const float* __restrict__ src, const Geom& g,
-                                          int x, int y, int z)
-{
-    const Wrap w(g, x, y, z);
-    static_for<0, Q>([&](auto qc) {
-        constexpr int q = decltype(qc)::value;
-        v[q] = __ldg(src + (long long)q * g.n + pull_src<q>(g, w, x, y, z));
-    });
-}
-
-template <bool kLap>
-__device__ __forceinline__ void stencil(const float* __restrict__ f, const Geom& g, const Mirror& m,
-                                        int x, int y, int z, long long c,
-                                        float& gx, float& gy, float& gz, float& lap)
-{
-    float ax = 0.f, ay = 0.f, az = 0.f, al = 0.f;
-    static_for<1, Q>([&](auto kc) {
-        constexpr int k = decltype(kc)::value;
-        const float val = __ldg(f + stencil_nb<k>(g, m, x, y, z));
-        ax = acc_signed<cx(k)>(ax, val);
-        ay = acc_signed<cy(k)>(ay, val);
-        az = acc_signed<cz(k)>(az, val);
-        if constexpr (kLap) al += val;
-    });
-    gx = ax * 0.1f;
-    gy = ay * 0.1f;
-    gz = az * 0.1f;
-    if constexpr (kLap) lap = (al - 14.f * __ldg(f + c)) * 0.2f;
-}
-
-struct MixPhys {
-    float rho_G, mu_G, mu_slope, inv_tauf, inv_taug, k_f, k_g, T, a, b, visc;
-    float fei_G, p0_G;          // gas rest state of f
-};
-
-// Per-cell constants of the mixed collision (CPU/Inamuro.cpp:134-250 in
-// deviation form: f_rest and E_q cancel in f - (f - f_eq)/tau).
-struct MixCell {
-    float inv_rho, mu, sum_fei, sum_rho, usq, chem_dev, dphi, kg_rho;
-};
-
-// The constants the g collision uses.
-__device__ __forceinline__ void mix_cell_g(const MixPhys& P, const CellDeriv<float>& d, MixCell& k)
-{
-    k.inv_rho = 1.f / d.lrho;
-    k.mu = (d.lrho - P.rho_G) * P.mu_slope + P.mu_G;
-    k.sum_rho = d.r_x * d.r_x + d.r_y * d.r_y + d.r_z * d.r_z;
-    k.usq = d.uu * d.uu + d.vv * d.vv + d.ww * d.ww;
-    k.kg_rho = P.k_g * k.inv_rho;
-}
-
-// The constants the f collision uses.
-__device__ __forceinline__ void mix_cell_f(const MixPhys& P, const CellDeriv<float>& d, MixCell& k)
-{
-    k.sum_fei = d.f_x * d.f_x + d.f_y * d.f_y + d.f_z * d.f_z;
-    const float p0 = d.fei * P.T / (1.f - P.b * d.fei) - P.a * d.fei * d.fei;
-    k.chem_dev = (p0 - P.p0_G) - P.k_f * d.fei * d.f_lap - P.k_f * k.sum_fei * (1.f / 6.f);
-    k.dphi = d.fei - P.fei_G;
-}
-
-// Post-collision f_q (deviation from f_rest,q); fin: the pulled, bounced f_q.
-template <int q, bool kFirst>
-__device__ __forceinline__ float mix_f_post(const MixPhys& P, const CellDeriv<float>& d, const MixCell& k,
-                                            float fin)
-{
-    constexpr float E = float(wE(q)), F = float(wF(q));
-    const float un = dotq<q>(d.uu, d.vv, d.ww);
-    const float fe = dotq<q>(d.f_x, d.f_y, d.f_z);
-    float feq;
-    if constexpr (q == 0) {
-        feq = k.dphi + F * k.chem_dev;
-    } else {
-        const float Gfei = 4.5f * fe * fe - 1.5f * float(csq(q)) * k.sum_fei;
-        feq = F * k.chem_dev + 3.f * E * d.fei * un + E * P.k_f * Gfei;
-    }
-    if constexpr (kFirst) return feq;
-    else return fin - (fin - feq) * P.inv_tauf;
-}
-
-// Post-collision g_q (deviation from E_q) with the viscous term.
-template <int q, bool kFirst>
-__device__ __forceinline__ float mix_g_post(const MixPhys& P, const CellDeriv<float>& d, const MixCell& k,
-                                            float gin)
-{
-    constexpr float E = float(wE(q)), F = float(wF(q));
-    const float un = dotq<q>(d.uu, d.vv, d.ww);
-    float geq;
-    if constexpr (q == 0) {
-        geq = -1.5f * E * k.usq - (2.f / 3.f) * F * k.kg_rho * k.sum_rho;
-    } else {
-        const float S = cc_contract<q>(d);
-        const float re = dotq<q>(d.r_x, d.r_y, d.r_z);
-        const float Grho = 4.5f * re * re - 1.5f * float(csq(q)) * k.sum_rho;
-        geq = E * (3.f * un - 1.5f * k.usq + 4.5f * un * un + P.visc * S) + E * k.kg_rho * Grho -
-              (2.f / 3.f) * F * k.kg_rho * k.sum_rho;
-    }
-    if constexpr (kFirst) return geq;
-    float out = gin - (gin - geq) * P.inv_taug;
-    if constexpr (q != 0) out += 3.f * E * k.inv_rho * k.mu * dotq<q>(d.u_lap, d.v_lap, d.w_lap);
-    return out;
-}
-
-// div = u_x + v_y + w_z into the source partial sums (sum, sum |.|, non-finite flag).
-__device__ __forceinline__ float mix_div(const CellDeriv<float>& d, double (&red)[3])
-{
-    const float div = d.u_x + d.v_y + d.w_z;
-    if (isfinite(div)) {
-        red[0] += div;
-        red[1] += fabs((double)div);
-    } else {
-        red[2] = 1.0;
-    }
-    return div;
-}
-
 // Plane-per-CTA collide for boxes the z-marching frame does not tile: stencil
 // neighbours gathered from global memory, 64-bit indices.
 template <bool kFirst>
@@ -190,51 +58,8 @@ collide_kernel(Geom g, MixPhys P, const float* __restrict__ fin, float* __restri
                double* __restrict__ part, long long nblocks)
 {
     int x, y, z;
-    const bool active = tile_coords(g, x, y, z);
     double red[3] = {0.0, 0.0, 0.0};
-    if (active) {
-        const long long c = cell_of(g, x, y, z);
-        const Mirror m(g, x, y, z);
-        CellDeriv<float> d;
-        float unused;
-        stencil<true>(u, g, m, x, y, z, c, d.u_x, d.u_y, d.u_z, d.u_lap);
-        stencil<true>(v, g, m, x, y, z, c, d.v_x, d.v_y, d.v_z, d.v_lap);
-        stencil<true>(w, g, m, x, y, z, c, d.w_x, d.w_y, d.w_z, d.w_lap);
-        stencil<false>(rho, g, m, x, y, z, c, d.r_x, d.r_y, d.r_z, unused);
-        stencil<true>(phi, g, m, x, y, z, c, d.f_x, d.f_y, d.f_z, d.f_lap);
-        (void)unused;
-        d.lrho = __ldg(rho + c);
-        d.fei = __ldg(phi + c);
-        d.uu = __ldg(u + c);
-        d.vv = __ldg(v + c);
-        d.ww = __ldg(w + c);
-        div_out[c] = mix_div(d, red);
-        MixCell k;
-        mix_cell_g(P, d, k);
-        mix_cell_f(P, d, k);
-        float fv[Q];
-        if constexpr (!kFirst) {
-            pull_regs(fv, fin, g, x, y, z);
-            bounce_regs(fv, g, x);
-        }
-        static_for<0, Q>([&](auto qc) {
-            constexpr int q = decltype(qc)::value;
-            float in = 0.f;
-            if constexpr (!kFirst) in = fv[q];
-            fout[(long long)q * g.n + c] = mix_f_post<q, kFirst>(P, d, k, in);
-        });
-        float gv[Q];
-        if constexpr (!kFirst) {
-            pull_regs(gv, gin, g, x, y, z);
-            bounce_regs(gv, g, x);
-        }
-        static_for<0, Q>([&](auto qc) {
-            constexpr int q = decltype(qc)::value;
-            float in = 0.f;
-            if constexpr (!kFirst) in = gv[q];
-            gout[(long long)q * g.n + c] = mix_g_post<q, kFirst>(P, d, k, in);
-        });
-    }
+    if (tile_coords(g, x, y, z)) mixc_collide<kFirst>(g, P, fin, fout, gin, gout, phi, rho, u, v, w, div_out, x, y, z, red);
     block_sum_store<3>(red, part, nblocks, block_linear());
 }
 
@@ -311,37 +136,9 @@ moments_kernel(Geom g, double fei_G, double fei_L, double rho_G, double rho_L, d
                double* __restrict__ part, long long nblocks)
 {
     int x, y, z;
-    const bool active = tile_coords(g, x, y, z);
     double red[1] = {0.0};
-    if (active) {
-        const long long c = cell_of(g, x, y, z);
-        float fv[Q];
-        pull_regs(fv, f, g, x, y, z);
-        bounce_regs(fv, g, x);
-        double dev = 0.0;
-        static_for<0, Q>([&](auto qc) { dev += (double)fv[decltype(qc)::value]; });
-        const double fei = fei_G + dev;
-        double density;
-        if (fei <= fei_G) density = rho_G;
-        else if (fei >= fei_L) density = rho_L;
-        else density = half_drho * (sin((fei - fei_avg) / dfei * CUDART_PI) + 1.0) + rho_G;
-        float gv[Q];
-        pull_regs(gv, gp, g, x, y, z);
-        bounce_regs(gv, g, x);
-        float uu = 0.f, vv = 0.f, ww = 0.f;
-        static_for<1, Q>([&](auto qc) {
-            constexpr int q = decltype(qc)::value;
-            uu = acc_signed<cx(q)>(uu, gv[q]);
-            vv = acc_signed<cy(q)>(vv, gv[q]);
-            ww = acc_signed<cz(q)>(ww, gv[q]);
-        });
-        phi[c] = (float)fei;
-        rho[c] = (float)density;
-        u[c] = uu;
-        v[c] = vv;
-        w[c] = ww;
-        red[0] = fei;
-    }
+    const MixMoments M{fei_G, fei_L, rho_G, rho_L, fei_avg, dfei, half_drho};
+    if (tile_coords(g, x, y, z)) mixc_moments(g, M, f, gp, phi, rho, u, v, w, x, y, z, red);
     block_sum_store<1>(red, part, nblocks, block_linear());
 }
 
@@ -352,42 +149,9 @@ prep_kernel(Geom g, const DevState* __restrict__ ds, const float* __restrict__ d
             float* __restrict__ omega, double* __restrict__ part, long long nblocks)
 {
     int x, y, z;
-    const bool active = tile_coords(g, x, y, z);
     double red[3] = {0.0, 0.0, 0.0};
-    if (active) {
-        const long long c = cell_of(g, x, y, z);
-        const float sv = (float)((double)div[c] - ds->div_mean);
-        s[c] = sv;
-        omega[c] = 1.f / (1.f / rho[c] + 0.5f);
-        if (isfinite(sv)) red[0] = sv; else red[1] = 1.0;
-        red[2] = p[c];
-    }
+    if (tile_coords(g, x, y, z)) mixc_prep(g, ds->div_mean, div, rho, p, s, omega, x, y, z, red);
     block_sum_store<3>(red, part, nblocks, block_linear());
-}
-
-// Kinetic collision of one population: h - (h - E p) omega - (E/3) s.
-template <int q>
-__device__ __forceinline__ float collide_h(float h, float p32, float om, float sv)
-{
-    constexpr float E = float(wE(q));
-    return h - (h - E * p32) * om - (E * (1.f / 3.f)) * sv;
-}
-
-__device__ __forceinline__ void collide_h_store(const float (&hv)[Q], double pv, float om, float sv,
-                                                float* __restrict__ hout, long long n, long long c)
-{
-    const float p32 = (float)pv;
-    static_for<0, Q>([&](auto qc) {
-        constexpr int q = decltype(qc)::value;
-        hout[(long long)q * n + c] = collide_h<q>(hv[q], p32, om, sv);
-    });
-}
-
-__device__ __forceinline__ double sum_q(const float (&hv)[Q])
-{
-    double acc = 0.0;
-    static_for<0, Q>([&](auto qc) { acc += (double)hv[decltype(qc)::value]; });
-    return acc;
 }
 
 __global__ void __launch_bounds__(256)
@@ -396,31 +160,7 @@ poisson_init_kernel(Geom g, int h_loaded, const float* __restrict__ hload, float
                     const float* __restrict__ s)
 {
     int x, y, z;
-    if (!tile_coords(g, x, y, z)) return;
-    const long long c = cell_of(g, x, y, z);
-    const double pv = p[c];
-    float hv[Q];
-    static_for<0, Q>([&](auto qc) {
-        constexpr int q = decltype(qc)::value;
-        hv[q] = h_loaded ? hload[(long long)q * g.n + c] : (float)(pv * wE(q));
-    });
-    collide_h_store(hv, pv, omega[c], s[c], hout, g.n, c);
-}
-
-// p = sum_q h in FP32, pairwise (plain sweeps; the check kernels sum in FP64).
-__device__ __forceinline__ float sum_q32(const float (&h)[Q])
-{
-    return (((h[0] + h[1]) + (h[2] + h[3])) + ((h[4] + h[5]) + (h[6] + h[7]))) +
-           (((h[8] + h[9]) + (h[10] + h[11])) + ((h[12] + h[13]) + h[14]));
-}
-
-__device__ __forceinline__ void collide_h_store32(const float (&hv)[Q], float p32, float om, float sv,
-                                                  float* __restrict__ hout, int n, int c)
-{
-    static_for<0, Q>([&](auto qc) {
-        constexpr int q = decltype(qc)::value;
-        hout[q * n + c] = collide_h<q>(hv[q], p32, om, sv);
-    });
+    if (tile_coords(g, x, y, z)) mixc_init(g, h_loaded != 0, hload, hout, p, omega, s, x, y, z);
 }
 
 // Plain sweep with 32-bit offsets (the launcher uses it when 15 n < 2^31).
@@ -429,13 +169,7 @@ sweep_kernel(Geom g, const float* __restrict__ hin, float* __restrict__ hout,
              const float* __restrict__ omega, const float* __restrict__ s)
 {
     int x, y, z;
-    if (!tile_coords(g, x, y, z)) return;
-    const int n = (int)g.n;
-    const int c = (z * g.ly + y) * g.lx + x;
-    float hv[Q];
-    pull_regs32(hv, hin, n, g, x, y, z);
-    bounce_regs(hv, g, x);
-    collide_h_store32(hv, sum_q32(hv), __ldg(omega + c), __ldg(s + c), hout, n, c);
+    if (tile_coords(g, x, y, z)) mixc_sweep32(g, hin, hout, omega, s, x, y, z);
 }
 
 // The same with 64-bit offsets for boxes with 15 n >= 2^31.
@@ -548,19 +282,7 @@ sweep_check_a_kernel(Geom g, int zrun, const float* __restrict__ hin, float* __r
     int x, y, z0, z1;
     const bool active = tile_zrun(g, zrun, x, y, z0, z1);
     double red[1] = {0.0};
-    for (int z = z0; active && z < z1; ++z) {
-        const long long c = cell_of(g, x, y, z);
-        float hv[Q];
-        pull_regs(hv, hin, g, x, y, z);
-        bounce_regs(hv, g, x);
-        const double pv = sum_q(hv);
-        static_for<0, Q>([&](auto qc) {
-            constexpr int q = decltype(qc)::value;
-            hout[(long long)q * g.n + c] = hv[q];
-        });
-        p_chk[c] = pv;
-        red[0] += pv;
-    }
+    for (int z = z0; active && z < z1; ++z) mixc_check_a(g, hin, hout, p_chk, x, y, z, red);
     block_sum_store<1>(red, part, nblocks, block_linear());
 }
 
@@ -578,30 +300,8 @@ sweep_check_b_kernel(Geom g, int zrun, const float* __restrict__ hin, float* __r
     double red[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     const double shift = ds->sigma;
     const double tgt = ds->target;
-    for (int z = z0; active && z < z1; ++z) {
-        const long long c = cell_of(g, x, y, z);
-        float hv[Q];
-        static_for<0, Q>([&](auto qc) {
-            constexpr int q = decltype(qc)::value;
-            hv[q] = (float)((double)__ldg(hin + (long long)q * g.n + c) - wE(q) * shift);
-        });
-        const double pv = p_chk[c] - shift;
-        if constexpr (kDual) {
-            static_for<0, Q>([&](auto qc) {
-                constexpr int q = decltype(qc)::value;
-                hc[(long long)q * g.n + c] = hv[q];
-            });
-            const double hsum = sum_q(hv);
-            red[2] += fabs(pv - hsum);
-            red[3] += fabs(pv - tgt);
-            red[4] += fabs(hsum - tgt);
-        }
-        red[0] += fabs(pv - p_prev[c]);
-        red[1] += fabs(pv);
-        p_prev[c] = pv;
-        p[c] = pv;
-        collide_h_store(hv, pv, __ldg(omega + c), __ldg(s + c), hout, g.n, c);
-    }
+    for (int z = z0; active && z < z1; ++z)
+        mixc_check_b<kDual>(g, hin, hout, hc, p_chk, p_prev, p, omega, s, shift, tgt, x, y, z, red);
     block_sum_store<5>(red, part, nblocks, block_linear());
 }
 
@@ -638,13 +338,7 @@ correct_kernel(Geom g, float* __restrict__ u, float* __restrict__ v, float* __re
                const double* __restrict__ p, const float* __restrict__ rho)
 {
     int x, y, z;
-    if (!tile_coords(g, x, y, z)) return;
-    const Mirror m(g, x, y, z);
-    const long long c = cell_of(g, x, y, z);
-    const double inv_2rho = 1.0 / (2.0 * (double)rho[c]);
-    u[c] = (float)((double)u[c] - (p[cell_of(g, m.xp, y, z)] - p[cell_of(g, m.xm, y, z)]) * inv_2rho);
-    v[c] = (float)((double)v[c] - (p[cell_of(g, x, m.yp, z)] - p[cell_of(g, x, m.ym, z)]) * inv_2rho);
-    w[c] = (float)((double)w[c] - (p[cell_of(g, x, y, m.zp)] - p[cell_of(g, x, y, m.zm)]) * inv_2rho);
+    if (tile_coords(g, x, y, z)) mixc_correct(g, u, v, w, p, rho, x, y, z);
 }
 
 __global__ void to_float_kernel(const double* __restrict__ src, float* __restrict__ dst, long long n)
@@ -659,26 +353,6 @@ __global__ void to_double_kernel(const float* __restrict__ src, double* __restri
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x)
         dst[i] = (double)src[i];
-}
-
-MixPhys mix_phys(const Phys& P)
-{
-    MixPhys M;
-    M.rho_G = (float)P.rho_G;
-    M.mu_G = (float)P.mu_G;
-    M.mu_slope = (float)P.mu_slope;
-    M.inv_tauf = (float)(1.0 / P.tauf);
-    M.inv_taug = (float)(1.0 / P.taug);
-    M.k_f = (float)P.k_f;
-    M.k_g = (float)P.k_g;
-    M.T = (float)P.T;
-    M.a = (float)P.a;
-    M.b = (float)P.b;
-    M.visc = (float)P.visc;
-    M.fei_G = (float)P.fei_G;
-    const double fg = P.fei_G;
-    M.p0_G = (float)(fg * P.T / (1.0 - P.b * fg) - P.a * fg * fg);
-    return M;
 }
 
 float* field_f(MixedBuffers& mb, int which)
