@@ -30,7 +30,7 @@ extern "C" {
 
 /* Bumped whenever a struct layout or a signature of this header changes;
    callers compare it with lbm_abi_version() of the loaded library. */
-#define LBM_B200_ABI_VERSION 2
+#define LBM_B200_ABI_VERSION 3
 
 typedef enum {
     LBM_OK = 0,
@@ -79,6 +79,9 @@ typedef struct {
     double init_center_x, init_center_y, init_center_z;
     double init_separation;
     double init_offset_x;
+    /* Not a reference mode: 1 makes x periodic instead of the reference's slip
+     * walls (params.in token boundary_x=periodic); default 0 (slip walls). */
+    int periodic_x;
 } lbm_params;
 
 /* Poisson stopping rule (InamuroCUDA::setPoissonConvergence /
@@ -301,6 +304,66 @@ lbm_status lbm_set_timing(lbm_handle* h, int enabled);
 const char* lbm_last_error(const lbm_handle* h);
 const char* lbm_status_string(lbm_status s);
 int lbm_abi_version(void);
+
+/* ---- batched boxes ------------------------------------------------------
+ * Many independent droplet boxes of different sizes and physics advanced
+ * together on one GPU, mixed precision (FP32 populations, FP64 pressure sums,
+ * reductions and exit tests, as LBM_PRECISION_MIXED).  The reference has no
+ * batched form; each instance follows the single-box step exactly (same
+ * kernels' cell arithmetic, same Poisson exit per instance), and every phase
+ * of a step is one launch over all instances: a persistent grid walks a work
+ * list of (instance, xy tile, z run) items.  Each instance leaves the Poisson
+ * loop at its own check; its items are skipped for the rest of the step.
+ * x boundary per instance as in the single box (slip walls, or periodic with
+ * lbm_params.periodic_x); the dual residual is not available
+ * (dual_residual must be 0). */
+typedef struct lbm_batch lbm_batch;
+
+/* Launch shape of the batched kernels (what lbm_batch_tune chooses). */
+typedef struct {
+    int tile_x, tile_y;      /* cells per CTA tile in x and y (tile_x * tile_y = 256) */
+    int zrun;                /* z planes per work item */
+    int ctas_per_sm;         /* persistent grid: ctas_per_sm CTAs per SM */
+    double sweep_ms;         /* measured time of one batched sweep (lbm_batch_tune), else 0 */
+} lbm_batch_tuning;
+
+/* One box per params[i] (its own lx, ly, lz and physics). */
+lbm_status lbm_batch_create(const lbm_params* params, int n_instances, int device, lbm_batch** out);
+void lbm_batch_destroy(lbm_batch* b);
+int lbm_batch_size(const lbm_batch* b);
+/* Initial macro fields of instance inst, physical layout (lbm_load_fields);
+ * NULL fields load as zero (p, u, v, w) or the gas state (phi, rho).  The
+ * next step restarts EVERY instance from its current macro fields
+ * (equilibrium populations, first Poisson solve from h = 0), as constructing
+ * the reference's class from a CPU object does: load all instances, then step. */
+lbm_status lbm_batch_load_fields(lbm_batch* b, int inst, const double* phi, const double* rho, const double* u,
+                                 const double* v, const double* w, const double* p);
+/* Poisson settings for every instance (lbm_set_poisson; dual_residual must be 0). */
+lbm_status lbm_batch_set_poisson(lbm_batch* b, const lbm_poisson_cfg* cfg);
+/* n_steps steps of every instance; stats (may be NULL): n_steps * n_instances
+ * entries, step-major (stats[s * n_instances + i]). */
+lbm_status lbm_batch_step(lbm_batch* b, int n_steps, lbm_step_stats* stats);
+/* The same with a fixed sweep count per step and instance (multiples of the
+ * check interval), sweeps[s * n_instances + i]. */
+lbm_status lbm_batch_step_replay(lbm_batch* b, int n_steps, const uint64_t* sweeps, lbm_step_stats* stats);
+/* A field of instance inst in the physical layout (lbm_download). */
+lbm_status lbm_batch_download(lbm_batch* b, int inst, lbm_field which, double* host);
+/* Autotuner: times the batched sweep, collide and check kernels over the
+ * candidate tiles (32x8, 16x16, 8x32), z runs (1, 2, 4, 8) and persistent
+ * grids (2, 4, 8 CTAs per SM) on the loaded state and keeps the fastest
+ * (the Poisson state is rebuilt at the next step, so tuning changes no
+ * result).  chosen may be NULL. */
+lbm_status lbm_batch_tune(lbm_batch* b, lbm_batch_tuning* chosen);
+lbm_status lbm_batch_set_tuning(lbm_batch* b, const lbm_batch_tuning* t);
+lbm_status lbm_batch_get_tuning(const lbm_batch* b, lbm_batch_tuning* out);
+/* Device time per kernel class summed over instances' launches (lbm_timing;
+ * sweeps = sweeps summed over steps and instances, sweep_kernels = batched
+ * sweep launches). */
+lbm_status lbm_batch_get_timing(const lbm_batch* b, lbm_timing* out);
+lbm_status lbm_batch_reset_timing(lbm_batch* b);
+/* Text of the last error on this batch ("" if none); with b == NULL: why the
+ * calling thread's last lbm_batch_create failed. */
+const char* lbm_batch_last_error(const lbm_batch* b);
 
 #ifdef __cplusplus
 }

@@ -41,7 +41,8 @@ class Params(C.Structure):
         [("init_single_droplet", C.c_int), ("init_tanh", C.c_int)] + \
         [(k, C.c_double) for k in ("init_velocity", "interface_width", "init_center_x",
                                     "init_center_y", "init_center_z", "init_separation",
-                                    "init_offset_x")]
+                                    "init_offset_x")] + \
+        [("periodic_x", C.c_int)]
 
     @property
     def shape(self):
@@ -82,6 +83,15 @@ class Timing(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BatchTuning(C.Structure):
+    """lbm_batch_tuning: launch shape of the batched kernels."""
+    _fields_ = [("tile_x", C.c_int), ("tile_y", C.c_int), ("zrun", C.c_int), ("ctas_per_sm", C.c_int),
+                ("sweep_ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class FieldStats(C.Structure):
     """lbm_field_stats: Inamuro::FieldStatistics (CPU/Inamuro.hpp:91-99) + sum."""
     _fields_ = [(k, C.c_double) for k in ("min", "max", "mean", "abs_max")] + \
@@ -102,7 +112,7 @@ class LBMError(RuntimeError):
 
 _lib = None
 # LBM_B200_ABI_VERSION of include/lbm_b200.h that the structures above mirror.
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 
 def load_library(path: str = LIB_PATH):
@@ -144,6 +154,23 @@ def load_library(path: str = LIB_PATH):
     L.lbm_status_string.argtypes = [C.c_int]
     L.lbm_status_string.restype = C.c_char_p
     L.lbm_abi_version.restype = C.c_int
+    B = C.c_void_p
+    L.lbm_batch_create.argtypes = [C.POINTER(Params), C.c_int, C.c_int, C.POINTER(B)]
+    L.lbm_batch_destroy.argtypes = [B]
+    L.lbm_batch_destroy.restype = None
+    L.lbm_batch_size.argtypes = [B]
+    L.lbm_batch_load_fields.argtypes = [B, C.c_int] + [C.c_void_p] * 6
+    L.lbm_batch_set_poisson.argtypes = [B, C.POINTER(PoissonCfg)]
+    L.lbm_batch_step.argtypes = [B, C.c_int, C.POINTER(StepStats)]
+    L.lbm_batch_step_replay.argtypes = [B, C.c_int, C.POINTER(C.c_uint64), C.POINTER(StepStats)]
+    L.lbm_batch_download.argtypes = [B, C.c_int, C.c_int, dp]
+    L.lbm_batch_tune.argtypes = [B, C.POINTER(BatchTuning)]
+    L.lbm_batch_set_tuning.argtypes = [B, C.POINTER(BatchTuning)]
+    L.lbm_batch_get_tuning.argtypes = [B, C.POINTER(BatchTuning)]
+    L.lbm_batch_get_timing.argtypes = [B, C.POINTER(Timing)]
+    L.lbm_batch_reset_timing.argtypes = [B]
+    L.lbm_batch_last_error.argtypes = [B]
+    L.lbm_batch_last_error.restype = C.c_char_p
     if L.lbm_abi_version() != ABI_VERSION:
         raise LBMError(7, f"{path} has ABI {L.lbm_abi_version()}, these bindings expect {ABI_VERSION}; "
                           "rebuild with lbm_b200.build.build()")
@@ -385,3 +412,118 @@ class InamuroCUDA:
 
     def set_timing(self, enabled: bool):
         self._check(self._lib.lbm_set_timing(self._h, int(enabled)), "set_timing")
+
+
+class Batch:
+    """Many independent mixed-precision boxes advanced together (lbm_batch_*):
+    one entry of `params` per instance, each with its own box and physics."""
+
+    def __init__(self, params: Sequence[Params], fields: Optional[Sequence[Dict[str, np.ndarray]]] = None,
+                 device: int = 0):
+        self._lib = load_library()
+        self.params = list(params)
+        arr = (Params * len(self.params))(*self.params)
+        h = C.c_void_p()
+        st = self._lib.lbm_batch_create(arr, len(self.params), device, C.byref(h))
+        if st != 0:
+            why = self._lib.lbm_batch_last_error(None)
+            raise LBMError(st, "lbm_batch_create: " + (why.decode() if why else ""))
+        self._h = h
+        if fields is not None:
+            for i, f in enumerate(fields):
+                self.load_fields(i, f)
+
+    def _check(self, st: int, what: str):
+        if st != 0:
+            msg = self._lib.lbm_batch_last_error(self._h)
+            raise LBMError(st, f"{what}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.lbm_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __len__(self):
+        return len(self.params)
+
+    def shape(self, i: int):
+        p = self.params[i]
+        return (p.lz, p.ly, p.lx)
+
+    def load_fields(self, i: int, fields: Dict[str, np.ndarray]):
+        arrs = []
+        for k in FIELDS:
+            a = fields.get(k)
+            if a is not None:
+                a = np.ascontiguousarray(a, dtype=np.float64)
+                if a.size != np.prod(self.shape(i)):
+                    raise LBMError(4, f"field {k} of instance {i} has {a.size} values, box has {np.prod(self.shape(i))}")
+            arrs.append(a)
+        ptrs = [a.ctypes.data if a is not None else None for a in arrs]
+        self._check(self._lib.lbm_batch_load_fields(self._h, i, *ptrs), "batch_load_fields")
+
+    def set_poisson(self, check_interval: int = 100, tolerance: float = 1e-3, max_sweeps: int = 0,
+                    fail_on_limit: bool = False):
+        cfg = PoissonCfg(check_interval, tolerance, 0, max_sweeps, int(fail_on_limit))
+        self._check(self._lib.lbm_batch_set_poisson(self._h, C.byref(cfg)), "batch_set_poisson")
+
+    def step(self, n: int = 1) -> List[List[Dict[str, float]]]:
+        """n steps; returns [step][instance] diagnostics."""
+        m = len(self)
+        stats = (StepStats * max(n * m, 1))()
+        self._check(self._lib.lbm_batch_step(self._h, n, stats), "batch_step")
+        return [[stats[s * m + i].as_dict() for i in range(m)] for s in range(n)]
+
+    def step_replay(self, sweeps: Sequence[Sequence[int]]) -> List[List[Dict[str, float]]]:
+        """One step per row of `sweeps` (one count per instance)."""
+        m = len(self)
+        n = len(sweeps)
+        flat = [int(c) for row in sweeps for c in row]
+        if len(flat) != n * m:
+            raise LBMError(4, "one sweep count per step and instance")
+        arr = (C.c_uint64 * len(flat))(*flat)
+        stats = (StepStats * max(n * m, 1))()
+        self._check(self._lib.lbm_batch_step_replay(self._h, n, arr, stats), "batch_step_replay")
+        return [[stats[s * m + i].as_dict() for i in range(m)] for s in range(n)]
+
+    def download(self, i: int, name: str) -> np.ndarray:
+        out = np.empty(self.shape(i), dtype=np.float64)
+        self._check(self._lib.lbm_batch_download(self._h, i, FIELD_ID[name], _dp(out)), "batch_download")
+        return out
+
+    def download_fields(self, i: int) -> Dict[str, np.ndarray]:
+        return {k: self.download(i, k) for k in FIELDS}
+
+    def tune(self) -> Dict[str, float]:
+        t = BatchTuning()
+        self._check(self._lib.lbm_batch_tune(self._h, C.byref(t)), "batch_tune")
+        return t.as_dict()
+
+    def set_tuning(self, tile_x: int, tile_y: int, zrun: int, ctas_per_sm: int):
+        t = BatchTuning(tile_x, tile_y, zrun, ctas_per_sm, 0.0)
+        self._check(self._lib.lbm_batch_set_tuning(self._h, C.byref(t)), "batch_set_tuning")
+
+    def tuning(self) -> Dict[str, float]:
+        t = BatchTuning()
+        self._check(self._lib.lbm_batch_get_tuning(self._h, C.byref(t)), "batch_get_tuning")
+        return t.as_dict()
+
+    def timing(self) -> Dict[str, float]:
+        t = Timing()
+        self._check(self._lib.lbm_batch_get_timing(self._h, C.byref(t)), "batch_timing")
+        return t.as_dict()
+
+    def reset_timing(self):
+        self._check(self._lib.lbm_batch_reset_timing(self._h), "batch_reset_timing")

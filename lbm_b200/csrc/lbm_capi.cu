@@ -30,6 +30,7 @@
 #include "field_stats.cuh"
 #include "lbm_solver.cuh"
 #include "lbm_mixed.cuh"
+#include "phys_host.hpp"
 
 using namespace lbm;
 
@@ -97,40 +98,6 @@ lbm_status fail(lbm_handle* h, lbm_status s, const std::string& msg)
             return fail((h), e_ == cudaErrorMemoryAllocation ? LBM_ERR_OOM : LBM_ERR_CUDA,    \
                         std::string(#call) + ": " + cudaGetErrorString(e_));                  \
     } while (0)
-
-bool is_pow2(double t)
-{
-    if (!(t > 0.0) || !std::isfinite(t)) return false;
-    int e = 0;
-    return std::frexp(t, &e) == 0.5;
-}
-
-Phys make_phys(const lbm_params& p)
-{
-    Phys P{};
-    P.rho_L = p.rho_L;
-    P.rho_G = p.rho_G;
-    P.mu_G = p.mu_G;
-    P.mu_slope = (p.mu_L - p.mu_G) / (p.rho_L - p.rho_G);
-    P.tauf = p.tauf;
-    P.taug = p.taug;
-    P.k_f = p.k_f;
-    P.k_g = p.k_g;
-    P.T = p.T;
-    P.a = p.a;
-    P.b = p.b;
-    P.fei_L = p.fei_L;
-    P.fei_G = p.fei_G;
-    P.fei_avg = (p.fei_L + p.fei_G) / 2.0;
-    P.dfei = p.fei_L - p.fei_G;
-    P.half_drho = (p.rho_L - p.rho_G) / 2.0;
-    P.visc = 1.5 * (p.taug - 0.5) * 2.0;
-    P.tauf_pow2 = is_pow2(p.tauf);
-    P.taug_pow2 = is_pow2(p.taug);
-    P.inv_tauf = 1.0 / p.tauf;
-    P.inv_taug = 1.0 / p.taug;
-    return P;
-}
 
 int pick_bx(int lx)
 {
@@ -588,7 +555,7 @@ lbm_status lbm_create(const lbm_params* prm, lbm_precision precision, int device
     h->geom.lx = prm->lx;
     h->geom.ly = prm->ly;
     h->geom.lz = prm->lz;
-    h->geom.periodic_x = 0;
+    h->geom.periodic_x = prm->periodic_x ? 1 : 0;
     h->geom.n = static_cast<long long>(prm->lx) * prm->ly * prm->lz;
     h->phys = make_phys(*prm);
     const int bx = pick_bx(prm->lx);

@@ -43,6 +43,7 @@ extern "C" void lbm_params_default(lbm_params* o)
     o->init_center_x = -1.0; o->init_center_y = -1.0; o->init_center_z = -1.0;
     o->init_separation = -1.0;
     o->init_offset_x = 0.0;
+    o->periodic_x = 0;
 }
 
 namespace {
@@ -111,6 +112,11 @@ extern "C" lbm_status lbm_params_load(const char* path, lbm_params* o)
             if (!num(o->init_separation)) return LBM_ERR_BAD_ARG;
         } else if (key == "init_offset_x") {
             if (!num(o->init_offset_x)) return LBM_ERR_BAD_ARG;
+        } else if (key == "boundary_x") {
+            // Not a reference key: periodic x instead of the slip walls.
+            if (value == "periodic") o->periodic_x = 1;
+            else if (value == "slip") o->periodic_x = 0;
+            else return LBM_ERR_BAD_ARG;
         }
         // Any other key (the CPU tree's output switches) is ignored.
     }

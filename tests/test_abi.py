@@ -25,14 +25,14 @@ def test_nm_lists_exports_as_c_symbols():
 
 def test_status_strings_and_version():
     lib = L.load_library()
-    assert lib.lbm_abi_version() == 2
+    assert lib.lbm_abi_version() == 3
     for s in range(9):
         assert lib.lbm_status_string(s)
 
 
 def test_struct_sizes_match_header():
     # lbm_params: 6 ints + 16 doubles + 2 ints + 7 doubles (natural alignment)
-    assert ctypes.sizeof(L.Params) == 6 * 4 + 16 * 8 + 2 * 4 + 7 * 8
+    assert ctypes.sizeof(L.Params) == 6 * 4 + 16 * 8 + 2 * 4 + 7 * 8 + 8   # periodic_x + tail padding
     assert ctypes.sizeof(L.PoissonCfg) == 40
     assert ctypes.sizeof(L.StepStats) == 8 + 16 * 8 + 6 * 4 + 8
     assert ctypes.sizeof(L.Timing) == 5 * 8 + 5 * 8

@@ -88,13 +88,14 @@ def test_mixed_field_statistics_and_ghosts():
     assert np.all(gh[0] == p.rho_G) and np.all(gh[-1] == p.rho_G)
 
 
-@pytest.mark.parametrize("zlen", ["32", "5", "1"])
-def test_two_sweep_pass_matches_single_sweeps(zlen, monkeypatch):
+@pytest.mark.parametrize("zlen,periodic", [("32", 0), ("5", 0), ("1", 0), ("32", 1)])
+def test_two_sweep_pass_matches_single_sweeps(zlen, periodic, monkeypatch):
     """The temporally blocked pass (two sweeps per launch, 2.5-D z march with a
     shared-memory plane ring) gives the same steps as single-sweep launches:
     same sweep counts, fields equal to FP32 rounding; z runs that do not divide
-    the box (5) and single-plane runs (1) included."""
+    the box (5), single-plane runs (1) and periodic x included."""
     p, f = laplace_case((64, 40, 24), DD=12.0, noise=1e-4)
+    p.periodic_x = periodic
     f["w"] = 0.01 * np.sin(2 * np.pi * np.arange(24) / 24)[:, None, None] * np.ones_like(f["w"])
     monkeypatch.setenv("LBM_SWEEP2_ZLEN", "0")
     a = L.InamuroCUDA(p, f, precision="mixed")
@@ -114,15 +115,16 @@ def test_two_sweep_pass_matches_single_sweeps(zlen, monkeypatch):
     assert tb["kernel_launches"] < ta["kernel_launches"]
 
 
-@pytest.mark.parametrize("zlen", ["16", "5", "1"])
-def test_zmarch_collide_matches_plane_collide(zlen, monkeypatch):
+@pytest.mark.parametrize("zlen,periodic", [("16", 0), ("5", 0), ("1", 0), ("16", 1)])
+def test_zmarch_collide_matches_plane_collide(zlen, periodic, monkeypatch):
     """The z-marching collide (macro fields staged in a shared-memory plane
     ring) computes the same cells as the plane-per-CTA collide: after the
     first step (equilibrium start, no reductions involved) phi and rho are
     bitwise equal; later steps differ only through the order of the source
-    sum, well inside FP32 rounding.  z runs that do not divide the box (5)
-    and single-plane runs (1) are covered."""
+    sum, well inside FP32 rounding.  z runs that do not divide the box (5),
+    single-plane runs (1) and periodic x are covered."""
     p, f = laplace_case((64, 40, 24), DD=12.0, noise=1e-4)
+    p.periodic_x = periodic
     f["u"] = 0.005 * np.cos(2 * np.pi * np.arange(40) / 40)[None, :, None] * np.ones_like(f["u"])
     f["w"] = 0.01 * np.sin(2 * np.pi * np.arange(24) / 24)[:, None, None] * np.ones_like(f["w"])
     monkeypatch.setenv("LBM_COLLIDE_ZLEN", "0")
@@ -140,3 +142,23 @@ def test_zmarch_collide_matches_plane_collide(zlen, monkeypatch):
     fa, fb = a.download_fields(), b.download_fields()
     for k in L.FIELDS:
         assert rel_err(fb[k], fa[k]) <= 1e-6, k
+
+
+def test_mixed_periodic_x_against_periodic_oracle():
+    """Periodic x (not a reference mode): the mixed box against the FP64
+    oracle run with periodic x, equal sweep counts; phi sum conserved to FP32
+    storage rounding."""
+    p, f = laplace_case((32, 24, 16), DD=8.0, noise=1e-4)
+    p.periodic_x = 1
+    f["u"] = 0.01 * np.sin(2 * np.pi * np.arange(24) / 24)[None, :, None] * np.ones_like(f["u"])
+    o = pyoracle.Oracle(p.shape, oracle_params(p), f, max_sweeps=CAP, periodic_x=True)
+    g = L.InamuroCUDA(p, f, precision="mixed")
+    g.set_poisson(max_sweeps=CAP, fail_on_limit=True)
+    masses = []
+    for _ in range(3):
+        info = o.step()
+        masses.append(g.step_replay([int(info["sweeps"])])[0]["mass"])
+    gf, of = g.download_fields(), o.fields()
+    for k, v in TOL.items():
+        assert rel_err(gf[k], of[k]) <= v, k
+    assert max(abs(m - masses[0]) for m in masses) <= 1e-10 * abs(masses[0])

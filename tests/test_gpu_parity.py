@@ -253,11 +253,13 @@ def test_full_size_256_translation_and_mirror():
     assert np.max(np.abs(c["w"])) > 0.0
 
 
-@pytest.mark.parametrize("zlen", ["32", "7"])
-def test_fp64_two_sweep_pass_is_bitwise(zlen, monkeypatch):
+@pytest.mark.parametrize("zlen,periodic", [("32", 0), ("7", 0), ("32", 1)])
+def test_fp64_two_sweep_pass_is_bitwise(zlen, periodic, monkeypatch):
     """The FP64 temporally blocked pass (two sweeps per launch) keeps every
-    cell's arithmetic, so it reproduces single-sweep launches bit for bit."""
+    cell's arithmetic, so it reproduces single-sweep launches bit for bit
+    (slip walls and periodic x)."""
     p, f = laplace_case((64, 12, 20), DD=8.0, noise=1e-4)
+    p.periodic_x = periodic
     f["w"] = 0.01 * np.sin(2 * np.pi * np.arange(20) / 20)[:, None, None] * np.ones_like(f["w"])
     monkeypatch.setenv("LBM_SWEEP2_ZLEN", "0")
     a = solver(p, f)
@@ -271,15 +273,16 @@ def test_fp64_two_sweep_pass_is_bitwise(zlen, monkeypatch):
     assert b.timing()["kernel_launches"] < a.timing()["kernel_launches"]
 
 
-@pytest.mark.parametrize("zlen,minb", [("16", "2"), ("5", "1"), ("1", "2")])
-def test_fp64_zmarch_collide_matches_plane_collide(zlen, minb, monkeypatch):
+@pytest.mark.parametrize("zlen,minb,periodic", [("16", "2", 0), ("5", "1", 0), ("1", "2", 0), ("16", "2", 1)])
+def test_fp64_zmarch_collide_matches_plane_collide(zlen, minb, periodic, monkeypatch):
     """The z-marching FP64 collide (macro fields staged in a shared-memory
     plane ring) evaluates every cell with the same operations as the plane
     collide: phi and rho after the first step are bitwise equal; later steps
     differ only through the order of the source sum (FP64 rounding).  z runs
-    that do not divide the box (5), single-plane runs (1) and both register
-    budgets are covered."""
+    that do not divide the box (5), single-plane runs (1), both register
+    budgets and periodic x are covered."""
     p, f = laplace_case((64, 40, 24), DD=12.0, noise=1e-4)
+    p.periodic_x = periodic
     f["u"] = 0.005 * np.cos(2 * np.pi * np.arange(40) / 40)[None, :, None] * np.ones_like(f["u"])
     f["w"] = 0.01 * np.sin(2 * np.pi * np.arange(24) / 24)[:, None, None] * np.ones_like(f["w"])
     monkeypatch.setenv("LBM_COLLIDE_ZLEN", "0")
@@ -298,3 +301,25 @@ def test_fp64_zmarch_collide_matches_plane_collide(zlen, minb, monkeypatch):
     fa, fb = a.download_fields(), b.download_fields()
     for k in L.FIELDS:
         assert rel_err(fb[k], fa[k]) <= 1e-12, k
+
+
+def test_fp64_periodic_x_matches_periodic_oracle_and_conserves_mass():
+    """Periodic x (not a reference mode; the configs' periodic boxes): the FP64
+    box against the oracle run with periodic x (same sweep counts, fields to
+    1e-10), and the phi sum conserved to 1e-12 relative over the steps (with
+    the reference's slip walls the scheme itself does not conserve it)."""
+    p, f = laplace_case((32, 24, 16), DD=8.0, noise=1e-4)
+    p.periodic_x = 1
+    f["u"] = 0.01 * np.sin(2 * np.pi * np.arange(24) / 24)[None, :, None] * np.ones_like(f["u"])
+    o = pyoracle.Oracle(p.shape, oracle_params(p), f, max_sweeps=CAP, periodic_x=True)
+    g = solver(p, f)
+    masses = []
+    for _ in range(3):
+        info = o.step()
+        st = g.step(1)[0]
+        assert st["iterations"] == info["sweeps"]
+        masses.append(st["mass"])
+    gf, of = g.download_fields(), o.fields()
+    for k in L.FIELDS:
+        assert rel_err(gf[k], of[k]) <= 1e-10, k
+    assert max(abs(m - masses[0]) for m in masses) <= 1e-12 * abs(masses[0])

@@ -74,3 +74,15 @@ def test_init_mode_fallbacks():
     assert p1.init_single_droplet == 0 and p1.init_tanh == 0
     for k in L.FIELDS:
         assert np.array_equal(L.init_droplets(p1)[k], L.init_droplets(p0)[k])
+
+
+def test_boundary_x_token():
+    """boundary_x=periodic|slip (not a reference key) sets lbm_params.periodic_x;
+    the reference's slip walls stay the default; other values are rejected."""
+    base = fixture("init_two_sharp")["params_text"].item()
+    assert params_from_text(base).periodic_x == 0
+    assert params_from_text(base + "boundary_x=periodic\n").periodic_x == 1
+    assert params_from_text(base + "boundary_x=slip\n").periodic_x == 0
+    with pytest.raises(L.LBMError) as e:
+        params_from_text(base + "boundary_x=open\n")
+    assert e.value.status == 4
