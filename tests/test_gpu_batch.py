@@ -128,7 +128,9 @@ def test_batch_sweep_cap_is_reported():
 def test_batch_workload_steps_and_conserves_mass():
     """Eight instances of the batched droplet-oscillation workload (periodic
     boxes) step with natural exits; every instance converges and keeps its
-    mass (phi sum) to FP32-storage rounding."""
+    mass (phi sum) to FP32-storage rounding: the populations' rounding is the
+    same in every cell of a uniform gas, so it adds up coherently (~1e-8 of
+    the mass per step), unlike the FP64 box (1e-12, tests/test_gpu_parity.py)."""
     params, fields = bench.batch_workload(8, seed=11)
     assert all(p.periodic_x == 1 for p in params)
     b = L.Batch(params, fields)
@@ -137,4 +139,4 @@ def test_batch_workload_steps_and_conserves_mass():
     s3 = b.step(2)[-1]
     for a, c in zip(s1, s3):
         assert a["converged"] == 1 and c["converged"] == 1
-        assert abs(c["mass"] - a["mass"]) <= 1e-10 * abs(a["mass"])
+        assert abs(c["mass"] - a["mass"]) <= 1e-6 * abs(a["mass"])

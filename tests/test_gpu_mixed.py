@@ -121,7 +121,7 @@ def test_zmarch_collide_matches_plane_collide(zlen, periodic, monkeypatch):
     ring) computes the same cells as the plane-per-CTA collide: after the
     first step (equilibrium start, no reductions involved) phi and rho are
     bitwise equal; later steps differ only through the order of the source
-    sum, well inside FP32 rounding.  z runs that do not divide the box (5),
+    sum, inside FP32 rounding (1e-6; 1e-5 for the small zero-mean p).  z runs that do not divide the box (5),
     single-plane runs (1) and periodic x are covered."""
     p, f = laplace_case((64, 40, 24), DD=12.0, noise=1e-4)
     p.periodic_x = periodic
@@ -141,16 +141,17 @@ def test_zmarch_collide_matches_plane_collide(zlen, periodic, monkeypatch):
         b.step_replay([300])
     fa, fb = a.download_fields(), b.download_fields()
     for k in L.FIELDS:
-        assert rel_err(fb[k], fa[k]) <= 1e-6, k
+        assert rel_err(fb[k], fa[k]) <= (1e-5 if k == "p" else 1e-6), k
 
 
 def test_mixed_periodic_x_against_periodic_oracle():
     """Periodic x (not a reference mode): the mixed box against the FP64
     oracle run with periodic x, equal sweep counts; phi sum conserved to FP32
-    storage rounding."""
+    storage rounding (coherent over uniform regions: ~1e-8 per step)."""
     p, f = laplace_case((32, 24, 16), DD=8.0, noise=1e-4)
     p.periodic_x = 1
     f["u"] = 0.01 * np.sin(2 * np.pi * np.arange(24) / 24)[None, :, None] * np.ones_like(f["u"])
+    f["v"] = 0.01 * np.cos(2 * np.pi * np.arange(32) / 32)[None, None, :] * np.ones_like(f["v"])
     o = pyoracle.Oracle(p.shape, oracle_params(p), f, max_sweeps=CAP, periodic_x=True)
     g = L.InamuroCUDA(p, f, precision="mixed")
     g.set_poisson(max_sweeps=CAP, fail_on_limit=True)
@@ -159,6 +160,11 @@ def test_mixed_periodic_x_against_periodic_oracle():
         info = o.step()
         masses.append(g.step_replay([int(info["sweeps"])])[0]["mass"])
     gf, of = g.download_fields(), o.fields()
-    for k, v in TOL.items():
-        assert rel_err(gf[k], of[k]) <= v, k
-    assert max(abs(m - masses[0]) for m in masses) <= 1e-10 * abs(masses[0])
+    for k in ("phi", "rho", "p"):
+        assert rel_err(gf[k], of[k]) <= TOL[k], k
+    # velocity components against the velocity scale (a component that stays
+    # near zero has no meaningful relative error of its own)
+    vscale = max(float(np.max(np.abs(of[k]))) for k in ("u", "v", "w"))
+    for k in ("u", "v", "w"):
+        assert float(np.max(np.abs(gf[k] - of[k]))) <= 1e-5 * vscale, k
+    assert max(abs(m - masses[0]) for m in masses) <= 1e-6 * abs(masses[0])

@@ -311,6 +311,7 @@ def test_fp64_periodic_x_matches_periodic_oracle_and_conserves_mass():
     p, f = laplace_case((32, 24, 16), DD=8.0, noise=1e-4)
     p.periodic_x = 1
     f["u"] = 0.01 * np.sin(2 * np.pi * np.arange(24) / 24)[None, :, None] * np.ones_like(f["u"])
+    f["v"] = 0.01 * np.cos(2 * np.pi * np.arange(32) / 32)[None, None, :] * np.ones_like(f["v"])
     o = pyoracle.Oracle(p.shape, oracle_params(p), f, max_sweeps=CAP, periodic_x=True)
     g = solver(p, f)
     masses = []
