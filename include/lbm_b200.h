@@ -30,7 +30,7 @@ extern "C" {
 
 /* Bumped whenever a struct layout or a signature of this header changes;
    callers compare it with lbm_abi_version() of the loaded library. */
-#define LBM_B200_ABI_VERSION 3
+#define LBM_B200_ABI_VERSION 4
 
 typedef enum {
     LBM_OK = 0,
@@ -324,7 +324,10 @@ typedef struct {
     int tile_x, tile_y;      /* cells per CTA tile in x and y (tile_x * tile_y = 256) */
     int zrun;                /* z planes per work item */
     int ctas_per_sm;         /* persistent grid: ctas_per_sm CTAs per SM */
-    double sweep_ms;         /* measured time of one batched sweep (lbm_batch_tune), else 0 */
+    int sweep2_zrun;         /* > 0: plain sweeps run two per launch (temporal blocking,
+                                16 x 8 tiles) on z runs of this length; 0: one per launch */
+    int reserved;
+    double sweep_ms;         /* measured time per sweep of the chosen form (lbm_batch_tune), else 0 */
 } lbm_batch_tuning;
 
 /* One box per params[i] (its own lx, ly, lz and physics). */
@@ -348,11 +351,11 @@ lbm_status lbm_batch_step(lbm_batch* b, int n_steps, lbm_step_stats* stats);
 lbm_status lbm_batch_step_replay(lbm_batch* b, int n_steps, const uint64_t* sweeps, lbm_step_stats* stats);
 /* A field of instance inst in the physical layout (lbm_download). */
 lbm_status lbm_batch_download(lbm_batch* b, int inst, lbm_field which, double* host);
-/* Autotuner: times the batched sweep, collide and check kernels over the
- * candidate tiles (32x8, 16x16, 8x32), z runs (1, 2, 4, 8) and persistent
- * grids (2, 4, 8 CTAs per SM) on the loaded state and keeps the fastest
- * (the Poisson state is rebuilt at the next step, so tuning changes no
- * result).  chosen may be NULL. */
+/* Autotuner: times the batched sweep over the candidate tiles (32x8, 16x16,
+ * 8x32), z runs (1, 2, 4, 8) and persistent grids (2, 4, 8 CTAs per SM), then
+ * the two-sweep pass on z runs of 8, 16 and 32, on the loaded state, and keeps
+ * the fastest per sweep (the Poisson state is rebuilt at the next step, so
+ * tuning changes no result).  chosen may be NULL. */
 lbm_status lbm_batch_tune(lbm_batch* b, lbm_batch_tuning* chosen);
 lbm_status lbm_batch_set_tuning(lbm_batch* b, const lbm_batch_tuning* t);
 lbm_status lbm_batch_get_tuning(const lbm_batch* b, lbm_batch_tuning* out);

@@ -86,7 +86,7 @@ class Timing(C.Structure):
 class BatchTuning(C.Structure):
     """lbm_batch_tuning: launch shape of the batched kernels."""
     _fields_ = [("tile_x", C.c_int), ("tile_y", C.c_int), ("zrun", C.c_int), ("ctas_per_sm", C.c_int),
-                ("sweep_ms", C.c_double)]
+                ("sweep2_zrun", C.c_int), ("reserved", C.c_int), ("sweep_ms", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -112,7 +112,7 @@ class LBMError(RuntimeError):
 
 _lib = None
 # LBM_B200_ABI_VERSION of include/lbm_b200.h that the structures above mirror.
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 
 def load_library(path: str = LIB_PATH):
@@ -511,8 +511,8 @@ class Batch:
         self._check(self._lib.lbm_batch_tune(self._h, C.byref(t)), "batch_tune")
         return t.as_dict()
 
-    def set_tuning(self, tile_x: int, tile_y: int, zrun: int, ctas_per_sm: int):
-        t = BatchTuning(tile_x, tile_y, zrun, ctas_per_sm, 0.0)
+    def set_tuning(self, tile_x: int, tile_y: int, zrun: int, ctas_per_sm: int, sweep2_zrun: int = 0):
+        t = BatchTuning(tile_x, tile_y, zrun, ctas_per_sm, sweep2_zrun, 0, 0.0)
         self._check(self._lib.lbm_batch_set_tuning(self._h, C.byref(t)), "batch_set_tuning")
 
     def tuning(self) -> Dict[str, float]:

@@ -180,6 +180,32 @@ b_sweep(const BItem* __restrict__ items, int n_items, const BInst* __restrict__ 
     }
 }
 
+// Two plain sweeps (flip index j: state in h[(parity + j) & 1], result in the
+// other buffer) for every active instance, 16 x 8 tiles with temporal
+// blocking (sweep2_run).
+constexpr int B2_TX = 16, B2_TY = 8;
+constexpr int B2_THREADS = sweep2_threads(B2_TX, B2_TY);   // 192
+constexpr int B2_SMEM = sweep2_smem(B2_TX, B2_TY);         // 43,200 B
+constexpr int B2_CTAS_PER_SM = 4;
+
+__global__ void __launch_bounds__(B2_THREADS, B2_CTAS_PER_SM)
+b_sweep2(const BItem* __restrict__ items, int n_items, const BInst* __restrict__ inst,
+         const BCtl* __restrict__ ctl, int j, BPool B)
+{
+    extern __shared__ float ring[];
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const BItem w = items[it];
+        const BCtl cw = ctl[w.inst];
+        if (!cw.active) continue;
+        const BInst I = inst[w.inst];
+        const bool odd = ((cw.parity + j) & 1) != 0;
+        const float* hin = (odd ? B.h[1] : B.h[0]) + I.pop;
+        float* hout = (odd ? B.h[0] : B.h[1]) + I.pop;
+        sweep2_run<B2_TX, B2_TY>(I.g, w.x0, w.y0, w.z0, w.z1, hin, hout, B.omega + I.fld, B.s + I.fld, ring);
+        __syncthreads();   // the ring is reused by the CTA's next item
+    }
+}
+
 __global__ void __launch_bounds__(256)
 b_check_a(const BItem* __restrict__ items, int n_items, const BInst* __restrict__ inst, int tile_x,
           const BCtl* __restrict__ ctl, int j, BPool B, double* __restrict__ part)
@@ -325,8 +351,10 @@ struct lbm_batch {
     long long pop_elems = 0;         // elements of one pooled population buffer
     long long item_capacity = 0;     // partial-sum slots allocated (largest work list of any tuning)
     int n_items = 0;
+    int n_items2 = 0;                // two-sweep work list (16 x 8 tiles, sweep2_zrun)
     BInst* inst_d = nullptr;
     BItem* items_d = nullptr;
+    BItem* items2_d = nullptr;
     DevState* ds = nullptr;
     DevState* ds_host = nullptr;     // pinned, n entries
     BCtl* ctl = nullptr;
@@ -335,7 +363,7 @@ struct lbm_batch {
     double *part_src = nullptr, *part_mass = nullptr, *part_prep = nullptr, *part_a = nullptr, *part_b = nullptr;
     double* scratch = nullptr;       // FP64 staging of one instance's field
     lbm_poisson_cfg pcfg{100, 1.0e-3, 0, 0, 0};
-    lbm_batch_tuning tune{32, 8, 4, 4, 0.0};
+    lbm_batch_tuning tune{32, 8, 4, 4, 0, 0, 0.0};
     int fcur = 0;
     bool first_step = true;
     std::map<int, cudaGraphExec_t> graphs;    // key: plain sweeps per segment
@@ -364,7 +392,8 @@ bool valid_tuning(const lbm_batch_tuning& t)
 {
     const bool tile = (t.tile_x == 32 && t.tile_y == 8) || (t.tile_x == 16 && t.tile_y == 16) ||
                       (t.tile_x == 8 && t.tile_y == 32);
-    return tile && t.zrun >= 1 && t.zrun <= 64 && t.ctas_per_sm >= 1 && t.ctas_per_sm <= 16;
+    return tile && t.zrun >= 1 && t.zrun <= 64 && t.ctas_per_sm >= 1 && t.ctas_per_sm <= 16 &&
+           t.sweep2_zrun >= 0 && t.sweep2_zrun <= 64;
 }
 
 long long count_items(const std::vector<lbm_params>& prm, int tx, int ty, int zrun)
@@ -396,6 +425,23 @@ lbm_status build_items(lbm_batch* b)
     b->items_d = nullptr;
     BCUDA(b, cudaMalloc(&b->items_d, items.size() * sizeof(BItem)));
     BCUDA(b, cudaMemcpy(b->items_d, items.data(), items.size() * sizeof(BItem), cudaMemcpyHostToDevice));
+    // the two-sweep list: 16 x 8 tiles, z runs of sweep2_zrun (no partial sums)
+    std::vector<BItem> items2;
+    if (t.sweep2_zrun > 0)
+        for (int i = 0; i < b->n; ++i) {
+            const BInst& I = b->inst_h[i];
+            for (int z0 = 0; z0 < I.g.lz; z0 += t.sweep2_zrun)
+                for (int y0 = 0; y0 < I.g.ly; y0 += B2_TY)
+                    for (int x0 = 0; x0 < I.g.lx; x0 += B2_TX)
+                        items2.push_back(BItem{i, x0, y0, z0, std::min(z0 + t.sweep2_zrun, I.g.lz)});
+        }
+    b->n_items2 = static_cast<int>(items2.size());
+    if (b->items2_d) cudaFree(b->items2_d);
+    b->items2_d = nullptr;
+    if (!items2.empty()) {
+        BCUDA(b, cudaMalloc(&b->items2_d, items2.size() * sizeof(BItem)));
+        BCUDA(b, cudaMemcpy(b->items2_d, items2.data(), items2.size() * sizeof(BItem), cudaMemcpyHostToDevice));
+    }
     BCUDA(b, cudaMemcpy(b->inst_d, b->inst_h.data(), b->n * sizeof(BInst), cudaMemcpyHostToDevice));
     for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
     b->graphs.clear();
@@ -426,6 +472,8 @@ void free_batch(lbm_batch* b)
     }
     if (b->inst_d) cudaFree(b->inst_d);
     if (b->items_d) cudaFree(b->items_d);
+    if (b->items2_d) cudaFree(b->items2_d);
+    b->items2_d = nullptr;
     if (b->ds) cudaFree(b->ds);
     if (b->ctl) cudaFree(b->ctl);
     if (b->ds_host) cudaFreeHost(b->ds_host);
@@ -482,13 +530,21 @@ lbm_status get_segment(lbm_batch* b, int n_normal, cudaGraphExec_t* out)
     const int grid = grid_of(b);
     const int tx = b->tune.tile_x;
     BCUDA(b, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    for (int j = 0; j < n_normal; ++j)
-        b_sweep<<<grid, 256, 0, st>>>(b->items_d, b->n_items, b->inst_d, tx, b->ctl, j, b->pool);
-    b_check_a<<<grid, 256, 0, st>>>(b->items_d, b->n_items, b->inst_d, tx, b->ctl, n_normal, b->pool, b->part_a);
+    // j counts buffer swaps: a two-sweep launch swaps once, a single sweep once
+    int j = 0;
+    int singles = n_normal;
+    if (b->n_items2 > 0) {
+        const int grid2 = std::max(1, std::min(b->n_items2, B2_CTAS_PER_SM * b->sm_count));
+        for (int k = 0; k + 1 < n_normal; k += 2)
+            b_sweep2<<<grid2, B2_THREADS, B2_SMEM, st>>>(b->items2_d, b->n_items2, b->inst_d, b->ctl, j++, b->pool);
+        singles = n_normal & 1;
+    }
+    for (int k = 0; k < singles; ++k)
+        b_sweep<<<grid, 256, 0, st>>>(b->items_d, b->n_items, b->inst_d, tx, b->ctl, j++, b->pool);
+    b_check_a<<<grid, 256, 0, st>>>(b->items_d, b->n_items, b->inst_d, tx, b->ctl, j++, b->pool, b->part_a);
     b_finalize<<<b->n, 256, 0, st>>>(FIN_SIGMA, b->ds, b->ctl, b->inst_d, b->part_a, b->n_items, 0);
-    b_check_b<<<grid, 256, 0, st>>>(b->items_d, b->n_items, b->inst_d, tx, b->ctl, b->ds, n_normal + 1, b->pool,
-                                    b->part_b);
-    b_finalize<<<b->n, 256, 0, st>>>(FIN_CHECK, b->ds, b->ctl, b->inst_d, b->part_b, b->n_items, n_normal + 2);
+    b_check_b<<<grid, 256, 0, st>>>(b->items_d, b->n_items, b->inst_d, tx, b->ctl, b->ds, j++, b->pool, b->part_b);
+    b_finalize<<<b->n, 256, 0, st>>>(FIN_CHECK, b->ds, b->ctl, b->inst_d, b->part_b, b->n_items, j);
     cudaMemcpyAsync(b->ctl_host, b->ctl, b->n * sizeof(BCtl), cudaMemcpyDeviceToHost, st);
     cudaGraph_t graph = nullptr;
     const cudaError_t e = cudaStreamEndCapture(st, &graph);
@@ -601,10 +657,13 @@ lbm_status batch_step_once(lbm_batch* b, const uint64_t* replay, lbm_step_stats*
     b->acc.poisson_ms += t[3];
     b->acc.correct_ms += t[4];
     b->acc.steps += 1;
-    // per segment: ci - 1 plain sweeps + check A + check B (together one sweep)
-    // + two finalisations; per step: 7 prologue launches and the correction
+    // per segment: ci - 1 plain sweeps (in pairs when two-sweep passes are on)
+    // + check A + check B (together one sweep) + two finalisations; per step:
+    // 7 prologue launches and the correction
     b->acc.sweep_kernels += segments * static_cast<uint64_t>(ci + 1);
-    b->acc.kernel_launches += 8 + segments * static_cast<uint64_t>(ci + 3);
+    const uint64_t plain = b->n_items2 > 0 ? static_cast<uint64_t>((ci - 1) / 2 + (ci - 1) % 2) : ci - 1;
+    b->acc.kernel_launches += 8 + segments * (plain + 4);
+    if (b->n_items2 > 0) b->acc.fused_sweeps += segments * static_cast<uint64_t>((ci - 1) / 2 * 2);
     lbm_status status = LBM_OK;
     for (int i = 0; i < b->n; ++i) {
         const DevState& d = b->ds_host[i];
@@ -718,8 +777,9 @@ lbm_status lbm_batch_create(const lbm_params* params, int n_instances, int devic
     cudaMemset(b->pool.omega, 0, fld * sizeof(float));
     if (const char* e = std::getenv("LBM_BATCH_TUNING")) {
         lbm_batch_tuning t{};
-        if (std::sscanf(e, "%d,%d,%d,%d", &t.tile_x, &t.tile_y, &t.zrun, &t.ctas_per_sm) == 4 && valid_tuning(t))
-            b->tune = t;
+        const int got = std::sscanf(e, "%d,%d,%d,%d,%d", &t.tile_x, &t.tile_y, &t.zrun, &t.ctas_per_sm,
+                                    &t.sweep2_zrun);
+        if (got >= 4 && valid_tuning(t)) b->tune = t;
     }
     lbm_status s = build_items(b);
     if (s != LBM_OK) return bail(s);
@@ -846,7 +906,7 @@ lbm_status lbm_batch_tune(lbm_batch* b, lbm_batch_tuning* chosen)
     for (auto& tl : tiles)
         for (int zr : zruns)
             for (int cp : ctas) {
-                const lbm_batch_tuning t{tl[0], tl[1], zr, cp, 0.0};
+                const lbm_batch_tuning t{tl[0], tl[1], zr, cp, 0, 0, 0.0};
                 b->tune = t;
                 lbm_status s = build_items(b);
                 if (s != LBM_OK) return s;
@@ -866,6 +926,31 @@ lbm_status lbm_batch_tune(lbm_batch* b, lbm_batch_tuning* chosen)
                     best.sweep_ms = ms / reps;
                 }
             }
+    // two sweeps per launch on z runs of 8, 16, 32 (per-sweep time = launch / 2)
+    const int zr2[3] = {8, 16, 32};
+    for (int zr : zr2) {
+        lbm_batch_tuning t = best;
+        t.sweep2_zrun = zr;
+        t.sweep_ms = 0.0;
+        b->tune = t;
+        lbm_status s = build_items(b);
+        if (s != LBM_OK) return s;
+        const int grid2 = std::max(1, std::min(b->n_items2, B2_CTAS_PER_SM * b->sm_count));
+        b_sweep2<<<grid2, B2_THREADS, B2_SMEM, st>>>(b->items2_d, b->n_items2, b->inst_d, b->ctl, 0, b->pool);
+        BCUDA(b, cudaEventRecord(b->ev[0], st));
+        for (int r = 0; r < reps / 2; ++r)
+            b_sweep2<<<grid2, B2_THREADS, B2_SMEM, st>>>(b->items2_d, b->n_items2, b->inst_d, b->ctl, r, b->pool);
+        BCUDA(b, cudaEventRecord(b->ev[1], st));
+        BCUDA(b, cudaGetLastError());
+        BCUDA(b, cudaEventSynchronize(b->ev[1]));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]);
+        const double per_sweep = ms / (reps / 2) / 2.0;
+        if (per_sweep < best.sweep_ms) {
+            best = t;
+            best.sweep_ms = per_sweep;
+        }
+    }
     b->tune = best;
     const lbm_status s = build_items(b);
     if (s != LBM_OK) return s;

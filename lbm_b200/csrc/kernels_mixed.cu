@@ -186,93 +186,23 @@ sweep_kernel64(Geom g, const float* __restrict__ hin, float* __restrict__ hout,
     collide_h_store(hv, (double)sum_q32(hv), __ldg(omega + c), __ldg(s + c), hout, g.n, c);
 }
 
-// Two sweeps in one pass (temporal blocking).  A CTA owns an xy tile of
-// TX x TY output cells and a run of `zlen` planes.  Marching in z it computes
-// sweep k on the tile plus a one-cell xy halo (pulling from global memory)
-// into a ring of shared-memory planes, then sweep k+1 on the tile by pulling
-// from that ring, and writes only the second result.  Halo cells use wrapped
-// coordinates, so the periodic stream and the x slip overwrite are those of
-// two single sweeps, and each cell's arithmetic is sweep_kernel's (collide_h,
-// sum_q32).
-// Each of the CTA's threads owns one cell of the halo region for the whole z
-// march and keeps the global pulls of the NEXT plane in flight (registers)
-// while the CTA works through the shared-memory phase of the current one, so
-// load latency overlaps the ring reads, the second collision and the stores.
-// The ring has four plane slots: the slot written at iteration z+1 was last
-// read at iteration z-1, which every thread has left when it passes the single
-// barrier of iteration z.
-// Requires lx % TX == 0, ly % TY == 0 and 15 n < 2^31 (the launcher checks).
+// Two sweeps in one pass (temporal blocking, sweep2_run in mixed_cells.cuh):
+// one CTA per 32 x 8 tile of output cells and run of `zlen` planes; sweep k
+// on the tile plus its one-cell halo goes into a shared-memory plane ring,
+// sweep k+1 pulls from the ring and only the second result is written.
+// Requires lx % 32 == 0, ly % 8 == 0 and 15 n < 2^31 (the launcher checks).
 constexpr int S2_TX = 32, S2_TY = 8;
-constexpr int S2_RX = S2_TX + 2, S2_RY = S2_TY + 2, S2_RC = S2_RX * S2_RY;
-constexpr int S2_THREADS = (S2_RC + 31) / 32 * 32;   // 352: one thread per region cell
-constexpr int S2_SLOTS = 4;
-constexpr int S2_SMEM = S2_SLOTS * Q * S2_RC * (int)sizeof(float);
+constexpr int S2_THREADS = sweep2_threads(S2_TX, S2_TY);   // 352: one thread per region cell
+constexpr int S2_SMEM = sweep2_smem(S2_TX, S2_TY);
 
 __global__ void __launch_bounds__(S2_THREADS, 2)
 sweep2_kernel(Geom g, int zlen, const float* __restrict__ hin, float* __restrict__ hout,
               const float* __restrict__ omega, const float* __restrict__ s)
 {
-    extern __shared__ float ring[];   // [S2_SLOTS][Q][S2_RC]
-    const int t = threadIdx.x;
-    const int n = (int)g.n;
-    const int x0 = blockIdx.x * S2_TX, y0 = blockIdx.y * S2_TY;
+    extern __shared__ float ring[];
     const int z0 = blockIdx.z * zlen;
-    const int z1 = min(z0 + zlen, g.lz);
-    // this thread's halo-region cell (wrapped coordinates)
-    const bool owner = t < S2_RC;
-    const int xw = (x0 - 1 + t % S2_RX + g.lx) % g.lx;
-    const int yw = (y0 - 1 + t / S2_RX + g.ly) % g.ly;
-    auto slot_of = [&](int zz) { return ring + ((zz + S2_SLOTS) & (S2_SLOTS - 1)) * (Q * S2_RC); };
-
-    float a[Q];
-    float a_om = 0.f, a_s = 0.f;
-    auto prefetch = [&](int zz) {        // issue sweep k's pulls for plane zz
-        if (!owner) return;
-        const int zw = zz < 0 ? zz + g.lz : (zz >= g.lz ? zz - g.lz : zz);
-        pull_regs32(a, hin, n, g, xw, yw, zw);
-        const int c = (zw * g.ly + yw) * g.lx + xw;
-        a_om = __ldg(omega + c);
-        a_s = __ldg(s + c);
-    };
-    auto finish = [&](int zz) {          // complete sweep k on plane zz into its ring slot
-        if (!owner) return;
-        bounce_regs(a, g, xw);
-        const float p32 = sum_q32(a);
-        float* slot = slot_of(zz);
-        static_for<0, Q>([&](auto qc) {
-            constexpr int q = decltype(qc)::value;
-            slot[q * S2_RC + t] = collide_h<q>(a[q], p32, a_om, a_s);
-        });
-    };
-
-    prefetch(z0 - 1);
-    finish(z0 - 1);
-    prefetch(z0);
-    finish(z0);
-    prefetch(z0 + 1);
-    const int tx = t % S2_TX, ty = t / S2_TX;
-    const int x = x0 + tx, y = y0 + ty;
-    const int rc = (ty + 1) * S2_RX + (tx + 1);
-    for (int z = z0; z < z1; ++z) {
-        finish(z + 1);
-        if (z + 1 < z1) prefetch(z + 2);
-        __syncthreads();
-        if (t < S2_TX * S2_TY) {
-            // sweep k+1 at (x, y, z): pull from the ring (planes z-1, z, z+1)
-            const float* sm = slot_of(z - 1);
-            const float* s0 = slot_of(z);
-            const float* sp = slot_of(z + 1);
-            float hv[Q];
-            static_for<0, Q>([&](auto qc) {
-                constexpr int q = decltype(qc)::value;
-                const float* slot = pick_t<-cz(q)>(sm, s0, sp);
-                hv[q] = slot[q * S2_RC + rc - cy(q) * S2_RX - cx(q)];
-            });
-            bounce_regs(hv, g, x);
-            const int c = (z * g.ly + y) * g.lx + x;
-            collide_h_store32(hv, sum_q32(hv), __ldg(omega + c), __ldg(s + c), hout, n, c);
-        }
-    }
+    sweep2_run<S2_TX, S2_TY>(g, blockIdx.x * S2_TX, blockIdx.y * S2_TY, z0, min(z0 + zlen, g.lz), hin, hout, omega,
+                             s, ring);
 }
 
 __global__ void __launch_bounds__(256)

@@ -106,6 +106,7 @@ def test_batch_tuning_changes_no_result():
     chosen = b.tune()
     assert (chosen["tile_x"], chosen["tile_y"]) in ((32, 8), (16, 16), (8, 32))
     assert chosen["zrun"] in (1, 2, 4, 8) and chosen["ctas_per_sm"] in (2, 4, 8) and chosen["sweep_ms"] > 0
+    assert chosen["sweep2_zrun"] in (0, 8, 16, 32)
     assert b.tuning()["zrun"] == chosen["zrun"]
     counts = [[200] * len(ps)] * 2
     a.step_replay(counts)
@@ -140,3 +141,25 @@ def test_batch_workload_steps_and_conserves_mass():
     for a, c in zip(s1, s3):
         assert a["converged"] == 1 and c["converged"] == 1
         assert abs(c["mass"] - a["mass"]) <= 1e-6 * abs(a["mass"])
+
+
+@pytest.mark.parametrize("zrun2", [8, 3])
+def test_batch_two_sweep_pass_matches_single_sweeps(zrun2):
+    """Two plain sweeps per launch (temporal blocking on 16 x 8 tiles, any box
+    side: partial x and z tiles included) evaluate every cell as single sweeps
+    do, so the instances' fields are bitwise equal."""
+    cases = uneven_cases()
+    ps, fs = [p for p, _ in cases], [f for _, f in cases]
+    a = L.Batch(ps, fs)
+    b = L.Batch(ps, fs)
+    a.set_tuning(32, 8, 4, 4, 0)
+    b.set_tuning(32, 8, 4, 4, zrun2)
+    counts = [[300, 200, 400, 100, 300]] * 2
+    for x in (a, b):
+        x.set_poisson(max_sweeps=CAP, fail_on_limit=True)
+        x.step_replay(counts)
+    for i in range(len(ps)):
+        fa, fb = a.download_fields(i), b.download_fields(i)
+        for k in L.FIELDS:
+            assert np.array_equal(fa[k], fb[k]), (i, k)
+    assert b.timing()["fused_sweeps"] > 0 and a.timing()["fused_sweeps"] == 0
