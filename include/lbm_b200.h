@@ -156,6 +156,14 @@ typedef struct {
     uint64_t valid_count;
 } lbm_field_stats;
 
+/* All step statistics at once (Inamuro::collectDiagnostics,
+ * CPU/Inamuro.cpp:412-507, the DiagnosticsSnapshot of CPU/Inamuro.hpp), in
+ * its field order: rho, phi (fei), u, v, w, velocity magnitude
+ * sqrt(u*u + v*v + w*w), p. */
+typedef struct {
+    lbm_field_stats rho, fei, u, v, w, velocity_magnitude, p;
+} lbm_diagnostics;
+
 /* One Poisson convergence check (the row InamuroCUDA::writePoissonDiagnostic
  * appends to the diagnostics CSV, GPU/InamuroCUDA.cu:2634-2682). */
 typedef struct {
@@ -268,6 +276,12 @@ lbm_status lbm_field_statistics(lbm_handle* h, lbm_field which, lbm_field_stats*
  * 458,752 bytes, plus one result record; every GPU that loads the library keeps
  * that much reserved until the process exits). */
 #define LBM_NOALLOC_MAX_CELLS 33554432ULL
+
+/* Inamuro::collectDiagnostics on the device: the statistics of every field
+ * and of the velocity magnitude in one call (fixed-order reductions; the
+ * mean of a field may differ from the reference's serial sum in the last
+ * bits).  The step_diagnostics.csv columns of CPU/InamuroSolver.cpp:276-334. */
+lbm_status lbm_diagnostics_snapshot(lbm_handle* h, lbm_diagnostics* out);
 
 /* Same statistics as lbm_field_statistics for a caller-owned device field of
  * n_cells doubles, without allocating anything.  It has no counterpart in the

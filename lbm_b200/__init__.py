@@ -102,6 +102,15 @@ class FieldStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Diagnostics(C.Structure):
+    """lbm_diagnostics: Inamuro::DiagnosticsSnapshot (CPU/Inamuro.cpp:412-507)."""
+    NAMES = ("rho", "fei", "u", "v", "w", "velocity_magnitude", "p")
+    _fields_ = [(k, FieldStats) for k in NAMES]
+
+    def as_dict(self):
+        return {k: getattr(self, k).as_dict() for k in self.NAMES}
+
+
 class LBMError(RuntimeError):
     def __init__(self, status: int, message: str = ""):
         name = STATUS.get(status, str(status))
@@ -146,6 +155,7 @@ def load_library(path: str = LIB_PATH):
     L.lbm_field_statistics.argtypes = [H, C.c_int, C.POINTER(FieldStats)]
     L.lbm_field_statistics_noalloc.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p,
                                                C.POINTER(FieldStats)]
+    L.lbm_diagnostics_snapshot.argtypes = [H, C.POINTER(Diagnostics)]
     L.lbm_get_timing.argtypes = [H, C.POINTER(Timing)]
     L.lbm_reset_timing.argtypes = [H]
     L.lbm_set_timing.argtypes = [H, C.c_int]
@@ -353,6 +363,12 @@ class InamuroCUDA:
         self._check(self._lib.lbm_field_statistics(self._h, FIELD_ID[name], C.byref(st)),
                     "field_statistics")
         return st.as_dict()
+
+    def diagnostics(self) -> Dict[str, Dict[str, float]]:
+        """Inamuro::collectDiagnostics on the device (lbm_diagnostics_snapshot)."""
+        d = Diagnostics()
+        self._check(self._lib.lbm_diagnostics_snapshot(self._h, C.byref(d)), "diagnostics_snapshot")
+        return d.as_dict()
 
     # -- Poisson configuration --------------------------------------------
     def set_poisson(self, check_interval: int = 100, tolerance: float = 1e-3, dual: bool = False,

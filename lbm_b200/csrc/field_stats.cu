@@ -22,9 +22,27 @@ namespace {
 
 enum { T_SUM = 0, T_CNT, T_NAN, T_INF, T_MIN, T_MAX, T_AMAX };
 
+// Value sources of the partial pass: a field, or the velocity magnitude
+// sqrt(u*u + v*v + w*w) of three fields (the reference's vel_mag, in FP64).
 template <class T>
+struct FieldSrc {
+    const T* f;
+    __device__ __forceinline__ double operator()(long long i) const { return static_cast<double>(f[i]); }
+};
+
+template <class T>
+struct VelMagSrc {
+    const T *u, *v, *w;
+    __device__ __forceinline__ double operator()(long long i) const
+    {
+        const double a = static_cast<double>(u[i]), b = static_cast<double>(v[i]), c = static_cast<double>(w[i]);
+        return sqrt(a * a + b * b + c * c);
+    }
+};
+
+template <class Src>
 __global__ void __launch_bounds__(256)
-stats_partial_kernel(const T* __restrict__ f, long long n, double* __restrict__ part, long long nblocks)
+stats_partial_kernel(Src src, long long n, double* __restrict__ part, long long nblocks)
 {
     double v[kStatsTerms] = {0.0, 0.0, 0.0, 0.0, CUDART_INF, -CUDART_INF, 0.0};
     const long long base = (long long)blockIdx.x * kStatsCellsPerBlock + threadIdx.x;
@@ -32,7 +50,7 @@ stats_partial_kernel(const T* __restrict__ f, long long n, double* __restrict__ 
     for (int k = 0; k < kStatsCellsPerBlock / 256; ++k) {
         const long long i = base + 256LL * k;
         if (i < n) {
-            const double x = static_cast<double>(f[i]);
+            const double x = src(i);
             if (isnan(x)) {
                 v[T_NAN] += 1.0;
             } else if (isinf(x)) {
@@ -125,13 +143,28 @@ cudaError_t field_stats(cudaStream_t st, const T* f, long long n, double* partia
 {
     const long long nb = stats_blocks(n);
     if (nb <= 0 || nb > 0x7fffffffLL) return cudaErrorInvalidValue;
-    stats_partial_kernel<T><<<static_cast<unsigned>(nb), 256, 0, st>>>(f, n, partials, nb);
+    stats_partial_kernel<<<static_cast<unsigned>(nb), 256, 0, st>>>(FieldSrc<T>{f}, n, partials, nb);
+    stats_final_kernel<<<1, 1024, 0, st>>>(partials, nb, dev_out);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t velmag_stats(cudaStream_t st, const T* u, const T* v, const T* w, long long n, double* partials,
+                         lbm_field_stats* dev_out)
+{
+    const long long nb = stats_blocks(n);
+    if (nb <= 0 || nb > 0x7fffffffLL) return cudaErrorInvalidValue;
+    stats_partial_kernel<<<static_cast<unsigned>(nb), 256, 0, st>>>(VelMagSrc<T>{u, v, w}, n, partials, nb);
     stats_final_kernel<<<1, 1024, 0, st>>>(partials, nb, dev_out);
     return cudaGetLastError();
 }
 
 template cudaError_t field_stats<double>(cudaStream_t, const double*, long long, double*, lbm_field_stats*);
 template cudaError_t field_stats<float>(cudaStream_t, const float*, long long, double*, lbm_field_stats*);
+template cudaError_t velmag_stats<double>(cudaStream_t, const double*, const double*, const double*, long long,
+                                          double*, lbm_field_stats*);
+template cudaError_t velmag_stats<float>(cudaStream_t, const float*, const float*, const float*, long long, double*,
+                                         lbm_field_stats*);
 
 }  // namespace lbm
 

@@ -20,4 +20,9 @@ template <class T>
 cudaError_t field_stats(cudaStream_t st, const T* f, long long n, double* partials,
                         lbm_field_stats* dev_out);
 
+// The same for the velocity magnitude sqrt(u*u + v*v + w*w).
+template <class T>
+cudaError_t velmag_stats(cudaStream_t st, const T* u, const T* v, const T* w, long long n, double* partials,
+                         lbm_field_stats* dev_out);
+
 }  // namespace lbm

@@ -77,7 +77,7 @@ struct lbm_handle {
     int fuse_zlen = 0;                   // FP64: >0 runs plain sweeps two per launch
     int collide_zlen = 0;                // FP64: >0 runs the z-marching collide
     double* stats_part = nullptr;        // field-statistics partials
-    lbm_field_stats* stats_dev = nullptr;
+    lbm_field_stats* stats_dev = nullptr;   // 7 results (lbm_diagnostics)
 };
 
 namespace {
@@ -572,7 +572,7 @@ lbm_status lbm_create(const lbm_params* prm, lbm_precision precision, int device
     if (cudaMalloc(&h->ds, sizeof(DevState)) != cudaSuccess) return bail(LBM_ERR_OOM);
     if (cudaMallocHost(&h->ds_host, sizeof(DevState)) != cudaSuccess) return bail(LBM_ERR_OOM);
     if (cudaMalloc(&h->stats_part, sizeof(double) * kStatsTerms * stats_blocks(h->geom.n)) != cudaSuccess ||
-        cudaMalloc(&h->stats_dev, sizeof(lbm_field_stats)) != cudaSuccess)
+        cudaMalloc(&h->stats_dev, 7 * sizeof(lbm_field_stats)) != cudaSuccess)
         return bail(LBM_ERR_OOM);
     std::memset(h->ds_host, 0, sizeof(DevState));
     if (precision == LBM_PRECISION_FP64) st = alloc_fp64(h);
@@ -795,6 +795,38 @@ lbm_status lbm_field_statistics(lbm_handle* h, lbm_field which, lbm_field_stats*
     if (e != cudaSuccess) return fail(h, LBM_ERR_CUDA, std::string("field statistics: ") + cudaGetErrorString(e));
     LBM_CUDA(h, cudaMemcpyAsync(out, h->stats_dev, sizeof(lbm_field_stats), cudaMemcpyDeviceToHost, h->stream));
     LBM_CUDA(h, cudaStreamSynchronize(h->stream));
+    return LBM_OK;
+}
+
+lbm_status lbm_diagnostics_snapshot(lbm_handle* h, lbm_diagnostics* out)
+{
+    if (check_handle(h) != LBM_OK || !out) return fail(h, LBM_ERR_BAD_ARG, "bad diagnostics request");
+    cudaSetDevice(h->device);
+    cudaStream_t st = h->stream;
+    const long long n = h->geom.n;
+    lbm_field_stats* dst[7] = {&out->rho, &out->fei, &out->u, &out->v, &out->w, &out->velocity_magnitude, &out->p};
+    // snapshot order -> field ids (velocity magnitude handled apart)
+    const lbm_field ids[7] = {LBM_FIELD_RHO, LBM_FIELD_PHI, LBM_FIELD_U, LBM_FIELD_V, LBM_FIELD_W,
+                              LBM_FIELD_U, LBM_FIELD_P};
+    for (int k = 0; k < 7; ++k) {
+        cudaError_t e;
+        lbm_field_stats* res = h->stats_dev + k;
+        if (h->precision == LBM_PRECISION_FP64) {
+            e = (k == 5) ? velmag_stats<double>(st, h->b.u, h->b.v, h->b.w, n, h->stats_part, res)
+                         : field_stats<double>(st, field_ptr(h, ids[k]), n, h->stats_part, res);
+        } else if (k == 5) {
+            e = velmag_stats<float>(st, h->mb.u, h->mb.v, h->mb.w, n, h->stats_part, res);
+        } else {
+            const void* f = mixed_field_ptr(h->mb, static_cast<int>(ids[k]));
+            e = (ids[k] == LBM_FIELD_P) ? field_stats<double>(st, static_cast<const double*>(f), n, h->stats_part, res)
+                                        : field_stats<float>(st, static_cast<const float*>(f), n, h->stats_part, res);
+        }
+        if (e != cudaSuccess) return fail(h, LBM_ERR_CUDA, std::string("diagnostics: ") + cudaGetErrorString(e));
+    }
+    lbm_field_stats host[7];
+    LBM_CUDA(h, cudaMemcpyAsync(host, h->stats_dev, sizeof(host), cudaMemcpyDeviceToHost, st));
+    LBM_CUDA(h, cudaStreamSynchronize(st));
+    for (int k = 0; k < 7; ++k) *dst[k] = host[k];
     return LBM_OK;
 }
 
