@@ -45,9 +45,10 @@ public:
         out_ << '\n';
     }
 
-    // One row for the handle's current fields.  Time step 0 (the initial
-    // state) writes zeros in the timing and solve columns, as the reference.
-    void record(lbm_handle* h, int time_step, double step_time_ms, const PressureSolveColumns& ps)
+    // One row for the handle's current fields; returns the statistics.  Time
+    // step 0 (the initial state) writes zeros in the timing and solve
+    // columns, as the reference.
+    lbm_diagnostics record(lbm_handle* h, int time_step, double step_time_ms, const PressureSolveColumns& ps)
     {
         lbm_diagnostics d;
         const lbm_status s = lbm_diagnostics_snapshot(h, &d);
@@ -64,6 +65,7 @@ public:
                  << f->inf_count;
         out_ << '\n';
         out_.flush();
+        return d;
     }
 
 private:

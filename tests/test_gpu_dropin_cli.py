@@ -102,3 +102,60 @@ def test_reference_main_production_flags(tmp_path):
     r = subprocess.run([DROPIN, "--mode", "gpu", "--params", str(pf), "--steps", "1", "--poisson", "onepass"],
                        cwd=tmp_path, capture_output=True, text=True, timeout=120)
     assert r.returncode == 1 and "not provided by liblbm_b200" in (r.stdout + r.stderr)
+
+
+CPU_DROPIN = os.path.join(ROOT, "oracle", "_ref", "lbm_cpu_dropin")
+LBM_SIM = os.path.join(ROOT, "oracle", "_ref", "lbm_sim")
+CPU_PARAMS = """16 24 16
+1
+3
+1
+50.0 1.0
+1.0 1.0
+0.008 0.00016
+0.5 0.0005
+0.035
+1.0
+6.7
+0.09714 0.01134
+0.092 0.015
+8.0
+enable_progress=0   # key=value switches of the CPU tree
+output_dir=out/
+"""
+
+
+@pytest.mark.skipif(not (os.path.exists(CPU_DROPIN) and os.path.exists(LBM_SIM)),
+                    reason="CPU-tree programs not built (need the reference sources)")
+def test_reference_cpu_program_over_gpu_solver_matches_reference(tmp_path):
+    """The reference's CPU/main.cpp and CPU/Inamuro.cpp, unchanged, over the
+    drop-in InamuroSolver (GPU steps) against the reference's own CPU program
+    on the same params.in: equal Tecplot fields to float32 rounding and the
+    same step_diagnostics.csv (columns, sweep counts, statistics to the
+    file's 11 digits)."""
+    outs = {}
+    for name, exe in (("gpu", CPU_DROPIN), ("cpu", LBM_SIM)):
+        d = tmp_path / name
+        d.mkdir()
+        (d / "params.in").write_text(CPU_PARAMS)
+        r = subprocess.run([exe, "params.in"], cwd=d, capture_output=True, text=True, timeout=900)
+        assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+        outs[name] = d / "out"
+    n = 16 * 24 * 16
+    for step in (0, 1, 2):
+        xg, vg = tecplot_points(outs["gpu"] / f"3D{step:09d}.plt", n)
+        xc, vc = tecplot_points(outs["cpu"] / f"3D{step:09d}.plt", n)
+        assert np.array_equal(xg, xc)
+        for j in range(6):
+            scale = float(np.max(np.abs(vc[:, j])))
+            assert float(np.max(np.abs(vg[:, j].astype(np.float64) - vc[:, j]))) <= 2e-6 * max(scale, 1e-30), (step, j)
+    rows = {k: list(csv.reader(open(v / "step_diagnostics.csv"))) for k, v in outs.items()}
+    assert rows["gpu"][0] == rows["cpu"][0]
+    assert len(rows["gpu"]) == len(rows["cpu"]) == 5
+    head = rows["cpu"][0]
+    for rg, rc in zip(rows["gpu"][1:], rows["cpu"][1:]):
+        for k, name in enumerate(head):
+            if name in ("step_time_ms", "pressure_solve_ms"):
+                continue
+            a, b = float(rg[k]), float(rc[k])
+            assert abs(a - b) <= 1e-9 * max(abs(b), 1e-12), (rg[0], name, a, b)
