@@ -319,6 +319,13 @@ const char* lbm_last_error(const lbm_handle* h);
 const char* lbm_status_string(lbm_status s);
 int lbm_abi_version(void);
 
+/* Self-check of the FP64 kernels' division (a correctly rounded a/b from a
+ * reciprocal computed once per divisor, exact_div.cuh) against the IEEE
+ * division on the current device: `samples` pseudo-random operand pairs of
+ * the kinds the kernels divide (stencil constants, relaxation times,
+ * densities, arbitrary normals); *mismatches = pairs whose bits differ. */
+lbm_status lbm_selftest_division(uint64_t samples, uint64_t seed, uint64_t* mismatches);
+
 /* ---- batched boxes ------------------------------------------------------
  * Many independent droplet boxes of different sizes and physics advanced
  * together on one GPU, mixed precision (FP32 populations, FP64 pressure sums,

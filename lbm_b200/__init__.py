@@ -164,6 +164,7 @@ def load_library(path: str = LIB_PATH):
     L.lbm_status_string.argtypes = [C.c_int]
     L.lbm_status_string.restype = C.c_char_p
     L.lbm_abi_version.restype = C.c_int
+    L.lbm_selftest_division.argtypes = [C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]
     B = C.c_void_p
     L.lbm_batch_create.argtypes = [C.POINTER(Params), C.c_int, C.c_int, C.POINTER(B)]
     L.lbm_batch_destroy.argtypes = [B]
@@ -543,3 +544,14 @@ class Batch:
 
     def reset_timing(self):
         self._check(self._lib.lbm_batch_reset_timing(self._h), "batch_reset_timing")
+
+
+def selftest_division(samples: int = 1 << 30, seed: int = 12345) -> int:
+    """lbm_selftest_division: number of pseudo-random operand pairs for which
+    the FP64 kernels' division from a reciprocal differs from IEEE a/b."""
+    lib = load_library()
+    out = C.c_uint64(0)
+    st = lib.lbm_selftest_division(samples, seed, C.byref(out))
+    if st != 0:
+        raise LBMError(st, "lbm_selftest_division")
+    return int(out.value)

@@ -37,6 +37,7 @@
 #include <math_constants.h>
 
 #include "collide_zm.cuh"
+#include "exact_div.cuh"
 #include "finalize.cuh"
 #include "lbm_solver.cuh"
 
@@ -427,6 +428,7 @@ poisson_init_kernel(Geom g, int h_loaded, const double* __restrict__ hload,
     const long long c = cell_of(g, x, y, z);
     const double pv = p[c];
     const double tauh = 1.0 / rho[c] + 0.5;
+    const double inv_tauh = 1.0 / tauh;
     const double sv = s[c];
     static_for<0, Q>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
@@ -434,7 +436,7 @@ poisson_init_kernel(Geom g, int h_loaded, const double* __restrict__ hload,
         // h = p * E_q after update_hh (CPU/Inamuro.cpp:835), or the loaded h.
         const double h0 = h_loaded ? hload[(long long)q * g.n + c] : pv * E;
         const double hequ = E * pv;
-        hout[(long long)q * g.n + c] = h0 - (h0 - hequ) / tauh - (E / 3.0) * sv;
+        hout[(long long)q * g.n + c] = h0 - div_rn(h0 - hequ, tauh, inv_tauh) - (E / 3.0) * sv;
     });
 }
 
@@ -443,11 +445,12 @@ template <class I>
 __device__ __forceinline__ void collide_h_store(const double (&hv)[Q], double pv, double tauh,
                                                 double sv, double* __restrict__ hout, I n, I c)
 {
+    const double inv_tauh = 1.0 / tauh;   // the 15 quotients by tau_h come from it (exact_div.cuh)
     static_for<0, Q>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
         constexpr double E = wE(q);
         const double hequ = E * pv;
-        hout[(I)q * n + c] = hv[q] - (hv[q] - hequ) / tauh - (E / 3.0) * sv;
+        hout[(I)q * n + c] = hv[q] - div_rn(hv[q] - hequ, tauh, inv_tauh) - (E / 3.0) * sv;
     });
 }
 

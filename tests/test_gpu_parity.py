@@ -324,3 +324,12 @@ def test_fp64_periodic_x_matches_periodic_oracle_and_conserves_mass():
     for k in L.FIELDS:
         assert rel_err(gf[k], of[k]) <= 1e-10, k
     assert max(abs(m - masses[0]) for m in masses) <= 1e-12 * abs(masses[0])
+
+
+def test_exact_division_matches_ieee_division():
+    """The FP64 Poisson kernels take their 15 quotients by tau_h per cell from
+    one reciprocal (two Markstein remainder corrections, exact_div.cuh).
+    Against CUDA's IEEE division on 2^32 pseudo-random operand pairs
+    (relaxation times, densities, stencil constants and arbitrary normal
+    divisors) every quotient must be bit-identical."""
+    assert L.selftest_division(1 << 32, seed=20261203) == 0
