@@ -389,6 +389,45 @@ lbm_status lbm_batch_reset_timing(lbm_batch* b);
  * calling thread's last lbm_batch_create failed. */
 const char* lbm_batch_last_error(const lbm_batch* b);
 
+/* ---- adjoints of the explicit FP64 kernels --------------------------------
+ * Forward/backward pairs over caller-owned DEVICE buffers of one box
+ * (cell = (z*ly + y)*lx + x, populations q-major: a[q*n + cell]); each call
+ * synchronises the device.  The reference computes no derivatives: these give
+ * the building blocks of a gradient through its step.  A forward call is the
+ * FP64 kernel of the solver (bitwise the same values); the matching backward
+ * call takes the adjoint (dJ/d output) of every output and returns the adjoint
+ * of every input at the same state, i.e. the transposed Jacobian applied to
+ * it.  Backward calls need lbm_params.periodic_x = 1 (LBM_ERR_BAD_ARG
+ * otherwise): the slip walls are not differentiated.
+ *
+ * Collide (CPU/Inamuro.cpp:134-250): pull of the previous post-collision
+ * populations fin/gin, then the f and g collisions with the stencils of phi,
+ * rho, u, v, w; outputs fout, gout and the velocity derivatives u_x, v_y,
+ * w_z (the Poisson source).  The map is affine in fin and gin, so the backward
+ * call does not read them (they may be NULL there). */
+lbm_status lbm_collide_forward(const lbm_params* p, const double* fin, const double* gin, const double* phi,
+                               const double* rho, const double* u, const double* v, const double* w, double* fout,
+                               double* gout, double* dux, double* dvy, double* dwz);
+lbm_status lbm_collide_backward(const lbm_params* p, const double* fin, const double* gin, const double* phi,
+                                const double* rho, const double* u, const double* v, const double* w,
+                                const double* lam_fout, const double* lam_gout, const double* lam_dux,
+                                const double* lam_dvy, const double* lam_dwz, double* lam_fin, double* lam_gin,
+                                double* lam_phi, double* lam_rho, double* lam_u, double* lam_v, double* lam_w);
+/* Moments (CPU/Inamuro.cpp:294-346): pull of f*, g*, then phi, rho(phi)
+ * (sine interpolation between fei_G and fei_L), u*, v*, w*. */
+lbm_status lbm_moments_forward(const lbm_params* p, const double* f, const double* g, double* phi, double* rho,
+                               double* u, double* v, double* w);
+lbm_status lbm_moments_backward(const lbm_params* p, const double* phi, const double* lam_phi,
+                                const double* lam_rho, const double* lam_u, const double* lam_v, const double* lam_w,
+                                double* lam_f, double* lam_g);
+/* Velocity correction (CPU/Inamuro.cpp:794-823), in place:
+ * u -= (p(x+1) - p(x-1)) / (2 rho), likewise v, w.  The adjoints of u*, v*,
+ * w* equal those of u, v, w; backward returns those of p and rho. */
+lbm_status lbm_correct_forward(const lbm_params* p, double* u, double* v, double* w, const double* press,
+                               const double* rho);
+lbm_status lbm_correct_backward(const lbm_params* p, const double* press, const double* rho, const double* lam_u,
+                                const double* lam_v, const double* lam_w, double* lam_p, double* lam_rho);
+
 #ifdef __cplusplus
 }
 #endif

@@ -182,6 +182,9 @@ def load_library(path: str = LIB_PATH):
     L.lbm_batch_reset_timing.argtypes = [B]
     L.lbm_batch_last_error.argtypes = [B]
     L.lbm_batch_last_error.restype = C.c_char_p
+    for name, n_ptr in (("lbm_collide_forward", 12), ("lbm_collide_backward", 19), ("lbm_moments_forward", 7),
+                        ("lbm_moments_backward", 8), ("lbm_correct_forward", 5), ("lbm_correct_backward", 7)):
+        getattr(L, name).argtypes = [C.POINTER(Params)] + [C.c_void_p] * n_ptr
     if L.lbm_abi_version() != ABI_VERSION:
         raise LBMError(7, f"{path} has ABI {L.lbm_abi_version()}, these bindings expect {ABI_VERSION}; "
                           "rebuild with lbm_b200.build.build()")
@@ -555,3 +558,39 @@ def selftest_division(samples: int = 1 << 30, seed: int = 12345) -> int:
     if st != 0:
         raise LBMError(st, "lbm_selftest_division")
     return int(out.value)
+
+
+# ---- adjoints of the explicit FP64 kernels ---------------------------------
+# Thin calls over caller-owned device buffers (integer device pointers, e.g.
+# torch.Tensor.data_ptr()); argument order and meaning as in lbm_b200.h.
+def _device_call(name: str, p: Params, ptrs) -> None:
+    lib = load_library()
+    st = getattr(lib, name)(C.byref(p), *[C.c_void_p(int(x)) if x else None for x in ptrs])
+    if st != 0:
+        raise LBMError(st, name)
+
+
+def collide_forward(p, fin, gin, phi, rho, u, v, w, fout, gout, dux, dvy, dwz) -> None:
+    _device_call("lbm_collide_forward", p, (fin, gin, phi, rho, u, v, w, fout, gout, dux, dvy, dwz))
+
+
+def collide_backward(p, fin, gin, phi, rho, u, v, w, lam_fout, lam_gout, lam_dux, lam_dvy, lam_dwz,
+                     lam_fin, lam_gin, lam_phi, lam_rho, lam_u, lam_v, lam_w) -> None:
+    _device_call("lbm_collide_backward", p, (fin, gin, phi, rho, u, v, w, lam_fout, lam_gout, lam_dux, lam_dvy,
+                                             lam_dwz, lam_fin, lam_gin, lam_phi, lam_rho, lam_u, lam_v, lam_w))
+
+
+def moments_forward(p, f, g, phi, rho, u, v, w) -> None:
+    _device_call("lbm_moments_forward", p, (f, g, phi, rho, u, v, w))
+
+
+def moments_backward(p, phi, lam_phi, lam_rho, lam_u, lam_v, lam_w, lam_f, lam_g) -> None:
+    _device_call("lbm_moments_backward", p, (phi, lam_phi, lam_rho, lam_u, lam_v, lam_w, lam_f, lam_g))
+
+
+def correct_forward(p, u, v, w, press, rho) -> None:
+    _device_call("lbm_correct_forward", p, (u, v, w, press, rho))
+
+
+def correct_backward(p, press, rho, lam_u, lam_v, lam_w, lam_p, lam_rho) -> None:
+    _device_call("lbm_correct_backward", p, (press, rho, lam_u, lam_v, lam_w, lam_p, lam_rho))
