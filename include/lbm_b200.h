@@ -428,6 +428,66 @@ lbm_status lbm_correct_forward(const lbm_params* p, double* u, double* v, double
 lbm_status lbm_correct_backward(const lbm_params* p, const double* press, const double* rho, const double* lam_u,
                                 const double* lam_v, const double* lam_w, double* lam_p, double* lam_rho);
 
+/* ---- adjoint runs: gradients through whole FP64 time steps ------------------
+ * A forward run of n steps of one periodic FP64 box (lbm_params.periodic_x =
+ * 1) from loaded macro fields, then its reverse pass: given the adjoint of the
+ * final fields (dJ/d phi_T, ... for an objective J of them), the gradient of J
+ * with respect to the loaded fields and to k_f (kappa_f).  The Poisson solve
+ * is differentiated implicitly: each step's reverse pass solves one adjoint
+ * problem of the solve's fixed point (the transposed kinetic sweep, iterated
+ * to the tolerance of lbm_adjoint_cfg) instead of unrolling its sweeps, so
+ * the gradient is that of the converged solve.  The forward run keeps the
+ * state every checkpoint_interval steps; the reverse pass recomputes each
+ * interval from its checkpoint (replaying the forward's sweep counts, so the
+ * recomputed states are bitwise the forward's) and walks it backwards.
+ * Device memory: about 288 B/cell per checkpoint plus 168 B/cell per step of
+ * one interval plus about 1 kB/cell of adjoint buffers.  The reference has no
+ * derivatives. */
+typedef struct lbm_adjoint lbm_adjoint;
+
+typedef struct {
+    int checkpoint_interval;   /* steps between stored states (>= 1) */
+    int check_interval;        /* adjoint Poisson: sweeps between convergence checks (>= 1) */
+    double tolerance;          /* adjoint Poisson: stop when sum|pi - pi_prev| / sum|pi| < tolerance,
+                                  pi = sum_q of the adjoint iterate, compared across checks */
+    uint64_t max_sweeps;       /* adjoint Poisson: cap per step; 0 = none.  Reaching it returns
+                                  LBM_ERR_POISSON_BUDGET */
+} lbm_adjoint_cfg;
+
+typedef struct {
+    double grad_kappa_f;       /* dJ/dk_f */
+    uint64_t forward_steps;    /* steps of the forward run */
+    uint64_t forward_sweeps;   /* Poisson sweeps of the forward run */
+    uint64_t recompute_steps;  /* steps recomputed from checkpoints by the reverse pass */
+    uint64_t adjoint_sweeps;   /* transposed Poisson sweeps of the reverse pass */
+    double forward_ms;         /* wall time of lbm_adjoint_forward */
+    double backward_ms;        /* wall time of lbm_adjoint_backward (recomputation included) */
+} lbm_adjoint_stats;
+
+lbm_status lbm_adjoint_create(const lbm_params* p, int device, const lbm_adjoint_cfg* cfg, lbm_adjoint** out);
+void lbm_adjoint_destroy(lbm_adjoint* a);
+/* Poisson settings of the forward run (lbm_set_poisson). */
+lbm_status lbm_adjoint_set_poisson(lbm_adjoint* a, const lbm_poisson_cfg* cfg);
+/* Loads the initial macro fields (host, physical layout; p may be NULL = 0)
+ * and runs n_steps steps, keeping checkpoints.  sweeps: NULL for the Poisson
+ * exits of the settings, else a fixed sweep count per step (lbm_step_replay). */
+lbm_status lbm_adjoint_forward(lbm_adjoint* a, const double* phi, const double* rho, const double* u,
+                               const double* v, const double* w, const double* p, int n_steps,
+                               const uint64_t* sweeps);
+/* Sweep count of each forward step (n_steps entries). */
+lbm_status lbm_adjoint_sweeps(const lbm_adjoint* a, uint64_t* out);
+/* A field of the forward run's final state (host, physical layout). */
+lbm_status lbm_adjoint_download(const lbm_adjoint* a, lbm_field which, double* host);
+/* Reverse pass.  lam_*: dJ/d(final field), host, NULL = 0.  grad_*: dJ/d(loaded
+ * field), host, NULL = not wanted.  stats may be NULL. */
+lbm_status lbm_adjoint_backward(lbm_adjoint* a, const double* lam_phi, const double* lam_rho, const double* lam_u,
+                                const double* lam_v, const double* lam_w, const double* lam_p, double* grad_phi,
+                                double* grad_rho, double* grad_u, double* grad_v, double* grad_w, double* grad_p,
+                                lbm_adjoint_stats* stats);
+/* Text of the last error on this object ("" if none); with a == NULL: why the
+ * calling thread's last lbm_adjoint_create failed. */
+const char* lbm_adjoint_last_error(const lbm_adjoint* a);
+
 #ifdef __cplusplus
 }
 #endif

@@ -111,6 +111,22 @@ class Diagnostics(C.Structure):
         return {k: getattr(self, k).as_dict() for k in self.NAMES}
 
 
+class AdjointCfg(C.Structure):
+    """lbm_adjoint_cfg: checkpoint interval and the adjoint Poisson solve's exit."""
+    _fields_ = [("checkpoint_interval", C.c_int), ("check_interval", C.c_int), ("tolerance", C.c_double),
+                ("max_sweeps", C.c_uint64)]
+
+
+class AdjointStats(C.Structure):
+    """lbm_adjoint_stats."""
+    _fields_ = [("grad_kappa_f", C.c_double)] + \
+        [(k, C.c_uint64) for k in ("forward_steps", "forward_sweeps", "recompute_steps", "adjoint_sweeps")] + \
+        [("forward_ms", C.c_double), ("backward_ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class LBMError(RuntimeError):
     def __init__(self, status: int, message: str = ""):
         name = STATUS.get(status, str(status))
@@ -185,6 +201,17 @@ def load_library(path: str = LIB_PATH):
     for name, n_ptr in (("lbm_collide_forward", 12), ("lbm_collide_backward", 19), ("lbm_moments_forward", 7),
                         ("lbm_moments_backward", 8), ("lbm_correct_forward", 5), ("lbm_correct_backward", 7)):
         getattr(L, name).argtypes = [C.POINTER(Params)] + [C.c_void_p] * n_ptr
+    A = C.c_void_p
+    L.lbm_adjoint_create.argtypes = [C.POINTER(Params), C.c_int, C.POINTER(AdjointCfg), C.POINTER(A)]
+    L.lbm_adjoint_destroy.argtypes = [A]
+    L.lbm_adjoint_destroy.restype = None
+    L.lbm_adjoint_set_poisson.argtypes = [A, C.POINTER(PoissonCfg)]
+    L.lbm_adjoint_forward.argtypes = [A] + [C.c_void_p] * 6 + [C.c_int, C.POINTER(C.c_uint64)]
+    L.lbm_adjoint_sweeps.argtypes = [A, C.POINTER(C.c_uint64)]
+    L.lbm_adjoint_download.argtypes = [A, C.c_int, dp]
+    L.lbm_adjoint_backward.argtypes = [A] + [C.c_void_p] * 12 + [C.POINTER(AdjointStats)]
+    L.lbm_adjoint_last_error.argtypes = [A]
+    L.lbm_adjoint_last_error.restype = C.c_char_p
     if L.lbm_abi_version() != ABI_VERSION:
         raise LBMError(7, f"{path} has ABI {L.lbm_abi_version()}, these bindings expect {ABI_VERSION}; "
                           "rebuild with lbm_b200.build.build()")
@@ -594,3 +621,71 @@ def correct_forward(p, u, v, w, press, rho) -> None:
 
 def correct_backward(p, press, rho, lam_u, lam_v, lam_w, lam_p, lam_rho) -> None:
     _device_call("lbm_correct_backward", p, (press, rho, lam_u, lam_v, lam_w, lam_p, lam_rho))
+
+
+class Adjoint:
+    """Gradients through whole FP64 steps of one periodic box (lbm_adjoint_*):
+    forward(fields, n_steps) runs and checkpoints, backward(lam) returns
+    dJ/d(loaded fields) and dJ/dk_f for the adjoint lam of the final fields."""
+
+    def __init__(self, params: Params, checkpoint_interval: int = 100, check_interval: int = 100,
+                 tolerance: float = 1e-12, max_sweeps: int = 0, device: int = 0):
+        self._lib = load_library()
+        self.params = params
+        self.cfg = AdjointCfg(checkpoint_interval, check_interval, tolerance, max_sweeps)
+        h = C.c_void_p()
+        st = self._lib.lbm_adjoint_create(C.byref(params), device, C.byref(self.cfg), C.byref(h))
+        if st != 0:
+            why = self._lib.lbm_adjoint_last_error(None)
+            raise LBMError(st, "lbm_adjoint_create: " + (why.decode() if why else ""))
+        self._h = h
+        self.n_steps = 0
+        self.shape = (params.lz, params.ly, params.lx)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.lbm_adjoint_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, st, what):
+        if st != 0:
+            msg = self._lib.lbm_adjoint_last_error(self._h)
+            raise LBMError(st, f"{what}: {msg.decode() if msg else ''}")
+
+    def set_poisson(self, **kw):
+        cfg = PoissonCfg(100, 1e-3, 0, 0, 0)
+        for k, v in kw.items():
+            setattr(cfg, k, v)
+        self._check(self._lib.lbm_adjoint_set_poisson(self._h, C.byref(cfg)), "adjoint_set_poisson")
+
+    def forward(self, fields: Dict[str, np.ndarray], n_steps: int, sweeps: Optional[Sequence[int]] = None):
+        arrs = [np.ascontiguousarray(fields[k], dtype=np.float64) if fields.get(k) is not None else None
+                for k in FIELDS]
+        ptrs = [a.ctypes.data_as(C.c_void_p) if a is not None else None for a in arrs]
+        sw = (C.c_uint64 * n_steps)(*sweeps) if sweeps is not None else None
+        self._check(self._lib.lbm_adjoint_forward(self._h, *ptrs, n_steps, sw), "adjoint_forward")
+        self.n_steps = n_steps
+
+    def sweeps(self) -> List[int]:
+        out = (C.c_uint64 * self.n_steps)()
+        self._check(self._lib.lbm_adjoint_sweeps(self._h, out), "adjoint_sweeps")
+        return [int(x) for x in out]
+
+    def download(self, which: str) -> np.ndarray:
+        out = np.empty(self.shape)
+        self._check(self._lib.lbm_adjoint_download(self._h, FIELDS.index(which), _dp(out)), "adjoint_download")
+        return out
+
+    def backward(self, lam: Dict[str, np.ndarray]):
+        """lam: adjoints of the final fields (missing = 0).  Returns (grads, stats):
+        grads[k] = dJ/d(loaded field k); stats['grad_kappa_f'] = dJ/dk_f."""
+        lams = [np.ascontiguousarray(lam[k], dtype=np.float64) if lam.get(k) is not None else None for k in FIELDS]
+        grads = {k: np.empty(self.shape) for k in FIELDS}
+        st = AdjointStats()
+        args = [a.ctypes.data_as(C.c_void_p) if a is not None else None for a in lams] + \
+            [grads[k].ctypes.data_as(C.c_void_p) for k in FIELDS]
+        self._check(self._lib.lbm_adjoint_backward(self._h, *args, C.byref(st)), "adjoint_backward")
+        return grads, st.as_dict()

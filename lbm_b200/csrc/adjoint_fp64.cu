@@ -23,6 +23,7 @@
 #include <string>
 
 #include "../../include/lbm_b200.h"
+#include "adjoint.hpp"
 #include "lbm_solver.cuh"
 #include "phys_host.hpp"
 
@@ -77,7 +78,10 @@ enum {
 // Collide, pass 1: local adjoints of one cell.  Writes the direct adjoints of
 // the cell's own phi, rho, u, v, w (stencil contributions follow in pass 2),
 // pushes the populations' adjoints to the cells they were pulled from, and
-// stores the stencil adjoints.
+// stores the stencil adjoints.  kFirst: the first collision of a run, which
+// writes the equilibria (no populations in, no viscous term); lfin and lgin
+// (may be null) get zeros.  lkf (may be null): the cell's term of dJ/dk_f.
+template <bool kFirst>
 __global__ void __launch_bounds__(256)
 collide_adjoint_local(Geom g, Phys P, const double* __restrict__ phi, const double* __restrict__ rho,
                       const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
@@ -85,7 +89,7 @@ collide_adjoint_local(Geom g, Phys P, const double* __restrict__ phi, const doub
                       const double* __restrict__ ldvy, const double* __restrict__ ldwz, double* __restrict__ lfin,
                       double* __restrict__ lgin, double* __restrict__ lphi, double* __restrict__ lrho_out,
                       double* __restrict__ lu, double* __restrict__ lv, double* __restrict__ lw,
-                      double* __restrict__ scratch)
+                      double* __restrict__ scratch, double* __restrict__ lkf)
 {
     int x, y, z;
     if (!cell_xyz(g, x, y, z)) return;
@@ -101,6 +105,7 @@ collide_adjoint_local(Geom g, Phys P, const double* __restrict__ phi, const doub
     (void)r_lap;
     const double fei = phi[c], lr = rho[c], uu = u[c], vv = v[c], ww = w[c];
     const double mu = (lr - P.rho_G) * P.mu_slope + P.mu_G;
+    const double sum_fei = f_x * f_x + f_y * f_y + f_z * f_z;
     const double sum_rho = r_x * r_x + r_y * r_y + r_z * r_z;
     const double den = 1.0 - P.b * fei;
     const double dp0 = P.T / (den * den) - 2.0 * P.a * fei;   // d p0 / d phi
@@ -110,6 +115,7 @@ collide_adjoint_local(Geom g, Phys P, const double* __restrict__ phi, const doub
     double a_ux = ldux[c], a_uy = 0, a_uz = 0, a_vx = 0, a_vy = ldvy[c], a_vz = 0, a_wx = 0, a_wy = 0,
            a_wz = ldwz[c];
     double a_ulap = 0, a_vlap = 0, a_wlap = 0;
+    double a_kf = 0;   // sum over q of E_q Gfei_q times the adjoint of f_eq_q (the k_f Gfei term)
     const double kf1 = 1.0 - 1.0 / P.tauf, kf2 = 1.0 / P.tauf;
     const double kg1 = 1.0 - 1.0 / P.taug, kg2 = 1.0 / P.taug;
     const Wrap wr(g, x, y, z);
@@ -120,8 +126,8 @@ collide_adjoint_local(Geom g, Phys P, const double* __restrict__ phi, const doub
         const long long src = pull_src<q>(g, wr, x, y, z);
         // ---- f: out = fv (1 - 1/tau_f) + feq / tau_f ----
         const double lF = lf[(long long)q * n + c];
-        lfin[(long long)q * n + src] = lF * kf1;
-        const double le = lF * kf2;   // adjoint of f_eq
+        if (lfin) lfin[(long long)q * n + src] = kFirst ? 0.0 : lF * kf1;
+        const double le = kFirst ? lF : lF * kf2;   // adjoint of f_eq
         if constexpr (q == 0) {
             a_fei += le;
             a_chem += F * le;
@@ -139,11 +145,12 @@ collide_adjoint_local(Geom g, Phys P, const double* __restrict__ phi, const doub
             a_fy += Y * a_fe;
             a_fz += Z * a_fe;
             a_sumfei += -1.5 * CS * E * P.k_f * le;
+            a_kf += E * (4.5 * fe * fe - 1.5 * CS * sum_fei) * le;
         }
         // ---- g: out = gv (1 - 1/tau_g) + geq / tau_g + 3 E mu lapdot / rho ----
         const double lG = lg[(long long)q * n + c];
-        lgin[(long long)q * n + src] = lG * kg1;
-        const double lq = lG * kg2;   // adjoint of g_eq
+        if (lgin) lgin[(long long)q * n + src] = kFirst ? 0.0 : lG * kg1;
+        const double lq = kFirst ? lG : lG * kg2;   // adjoint of g_eq
         const double Cq = -2.0 / 3.0 * F * P.k_g;   // (2/3 F k_g / rho) sum_rho term coefficient
         a_sumrho += Cq / lr * lq;
         a_lr += -Cq * sum_rho / (lr * lr) * lq;
@@ -175,17 +182,20 @@ collide_adjoint_local(Geom g, Phys P, const double* __restrict__ phi, const doub
             a_rz += Z * a_re;
             a_sumrho += kq * (-1.5 * CS) * lq;
             a_lr += -E * P.k_g * Grho / (lr * lr) * lq;
-            // viscous term 3 E mu (c . lap u) / rho, on the output directly
-            const double lapdot = X * u_lap + Y * v_lap + Z * w_lap;
-            a_mu += 3.0 * E * lapdot / lr * lG;
-            a_lr += -3.0 * E * mu * lapdot / (lr * lr) * lG;
-            const double a_ld = 3.0 * E * mu / lr * lG;
-            a_ulap += X * a_ld;
-            a_vlap += Y * a_ld;
-            a_wlap += Z * a_ld;
+            if constexpr (!kFirst) {
+                // viscous term 3 E mu (c . lap u) / rho, on the output directly
+                const double lapdot = X * u_lap + Y * v_lap + Z * w_lap;
+                a_mu += 3.0 * E * lapdot / lr * lG;
+                a_lr += -3.0 * E * mu * lapdot / (lr * lr) * lG;
+                const double a_ld = 3.0 * E * mu / lr * lG;
+                a_ulap += X * a_ld;
+                a_vlap += Y * a_ld;
+                a_wlap += Z * a_ld;
+            }
         }
     });
     // chem = p0(phi) - k_f phi lap(phi) - k_f sum_fei / 6
+    if (lkf) lkf[c] = a_chem * (-fei * f_lap - sum_fei / 6.0) + a_kf;
     a_fei += dp0 * a_chem - P.k_f * f_lap * a_chem;
     a_flap += -P.k_f * fei * a_chem;
     a_sumfei += -P.k_f / 6.0 * a_chem;
@@ -248,6 +258,8 @@ collide_adjoint_gather(Geom g, const double* __restrict__ scratch, double* __res
 
 // Moments backward: phi = sum_q f*(x - c_q), rho = rho(phi) (the sine
 // interpolation, CPU/Inamuro.cpp:315-327), u* = sum_q c_q g*(x - c_q).
+// kAdd: add to lf, lg instead of overwriting them.
+template <bool kAdd>
 __global__ void __launch_bounds__(256)
 moments_adjoint(Geom g, Phys P, const double* __restrict__ phi, const double* __restrict__ lphi,
                 const double* __restrict__ lrho, const double* __restrict__ lu, const double* __restrict__ lv,
@@ -269,14 +281,21 @@ moments_adjoint(Geom g, Phys P, const double* __restrict__ phi, const double* __
     static_for<0, Q>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
         const long long src = pull_src<q>(g, wr, x, y, z);
-        lf[(long long)q * n + src] = a_phi;
-        lg[(long long)q * n + src] = cx(q) * au + cy(q) * av + cz(q) * aw;
+        const double vf = a_phi, vg = cx(q) * au + cy(q) * av + cz(q) * aw;
+        if constexpr (kAdd) {
+            lf[(long long)q * n + src] += vf;
+            lg[(long long)q * n + src] += vg;
+        } else {
+            lf[(long long)q * n + src] = vf;
+            lg[(long long)q * n + src] = vg;
+        }
     });
 }
 
 // Correction backward: u = u* - (p(x+1) - p(x-1)) / (2 rho), likewise v, w.
 // lu, lv, lw: adjoints of u, v, w (= those of u*, v*, w*); outputs the
-// adjoints of p and rho.
+// adjoints of p and rho (kAdd: added to lp, lrho).
+template <bool kAdd>
 __global__ void __launch_bounds__(256)
 correct_adjoint(Geom g, const double* __restrict__ p, const double* __restrict__ rho,
                 const double* __restrict__ lu, const double* __restrict__ lv, const double* __restrict__ lw,
@@ -296,11 +315,212 @@ correct_adjoint(Geom g, const double* __restrict__ p, const double* __restrict__
         const double grad = p[cp] - p[cm];
         ar += la[a][t] * grad / (2.0 * rho[t] * rho[t]);
     }
-    lp[t] = ap;
-    lrho[t] = ar;
+    if constexpr (kAdd) {
+        lp[t] += ap;
+        lrho[t] += ar;
+    } else {
+        lp[t] = ap;
+        lrho[t] = ar;
+    }
+}
+
+// ---- the implicit adjoint of the kinetic Poisson solve ---------------------
+// The forward solve iterates h <- K h - E s / 3 to its fixed point, with
+// K = M R: R the pull stream, M the per-cell relaxation
+// hv -> hv - (hv - E sum(hv)) / tau_h, tau_h = 1/rho + 0.5
+// (CPU/Inamuro.cpp:755-778), and p = sum_q (R h)_q.  With lam_p the adjoint
+// of p (zero mean; its mean belongs to the gauge), the multiplier mu of the
+// fixed-point equation solves mu = K^T mu + R^T 1 lam_p, K^T = R^T M^T:
+// M^T m = (1 - 1/tau) m + (sum_k E_k m_k) / tau per cell, and R^T pulls
+// from x + c_q where R pulls from x - c_q.  Iterated on y = M^T mu + lam_p:
+//   y <- M^T (pull from x + c_q of y) + lam_p,   mu_q(x) = y_q(x + c_q),
+// one sweep costs what a forward sweep does.  Then
+//   dJ/ds   = -sum_q E_q mu_q / 3,
+//   dJ/drho = -sum_q mu_q (hv_q - E_q p) / (tau^2 rho^2)   (hv = R h*).
+// The constant mode (K^T 1 = 1) only shifts dJ/ds by a constant, which the
+// source's mean projection and the periodic stencils' transposes remove.
+
+// y_q(x) = lp(x) for every q.
+__global__ void __launch_bounds__(256)
+padj_init(Geom g, const double* __restrict__ lp, double* __restrict__ y)
+{
+    int x, yy, z;
+    if (!cell_xyz(g, x, yy, z)) return;
+    const long long c = cell_of(g, x, yy, z);
+    const double v = lp[c];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) y[(long long)q * g.n + c] = v;
+}
+
+// One transposed sweep.  kCheck: also the relative change of
+// pi = sum_q y_q against the copy kept from the previous check (block
+// partials of sum |pi - pi_prev| and sum |pi|), and the new copy.
+template <bool kCheck>
+__global__ void __launch_bounds__(256)
+padj_sweep(Geom g, const double* __restrict__ yin, double* __restrict__ yout, const double* __restrict__ rho,
+           const double* __restrict__ lp, double* __restrict__ pi_prev, double* __restrict__ part,
+           long long nblocks)
+{
+    int x, yy, z;
+    const bool active = cell_xyz(g, x, yy, z);
+    double red[2] = {0.0, 0.0};
+    if (active) {
+        const long long n = g.n;
+        const long long c = cell_of(g, x, yy, z);
+        double m[Q];
+        double S = 0.0;
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            m[q] = yin[(long long)q * n + nb(g, x, yy, z, cx(q), cy(q), cz(q))];
+            S += wE(q) * m[q];
+        });
+        const double tau = 1.0 / rho[c] + 0.5;
+        const double a = 1.0 - 1.0 / tau, b = S / tau, l = lp[c];
+        double pi = 0.0;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const double v = a * m[q] + b + l;
+            yout[(long long)q * n + c] = v;
+            pi += v;
+        }
+        if constexpr (kCheck) {
+            red[0] = fabs(pi - pi_prev[c]);
+            red[1] = fabs(pi);
+            pi_prev[c] = pi;
+        }
+    }
+    if constexpr (kCheck) block_sum_store<2>(red, part, nblocks, block_linear());
+}
+
+// mu from the converged y; dJ/ds into ls, dJ/drho added to lrho.  h: the
+// forward solve's converged (post-collision) h.
+__global__ void __launch_bounds__(256)
+padj_final(Geom g, const double* __restrict__ y, const double* __restrict__ h, const double* __restrict__ rho,
+           double* __restrict__ ls, double* __restrict__ lrho)
+{
+    int x, yy, z;
+    if (!cell_xyz(g, x, yy, z)) return;
+    const long long n = g.n;
+    const long long c = cell_of(g, x, yy, z);
+    double mu[Q], hv[Q];
+    double p = 0.0, smu = 0.0;
+    static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        mu[q] = y[(long long)q * n + nb(g, x, yy, z, cx(q), cy(q), cz(q))];
+        hv[q] = h[(long long)q * n + nb(g, x, yy, z, -cx(q), -cy(q), -cz(q))];
+        p += hv[q];
+        smu += wE(q) * mu[q];
+    });
+    double t = 0.0;
+    static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        t += mu[q] * (hv[q] - wE(q) * p);
+    });
+    const double r = rho[c];
+    const double tau = 1.0 / r + 0.5;
+    ls[c] = -smu / 3.0;
+    lrho[c] += -t / (tau * tau * r * r);
+}
+
+// Source projection backward: s = (u_x - mean(u_x)) + v_y + w_z
+// (CPU/Inamuro.cpp:652-668).
+__global__ void __launch_bounds__(256)
+prep_adjoint(Geom g, const double* __restrict__ ls, double mean_ls, double* __restrict__ ldux,
+             double* __restrict__ ldvy, double* __restrict__ ldwz)
+{
+    int x, y, z;
+    if (!cell_xyz(g, x, y, z)) return;
+    const long long c = cell_of(g, x, y, z);
+    const double v = ls[c];
+    ldux[c] = v - mean_ls;
+    ldvy[c] = v;
+    ldwz[c] = v;
+}
+
+// Block partial sums of a[0..n) on a fixed grid (deterministic order).
+__global__ void __launch_bounds__(256)
+sum_partials(const double* __restrict__ a, long long n, double* __restrict__ part)
+{
+    double v[1] = {0.0};
+    for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256) v[0] += a[i];
+    block_sum_store<1>(v, part, gridDim.x, blockIdx.x);
+}
+
+__global__ void __launch_bounds__(256)
+add_const(double* __restrict__ a, long long n, double alpha)
+{
+    for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256) a[i] += alpha;
 }
 
 }  // namespace
+
+namespace adj {
+
+void collide_backward(cudaStream_t st, const Launch& L, const Geom& g, const Phys& P, bool first,
+                      const double* phi, const double* rho, const double* u, const double* v, const double* w,
+                      const double* lf, const double* lg, const double* ldux, const double* ldvy,
+                      const double* ldwz, double* lfin, double* lgin, double* lphi, double* lrho, double* lu,
+                      double* lv, double* lw, double* scratch, double* lkf)
+{
+    if (first)
+        collide_adjoint_local<true><<<L.grid, L.block, 0, st>>>(g, P, phi, rho, u, v, w, lf, lg, ldux, ldvy, ldwz,
+                                                                lfin, lgin, lphi, lrho, lu, lv, lw, scratch, lkf);
+    else
+        collide_adjoint_local<false><<<L.grid, L.block, 0, st>>>(g, P, phi, rho, u, v, w, lf, lg, ldux, ldvy, ldwz,
+                                                                 lfin, lgin, lphi, lrho, lu, lv, lw, scratch, lkf);
+    collide_adjoint_gather<<<L.grid, L.block, 0, st>>>(g, scratch, lphi, lrho, lu, lv, lw);
+}
+
+void moments_backward_add(cudaStream_t st, const Launch& L, const Geom& g, const Phys& P, const double* phi,
+                          const double* lphi, const double* lrho, const double* lu, const double* lv,
+                          const double* lw, double* lf, double* lg)
+{
+    moments_adjoint<true><<<L.grid, L.block, 0, st>>>(g, P, phi, lphi, lrho, lu, lv, lw, lf, lg);
+}
+
+void correct_backward_add(cudaStream_t st, const Launch& L, const Geom& g, const double* p, const double* rho,
+                          const double* lu, const double* lv, const double* lw, double* lp, double* lrho)
+{
+    correct_adjoint<true><<<L.grid, L.block, 0, st>>>(g, p, rho, lu, lv, lw, lp, lrho);
+}
+
+void poisson_init(cudaStream_t st, const Launch& L, const Geom& g, const double* lp, double* y)
+{
+    padj_init<<<L.grid, L.block, 0, st>>>(g, lp, y);
+}
+
+void poisson_sweep(cudaStream_t st, const Launch& L, const Geom& g, bool check, const double* yin, double* yout,
+                   const double* rho, const double* lp, double* pi_prev, double* part)
+{
+    if (check)
+        padj_sweep<true><<<L.grid, L.block, 0, st>>>(g, yin, yout, rho, lp, pi_prev, part, L.nblocks);
+    else
+        padj_sweep<false><<<L.grid, L.block, 0, st>>>(g, yin, yout, rho, lp, pi_prev, part, L.nblocks);
+}
+
+void poisson_final(cudaStream_t st, const Launch& L, const Geom& g, const double* y, const double* h,
+                   const double* rho, double* ls, double* lrho)
+{
+    padj_final<<<L.grid, L.block, 0, st>>>(g, y, h, rho, ls, lrho);
+}
+
+void prep_backward(cudaStream_t st, const Launch& L, const Geom& g, const double* ls, double mean_ls,
+                   double* ldux, double* ldvy, double* ldwz)
+{
+    prep_adjoint<<<L.grid, L.block, 0, st>>>(g, ls, mean_ls, ldux, ldvy, ldwz);
+}
+
+void sum_partials(cudaStream_t st, const double* a, long long n, double* part)
+{
+    lbm::sum_partials<<<kSumBlocks, 256, 0, st>>>(a, n, part);
+}
+
+void add_const(cudaStream_t st, double* a, long long n, double alpha)
+{
+    lbm::add_const<<<kSumBlocks, 256, 0, st>>>(a, n, alpha);
+}
+
+}  // namespace adj
 }  // namespace lbm
 
 using namespace lbm;
@@ -371,9 +591,9 @@ lbm_status lbm_collide_backward(const lbm_params* prm, const double* fin, const 
     (void)gin;
     double* scratch = nullptr;
     if (cudaMalloc(&scratch, static_cast<size_t>(A_N) * b.g.n * sizeof(double)) != cudaSuccess) return LBM_ERR_OOM;
-    collide_adjoint_local<<<b.L.grid, b.L.block>>>(b.g, b.P, phi, rho, u, v, w, lam_fout, lam_gout, lam_dux,
-                                                   lam_dvy, lam_dwz, lam_fin, lam_gin, lam_phi, lam_rho, lam_u,
-                                                   lam_v, lam_w, scratch);
+    collide_adjoint_local<false><<<b.L.grid, b.L.block>>>(b.g, b.P, phi, rho, u, v, w, lam_fout, lam_gout,
+                                                          lam_dux, lam_dvy, lam_dwz, lam_fin, lam_gin, lam_phi,
+                                                          lam_rho, lam_u, lam_v, lam_w, scratch, nullptr);
     collide_adjoint_gather<<<b.L.grid, b.L.block>>>(b.g, scratch, lam_phi, lam_rho, lam_u, lam_v, lam_w);
     const lbm_status r = finish(cudaSuccess);
     cudaFree(scratch);
@@ -403,7 +623,7 @@ lbm_status lbm_moments_backward(const lbm_params* prm, const double* phi, const 
     const lbm_status s = make_box(prm, true, b);
     if (s != LBM_OK) return s;
     if (!phi || !lam_phi || !lam_rho || !lam_u || !lam_v || !lam_w || !lam_f || !lam_g) return LBM_ERR_BAD_ARG;
-    moments_adjoint<<<b.L.grid, b.L.block>>>(b.g, b.P, phi, lam_phi, lam_rho, lam_u, lam_v, lam_w, lam_f, lam_g);
+    moments_adjoint<false><<<b.L.grid, b.L.block>>>(b.g, b.P, phi, lam_phi, lam_rho, lam_u, lam_v, lam_w, lam_f, lam_g);
     return finish(cudaSuccess);
 }
 
@@ -425,7 +645,7 @@ lbm_status lbm_correct_backward(const lbm_params* prm, const double* p, const do
     const lbm_status s = make_box(prm, true, b);
     if (s != LBM_OK) return s;
     if (!p || !rho || !lam_u || !lam_v || !lam_w || !lam_p || !lam_rho) return LBM_ERR_BAD_ARG;
-    correct_adjoint<<<b.L.grid, b.L.block>>>(b.g, p, rho, lam_u, lam_v, lam_w, lam_p, lam_rho);
+    correct_adjoint<false><<<b.L.grid, b.L.block>>>(b.g, p, rho, lam_u, lam_v, lam_w, lam_p, lam_rho);
     return finish(cudaSuccess);
 }
 

@@ -1,0 +1,476 @@
+// adjoint_run.cu -- gradients through whole FP64 time steps (lbm_adjoint_*).
+//
+// The forward run is an ordinary FP64 box (lbm_handle) stepped one step at a
+// time; every checkpoint_interval steps its state (post-collision f and g,
+// the six macro fields) is copied aside.  The reverse pass walks the
+// intervals from the last: it restores the interval's checkpoint, recomputes
+// the interval with the forward's sweep counts (bitwise the same states),
+// keeping each step's macro fields and final Poisson h, then runs the steps'
+// adjoints backwards.  One step (CPU/Inamuro.cpp:347-363) and its adjoint:
+//
+//   forward                                    reverse
+//   F', G', s' = collide(F, G, X)              4. collide^T -> lam F, G, X
+//   X* = moments(F', G')                       3. moments^T (added to lam F', G')
+//   p' = poisson(s, rho') + mean(p)            2. adjoint solve -> lam s, lam rho'
+//   u' = correct(u*, p', rho')                 1. correct^T -> lam p', lam rho'
+//
+// X = (phi, rho, u, v, w, p).  p enters the next step only through the
+// gauge target (the mean of p, CPU/Inamuro.cpp:699-705) and the solve's
+// starting guess, which the converged solve forgets: the mean of lam p' goes
+// to lam p uniformly, the rest drives the adjoint solve.  The source
+// projection s = (u_x - mean u_x) + v_y + w_z is linear.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "../../include/lbm_b200.h"
+#include "adjoint.hpp"
+#include "handle_internal.hpp"
+#include "lbm_solver.cuh"
+
+using namespace lbm;
+
+namespace {
+
+thread_local std::string g_adj_create_error;
+
+}  // namespace
+
+struct lbm_adjoint {
+    lbm_params prm{};
+    lbm_adjoint_cfg cfg{};
+    int device = 0;
+    lbm_handle* fwd = nullptr;
+    Fp64View view{};
+    long long n = 0;
+    std::string err;
+    int n_steps = 0;
+    bool have_forward = false;
+    std::vector<uint64_t> sweeps;       // per forward step
+    std::vector<double*> ckpt;          // ckpt[k]: state after step k * interval (k >= 1): f, g, 6 macro
+    double* init = nullptr;             // loaded macro fields (6 n)
+    double* final_state = nullptr;      // macro fields after the last step (6 n)
+    double* seg_macro = nullptr;        // (interval + 1) x 6 n
+    double* seg_h = nullptr;            // interval x 15 n
+    double* lpop[2][2] = {};            // [parity][f, g] adjoints of the populations, 15 n each
+    double* lmac[2] = {};               // [parity] adjoints of the 6 macro fields, 6 n each
+    double* y[2] = {};                  // adjoint Poisson iterates, 15 n each
+    double* pi_prev = nullptr;
+    double* scratch = nullptr;          // adj::kCollideScratch n
+    double* ls = nullptr;
+    double* lsrc = nullptr;             // dux, dvy, dwz adjoints, 3 n
+    double* lkf = nullptr;
+    double* part = nullptr;             // max(2 nblocks, kSumBlocks) partials
+    double* part_host = nullptr;        // pinned copy
+    size_t part_len = 0;
+    double forward_ms = 0.0;
+    uint64_t forward_sweeps = 0;
+};
+
+namespace {
+
+lbm_status afail(lbm_adjoint* a, lbm_status s, const std::string& msg)
+{
+    if (a) a->err = msg;
+    return s;
+}
+
+#define ADJ_CUDA(a, call)                                                                         \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            return afail((a), e_ == cudaErrorMemoryAllocation ? LBM_ERR_OOM : LBM_ERR_CUDA,       \
+                         std::string(#call) + ": " + cudaGetErrorString(e_));                     \
+    } while (0)
+
+#define ADJ_TRY(a, call, what)                                                                    \
+    do {                                                                                          \
+        const lbm_status s_ = (call);                                                             \
+        if (s_ != LBM_OK) {                                                                       \
+            const char* t_ = lbm_last_error((a)->fwd);                                            \
+            return afail((a), s_, std::string(what) + (t_ && *t_ ? std::string(": ") + t_ : "")); \
+        }                                                                                         \
+    } while (0)
+
+double* dalloc(size_t count, cudaError_t* e)
+{
+    void* p = nullptr;
+    *e = cudaMalloc(&p, count * sizeof(double));
+    return *e == cudaSuccess ? static_cast<double*>(p) : nullptr;
+}
+
+void free_all(lbm_adjoint* a)
+{
+    for (double* p : a->ckpt) cudaFree(p);
+    a->ckpt.clear();
+    double* bufs[] = {a->init, a->final_state, a->seg_macro, a->seg_h, a->lpop[0][0], a->lpop[0][1],
+                      a->lpop[1][0], a->lpop[1][1], a->lmac[0], a->lmac[1], a->y[0], a->y[1], a->pi_prev,
+                      a->scratch, a->ls, a->lsrc, a->lkf, a->part};
+    for (double* p : bufs) cudaFree(p);
+    if (a->part_host) cudaFreeHost(a->part_host);
+    if (a->fwd) lbm_destroy(a->fwd);
+}
+
+// Deterministic sum of a[0..n) (fixed device tree, then the host in order).
+lbm_status dsum(lbm_adjoint* a, const double* v, long long n, double* out)
+{
+    cudaStream_t st = a->view.stream;
+    adj::sum_partials(st, v, n, a->part);
+    ADJ_CUDA(a, cudaMemcpyAsync(a->part_host, a->part, adj::kSumBlocks * sizeof(double), cudaMemcpyDeviceToHost,
+                                st));
+    ADJ_CUDA(a, cudaStreamSynchronize(st));
+    double s = 0.0;
+    for (int i = 0; i < adj::kSumBlocks; ++i) s += a->part_host[i];
+    *out = s;
+    return LBM_OK;
+}
+
+}  // namespace
+
+namespace {
+
+double* slot(double* base, long long n, int i) { return base + static_cast<long long>(i) * n; }
+
+// Adjoint of one step X_n -> X_{n+1}.  On entry lpop[cur], lmac[cur] hold the
+// adjoint of X_{n+1} (F', G' and the six macro fields); on return
+// lpop[1-cur], lmac[1-cur] hold that of X_n and *kf has gained the step's
+// dJ/dk_f.  xn, x1: macro fields of X_n and X_{n+1}; h1: the h the step's
+// Poisson solve ended with.
+lbm_status step_adjoint(lbm_adjoint* a, bool first, double* const xn, double* const x1, const double* h1, int cur,
+                        uint64_t* adj_sweeps, double* kf)
+{
+    const Geom& g = a->view.geom;
+    const Phys& P = a->view.phys;
+    const Launch& L = a->view.L;
+    cudaStream_t st = a->view.stream;
+    const long long n = a->n;
+    double* lm = a->lmac[cur];
+    double* lf = a->lpop[cur][0];
+    double* lg = a->lpop[cur][1];
+    auto X1 = [&](int i) { return slot(x1, n, i); };
+    auto XN = [&](int i) { return slot(xn, n, i); };
+    auto LM = [&](int i) { return slot(lm, n, i); };
+    // 1. velocity correction
+    adj::correct_backward_add(st, L, g, X1(5), X1(1), LM(2), LM(3), LM(4), LM(5), LM(1));
+    // 2. the gauge takes the mean of lam p; the rest drives the adjoint solve
+    double sum_lp = 0.0;
+    lbm_status s = dsum(a, LM(5), n, &sum_lp);
+    if (s != LBM_OK) return s;
+    const double mean_lp = sum_lp / static_cast<double>(n);
+    adj::add_const(st, LM(5), n, -mean_lp);
+    adj::poisson_init(st, L, g, LM(5), a->y[0]);
+    ADJ_CUDA(a, cudaMemsetAsync(a->pi_prev, 0, n * sizeof(double), st));
+    const int ci = a->cfg.check_interval;
+    int yc = 0;
+    uint64_t it = 0;
+    for (;;) {
+        for (int i = 0; i < ci; ++i) {
+            const bool check = i == ci - 1;
+            adj::poisson_sweep(st, L, g, check, a->y[yc], a->y[1 - yc], X1(1), LM(5), a->pi_prev, a->part);
+            yc = 1 - yc;
+        }
+        it += static_cast<uint64_t>(ci);
+        ADJ_CUDA(a, cudaGetLastError());
+        ADJ_CUDA(a, cudaMemcpyAsync(a->part_host, a->part, 2 * L.nblocks * sizeof(double), cudaMemcpyDeviceToHost,
+                                    st));
+        ADJ_CUDA(a, cudaStreamSynchronize(st));
+        double d = 0.0, nrm = 0.0;
+        for (long long b = 0; b < L.nblocks; ++b) d += a->part_host[b];
+        for (long long b = 0; b < L.nblocks; ++b) nrm += a->part_host[L.nblocks + b];
+        if (!std::isfinite(d) || !std::isfinite(nrm))
+            return afail(a, LBM_ERR_NONFINITE, "adjoint Poisson iterate contains NaN/Inf");
+        if (nrm == 0.0 || d < a->cfg.tolerance * nrm) break;
+        if (a->cfg.max_sweeps && it >= a->cfg.max_sweeps)
+            return afail(a, LBM_ERR_POISSON_BUDGET, "adjoint Poisson sweep limit reached without convergence");
+    }
+    *adj_sweeps += it;
+    adj::poisson_final(st, L, g, a->y[yc], h1, X1(1), a->ls, LM(1));
+    // 3. source projection
+    double sum_ls = 0.0;
+    s = dsum(a, a->ls, n, &sum_ls);
+    if (s != LBM_OK) return s;
+    double* ldux = slot(a->lsrc, n, 0);
+    double* ldvy = slot(a->lsrc, n, 1);
+    double* ldwz = slot(a->lsrc, n, 2);
+    adj::prep_backward(st, L, g, a->ls, sum_ls / static_cast<double>(n), ldux, ldvy, ldwz);
+    // 4. moments, added to the adjoints of F', G'
+    adj::moments_backward_add(st, L, g, P, X1(0), LM(0), LM(1), LM(2), LM(3), LM(4), lf, lg);
+    // 5. collide, into the adjoint of X_n
+    const int nx = 1 - cur;
+    double* ln = a->lmac[nx];
+    adj::collide_backward(st, L, g, P, first, XN(0), XN(1), XN(2), XN(3), XN(4), lf, lg, ldux, ldvy, ldwz,
+                          a->lpop[nx][0], a->lpop[nx][1], slot(ln, n, 0), slot(ln, n, 1), slot(ln, n, 2),
+                          slot(ln, n, 3), slot(ln, n, 4), a->scratch, a->lkf);
+    ADJ_CUDA(a, cudaMemsetAsync(slot(ln, n, 5), 0, n * sizeof(double), st));
+    adj::add_const(st, slot(ln, n, 5), n, mean_lp);
+    ADJ_CUDA(a, cudaGetLastError());
+    double k = 0.0;
+    s = dsum(a, a->lkf, n, &k);
+    if (s != LBM_OK) return s;
+    *kf += k;
+    return LBM_OK;
+}
+
+// Restores the state at step s0 and recomputes steps s0+1 .. s1, keeping
+// X_{s0} .. X_{s1} (macro fields) and each step's final h.
+lbm_status recompute(lbm_adjoint* a, int s0, int s1)
+{
+    const long long n = a->n;
+    const size_t fbytes = static_cast<size_t>(n) * sizeof(double);
+    cudaStream_t st = a->view.stream;
+    const double* src_macro = nullptr;
+    if (s0 == 0) {
+        ADJ_TRY(a, lbm_load_fields_device(a->fwd, slot(a->init, n, 0), slot(a->init, n, 1), slot(a->init, n, 2),
+                                          slot(a->init, n, 3), slot(a->init, n, 4), slot(a->init, n, 5)),
+                "reload of the initial fields");
+        src_macro = a->init;
+    } else {
+        double* ck = a->ckpt[s0 / a->cfg.checkpoint_interval - 1];
+        const double* m[6];
+        for (int i = 0; i < 6; ++i) m[i] = slot(ck, n, 30 + i);
+        ADJ_TRY(a, fp64_restore(a->fwd, ck, slot(ck, n, 15), m), "checkpoint restore");
+        src_macro = slot(ck, n, 30);
+    }
+    ADJ_CUDA(a, cudaMemcpyAsync(a->seg_macro, src_macro, 6 * fbytes, cudaMemcpyDeviceToDevice, st));
+    for (int k = s0; k < s1; ++k) {
+        ADJ_TRY(a, lbm_step_replay(a->fwd, 1, &a->sweeps[k], nullptr), "recomputation step");
+        ADJ_TRY(a, fp64_view(a->fwd, &a->view), "state view");
+        double* dst = slot(a->seg_macro, 6 * n, k - s0 + 1);
+        for (int i = 0; i < 6; ++i)
+            ADJ_CUDA(a, cudaMemcpyAsync(slot(dst, n, i), a->view.macro[i], fbytes, cudaMemcpyDeviceToDevice, st));
+        ADJ_CUDA(a, cudaMemcpyAsync(slot(a->seg_h, 15 * n, k - s0), a->view.h_last, 15 * fbytes,
+                                    cudaMemcpyDeviceToDevice, st));
+    }
+    ADJ_CUDA(a, cudaStreamSynchronize(st));
+    return LBM_OK;
+}
+
+double ms_since(std::chrono::steady_clock::time_point t0)
+{
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+}  // namespace
+
+extern "C" {
+
+lbm_status lbm_adjoint_create(const lbm_params* p, int device, const lbm_adjoint_cfg* cfg, lbm_adjoint** out)
+{
+    g_adj_create_error.clear();
+    if (!p || !cfg || !out) {
+        g_adj_create_error = "null argument";
+        return LBM_ERR_BAD_ARG;
+    }
+    *out = nullptr;
+    if (!p->periodic_x) {
+        g_adj_create_error = "adjoint runs need periodic_x = 1 (the slip walls are not differentiated)";
+        return LBM_ERR_BAD_ARG;
+    }
+    if (cfg->checkpoint_interval < 1 || cfg->check_interval < 1 || !(cfg->tolerance > 0.0) ||
+        (cfg->max_sweeps && cfg->max_sweeps % static_cast<uint64_t>(cfg->check_interval) != 0)) {
+        g_adj_create_error = "adjoint settings: checkpoint_interval >= 1, check_interval >= 1, tolerance > 0, "
+                             "max_sweeps a multiple of check_interval";
+        return LBM_ERR_BAD_ARG;
+    }
+    lbm_adjoint* a = new lbm_adjoint();
+    a->prm = *p;
+    a->cfg = *cfg;
+    a->device = device;
+    lbm_status s = lbm_create(p, LBM_PRECISION_FP64, device, &a->fwd);
+    if (s != LBM_OK) {
+        g_adj_create_error = std::string("forward box: ") + lbm_last_error(nullptr);
+        delete a;
+        return s;
+    }
+    s = fp64_view(a->fwd, &a->view);
+    if (s != LBM_OK) {
+        g_adj_create_error = "forward box is not FP64";
+        free_all(a);
+        delete a;
+        return s;
+    }
+    const long long n = a->view.geom.n;
+    a->n = n;
+    const size_t K = static_cast<size_t>(cfg->checkpoint_interval);
+    cudaError_t e = cudaSuccess;
+    struct Req { double** dst; size_t count; };
+    const Req reqs[] = {
+        {&a->init, 6 * (size_t)n}, {&a->final_state, 6 * (size_t)n}, {&a->seg_macro, (K + 1) * 6 * (size_t)n},
+        {&a->seg_h, K * 15 * (size_t)n}, {&a->lpop[0][0], 15 * (size_t)n}, {&a->lpop[0][1], 15 * (size_t)n},
+        {&a->lpop[1][0], 15 * (size_t)n}, {&a->lpop[1][1], 15 * (size_t)n}, {&a->lmac[0], 6 * (size_t)n},
+        {&a->lmac[1], 6 * (size_t)n}, {&a->y[0], 15 * (size_t)n}, {&a->y[1], 15 * (size_t)n},
+        {&a->pi_prev, (size_t)n}, {&a->scratch, adj::kCollideScratch * (size_t)n}, {&a->ls, (size_t)n},
+        {&a->lsrc, 3 * (size_t)n}, {&a->lkf, (size_t)n}};
+    for (const Req& r : reqs) {
+        *r.dst = dalloc(r.count, &e);
+        if (e != cudaSuccess) break;
+    }
+    a->part_len = std::max<size_t>(2 * static_cast<size_t>(a->view.L.nblocks), adj::kSumBlocks);
+    if (e == cudaSuccess) a->part = dalloc(a->part_len, &e);
+    if (e == cudaSuccess) e = cudaMallocHost(&a->part_host, a->part_len * sizeof(double));
+    if (e != cudaSuccess) {
+        g_adj_create_error = std::string("adjoint buffers: ") + cudaGetErrorString(e);
+        free_all(a);
+        delete a;
+        return e == cudaErrorMemoryAllocation ? LBM_ERR_OOM : LBM_ERR_CUDA;
+    }
+    *out = a;
+    return LBM_OK;
+}
+
+void lbm_adjoint_destroy(lbm_adjoint* a)
+{
+    if (!a) return;
+    cudaSetDevice(a->device);
+    free_all(a);
+    delete a;
+}
+
+lbm_status lbm_adjoint_set_poisson(lbm_adjoint* a, const lbm_poisson_cfg* cfg)
+{
+    if (!a) return LBM_ERR_BAD_ARG;
+    ADJ_TRY(a, lbm_set_poisson(a->fwd, cfg), "forward Poisson settings");
+    return LBM_OK;
+}
+
+lbm_status lbm_adjoint_forward(lbm_adjoint* a, const double* phi, const double* rho, const double* u,
+                               const double* v, const double* w, const double* p, int n_steps,
+                               const uint64_t* sweeps)
+{
+    if (!a) return LBM_ERR_BAD_ARG;
+    if (!phi || !rho || !u || !v || !w || n_steps < 1) return afail(a, LBM_ERR_BAD_ARG, "null field or n_steps < 1");
+    cudaSetDevice(a->device);
+    const auto t0 = std::chrono::steady_clock::now();
+    a->have_forward = false;
+    const long long n = a->n;
+    const size_t fbytes = static_cast<size_t>(n) * sizeof(double);
+    cudaStream_t st = a->view.stream;
+    const double* src[6] = {phi, rho, u, v, w, p};
+    for (int i = 0; i < 6; ++i) {
+        if (src[i]) ADJ_CUDA(a, cudaMemcpyAsync(slot(a->init, n, i), src[i], fbytes, cudaMemcpyHostToDevice, st));
+        else ADJ_CUDA(a, cudaMemsetAsync(slot(a->init, n, i), 0, fbytes, st));
+    }
+    ADJ_CUDA(a, cudaStreamSynchronize(st));
+    for (double* c : a->ckpt) cudaFree(c);
+    a->ckpt.clear();
+    const int K = a->cfg.checkpoint_interval;
+    const int n_ckpt = (n_steps - 1) / K;
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < n_ckpt; ++k) {
+        double* c = dalloc(36 * static_cast<size_t>(n), &e);
+        if (e != cudaSuccess) return afail(a, LBM_ERR_OOM, "checkpoint allocation failed");
+        a->ckpt.push_back(c);
+    }
+    ADJ_TRY(a, lbm_load_fields_device(a->fwd, slot(a->init, n, 0), slot(a->init, n, 1), slot(a->init, n, 2),
+                                      slot(a->init, n, 3), slot(a->init, n, 4), slot(a->init, n, 5)),
+            "load");
+    a->sweeps.assign(n_steps, 0);
+    a->forward_sweeps = 0;
+    for (int k = 0; k < n_steps; ++k) {
+        lbm_step_stats stt{};
+        if (sweeps) ADJ_TRY(a, lbm_step_replay(a->fwd, 1, &sweeps[k], &stt), "forward step");
+        else ADJ_TRY(a, lbm_step(a->fwd, 1, &stt), "forward step");
+        a->sweeps[k] = stt.iterations;
+        a->forward_sweeps += stt.iterations;
+        ADJ_TRY(a, fp64_view(a->fwd, &a->view), "state view");
+        const int done = k + 1;
+        double* dst = nullptr;
+        if (done < n_steps && done % K == 0) {
+            double* c = a->ckpt[done / K - 1];
+            ADJ_CUDA(a, cudaMemcpyAsync(c, a->view.f, 15 * fbytes, cudaMemcpyDeviceToDevice, st));
+            ADJ_CUDA(a, cudaMemcpyAsync(slot(c, n, 15), a->view.gpop, 15 * fbytes, cudaMemcpyDeviceToDevice, st));
+            dst = slot(c, n, 30);
+        } else if (done == n_steps) {
+            dst = a->final_state;
+        }
+        if (dst)
+            for (int i = 0; i < 6; ++i)
+                ADJ_CUDA(a, cudaMemcpyAsync(slot(dst, n, i), a->view.macro[i], fbytes, cudaMemcpyDeviceToDevice, st));
+    }
+    ADJ_CUDA(a, cudaStreamSynchronize(st));
+    a->n_steps = n_steps;
+    a->have_forward = true;
+    a->forward_ms = ms_since(t0);
+    return LBM_OK;
+}
+
+lbm_status lbm_adjoint_sweeps(const lbm_adjoint* a, uint64_t* out)
+{
+    if (!a || !out || !a->have_forward) return LBM_ERR_BAD_ARG;
+    for (int k = 0; k < a->n_steps; ++k) out[k] = a->sweeps[k];
+    return LBM_OK;
+}
+
+lbm_status lbm_adjoint_download(const lbm_adjoint* a, lbm_field which, double* host)
+{
+    if (!a || !host || !a->have_forward || which < LBM_FIELD_PHI || which > LBM_FIELD_P) return LBM_ERR_BAD_ARG;
+    cudaSetDevice(a->device);
+    const cudaError_t e = cudaMemcpy(host, a->final_state + static_cast<long long>(which) * a->n,
+                                     static_cast<size_t>(a->n) * sizeof(double), cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? LBM_OK : LBM_ERR_CUDA;
+}
+
+lbm_status lbm_adjoint_backward(lbm_adjoint* a, const double* lam_phi, const double* lam_rho, const double* lam_u,
+                                const double* lam_v, const double* lam_w, const double* lam_p, double* grad_phi,
+                                double* grad_rho, double* grad_u, double* grad_v, double* grad_w, double* grad_p,
+                                lbm_adjoint_stats* stats)
+{
+    if (!a) return LBM_ERR_BAD_ARG;
+    if (!a->have_forward) return afail(a, LBM_ERR_BAD_ARG, "no forward run");
+    cudaSetDevice(a->device);
+    const auto t0 = std::chrono::steady_clock::now();
+    const long long n = a->n;
+    const size_t fbytes = static_cast<size_t>(n) * sizeof(double);
+    cudaStream_t st = a->view.stream;
+    int cur = 0;
+    ADJ_CUDA(a, cudaMemsetAsync(a->lpop[cur][0], 0, 15 * fbytes, st));
+    ADJ_CUDA(a, cudaMemsetAsync(a->lpop[cur][1], 0, 15 * fbytes, st));
+    const double* lam[6] = {lam_phi, lam_rho, lam_u, lam_v, lam_w, lam_p};
+    for (int i = 0; i < 6; ++i) {
+        if (lam[i]) ADJ_CUDA(a, cudaMemcpyAsync(slot(a->lmac[cur], n, i), lam[i], fbytes, cudaMemcpyHostToDevice, st));
+        else ADJ_CUDA(a, cudaMemsetAsync(slot(a->lmac[cur], n, i), 0, fbytes, st));
+    }
+    const int K = a->cfg.checkpoint_interval;
+    const int T = a->n_steps;
+    const int n_seg = (T + K - 1) / K;
+    double kf = 0.0;
+    uint64_t adj_sweeps = 0, recomputed = 0;
+    for (int seg = n_seg - 1; seg >= 0; --seg) {
+        const int s0 = seg * K;
+        const int s1 = std::min(T, s0 + K);
+        const lbm_status s = recompute(a, s0, s1);
+        if (s != LBM_OK) return s;
+        recomputed += static_cast<uint64_t>(s1 - s0);
+        for (int n1 = s1; n1 > s0; --n1) {
+            const int j = n1 - s0;
+            const lbm_status s2 = step_adjoint(a, n1 == 1, slot(a->seg_macro, 6 * n, j - 1),
+                                               slot(a->seg_macro, 6 * n, j), slot(a->seg_h, 15 * n, j - 1), cur,
+                                               &adj_sweeps, &kf);
+            if (s2 != LBM_OK) return s2;
+            cur = 1 - cur;
+        }
+    }
+    double* grads[6] = {grad_phi, grad_rho, grad_u, grad_v, grad_w, grad_p};
+    for (int i = 0; i < 6; ++i)
+        if (grads[i])
+            ADJ_CUDA(a, cudaMemcpyAsync(grads[i], slot(a->lmac[cur], n, i), fbytes, cudaMemcpyDeviceToHost, st));
+    ADJ_CUDA(a, cudaStreamSynchronize(st));
+    if (stats) {
+        stats->grad_kappa_f = kf;
+        stats->forward_steps = static_cast<uint64_t>(T);
+        stats->forward_sweeps = a->forward_sweeps;
+        stats->recompute_steps = recomputed;
+        stats->adjoint_sweeps = adj_sweeps;
+        stats->forward_ms = a->forward_ms;
+        stats->backward_ms = ms_since(t0);
+    }
+    return LBM_OK;
+}
+
+const char* lbm_adjoint_last_error(const lbm_adjoint* a) { return a ? a->err.c_str() : g_adj_create_error.c_str(); }
+
+}  // extern "C"

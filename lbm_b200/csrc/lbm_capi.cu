@@ -28,6 +28,7 @@
 
 #include "../../include/lbm_b200.h"
 #include "field_stats.cuh"
+#include "handle_internal.hpp"
 #include "lbm_solver.cuh"
 #include "lbm_mixed.cuh"
 #include "phys_host.hpp"
@@ -78,6 +79,7 @@ struct lbm_handle {
     int collide_zlen = 0;                // FP64: >0 runs the z-marching collide
     double* stats_part = nullptr;        // field-statistics partials
     lbm_field_stats* stats_dev = nullptr;   // 7 results (lbm_diagnostics)
+    int h_last = 0;                      // h buffer the last Poisson solve ended in
 };
 
 namespace {
@@ -360,6 +362,7 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
         LBM_CUDA(h, cudaGraphLaunch(ex, st));
         LBM_CUDA(h, cudaStreamSynchronize(st));
         hcur = end_parity;
+        h->h_last = hcur;
         // sweep-equivalents executed (plain, A, B, C) and actual launches
         // (two plain sweeps per launch where the mixed box fuses them)
         kernels += static_cast<uint64_t>(n_normal) + 2 + (dual ? 1 : 0);
@@ -495,6 +498,43 @@ void default_ghosts(lbm_handle* h)
 }
 
 }  // namespace
+
+namespace lbm {
+
+lbm_status fp64_view(lbm_handle* h, Fp64View* out)
+{
+    if (check_handle(h) != LBM_OK || !out || h->precision != LBM_PRECISION_FP64) return LBM_ERR_BAD_ARG;
+    out->geom = h->geom;
+    out->phys = h->phys;
+    out->L = h->L;
+    out->stream = h->stream;
+    out->f = h->b.f[h->fcur];
+    out->gpop = h->b.g[h->fcur];
+    double* m[6] = {h->b.phi, h->b.rho, h->b.u, h->b.v, h->b.w, h->b.p};
+    for (int i = 0; i < 6; ++i) out->macro[i] = m[i];
+    out->h_last = h->b.h[h->h_last];
+    return LBM_OK;
+}
+
+lbm_status fp64_restore(lbm_handle* h, const double* f, const double* gpop, const double* const macro[6])
+{
+    if (check_handle(h) != LBM_OK || h->precision != LBM_PRECISION_FP64 || !f || !gpop) return LBM_ERR_BAD_ARG;
+    const size_t bytes = static_cast<size_t>(h->geom.n) * sizeof(double);
+    cudaStream_t st = h->stream;
+    LBM_CUDA(h, cudaMemcpyAsync(h->b.f[h->fcur], f, 15 * bytes, cudaMemcpyDeviceToDevice, st));
+    LBM_CUDA(h, cudaMemcpyAsync(h->b.g[h->fcur], gpop, 15 * bytes, cudaMemcpyDeviceToDevice, st));
+    double* m[6] = {h->b.phi, h->b.rho, h->b.u, h->b.v, h->b.w, h->b.p};
+    for (int i = 0; i < 6; ++i) {
+        if (!macro[i]) return LBM_ERR_BAD_ARG;
+        LBM_CUDA(h, cudaMemcpyAsync(m[i], macro[i], bytes, cudaMemcpyDeviceToDevice, st));
+    }
+    LBM_CUDA(h, cudaStreamSynchronize(st));
+    h->first_step = false;
+    h->h_loaded = false;
+    return LBM_OK;
+}
+
+}  // namespace lbm
 
 extern "C" {
 

@@ -1,0 +1,157 @@
+"""Gradients through whole FP64 steps (lbm_adjoint_*): the implicit adjoint
+of the Poisson solve, the step adjoints chained backwards, checkpoints with
+recomputation.
+
+The objective mirrors the adjoint calibration workload on a small periodic
+box: J = 0.5 sum (phi_T - phi_target)^2, phi_target the final phi of a run
+with k_f raised by 5 % (plus fixed random weights on rho_T, u_T and p_T, so
+that every final field's adjoint path is exercised).  Directional
+derivatives from the reverse pass are checked against FP64 centred finite
+differences of forward runs (step 1e-6 of each field's scale) along seeded
+random directions of the loaded phi, rho, u, p and along k_f, to 1e-6
+relative.  The loaded rho enters J only through the O(k_g) capillary terms
+of the first g collision, so its directional derivative is small against J:
+at step 1e-6 the forward runs' rounding (the last bits of J move with the
+inputs, ~1e-10 of that derivative per 1e-16 of J) is of the order of the
+tolerance, so that direction uses step 1e-5 (truncation ~1e-10 relative).
+The finite-difference runs replay the base run's sweep counts, so
+J is a smooth function of the inputs; the base run's Poisson exit (relative
+change 1e-11 between checks) and the adjoint solve's (1e-13) make the
+implicit derivative and that of the replayed run agree far below 1e-6.
+Seven steps with checkpoints every three: two recomputed intervals and a
+partial one."""
+import numpy as np
+import pytest
+
+import lbm_b200 as L
+from tests.helpers import laplace_case
+
+pytestmark = pytest.mark.gpu
+SHAPE = (20, 16, 12)
+STEPS = 7
+KINT = 3
+FD_STEP = 1e-6
+TOL = 1e-6
+
+
+def setup_case():
+    p, f = laplace_case(SHAPE, DD=7.0, noise=1e-4, seed=21)
+    p.periodic_x = 1
+    rng = np.random.default_rng(5)
+    shp = f["phi"].shape
+    f["u"] = 0.005 * np.sin(2 * np.pi * np.arange(SHAPE[0]) / SHAPE[0])[None, None, :] * np.ones(shp)
+    f["w"] = 0.002 * rng.standard_normal(shp)
+    return p, f
+
+
+def poisson(obj):
+    obj.set_poisson(check_interval=100, tolerance=1e-11, max_sweeps=400000, fail_on_limit=1)
+
+
+def final_fields(p, f, sweeps=None):
+    a = L.Adjoint(p, checkpoint_interval=KINT)
+    poisson(a)
+    a.forward(f, STEPS, sweeps)
+    out = {k: a.download(k) for k in L.FIELDS}
+    counts = a.sweeps()
+    a.close()
+    return out, counts
+
+
+class Objective:
+    def __init__(self, p, f):
+        rng = np.random.default_rng(77)
+        pt = L.make_params(**{k: getattr(p, k) for k, _ in L.Params._fields_})
+        pt.k_f = p.k_f * 1.05
+        self.target = final_fields(pt, f)[0]["phi"]
+        shp = f["phi"].shape
+        self.w_rho = 1e-3 * rng.standard_normal(shp)
+        self.w_u = 1e-1 * rng.standard_normal(shp)
+        self.w_p = 1e-1 * rng.standard_normal(shp)
+
+    def value(self, y):
+        return (0.5 * np.sum((y["phi"] - self.target) ** 2) + np.sum(self.w_rho * y["rho"]) +
+                np.sum(self.w_u * y["u"]) + np.sum(self.w_p * y["p"]))
+
+    def adjoint(self, y):
+        return {"phi": y["phi"] - self.target, "rho": self.w_rho, "u": self.w_u, "p": self.w_p}
+
+
+@pytest.fixture(scope="module")
+def run():
+    p, f = setup_case()
+    obj = Objective(p, f)
+    a = L.Adjoint(p, checkpoint_interval=KINT, check_interval=50, tolerance=1e-13, max_sweeps=2000000)
+    poisson(a)
+    a.forward(f, STEPS)
+    y = {k: a.download(k) for k in L.FIELDS}
+    sweeps = a.sweeps()
+    grads, stats = a.backward(obj.adjoint(y))
+    return p, f, obj, y, sweeps, grads, stats, a
+
+
+def fd(p, f, obj, sweeps, field=None, d=None, kf=False, step=FD_STEP):
+    vals = []
+    for sgn in (1.0, -1.0):
+        pp = L.make_params(**{k: getattr(p, k) for k, _ in L.Params._fields_})
+        ff = dict(f)
+        if kf:
+            h = step * p.k_f
+            pp.k_f = p.k_f + sgn * h
+        else:
+            h = step
+            ff[field] = f[field] + sgn * h * d
+        vals.append(obj.value(final_fields(pp, ff, sweeps)[0]))
+    return (vals[0] - vals[1]) / (2 * h)
+
+
+def test_forward_matches_the_solver(run):
+    """The adjoint object's forward run is the FP64 solver's run."""
+    p, f, obj, y, sweeps, grads, stats, a = run
+    g = L.InamuroCUDA(p, f, precision="fp64")
+    g.set_poisson(check_interval=100, tolerance=1e-11, max_sweeps=400000, fail_on_limit=True)
+    st = g.step(STEPS)
+    assert [int(s["iterations"]) for s in st] == sweeps
+    for k in L.FIELDS:
+        assert np.array_equal(g.download(k), y[k]), k
+
+
+@pytest.mark.parametrize("field,seed,step", [("phi", 1, FD_STEP), ("phi", 2, FD_STEP), ("rho", 3, 1e-5),
+                                             ("u", 4, FD_STEP), ("p", 5, FD_STEP)])
+def test_gradient_matches_finite_differences(run, field, seed, step):
+    p, f, obj, y, sweeps, grads, stats, a = run
+    rng = np.random.default_rng(seed)
+    scale = max(float(np.max(np.abs(f[field]))), 1e-2)
+    d = scale * rng.standard_normal(f[field].shape)
+    want = fd(p, f, obj, sweeps, field, d, step=step)
+    got = float(np.sum(grads[field] * d))
+    assert abs(got - want) <= TOL * abs(want), (field, got, want)
+
+
+def test_kappa_f_gradient_matches_finite_differences(run):
+    p, f, obj, y, sweeps, grads, stats, a = run
+    want = fd(p, f, obj, sweeps, kf=True)
+    got = stats["grad_kappa_f"]
+    assert abs(got - want) <= TOL * abs(want), (got, want)
+
+
+def test_reverse_pass_bookkeeping(run):
+    p, f, obj, y, sweeps, grads, stats, a = run
+    assert stats["forward_steps"] == STEPS and stats["recompute_steps"] == STEPS
+    assert stats["forward_sweeps"] == sum(sweeps) and stats["adjoint_sweeps"] > 0
+    # p enters only through its mean (the gauge target): its gradient is uniform
+    gp = grads["p"]
+    assert np.ptp(gp) <= 1e-12 * max(np.max(np.abs(gp)), 1e-300)
+    # a second reverse pass on the same forward run gives the same gradient
+    g2, s2 = a.backward(obj.adjoint(y))
+    for k in L.FIELDS:
+        assert np.array_equal(g2[k], grads[k]), k
+    assert s2["grad_kappa_f"] == stats["grad_kappa_f"]
+
+
+def test_adjoint_needs_periodic_x():
+    p, f = setup_case()
+    p.periodic_x = 0
+    with pytest.raises(L.LBMError) as e:
+        L.Adjoint(p)
+    assert e.value.status == 4 and "periodic" in str(e.value)
