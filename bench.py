@@ -115,6 +115,29 @@ def batch_workload(n_instances=64, seed=2024, noise=1e-4):
     return params, fields
 
 
+def adjoint_workload(n=64, e=0.0, kf_scale=1.0, seed=31, noise=1e-4):
+    """Adjoint calibration box: n^3 periodic, one drop R = n/4 at the centre
+    (semi-axes R(1+e), R, R/(1+e); e = 0 a sphere), tanh interface W = 4,
+    rho_L/rho_G = 100, mu = 0.1 rho, a = 1, b = 6.7, T = 0.035,
+    kappa_f = 0.06 kf_scale, kappa_g = 6e-6, tau = 1, at rest, seeded phi
+    noise.  Returns (params, fields)."""
+    import lbm_b200 as L
+    R = n / 4.0
+    p = L.make_params(lx=n, ly=n, lz=n, rho_L=100.0, rho_G=1.0, mu_L=10.0, mu_G=0.1, tauf=1.0, taug=1.0,
+                      k_f=0.06 * kf_scale, k_g=6e-6, T=0.035, a=1.0, b=6.7, DD=2.0 * R, init_single_droplet=1,
+                      init_tanh=1, interface_width=2.0, init_velocity=0.0, periodic_x=1)
+    axes = (R * (1.0 + e), R, R / (1.0 + e))
+    c = (n - 1) / 2.0
+    z, y, x = np.meshgrid(np.arange(n) - c, np.arange(n) - c, np.arange(n) - c, indexing="ij")
+    re = R * np.sqrt((x / axes[0]) ** 2 + (y / axes[1]) ** 2 + (z / axes[2]) ** 2)
+    frac = 0.5 * (1.0 - np.tanh(2.0 * (re - R) / 4.0))
+    rng = np.random.default_rng(seed)
+    phi = p.fei_min + frac * (p.fei_max - p.fei_min) + rng.uniform(-noise, noise, size=frac.shape)
+    rho = p.rho_G + frac * (p.rho_L - p.rho_G)
+    zero = np.zeros_like(phi)
+    return p, {"phi": phi, "rho": rho, "u": zero, "v": zero, "w": zero, "p": zero}
+
+
 def config_dict(n, precision, dual=False):
     return {"workload": f"head-on binary droplet collision {n}^3, 2 x R=32 drops 96 apart, "
                         f"+-0.02, rho_L/rho_G=100",
@@ -503,6 +526,92 @@ def run_batch(args):
     return 0
 
 
+def run_adjoint(args):
+    """Adjoint calibration (FP64, periodic n^3, bounded sample of the
+    2000-step run): J = 0.5 sum (phi_T - phi_target)^2, phi_target the final
+    phi of a run from an ellipsoidal drop (e = 0.2) with kappa_f + 5 %.  W
+    warm-up steps on a separate box, then one forward run of K steps
+    (checkpoints every min(100, K) steps) and its reverse pass (recomputation
+    included), timed on the wall clock around the synchronous calls; the
+    gradient along kappa_f and along seeded random directions of phi_0 is
+    checked against centred finite differences (step 1e-6) of replayed runs."""
+    import lbm_b200 as L
+    n, K = args.adjoint_size, args.steps
+    tol_f, tol_a = 1e-10, 1e-13
+    p, f = adjoint_workload(n)
+    pt, ft = adjoint_workload(n, e=0.2, kf_scale=1.05)
+
+    def forward(pp, ff, sweeps=None):
+        a = L.Adjoint(pp, checkpoint_interval=min(100, K), check_interval=100, tolerance=tol_a)
+        a.set_poisson(check_interval=100, tolerance=tol_f, max_sweeps=args.max_sweeps, fail_on_limit=1)
+        a.forward(ff, K, sweeps)
+        return a
+
+    if args.warmup:
+        w = L.InamuroCUDA(p, f, precision="fp64")
+        w.set_poisson(check_interval=100, tolerance=tol_f, max_sweeps=args.max_sweeps, fail_on_limit=True)
+        w.step(args.warmup)
+        w.close()
+    tgt = forward(pt, ft)
+    target = tgt.download("phi")
+    tgt.close()
+    clk = ClockSampler(0)
+    clk.start()
+    a = forward(p, f)
+    phi_T = a.download("phi")
+    grads, st = a.backward({"phi": phi_T - target})
+    clocks = clk.stop()
+    sweeps = a.sweeps()
+    J = 0.5 * float(np.sum((phi_T - target) ** 2))
+
+    def J_of(pp, ff):
+        b = forward(pp, ff, sweeps)
+        v = 0.5 * float(np.sum((b.download("phi") - target) ** 2))
+        b.close()
+        return v
+
+    checks = []
+    h = 1e-6
+    pp = [L.make_params(**{k: getattr(p, k) for k, _ in L.Params._fields_}) for _ in range(2)]
+    pp[0].k_f, pp[1].k_f = p.k_f * (1 + h), p.k_f * (1 - h)
+    fd = (J_of(pp[0], f) - J_of(pp[1], f)) / (2 * h * p.k_f)
+    checks.append({"along": "kappa_f", "adjoint": st["grad_kappa_f"], "fd": fd,
+                   "rel_err": abs(st["grad_kappa_f"] - fd) / abs(fd)})
+    rng = np.random.default_rng(7)
+    for i in range(args.adjoint_directions):
+        d = 0.05 * rng.standard_normal(f["phi"].shape)
+        vals = []
+        for sgn in (1.0, -1.0):
+            ff = dict(f)
+            ff["phi"] = f["phi"] + sgn * h * d
+            vals.append(J_of(p, ff))
+        fd = (vals[0] - vals[1]) / (2 * h)
+        got = float(np.sum(grads["phi"] * d))
+        checks.append({"along": f"phi_0 direction {i}", "adjoint": got, "fd": fd, "rel_err": abs(got - fd) / abs(fd)})
+    cells = n ** 3
+    fwd_s, bwd_s = st["forward_ms"] / 1e3, st["backward_ms"] / 1e3
+    fwd_updates = cells * (K + st["forward_sweeps"])
+    bwd_updates = cells * (2 * st["recompute_steps"] + st["forward_sweeps"] + st["adjoint_sweeps"])
+    line = {"metric": "MLUPS (Poisson sweeps counted) of the adjoint calibration run (forward + reverse pass)",
+            "value": (fwd_updates + bwd_updates) / (fwd_s + bwd_s) / 1e6, "unit": "MLUPS", "n_gpus": 1,
+            "steps": K, "warmup": args.warmup, "ms_per_step": (st["forward_ms"] + st["backward_ms"]) / K,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded phi noise 1e-4; target from an ellipsoidal drop e=0.2, kappa_f +5%)",
+            "config": {"workload": f"adjoint calibration {n}^3 periodic, R={n // 4}, rho_L/rho_G=100, "
+                                   f"{K} of 2000 steps (bounded sample), checkpoints every {min(100, K)} steps",
+                       "poisson": {"forward_tolerance": tol_f, "adjoint_tolerance": tol_a, "check_interval": 100},
+                       "l2": "per-step state larger than L2" if cells * 288 > 126e6 else "state fits in L2"},
+            "forward_mlups": fwd_updates / fwd_s / 1e6, "reverse_mlups": bwd_updates / bwd_s / 1e6,
+            "adjoint_forward_time_ratio": bwd_s / fwd_s,
+            "forward_ms": st["forward_ms"], "backward_ms": st["backward_ms"],
+            "sweeps_per_step": {"forward": st["forward_sweeps"] / K, "adjoint": st["adjoint_sweeps"] / K},
+            "objective": J, "gradient_checks": checks,
+            "max_rel_err": max(c["rel_err"] for c in checks), "clocks": clocks}
+    print(json.dumps(line))
+    a.close()
+    return 0
+
+
 def run_ours(args):
     world, rank, local = dist_setup(args.gpus)
     n = args.size
@@ -607,8 +716,12 @@ def main(argv=None):
     ap.add_argument("--phase-timing", action="store_true",
                     help="time the non-Poisson kernels per step with --phase-sweeps sweeps per step")
     ap.add_argument("--phase-sweeps", type=int, default=100)
-    ap.add_argument("--workload", choices=("headon", "batch"), default="headon",
-                    help="batch: the batched droplet oscillation (64 uneven boxes, mixed precision)")
+    ap.add_argument("--workload", choices=("headon", "batch", "adjoint"), default="headon",
+                    help="batch: the batched droplet oscillation (64 uneven boxes, mixed precision); "
+                         "adjoint: the adjoint calibration run (FP64, 64^3), --steps forward steps")
+    ap.add_argument("--adjoint-size", type=int, default=64)
+    ap.add_argument("--adjoint-directions", type=int, default=2,
+                    help="seeded random phi_0 directions checked by finite differences")
     ap.add_argument("--batch-instances", type=int, default=64)
     ap.add_argument("--batch-seed", type=int, default=2024)
     args = ap.parse_args(argv)
@@ -618,6 +731,8 @@ def main(argv=None):
         return run_phase_timing(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "adjoint":
+        return run_adjoint(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_ours(args)

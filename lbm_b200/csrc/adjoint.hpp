@@ -33,6 +33,8 @@ void correct_backward_add(cudaStream_t st, const Launch& L, const Geom& g, const
 // relative-change partials, 2 x L.nblocks doubles); the final multiplier's
 // dJ/ds (ls) and dJ/drho (added to lrho).
 void poisson_init(cudaStream_t st, const Launch& L, const Geom& g, const double* lp, double* y);
+// pi = sum_q y_q (the first check's reference for a given starting iterate).
+void poisson_pi(cudaStream_t st, const Launch& L, const Geom& g, const double* y, double* pi);
 void poisson_sweep(cudaStream_t st, const Launch& L, const Geom& g, bool check, const double* yin, double* yout,
                    const double* rho, const double* lp, double* pi_prev, double* part);
 void poisson_final(cudaStream_t st, const Launch& L, const Geom& g, const double* y, const double* h,

@@ -352,6 +352,19 @@ padj_init(Geom g, const double* __restrict__ lp, double* __restrict__ y)
     for (int q = 0; q < Q; ++q) y[(long long)q * g.n + c] = v;
 }
 
+// pi = sum_q y_q of a starting iterate (the reference of the first check).
+__global__ void __launch_bounds__(256)
+padj_pi(Geom g, const double* __restrict__ y, double* __restrict__ pi)
+{
+    int x, yy, z;
+    if (!cell_xyz(g, x, yy, z)) return;
+    const long long c = cell_of(g, x, yy, z);
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) s += y[(long long)q * g.n + c];
+    pi[c] = s;
+}
+
 // One transposed sweep.  kCheck: also the relative change of
 // pi = sum_q y_q against the copy kept from the previous check (block
 // partials of sum |pi - pi_prev| and sum |pi|), and the new copy.
@@ -487,6 +500,11 @@ void correct_backward_add(cudaStream_t st, const Launch& L, const Geom& g, const
 void poisson_init(cudaStream_t st, const Launch& L, const Geom& g, const double* lp, double* y)
 {
     padj_init<<<L.grid, L.block, 0, st>>>(g, lp, y);
+}
+
+void poisson_pi(cudaStream_t st, const Launch& L, const Geom& g, const double* y, double* pi)
+{
+    padj_pi<<<L.grid, L.block, 0, st>>>(g, y, pi);
 }
 
 void poisson_sweep(cudaStream_t st, const Launch& L, const Geom& g, bool check, const double* yin, double* yout,

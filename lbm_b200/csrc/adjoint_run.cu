@@ -69,6 +69,7 @@ struct lbm_adjoint {
     size_t part_len = 0;
     double forward_ms = 0.0;
     uint64_t forward_sweeps = 0;
+    int y_warm = -1;                    // y buffer holding the last converged adjoint iterate, -1: none
 };
 
 namespace {
@@ -162,10 +163,16 @@ lbm_status step_adjoint(lbm_adjoint* a, bool first, double* const xn, double* co
     if (s != LBM_OK) return s;
     const double mean_lp = sum_lp / static_cast<double>(n);
     adj::add_const(st, LM(5), n, -mean_lp);
-    adj::poisson_init(st, L, g, LM(5), a->y[0]);
-    ADJ_CUDA(a, cudaMemsetAsync(a->pi_prev, 0, n * sizeof(double), st));
-    const int ci = a->cfg.check_interval;
+    // Start from the previous reverse step's converged iterate (the adjoint
+    // fields change little from one step to the next), else from y = lam p.
     int yc = 0;
+    if (a->y_warm >= 0) {
+        yc = a->y_warm;
+    } else {
+        adj::poisson_init(st, L, g, LM(5), a->y[0]);
+    }
+    adj::poisson_pi(st, L, g, a->y[yc], a->pi_prev);
+    const int ci = a->cfg.check_interval;
     uint64_t it = 0;
     for (;;) {
         for (int i = 0; i < ci; ++i) {
@@ -188,6 +195,7 @@ lbm_status step_adjoint(lbm_adjoint* a, bool first, double* const xn, double* co
             return afail(a, LBM_ERR_POISSON_BUDGET, "adjoint Poisson sweep limit reached without convergence");
     }
     *adj_sweeps += it;
+    a->y_warm = yc;
     adj::poisson_final(st, L, g, a->y[yc], h1, X1(1), a->ls, LM(1));
     // 3. source projection
     double sum_ls = 0.0;
@@ -439,6 +447,7 @@ lbm_status lbm_adjoint_backward(lbm_adjoint* a, const double* lam_phi, const dou
     const int n_seg = (T + K - 1) / K;
     double kf = 0.0;
     uint64_t adj_sweeps = 0, recomputed = 0;
+    a->y_warm = -1;
     for (int seg = n_seg - 1; seg >= 0; --seg) {
         const int s0 = seg * K;
         const int s1 = std::min(T, s0 + K);
