@@ -612,6 +612,62 @@ def run_adjoint(args):
     return 0
 
 
+def run_poisson_forms(args):
+    """The head-on workload in FP64 with each Poisson form (kinetic: the
+    production solve; scalar: the reference's scalar Jacobi form; scalar-rb:
+    red-black SOR of the same scalar equation), natural exits at the 1e-3
+    contract: W warm-up steps, K timed steps per form from the same initial
+    fields, device time from the handle's CUDA events.  Reports sweeps per
+    step, MLUPS (sweeps counted and the reference definition), the Poisson
+    phase's bandwidth on the form's algorithmic bytes (kinetic 272 B, scalar 32
+    B per cell and sweep: p in, p out, rho, s) and the error of each form's
+    fields after the run against the kinetic form's."""
+    import lbm_b200 as L
+    n = args.size
+    p = workload_params(n)
+    f = workload_fields(p)
+    cells = float(n ** 3)
+    peak, peak_kind = measured_peaks()
+    out, fields = {}, {}
+    for form in ("kinetic", "scalar", "scalar-rb"):
+        g = L.InamuroCUDA(p, f, precision="fp64")
+        g.set_poisson(check_interval=100, tolerance=1e-3, max_sweeps=args.max_sweeps)
+        g.set_poisson_form(form)
+        g.step(args.warmup)
+        g.reset_timing()
+        clk = ClockSampler(0)
+        clk.start()
+        stats = g.step(args.steps)
+        clocks = clk.stop()
+        tm = g.timing()
+        dev_s = sum(st["device_ms"] for st in stats) / 1e3
+        sweeps = sum(st["iterations"] for st in stats)
+        bytes_cell = SWEEP_BYTES["fp64"] if form == "kinetic" else 32.0
+        gbs = bytes_cell * cells * sweeps / (tm["poisson_ms"] / 1e3) / 1e9
+        out[form] = {"mlups": cells * (args.steps + sweeps) / dev_s / 1e6,
+                     "mlups_reference_definition": cells * args.steps / dev_s / 1e6,
+                     "ms_per_step": dev_s * 1e3 / args.steps, "sweeps_per_step": sweeps / args.steps,
+                     "poisson_ms_per_step": tm["poisson_ms"] / args.steps,
+                     "poisson_gbs": gbs, "poisson_frac": gbs / peak, "bytes_per_cell_sweep": bytes_cell,
+                     "converged_steps": int(sum(st["converged"] for st in stats)),
+                     "omega": g.poisson_form()["omega"], "gpu_launches": tm["kernel_launches"], "clocks": clocks}
+        fields[form] = g.download_fields()
+        g.close()
+    for form in ("scalar", "scalar-rb"):
+        out[form]["rel_err_vs_kinetic"] = {k: float(np.max(np.abs(fields[form][k] - fields["kinetic"][k])) /
+                                                    np.max(np.abs(fields["kinetic"][k]))) for k in ("phi", "u", "w", "p")}
+    out["scalar-rb"]["rel_err_vs_scalar"] = {k: float(np.max(np.abs(fields["scalar-rb"][k] - fields["scalar"][k])) /
+                                                      np.max(np.abs(fields["scalar"][k]))) for k in ("phi", "u", "w", "p")}
+    line = {"metric": "MLUPS (Poisson sweeps counted) of the Inamuro D3Q15 droplet step per Poisson form",
+            "value": out["scalar-rb"]["mlups_reference_definition"], "unit": "MLUPS (reference definition)",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(config_dict(n, "fp64"), poisson={"check_interval": 100, "tolerance": 1e-3}),
+            "peak": peak, "peak_kind": peak_kind, "forms": out}
+    print(json.dumps(line))
+    return 0
+
+
 def run_ours(args):
     world, rank, local = dist_setup(args.gpus)
     n = args.size
@@ -716,7 +772,7 @@ def main(argv=None):
     ap.add_argument("--phase-timing", action="store_true",
                     help="time the non-Poisson kernels per step with --phase-sweeps sweeps per step")
     ap.add_argument("--phase-sweeps", type=int, default=100)
-    ap.add_argument("--workload", choices=("headon", "batch", "adjoint"), default="headon",
+    ap.add_argument("--workload", choices=("headon", "batch", "adjoint", "poisson-forms"), default="headon",
                     help="batch: the batched droplet oscillation (64 uneven boxes, mixed precision); "
                          "adjoint: the adjoint calibration run (FP64, 64^3), --steps forward steps")
     ap.add_argument("--adjoint-size", type=int, default=64)
@@ -733,6 +789,8 @@ def main(argv=None):
         return run_batch(args)
     if args.workload == "adjoint":
         return run_adjoint(args)
+    if args.workload == "poisson-forms":
+        return run_poisson_forms(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_ours(args)

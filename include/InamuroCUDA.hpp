@@ -129,6 +129,10 @@ public:
             iteration_limit_ = o.iteration_limit_;
             dual_ = o.dual_;
             shadow_ = o.shadow_;
+            fused_ = o.fused_;
+            fused_boundary_ = o.fused_boundary_;
+            scalar_ = o.scalar_;
+            scalar_scale_ = o.scalar_scale_;
             diag_ = o.diag_;
             csv_path_ = o.csv_path_;
             if (h_) lbm_set_check_callback(h_, &InamuroCUDA::onCheck, this);
@@ -141,6 +145,11 @@ public:
     // One time step (performTimeStepGPU, GPU/InamuroCUDA.cu:2372-2442).
     void performTimeStepGPU()
     {
+        // The reference's own guard (GPU/InamuroCUDA.cu:1846-1856).
+        if ((dual_ || shadow_) && (fused_ || fused_boundary_ || scalar_))
+            throw std::runtime_error(
+                "fixed-point residual requires frozen split+split Poisson with unit relaxation and all "
+                "accelerators disabled");
         lbm_step_stats st{};
         const lbm_status s = lbm_step(h_, 1, &st);
         if (s == LBM_ERR_BAD_ARG) throw std::invalid_argument(lbm_last_error(h_));
@@ -196,15 +205,28 @@ public:
     const PoissonStepDiagnostics& getLastPoissonDiagnostics() const { return diag_; }
 
     // ---- settings (GPU/InamuroCUDA.hpp:67-88) ----
-    // The reference's non-production Poisson accelerators are not provided by the
-    // library; enabling one is rejected, disabling is accepted.
-    void setUseFusedPoisson(bool e) { rejectAccelerator(e, "fused Poisson"); }
+    // The fused Poisson kernel and the fused boundary+pressure kernel of the
+    // reference do the split form's arithmetic in fewer launches
+    // (GPU/InamuroCUDA.cu:539-584, 732-778): the library's sweep is that form.
+    void setUseFusedPoisson(bool e) { fused_ = e; }
+    void setUseFusedBoundaryPressure(bool e) { fused_boundary_ = e; }
+    // The scalar form (GPU/InamuroCUDA.cu:864-901): lbm_set_poisson_form.
+    void setUseScalarPoisson(bool e)
+    {
+        scalar_ = e;
+        applyPoissonForm();
+    }
+    void setScalarPoissonSourceScale(double scale)
+    {
+        scalar_scale_ = scale;
+        applyPoissonForm();
+    }
+    // The other non-production accelerators are not provided by the library;
+    // enabling one is rejected, disabling is accepted.
     void setUseOnePassPoisson(bool e) { rejectAccelerator(e, "one-pass Poisson"); }
-    void setUseScalarPoisson(bool e) { rejectAccelerator(e, "scalar Poisson"); }
     void setUseSourceAwareHHInit(bool e) { rejectAccelerator(e, "source-aware hh init"); }
     void setUsePoissonAndersonM1(bool e) { rejectAccelerator(e, "Anderson-m1"); }
     void setUsePoissonTwoGridCorrection(bool e) { rejectAccelerator(e, "two-grid correction"); }
-    void setUseFusedBoundaryPressure(bool e) { rejectAccelerator(e, "fused boundary+pressure"); }
     void setUsePoissonSpatialDiagnostics(bool e) { rejectAccelerator(e, "spatial diagnostics"); }
     // Every Poisson segment already runs as a captured CUDA graph.
     void setUsePoissonGraph(bool) {}
@@ -212,7 +234,6 @@ public:
     void setEnablePoissonDetailTiming(bool) {}
     // Reductions are always fixed-order (deterministic).
     void setUsePoissonDeterministicReductions(bool) {}
-    void setScalarPoissonSourceScale(double) {}
     void setSourceAwareHHScale(double) {}
     void setPressureRelaxScale(double scale)
     {
@@ -333,6 +354,10 @@ private:
     std::uint64_t iteration_limit_ = 0;
     bool dual_ = false;
     bool shadow_ = false;
+    bool fused_ = false;
+    bool fused_boundary_ = false;
+    bool scalar_ = false;
+    double scalar_scale_ = 2.0;
     PoissonStepDiagnostics diag_;
     std::string csv_path_;
 
@@ -356,8 +381,15 @@ private:
     {
         if (enabled)
             throw std::invalid_argument(std::string(name) +
-                                        ": the experimental Poisson accelerators are not provided by "
-                                        "liblbm_b200 (split Poisson only)");
+                                        ": this experimental Poisson accelerator is not provided by "
+                                        "liblbm_b200 (split, fused and scalar Poisson only)");
+    }
+
+    void applyPoissonForm()
+    {
+        if (!h_) return;
+        check(lbm_set_poisson_form(h_, scalar_ ? LBM_POISSON_SCALAR_JACOBI : LBM_POISSON_KINETIC, scalar_scale_, 0.0),
+              "setUseScalarPoisson");
     }
 
     void applyPoissonConfig()

@@ -236,6 +236,31 @@ lbm_status lbm_load_fields_device(lbm_handle* h, const double* phi, const double
 lbm_status lbm_set_poisson(lbm_handle* h, const lbm_poisson_cfg* cfg);
 lbm_status lbm_get_poisson(const lbm_handle* h, lbm_poisson_cfg* cfg);
 
+/* Poisson form.  LBM_POISSON_KINETIC is the reference's production solve (its
+ * split form; its fused form and fused boundary do the same arithmetic, so
+ * they are this form too).  The scalar forms are the reference's
+ * non-production scalar option (InamuroCUDA::setUseScalarPoisson,
+ * GPU/InamuroCUDA.cu:864-901, 2207-2218): the 14-neighbour stencil
+ * lap p = (sum_nb p - 14 p)/5 solved for lap p = source_scale rho s, with the
+ * same gauge and relative-change exit; its result differs from the kinetic
+ * form's (another equation).  LBM_POISSON_SCALAR_JACOBI sweeps as the
+ * reference does (Jacobi); LBM_POISSON_SCALAR_RB solves the same equation by
+ * red-black SOR (its right-hand side's mean removed, which the gauge makes
+ * immaterial), reaching the Jacobi sweeps' fixed point in far fewer sweeps.
+ * Scalar forms: FP64 only, no dual residual; red-black needs even ly, lz
+ * (and lx with periodic_x).  source_scale: the reference's
+ * --scalar-source-scale (default 2.0); omega: SOR relaxation in (0, 2), 0 =
+ * the optimum for the box's slowest mode. */
+typedef enum {
+    LBM_POISSON_KINETIC = 0,
+    LBM_POISSON_SCALAR_JACOBI = 1,
+    LBM_POISSON_SCALAR_RB = 2
+} lbm_poisson_form;
+lbm_status lbm_set_poisson_form(lbm_handle* h, lbm_poisson_form form, double source_scale, double omega);
+/* Current form, source scale and the relaxation in use (the computed optimum
+ * when 0 was set); any pointer may be NULL. */
+lbm_status lbm_get_poisson_form(const lbm_handle* h, lbm_poisson_form* form, double* source_scale, double* omega);
+
 /* Advances n_steps time steps (InamuroCUDA::performTimeStepGPU,
  * GPU/InamuroCUDA.cu:2372-2442).  `stats` (may be NULL) receives n_steps
  * entries.  On error the state is left as of the failing step. */

@@ -161,6 +161,8 @@ def load_library(path: str = LIB_PATH):
         getattr(L, name).argtypes = [H] + [C.c_void_p] * 6
     L.lbm_set_poisson.argtypes = [H, C.POINTER(PoissonCfg)]
     L.lbm_get_poisson.argtypes = [H, C.POINTER(PoissonCfg)]
+    L.lbm_set_poisson_form.argtypes = [H, C.c_int, C.c_double, C.c_double]
+    L.lbm_get_poisson_form.argtypes = [H, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.lbm_step.argtypes = [H, C.c_int, C.POINTER(StepStats)]
     L.lbm_step_replay.argtypes = [H, C.c_int, C.POINTER(C.c_uint64), C.POINTER(StepStats)]
     L.lbm_download.argtypes = [H, C.c_int, dp]
@@ -406,6 +408,22 @@ class InamuroCUDA:
                     max_sweeps: int = 0, fail_on_limit: bool = False):
         cfg = PoissonCfg(check_interval, tolerance, int(dual), max_sweeps, int(fail_on_limit))
         self._check(self._lib.lbm_set_poisson(self._h, C.byref(cfg)), "set_poisson")
+
+    POISSON_FORMS = {"kinetic": 0, "scalar": 1, "scalar-rb": 2}
+
+    def set_poisson_form(self, form: str = "kinetic", source_scale: float = 2.0, omega: float = 0.0):
+        """lbm_set_poisson_form: "kinetic" (the production solve), "scalar"
+        (the reference's scalar Jacobi form) or "scalar-rb" (red-black SOR of
+        the same scalar equation; omega 0 = the optimum for the box)."""
+        self._check(self._lib.lbm_set_poisson_form(self._h, self.POISSON_FORMS[form], source_scale, omega),
+                    "set_poisson_form")
+
+    def poisson_form(self) -> Dict[str, float]:
+        f, sc, om = C.c_int(), C.c_double(), C.c_double()
+        self._check(self._lib.lbm_get_poisson_form(self._h, C.byref(f), C.byref(sc), C.byref(om)),
+                    "get_poisson_form")
+        names = {v: k for k, v in self.POISSON_FORMS.items()}
+        return {"form": names[f.value], "source_scale": sc.value, "omega": om.value}
 
     # reference setter names (GPU/InamuroCUDA.hpp:83-86)
     def set_poisson_convergence(self, check_interval: int, tolerance: float):

@@ -123,6 +123,14 @@ __device__ void finalize_body(int kind, DevState* __restrict__ ds, const double*
         double r[1];
         reduce_partials<1>(part, stride, count, r);
         if (threadIdx.x == 0) ds->mass = r[0];
+    } else if (kind == FIN_RHS) {
+        double r[3];
+        reduce_partials<3>(part, stride, count, r);
+        if (threadIdx.x == 0) {
+            ds->rhs_mean = r[0] / r[2];
+            ds->rhs_chk = r[1] / r[2];
+            if (!isfinite(r[0]) || !isfinite(r[1])) set_error(ds, SITE_PROJECTED);
+        }
     }
 }
 

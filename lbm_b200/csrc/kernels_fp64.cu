@@ -671,6 +671,125 @@ sweep_check_c_kernel(Geom g, int zrun, const double* __restrict__ hin, double* _
     block_sum_store<3>(red, part, nblocks, block_linear());
 }
 
+// ---- scalar Poisson forms -------------------------------------------------
+// The reference's scalar form (scalarPressureJacobiKernel,
+// GPU/InamuroCUDA.cu:864-901): one Jacobi sweep of the 14-neighbour stencil,
+// p' = (sum_{q=1..14} p(x - c_q) - 5 scale rho s) / 14, x neighbours mirrored
+// at the slip walls (its pressure_bounce_direction, .cu:846-862), in the
+// reference's operand order.  Its fixed point solves lap p = scale rho s
+// with lap = (sum_nb - 14 p) / 5.
+__device__ __forceinline__ double scalar_nsum(const double* __restrict__ p, const Geom& g, const Mirror& m, int x,
+                                              int y, int z)
+{
+    double nsum = 0.0;
+    static_for<1, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        nsum = nsum + __ldg(p + cell_of(g, pick<-cx(q)>(m.xm, x, m.xp), pick<-cy(q)>(m.ym, y, m.yp),
+                                        pick<-cz(q)>(m.zm, z, m.zp)));
+    });
+    return nsum;
+}
+
+__global__ void __launch_bounds__(256)
+scalar_jacobi_kernel(Geom g, const double* __restrict__ pin, double* __restrict__ pout,
+                     const double* __restrict__ rho, const double* __restrict__ s, double scale)
+{
+    int x, y, z;
+    if (!tile_coords(g, x, y, z)) return;
+    const Mirror m(g, x, y, z);
+    const long long c = cell_of(g, x, y, z);
+    const double nsum = scalar_nsum(pin, g, m, x, y, z);
+    const double rhs = scale * __ldg(rho + c) * __ldg(s + c);
+    pout[c] = (nsum - 5.0 * rhs) / 14.0;
+}
+
+// Red-black SOR on the same equation, in place: cells with (x + y + z) % 2 ==
+// color move to p + omega (p_J - p), p_J the Jacobi value above.  The 14
+// neighbours of a cell all have the other colour (axis and body-diagonal
+// offsets are odd; even periodic extents keep it so across the wrap), so a
+// half-sweep reads only values it does not write.  For the same reason the
+// Jacobi sweep maps the checkerboard chi = (-1)^(x+y+z) to -chi: at the even
+// sweep counts of its checks it never takes up the right-hand side's chi
+// component, and the constant one is the gauge's.  Both are removed from the
+// right-hand side here (ds->rhs_mean, ds->rhs_chk), so SOR converges to the
+// Jacobi sweeps' gauged limit.
+__global__ void __launch_bounds__(256)
+rb_sor_kernel(Geom g, double* __restrict__ p, const double* __restrict__ rho, const double* __restrict__ s,
+              double scale, double omega, int color, const DevState* __restrict__ ds)
+{
+    int x, y, z;
+    if (!tile_coords(g, x, y, z) || ((x + y + z) & 1) != color) return;
+    const Mirror m(g, x, y, z);
+    const long long c = cell_of(g, x, y, z);
+    double nsum = 0.0;
+    static_for<1, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        nsum = nsum + p[cell_of(g, pick<-cx(q)>(m.xm, x, m.xp), pick<-cy(q)>(m.ym, y, m.yp),
+                                pick<-cz(q)>(m.zm, z, m.zp))];
+    });
+    const double rhs = scale * __ldg(rho + c) * __ldg(s + c) - ds->rhs_mean - (color ? -ds->rhs_chk : ds->rhs_chk);
+    const double pj = (nsum - 5.0 * rhs) / 14.0;
+    const double pv = p[c];
+    p[c] = pv + omega * (pj - pv);
+}
+
+// Block partial sums of w f, w chi f and w, f = scale rho s: the constant and
+// checkerboard components the red-black form removes, projected with the
+// weights w under which the mirrored stencil is symmetric (1/2 on the two
+// slip-wall planes, whose cells see their inner neighbours twice; 1 elsewhere).
+__global__ void __launch_bounds__(256)
+scalar_rhs_sum_kernel(Geom g, int zrun, const double* __restrict__ rho, const double* __restrict__ s,
+                      double scale, double* __restrict__ part, long long nblocks)
+{
+    int x, y, z0, z1;
+    const bool active = tile_zrun(g, zrun, x, y, z0, z1);
+    double red[3] = {0.0, 0.0, 0.0};
+    const double w = (!g.periodic_x && (x == 0 || x == g.lx - 1)) ? 0.5 : 1.0;
+    for (int z = z0; active && z < z1; ++z) {
+        const long long c = cell_of(g, x, y, z);
+        const double f = w * (scale * __ldg(rho + c) * __ldg(s + c));
+        red[0] += f;
+        red[1] += ((x + y + z) & 1) ? -f : f;
+        red[2] += w;
+    }
+    block_sum_store<3>(red, part, nblocks, block_linear());
+}
+
+// Block partial sums of p (the gauge mean of a check).
+__global__ void __launch_bounds__(256)
+p_sum_kernel(Geom g, int zrun, const double* __restrict__ p, double* __restrict__ part, long long nblocks)
+{
+    int x, y, z0, z1;
+    const bool active = tile_zrun(g, zrun, x, y, z0, z1);
+    double red[1] = {0.0};
+    for (int z = z0; active && z < z1; ++z) red[0] += p[cell_of(g, x, y, z)];
+    block_sum_store<1>(red, part, nblocks, block_linear());
+}
+
+// Check of the scalar forms: gauge p -= shift (CPU/Inamuro.cpp:699-705; the
+// h shift is moot, h = E p after the solve), relative change against the
+// previous check (:726-753), result into p.  Same partial layout as
+// sweep_check_b_kernel with the dual terms zero.
+__global__ void __launch_bounds__(256)
+scalar_check_kernel(Geom g, int zrun, const double* __restrict__ pin, double* __restrict__ p,
+                    double* __restrict__ p_prev, const DevState* __restrict__ ds, double* __restrict__ part,
+                    long long nblocks)
+{
+    int x, y, z0, z1;
+    const bool active = tile_zrun(g, zrun, x, y, z0, z1);
+    double red[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const double shift = ds->sigma;
+    for (int z = z0; active && z < z1; ++z) {
+        const long long c = cell_of(g, x, y, z);
+        const double pv = pin[c] - shift;
+        red[0] += fabs(pv - p_prev[c]);
+        red[1] += fabs(pv);
+        p_prev[c] = pv;
+        p[c] = pv;
+    }
+    block_sum_store<5>(red, part, nblocks, block_linear());
+}
+
 __global__ void __launch_bounds__(256)
 correct_kernel(Geom g, double* __restrict__ u, double* __restrict__ v, double* __restrict__ w,
                const double* __restrict__ p, const double* __restrict__ rho)
@@ -804,6 +923,36 @@ void sweep_check_c(cudaStream_t st, const Launch& L, const Geom& g, const double
 {
     sweep_check_c_kernel<<<L.cgrid, L.block, 0, st>>>(g, L.zrun, hin, hout, hc, rho, s, ds, part,
                                                       L.cnblocks);
+}
+
+void scalar_jacobi(cudaStream_t st, const Launch& L, const Geom& g, const double* pin, double* pout,
+                   const double* rho, const double* s, double scale)
+{
+    scalar_jacobi_kernel<<<L.grid, L.block, 0, st>>>(g, pin, pout, rho, s, scale);
+}
+
+void rb_sor(cudaStream_t st, const Launch& L, const Geom& g, double* p, const double* rho, const double* s,
+            double scale, double omega, const DevState* ds)
+{
+    rb_sor_kernel<<<L.grid, L.block, 0, st>>>(g, p, rho, s, scale, omega, 0, ds);
+    rb_sor_kernel<<<L.grid, L.block, 0, st>>>(g, p, rho, s, scale, omega, 1, ds);
+}
+
+void scalar_rhs_sum(cudaStream_t st, const Launch& L, const Geom& g, const double* rho, const double* s,
+                    double scale, double* part)
+{
+    scalar_rhs_sum_kernel<<<L.cgrid, L.block, 0, st>>>(g, L.zrun, rho, s, scale, part, L.cnblocks);
+}
+
+void p_sum(cudaStream_t st, const Launch& L, const Geom& g, const double* p, double* part)
+{
+    p_sum_kernel<<<L.cgrid, L.block, 0, st>>>(g, L.zrun, p, part, L.cnblocks);
+}
+
+void scalar_check(cudaStream_t st, const Launch& L, const Geom& g, const double* pin, double* p, double* p_prev,
+                  const DevState* ds, double* part)
+{
+    scalar_check_kernel<<<L.cgrid, L.block, 0, st>>>(g, L.zrun, pin, p, p_prev, ds, part, L.cnblocks);
 }
 
 void correct(cudaStream_t st, const Launch& L, const Geom& g, double* u, double* v, double* w,

@@ -39,11 +39,13 @@ namespace {
 
 struct SegKey {
     int start_parity, n_normal, dual;
+    int form = 0;   // lbm_poisson_form
     bool operator<(const SegKey& o) const
     {
         if (start_parity != o.start_parity) return start_parity < o.start_parity;
         if (n_normal != o.n_normal) return n_normal < o.n_normal;
-        return dual < o.dual;
+        if (dual != o.dual) return dual < o.dual;
+        return form < o.form;
     }
 };
 
@@ -80,6 +82,9 @@ struct lbm_handle {
     double* stats_part = nullptr;        // field-statistics partials
     lbm_field_stats* stats_dev = nullptr;   // 7 results (lbm_diagnostics)
     int h_last = 0;                      // h buffer the last Poisson solve ended in
+    int pform = LBM_POISSON_KINETIC;     // lbm_poisson_form
+    double scalar_scale = 2.0;           // scalar forms: source scale (reference default 2.0)
+    double sor_omega = 0.0;              // red-black form: relaxation (0: from the box size)
 };
 
 namespace {
@@ -199,7 +204,24 @@ lbm_status build_segment(lbm_handle* h, const SegKey& key, cudaGraphExec_t* out,
     int cur = key.start_parity;
     const Geom& g = h->geom;
     const Launch& L = h->L;
-    if (h->precision == LBM_PRECISION_FP64) {
+    if (key.form != LBM_POISSON_KINETIC) {
+        // Scalar forms: n_normal sweeps, the gauge mean, the check; p ends in b.p.
+        Fp64Buffers& b = h->b;
+        double* P[2] = {b.p, b.p_chk};
+        int pc = 0;
+        for (int i = 0; i < key.n_normal; ++i) {
+            if (key.form == LBM_POISSON_SCALAR_JACOBI) {
+                fp64::scalar_jacobi(st, L, g, P[pc], P[1 - pc], b.rho, b.s, h->scalar_scale);
+                pc = 1 - pc;
+            } else {
+                fp64::rb_sor(st, L, g, b.p, b.rho, b.s, h->scalar_scale, h->sor_omega, h->ds);
+            }
+        }
+        fp64::p_sum(st, L, g, P[pc], b.part_a);
+        finalize(st, FIN_SIGMA, h->ds, b.part_a, L.cnblocks, nullptr, 0, nullptr, 0);
+        fp64::scalar_check(st, L, g, P[pc], b.p, b.p_prev, h->ds, b.part_b);
+        finalize(st, FIN_CHECK, h->ds, b.part_b, L.cnblocks, nullptr, 0, nullptr, 0);
+    } else if (h->precision == LBM_PRECISION_FP64) {
         Fp64Buffers& b = h->b;
         int n_single = key.n_normal;
         if (h->fuse_zlen > 0) {
@@ -306,6 +328,10 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
     const Launch& L = h->L;
     const int ci = h->pcfg.check_interval;
     const int dual = h->pcfg.dual_residual != 0;   // residual kernels run in exit and shadow mode
+    const int form = h->pform;
+    if (form != LBM_POISSON_KINETIC && dual)
+        return fail(h, LBM_ERR_BAD_ARG,
+                    "fixed-point residual requires the kinetic (split) Poisson form");
     if (dual) {
         const lbm_status s = ensure_dual_buffer(h);
         if (s != LBM_OK) return s;
@@ -333,7 +359,12 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
         finalize(st, FIN_MASS, h->ds, b.part_mass, L.nblocks, nullptr, 0, nullptr, 0);
         fp64::prep(st, L, g, h->ds, b.dux, b.dvy, b.dwz, b.p, b.s, b.part_prep);
         finalize(st, FIN_PREP, h->ds, b.part_prep, L.nblocks, nullptr, 0, nullptr, 0);
-        fp64::poisson_init(st, L, g, h->h_loaded, b.h[1], b.h[0], b.p, b.rho, b.s);
+        if (form == LBM_POISSON_KINETIC) {
+            fp64::poisson_init(st, L, g, h->h_loaded, b.h[1], b.h[0], b.p, b.rho, b.s);
+        } else if (form == LBM_POISSON_SCALAR_RB) {
+            fp64::scalar_rhs_sum(st, L, g, b.rho, b.s, h->scalar_scale, b.part_a);
+            finalize(st, FIN_RHS, h->ds, b.part_a, L.cnblocks, nullptr, 0, nullptr, 0);
+        }
     } else {
         const lbm_status s2 = mixed_prologue(st, h->mb, L, g, h->phys, h->first_step, h->fcur,
                                              h->h_loaded, h->ds, h->timing ? h->ev : nullptr);
@@ -351,10 +382,13 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
     uint64_t kernels = 0;
     // collide, moments, 2 finalize, prep, finalize, poisson_init (+ correct below)
     uint64_t launches = 7;
+    if (form == LBM_POISSON_SCALAR_JACOBI) launches = 6;   // no h initialisation
+    if (form == LBM_POISSON_SCALAR_RB) launches = 8;       // no h initialisation; right-hand-side mean
     uint64_t fused_sweeps = 0;
     for (;;) {
-        const int n_normal = dual ? (first_seg ? ci - 1 : ci - 2) : ci - 1;
-        SegKey key{hcur, n_normal, dual};
+        const int n_normal =
+            form != LBM_POISSON_KINETIC ? ci : (dual ? (first_seg ? ci - 1 : ci - 2) : ci - 1);
+        SegKey key{hcur, n_normal, dual, form};
         cudaGraphExec_t ex = nullptr;
         int end_parity = hcur;
         const lbm_status gs = get_segment(h, key, &ex, &end_parity);
@@ -365,12 +399,18 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
         h->h_last = hcur;
         // sweep-equivalents executed (plain, A, B, C) and actual launches
         // (two plain sweeps per launch where the mixed box fuses them)
-        kernels += static_cast<uint64_t>(n_normal) + 2 + (dual ? 1 : 0);
-        const bool fused = h->precision == LBM_PRECISION_MIXED ? h->mb.fuse_zlen > 0 : h->fuse_zlen > 0;
-        const uint64_t plain_launches = fused ? static_cast<uint64_t>(n_normal / 2 + n_normal % 2)
-                                              : static_cast<uint64_t>(n_normal);
-        launches += plain_launches + 4 + (dual ? 1 : 0);
-        if (fused) fused_sweeps += static_cast<uint64_t>(n_normal / 2) * 2;
+        if (form != LBM_POISSON_KINETIC) {
+            // scalar sweeps (red-black: two launches each), p sum, check, 2 finalize
+            kernels += static_cast<uint64_t>(n_normal);
+            launches += static_cast<uint64_t>(n_normal) * (form == LBM_POISSON_SCALAR_RB ? 2 : 1) + 4;
+        } else {
+            kernels += static_cast<uint64_t>(n_normal) + 2 + (dual ? 1 : 0);
+            const bool fused = h->precision == LBM_PRECISION_MIXED ? h->mb.fuse_zlen > 0 : h->fuse_zlen > 0;
+            const uint64_t plain_launches = fused ? static_cast<uint64_t>(n_normal / 2 + n_normal % 2)
+                                                  : static_cast<uint64_t>(n_normal);
+            launches += plain_launches + 4 + (dual ? 1 : 0);
+            if (fused) fused_sweeps += static_cast<uint64_t>(n_normal / 2) * 2;
+        }
         first_seg = false;
         if (dh.error) {
             return fail(h, static_cast<lbm_status>(dh.error), site_text(dh.error_site));
@@ -711,6 +751,48 @@ lbm_status lbm_set_poisson(lbm_handle* h, const lbm_poisson_cfg* cfg)
         h->graphs.clear();
     }
     h->pcfg = *cfg;
+    return LBM_OK;
+}
+
+lbm_status lbm_set_poisson_form(lbm_handle* h, lbm_poisson_form form, double source_scale, double omega)
+{
+    if (check_handle(h) != LBM_OK) return LBM_ERR_BAD_ARG;
+    if (form != LBM_POISSON_KINETIC && form != LBM_POISSON_SCALAR_JACOBI && form != LBM_POISSON_SCALAR_RB)
+        return fail(h, LBM_ERR_BAD_ARG, "unknown Poisson form");
+    if (form != LBM_POISSON_KINETIC && h->precision != LBM_PRECISION_FP64)
+        return fail(h, LBM_ERR_BAD_ARG, "the scalar Poisson forms run in FP64 precision only");
+    if (!std::isfinite(source_scale)) return fail(h, LBM_ERR_BAD_ARG, "scalar source scale must be finite");
+    if (!(omega == 0.0 || (omega > 0.0 && omega < 2.0)))
+        return fail(h, LBM_ERR_BAD_ARG, "SOR relaxation must be 0 (automatic) or in (0, 2)");
+    const Geom& g = h->geom;
+    if (form == LBM_POISSON_SCALAR_RB && (g.ly % 2 || g.lz % 2 || (g.periodic_x && g.lx % 2)))
+        return fail(h, LBM_ERR_BAD_ARG, "the red-black form needs even extents along the periodic axes");
+    double w = omega;
+    if (form == LBM_POISSON_SCALAR_RB && w == 0.0) {
+        // Optimal SOR for the Jacobi iteration of the 14-neighbour stencil:
+        // its slowest mode (wave number k) has rho_J = (10 cos k + 4) / 14.
+        const double pi = 3.14159265358979323846;
+        double k = std::min(2.0 * pi / g.ly, 2.0 * pi / g.lz);
+        k = std::min(k, g.periodic_x ? 2.0 * pi / g.lx : pi / std::max(1, g.lx - 1));
+        const double rj = (10.0 * std::cos(k) + 4.0) / 14.0;
+        w = 2.0 / (1.0 + std::sqrt(std::max(0.0, 1.0 - rj * rj)));
+    }
+    if (form != h->pform || source_scale != h->scalar_scale || w != h->sor_omega) {
+        for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second.first);
+        h->graphs.clear();
+    }
+    h->pform = form;
+    h->scalar_scale = source_scale;
+    h->sor_omega = w;
+    return LBM_OK;
+}
+
+lbm_status lbm_get_poisson_form(const lbm_handle* h, lbm_poisson_form* form, double* source_scale, double* omega)
+{
+    if (!h) return LBM_ERR_BAD_ARG;
+    if (form) *form = static_cast<lbm_poisson_form>(h->pform);
+    if (source_scale) *source_scale = h->scalar_scale;
+    if (omega) *omega = h->sor_omega;
     return LBM_OK;
 }
 

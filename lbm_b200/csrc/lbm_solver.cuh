@@ -50,6 +50,8 @@ struct DevState {
     int dual;
     double tolerance;
     double n_cells;             // (double)lx * ly * lz
+    double rhs_mean;            // scalar red-black form: weighted mean of f = scale rho s (per step)
+    double rhs_chk;             // ... and of chi f, chi = (-1)^(x+y+z)
 };
 
 enum ErrorSite {
@@ -136,11 +138,24 @@ void sweep_check_c(cudaStream_t st, const Launch& L, const Geom& g, const double
                    const DevState* ds, double* part);
 void correct(cudaStream_t st, const Launch& L, const Geom& g, double* u, double* v, double* w,
              const double* p, const double* rho);
+// Scalar Poisson forms: a Jacobi sweep of the reference's scalar form, a
+// red-black SOR sweep (two launches) of the same equation, the partial sums
+// of its right-hand side (FIN_RHS) and of p (FIN_SIGMA), and the check
+// (gauge, relative change; FIN_CHECK layout).
+void scalar_jacobi(cudaStream_t st, const Launch& L, const Geom& g, const double* pin, double* pout,
+                   const double* rho, const double* s, double scale);
+void rb_sor(cudaStream_t st, const Launch& L, const Geom& g, double* p, const double* rho, const double* s,
+            double scale, double omega, const DevState* ds);
+void scalar_rhs_sum(cudaStream_t st, const Launch& L, const Geom& g, const double* rho, const double* s,
+                    double scale, double* part);
+void p_sum(cudaStream_t st, const Launch& L, const Geom& g, const double* p, double* part);
+void scalar_check(cudaStream_t st, const Launch& L, const Geom& g, const double* pin, double* p, double* p_prev,
+                  const DevState* ds, double* part);
 }  // namespace fp64
 
 // Finalisation kernels (kernels_fp64.cu): reduce block partials in a fixed
 // order and update DevState.
-enum FinKind { FIN_SOURCE = 0, FIN_PREP = 1, FIN_SIGMA = 2, FIN_CHECK = 3, FIN_MASS = 4 };
+enum FinKind { FIN_SOURCE = 0, FIN_PREP = 1, FIN_SIGMA = 2, FIN_CHECK = 3, FIN_MASS = 4, FIN_RHS = 5 };
 void finalize(cudaStream_t st, FinKind kind, DevState* ds, const double* part,
               long long nblocks, const double* part2, long long nblocks2,
               const double* part3, long long nblocks3);

@@ -350,6 +350,79 @@ static int dual_residual(orc_state* s, double g, orc_step_info* info)
     return ORC_OK;
 }
 
+/* The reference's scalar Poisson form (GPU only there): Jacobi sweeps of
+ * scalarPressureJacobiKernel, GPU/InamuroCUDA.cu:864-901 (x neighbours
+ * mirrored at the slip walls, pressure_bounce_direction :846-862), with the
+ * gauge and relative-change check of check_residual (:1977-2140) every
+ * check_interval sweeps.  u_x is already projected.  x-outer sums. */
+static int poisson_scalar(orc_state* s, uint64_t replay, orc_step_info* info, double target)
+{
+    const orc_params* P = &s->P;
+    const int lx = P->lx, ly = P->ly, lz = P->lz;
+    const long N = s->N;
+    const double cell_count = (double)lx * ly * lz;
+    const double* ux = s->d[D_UX];
+    const double* vy = s->d[D_VY];
+    const double* wz = s->d[D_WZ];
+    uint64_t iter = 0;
+    for (;;) {
+        ++iter;
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int z = 0; z < lz; ++z)
+            for (int y = 0; y < ly; ++y)
+                for (int x = 0; x < lx; ++x) {
+                    double nsum = 0.0;
+                    for (int q = 1; q < Q; ++q) {
+                        int xs = x - EX[q], ys = y - EY[q], zs = z - EZ[q];
+                        if (!P->periodic_x && xs < 0) xs = 1;
+                        else if (!P->periodic_x && xs >= lx) xs = lx - 2;
+                        else if (xs < 0) xs += lx;
+                        else if (xs >= lx) xs -= lx;
+                        if (ys < 0) ys += ly; else if (ys >= ly) ys -= ly;
+                        if (zs < 0) zs += lz; else if (zs >= lz) zs -= lz;
+                        nsum += s->p[idx(s, xs, ys, zs)];
+                    }
+                    const long c = idx(s, x, y, z);
+                    const double div_u = ux[c] + vy[c] + wz[c];
+                    const double rhs = P->scalar_source_scale * s->rho[c] * div_u;
+                    s->pf[c] = (nsum - 5.0 * rhs) / 14.0;
+                }
+        memcpy(s->p, s->pf, sizeof(double) * N);
+        int converged = 0;
+        if (iter % (uint64_t)P->check_interval == 0) {
+            const double shift = sum_xouter(s, s->p) / cell_count - target;
+            if (!isfinite(shift)) return ORC_ERR_NONFINITE;
+            if (fabs(shift) > info->gauge_max_shift) info->gauge_max_shift = fabs(shift);
+            for (long c = 0; c < N; ++c) s->p[c] -= shift;
+            double err1 = 0.0, err2 = 0.0;
+            for (int x = 0; x < lx; ++x)
+                for (int y = 0; y < ly; ++y)
+                    for (int z = 0; z < lz; ++z) {
+                        const long c = idx(s, x, y, z);
+                        err1 += fabs(s->p[c] - s->p_prev[c]);
+                        err2 += fabs(s->p[c]);
+                        s->p_prev[c] = s->p[c];
+                    }
+            if (!isfinite(err1) || !isfinite(err2)) return ORC_ERR_NONFINITE;
+            info->pressure_l1_delta = err1;
+            info->pressure_l1_norm = err2;
+            info->relative_error = relative(err1, err2);
+            converged = info->relative_error < P->tol;
+        }
+        if (replay) {
+            if (iter == replay) break;
+        } else if (converged) {
+            break;
+        }
+        if (!replay && P->max_sweeps && iter >= P->max_sweeps) {
+            info->sweeps = iter;
+            return ORC_ERR_BUDGET;
+        }
+    }
+    info->sweeps = iter;
+    return ORC_OK;
+}
+
 /* solvePressurePoisson: CPU/Inamuro.cpp:624-724 */
 static int poisson(orc_state* s, uint64_t replay, orc_step_info* info)
 {
@@ -374,6 +447,7 @@ static int poisson(orc_state* s, uint64_t replay, orc_step_info* info)
     info->divergence_mean = divergence_mean;
     info->gauge_target = target;
     info->gauge_max_shift = 0.0;
+    if (P->poisson_form == 1) return poisson_scalar(s, replay, info, target);
 
     uint64_t iter = 0;
     for (;;) {
@@ -486,6 +560,7 @@ orc_state* orc_create(const orc_params* prm,
                       const double* p)
 {
     if (!prm || prm->lx < 2 || prm->ly < 1 || prm->lz < 1 || prm->check_interval <= 0) return NULL;
+    if (prm->poisson_form < 0 || prm->poisson_form > 1 || (prm->poisson_form == 1 && prm->dual)) return NULL;
     orc_state* s = (orc_state*)calloc(1, sizeof(orc_state));
     if (!s) return NULL;
     s->P = *prm;

@@ -49,6 +49,8 @@ typedef struct {
     int dual;                /* 1: also require the kinetic fixed-point residual < tol */
     uint64_t max_sweeps;     /* 0 = unbounded (reference contract); else error when hit */
     int periodic_x;          /* 1: periodic x (no slip walls) -- not a reference mode */
+    int poisson_form;        /* 0: kinetic (production); 1: the reference's scalar Jacobi form */
+    double scalar_source_scale;  /* scalar form: --scalar-source-scale (reference default 2.0) */
 } orc_params;
 
 typedef struct {

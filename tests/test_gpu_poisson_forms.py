@@ -1,0 +1,169 @@
+"""Poisson forms (lbm_set_poisson_form) and the reference's own GPU program.
+
+* The scalar form (the reference's --poisson scalar, GPU/InamuroCUDA.cu:864-901)
+  against the oracle's restatement of it: same sweep counts at natural exits,
+  fields within the FP64 bar (1e-10 relative; the device sums run in another
+  order than the oracle's x-outer loops).
+* The red-black SOR form reaches the Jacobi sweeps' fixed point (tight
+  tolerance on both: fields within 1e-8) in a fraction of the sweeps.
+* oracle/_ref/lbm_gpu_ref, the reference's GPU program compiled from its
+  sources, against the reference's GPU/main.cpp over this library
+  (oracle/_ref/lbm_gpu_dropin) on the same params.in with the split and the
+  fused Poisson flags: Tecplot fields to float32 rounding and the same sweep
+  count at every step.
+* With --poisson scalar the reference program does not solve the scalar
+  equation: after each Jacobi sweep its loop still runs the split form's
+  bounce + computePressure on the unchanged h (the block after the sweep is
+  guarded only by !use_onepass_poisson, GPU/InamuroCUDA.cu:2307-2329), so p is
+  reset to sum_q h = its start value every sweep.  The test records that
+  behaviour (p stays 0 from the zero start, each solve exits at its first
+  check); this library's scalar form solves the equation its kernel states
+  (pinned to the oracle above)."""
+import csv
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import lbm_b200 as L
+from oracle import pyoracle
+from tests.helpers import laplace_case, oracle_params, rel_err
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GPU_REF = os.path.join(ROOT, "oracle", "_ref", "lbm_gpu_ref")
+DROPIN = os.path.join(ROOT, "oracle", "_ref", "lbm_gpu_dropin")
+SHAPE = (16, 12, 10)
+
+
+def case(periodic):
+    p, f = laplace_case(SHAPE, DD=6.0, noise=1e-4, seed=3)
+    p.periodic_x = int(periodic)
+    f["w"] = 0.01 * np.sin(2 * np.pi * np.arange(SHAPE[2]) / SHAPE[2])[:, None, None] * np.ones_like(f["w"])
+    return p, f
+
+
+def gpu_box(p, f, form, tol, cap=400000):
+    g = L.InamuroCUDA(p, f, precision="fp64")
+    g.set_poisson(check_interval=100, tolerance=tol, max_sweeps=cap, fail_on_limit=True)
+    g.set_poisson_form(form)
+    return g
+
+
+@pytest.mark.parametrize("periodic", [False, True])
+def test_scalar_form_matches_oracle(periodic):
+    p, f = case(periodic)
+    g = gpu_box(p, f, "scalar", 1e-3)
+    o = pyoracle.Oracle(SHAPE, oracle_params(p), f, tol=1e-3, periodic_x=periodic, poisson_form=1)
+    for step in range(3):
+        want = o.step()
+        got = g.step(1)[0]
+        assert got["iterations"] == want["sweeps"], step
+        assert got["converged"] == 1
+    of, gf = o.fields(), g.download_fields()
+    for k in L.FIELDS:
+        assert rel_err(gf[k], of[k]) <= 1e-10, k
+
+
+def test_red_black_reaches_the_jacobi_fixed_point():
+    p, f = case(True)
+    a = gpu_box(p, f, "scalar", 1e-12)
+    b = gpu_box(p, f, "scalar-rb", 1e-12)
+    assert 1.0 < b.poisson_form()["omega"] < 2.0
+    sa = [s["iterations"] for s in a.step(2)]
+    sb = [s["iterations"] for s in b.step(2)]
+    assert all(x * 3 <= y for x, y in zip(sb, sa)), (sa, sb)
+    fa, fb = a.download_fields(), b.download_fields()
+    for k in ("p", "u", "v", "w"):
+        assert rel_err(fb[k], fa[k]) <= 1e-8, k
+    for k in ("phi", "rho"):
+        assert rel_err(fb[k], fa[k]) <= 1e-12, k
+
+
+def test_scalar_form_rejections():
+    p, f = case(True)
+    m = L.InamuroCUDA(p, f, precision="mixed")
+    with pytest.raises(L.LBMError) as e:
+        m.set_poisson_form("scalar")
+    assert e.value.status == 4
+    p2, f2 = laplace_case((16, 11, 10), DD=6.0)
+    g = L.InamuroCUDA(p2, f2, precision="fp64")
+    with pytest.raises(L.LBMError) as e:
+        g.set_poisson_form("scalar-rb")
+    assert e.value.status == 4 and "even" in str(e.value)
+    g2 = L.InamuroCUDA(p, f, precision="fp64")
+    g2.set_poisson(dual=True)
+    g2.set_poisson_form("scalar")
+    with pytest.raises(L.LBMError) as e:
+        g2.step(1)
+    assert e.value.status == 4 and "kinetic" in str(e.value)
+
+
+PARAMS = """16 32 32
+1
+3
+1
+50.0 1.0
+1.0 1.0
+0.008 0.00016
+0.5 0.0005
+0.035
+1.0
+6.7
+0.09714 0.01134
+0.092 0.015
+8.0
+"""
+
+
+def tecplot_points(path, n):
+    raw = open(path, "rb").read()
+    data = np.frombuffer(raw[len(raw) - 36 * n:], dtype=np.dtype([("xyz", "<i4", 3), ("val", "<f4", 6)]))
+    return data["xyz"], data["val"]
+
+
+def final_counts(path):
+    finals = {}
+    for r in csv.DictReader(open(path)):
+        if r["converged"] == "1":
+            finals[int(r["step"])] = int(r["iteration"])
+    return finals
+
+
+def run_program(exe, d, pf, flags):
+    d.mkdir()
+    args = [exe, "--mode", "gpu", "--params", str(pf), "--steps", "3", "--write-output", "--output-steps",
+            "3", "--no-roofline", "--poisson-diagnostics", "diag.csv"] + flags
+    r = subprocess.run(args, cwd=d, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, (exe, r.stdout[-2000:] + r.stderr[-2000:])
+    return d
+
+
+@pytest.mark.skipif(not (os.path.exists(GPU_REF) and os.path.exists(DROPIN)),
+                    reason="reference GPU program or drop-in CLI not built (needs the reference sources)")
+@pytest.mark.parametrize("flags", [["--poisson", "split"],
+                                   ["--poisson", "fused", "--pressure-boundary", "fused"]])
+def test_reference_gpu_program_matches_dropin(tmp_path, flags):
+    pf = tmp_path / "params.in"
+    pf.write_text(PARAMS)
+    outs = {name: run_program(exe, tmp_path / name, pf, flags) for name, exe in (("ref", GPU_REF), ("ours", DROPIN))}
+    n = 16 * 32 * 32
+    xr, vr = tecplot_points(outs["ref"] / "out" / "3D000000003.plt", n)
+    xo, vo = tecplot_points(outs["ours"] / "out" / "3D000000003.plt", n)
+    assert np.array_equal(xr, xo)
+    for j, name in enumerate(("u", "v", "w", "rho", "fei", "press")):
+        scale = float(np.max(np.abs(vr[:, j])))
+        err = float(np.max(np.abs(vo[:, j].astype(np.float64) - vr[:, j])))
+        assert err <= 2e-6 * max(scale, 1e-30), (name, err, scale)
+    assert final_counts(outs["ours"] / "diag.csv") == final_counts(outs["ref"] / "diag.csv")
+
+
+@pytest.mark.skipif(not os.path.exists(GPU_REF), reason="reference GPU program not built (needs the reference sources)")
+def test_reference_scalar_option_keeps_its_start_pressure(tmp_path):
+    pf = tmp_path / "params.in"
+    pf.write_text(PARAMS)
+    d = run_program(GPU_REF, tmp_path / "ref", pf, ["--poisson", "scalar"])
+    _, v = tecplot_points(d / "out" / "3D000000003.plt", 16 * 32 * 32)
+    assert np.all(v[:, 5] == 0.0)
+    assert final_counts(d / "diag.csv") == {1: 100, 2: 100, 3: 100}
