@@ -466,8 +466,8 @@ lbm_status lbm_correct_backward(const lbm_params* p, const double* press, const 
  * interval from its checkpoint (replaying the forward's sweep counts, so the
  * recomputed states are bitwise the forward's) and walks it backwards.
  * Device memory: about 288 B/cell per checkpoint plus 168 B/cell per step of
- * one interval plus about 1 kB/cell of adjoint buffers.  The reference has no
- * derivatives. */
+ * one interval (uniform) or of one step (binomial) plus about 1 kB/cell of
+ * adjoint buffers.  The reference has no derivatives. */
 typedef struct lbm_adjoint lbm_adjoint;
 
 typedef struct {
@@ -477,6 +477,10 @@ typedef struct {
                                   pi = sum_q of the adjoint iterate, compared across checks */
     uint64_t max_sweeps;       /* adjoint Poisson: cap per step; 0 = none.  Reaching it returns
                                   LBM_ERR_POISSON_BUDGET */
+    int binomial_checkpoints;  /* 0: uniform checkpoints every checkpoint_interval steps.  > 0:
+                                  binomial checkpointing (Griewank's revolve schedule) with at most
+                                  this many stored states besides the loaded one; the forward run
+                                  then keeps no states, and the reverse pass keeps one step's */
 } lbm_adjoint_cfg;
 
 typedef struct {
@@ -512,6 +516,10 @@ lbm_status lbm_adjoint_backward(lbm_adjoint* a, const double* lam_phi, const dou
 /* Text of the last error on this object ("" if none); with a == NULL: why the
  * calling thread's last lbm_adjoint_create failed. */
 const char* lbm_adjoint_last_error(const lbm_adjoint* a);
+/* The binomial schedule of a reverse pass over n_steps steps with at most
+ * `checkpoints` stored states, run dry (no device work): the forward steps it
+ * recomputes and the most states it holds at once.  For sizing runs. */
+lbm_status lbm_adjoint_schedule(int n_steps, int checkpoints, uint64_t* recompute_steps, int* peak_checkpoints);
 
 #ifdef __cplusplus
 }

@@ -114,7 +114,7 @@ class Diagnostics(C.Structure):
 class AdjointCfg(C.Structure):
     """lbm_adjoint_cfg: checkpoint interval and the adjoint Poisson solve's exit."""
     _fields_ = [("checkpoint_interval", C.c_int), ("check_interval", C.c_int), ("tolerance", C.c_double),
-                ("max_sweeps", C.c_uint64)]
+                ("max_sweeps", C.c_uint64), ("binomial_checkpoints", C.c_int)]
 
 
 class AdjointStats(C.Structure):
@@ -214,6 +214,7 @@ def load_library(path: str = LIB_PATH):
     L.lbm_adjoint_backward.argtypes = [A] + [C.c_void_p] * 12 + [C.POINTER(AdjointStats)]
     L.lbm_adjoint_last_error.argtypes = [A]
     L.lbm_adjoint_last_error.restype = C.c_char_p
+    L.lbm_adjoint_schedule.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_uint64), C.POINTER(C.c_int)]
     if L.lbm_abi_version() != ABI_VERSION:
         raise LBMError(7, f"{path} has ABI {L.lbm_abi_version()}, these bindings expect {ABI_VERSION}; "
                           "rebuild with lbm_b200.build.build()")
@@ -647,10 +648,10 @@ class Adjoint:
     dJ/d(loaded fields) and dJ/dk_f for the adjoint lam of the final fields."""
 
     def __init__(self, params: Params, checkpoint_interval: int = 100, check_interval: int = 100,
-                 tolerance: float = 1e-12, max_sweeps: int = 0, device: int = 0):
+                 tolerance: float = 1e-12, max_sweeps: int = 0, binomial_checkpoints: int = 0, device: int = 0):
         self._lib = load_library()
         self.params = params
-        self.cfg = AdjointCfg(checkpoint_interval, check_interval, tolerance, max_sweeps)
+        self.cfg = AdjointCfg(checkpoint_interval, check_interval, tolerance, max_sweeps, binomial_checkpoints)
         h = C.c_void_p()
         st = self._lib.lbm_adjoint_create(C.byref(params), device, C.byref(self.cfg), C.byref(h))
         if st != 0:
@@ -707,3 +708,13 @@ class Adjoint:
             [grads[k].ctypes.data_as(C.c_void_p) for k in FIELDS]
         self._check(self._lib.lbm_adjoint_backward(self._h, *args, C.byref(st)), "adjoint_backward")
         return grads, st.as_dict()
+
+
+def adjoint_schedule(n_steps: int, checkpoints: int) -> Dict[str, int]:
+    """lbm_adjoint_schedule: forward steps a binomial reverse pass recomputes
+    and the most checkpoints it holds at once (no device work)."""
+    steps, peak = C.c_uint64(), C.c_int()
+    st = load_library().lbm_adjoint_schedule(n_steps, checkpoints, C.byref(steps), C.byref(peak))
+    if st != 0:
+        raise LBMError(st, "lbm_adjoint_schedule")
+    return {"recompute_steps": int(steps.value), "peak_checkpoints": int(peak.value)}

@@ -70,6 +70,8 @@ struct lbm_adjoint {
     double forward_ms = 0.0;
     uint64_t forward_sweeps = 0;
     int y_warm = -1;                    // y buffer holding the last converged adjoint iterate, -1: none
+    std::vector<double*> bslot;         // binomial mode: checkpoint slots (36 n each), allocated on first use
+    std::vector<int> bfree;             // free slot indices
 };
 
 namespace {
@@ -108,6 +110,8 @@ void free_all(lbm_adjoint* a)
 {
     for (double* p : a->ckpt) cudaFree(p);
     a->ckpt.clear();
+    for (double* p : a->bslot) cudaFree(p);
+    a->bslot.clear();
     double* bufs[] = {a->init, a->final_state, a->seg_macro, a->seg_h, a->lpop[0][0], a->lpop[0][1],
                       a->lpop[1][0], a->lpop[1][1], a->lmac[0], a->lmac[1], a->y[0], a->y[1], a->pi_prev,
                       a->scratch, a->ls, a->lsrc, a->lkf, a->part};
@@ -257,6 +261,169 @@ lbm_status recompute(lbm_adjoint* a, int s0, int s1)
     return LBM_OK;
 }
 
+// ---- binomial checkpointing ------------------------------------------------
+// Griewank's revolve schedule, recursive form: to reverse steps [a, b) from
+// a stored state at a with c free slots, when b - a > 1 and c > 0 advance to
+// m, store the state there, reverse [m, b) with c - 1 slots, free it and
+// reverse [a, m) with c.  With r the least repetition count with
+// beta(c, r) = C(c + r, c) >= b - a, the split keeps [m, b) within
+// beta(c - 1, r) and [a, m) within beta(c, r - 1) (beta(c, r) =
+// beta(c - 1, r) + beta(c, r - 1)), so no step is recomputed more than r
+// times.  With no slot left, each step of [a, b) is reached from a in turn.
+// A leaf n restores the base state at a, advances to n, runs step n + 1
+// keeping X_n, X_{n+1} and its final h, and runs that step's adjoint.
+double beta(int c, int r)
+{
+    double v = 1.0;
+    for (int i = 1; i <= c; ++i) v = v * (r + i) / i;
+    return v;
+}
+
+template <class Ops>
+lbm_status revolve(Ops& ops, int a, int b, int c, int base)
+{
+    const int l = b - a;
+    if (l == 1) return ops.leaf(a, a, base);
+    if (c <= 0) {
+        for (int n = b - 1; n >= a; --n) {
+            const lbm_status s = ops.leaf(n, a, base);
+            if (s != LBM_OK) return s;
+        }
+        return LBM_OK;
+    }
+    int r = 1;
+    while (beta(c, r) < l) ++r;
+    const double right_cap = beta(c - 1, r);
+    int l1 = right_cap >= l ? 1 : static_cast<int>(l - right_cap);
+    l1 = std::max(1, std::min(l1, l - 1));
+    const int m = a + l1;
+    int slot = -1;
+    lbm_status s = ops.save_at(base, a, m, &slot);
+    if (s != LBM_OK) return s;
+    s = revolve(ops, m, b, c - 1, slot);
+    if (s != LBM_OK) return s;
+    ops.release(slot);
+    return revolve(ops, a, m, c, base);
+}
+
+// Counts what a schedule does, without device work.
+struct DryOps {
+    uint64_t steps = 0;
+    int live = 0, peak = 0;
+    lbm_status leaf(int n, int a, int) { steps += static_cast<uint64_t>(n - a) + 1; return LBM_OK; }
+    lbm_status save_at(int, int a, int m, int* slot)
+    {
+        steps += static_cast<uint64_t>(m - a);
+        *slot = live++;
+        peak = std::max(peak, live);
+        return LBM_OK;
+    }
+    void release(int) { --live; }
+};
+
+lbm_status restore_state(lbm_adjoint* a, int base);
+lbm_status advance(lbm_adjoint* a, int from, int to, uint64_t* counted);
+
+// Device schedule: base -1 is the loaded state (step 0), else a slot.
+struct GpuOps {
+    lbm_adjoint* a;
+    int cur = 0;
+    double kf = 0.0;
+    uint64_t adj_sweeps = 0, recomputed = 0;
+
+    lbm_status leaf(int n, int from, int base)
+    {
+        lbm_status s = restore_state(a, base);
+        if (s != LBM_OK) return s;
+        s = advance(a, from, n, &recomputed);
+        if (s != LBM_OK) return s;
+        s = recompute_from_current(n);
+        if (s != LBM_OK) return s;
+        s = step_adjoint(a, n == 0, a->seg_macro, slot(a->seg_macro, 6 * a->n, 1), a->seg_h, cur, &adj_sweeps, &kf);
+        cur = 1 - cur;
+        return s;
+    }
+
+    // X_n (the box's current state) and step n + 1 into the one-step buffers.
+    lbm_status recompute_from_current(int n)
+    {
+        const long long nn = a->n;
+        const size_t fbytes = static_cast<size_t>(nn) * sizeof(double);
+        cudaStream_t st = a->view.stream;
+        ADJ_TRY(a, fp64_view(a->fwd, &a->view), "state view");
+        for (int i = 0; i < 6; ++i)
+            ADJ_CUDA(a, cudaMemcpyAsync(slot(a->seg_macro, nn, i), a->view.macro[i], fbytes,
+                                        cudaMemcpyDeviceToDevice, st));
+        ADJ_TRY(a, lbm_step_replay(a->fwd, 1, &a->sweeps[n], nullptr), "recomputation step");
+        ++recomputed;
+        ADJ_TRY(a, fp64_view(a->fwd, &a->view), "state view");
+        double* dst = slot(a->seg_macro, 6 * nn, 1);
+        for (int i = 0; i < 6; ++i)
+            ADJ_CUDA(a, cudaMemcpyAsync(slot(dst, nn, i), a->view.macro[i], fbytes, cudaMemcpyDeviceToDevice, st));
+        ADJ_CUDA(a, cudaMemcpyAsync(a->seg_h, a->view.h_last, 15 * fbytes, cudaMemcpyDeviceToDevice, st));
+        ADJ_CUDA(a, cudaStreamSynchronize(st));
+        return LBM_OK;
+    }
+
+    lbm_status save_at(int base, int from, int m, int* out)
+    {
+        lbm_status s = restore_state(a, base);
+        if (s != LBM_OK) return s;
+        s = advance(a, from, m, &recomputed);
+        if (s != LBM_OK) return s;
+        int k;
+        if (!a->bfree.empty()) {
+            k = a->bfree.back();
+            a->bfree.pop_back();
+        } else {
+            cudaError_t e = cudaSuccess;
+            double* buf = dalloc(36 * static_cast<size_t>(a->n), &e);
+            if (e != cudaSuccess) return afail(a, LBM_ERR_OOM, "binomial checkpoint allocation failed");
+            a->bslot.push_back(buf);
+            k = static_cast<int>(a->bslot.size()) - 1;
+        }
+        const size_t fbytes = static_cast<size_t>(a->n) * sizeof(double);
+        cudaStream_t st = a->view.stream;
+        double* c = a->bslot[k];
+        ADJ_TRY(a, fp64_view(a->fwd, &a->view), "state view");
+        ADJ_CUDA(a, cudaMemcpyAsync(c, a->view.f, 15 * fbytes, cudaMemcpyDeviceToDevice, st));
+        ADJ_CUDA(a, cudaMemcpyAsync(slot(c, a->n, 15), a->view.gpop, 15 * fbytes, cudaMemcpyDeviceToDevice, st));
+        for (int i = 0; i < 6; ++i)
+            ADJ_CUDA(a, cudaMemcpyAsync(slot(c, a->n, 30 + i), a->view.macro[i], fbytes, cudaMemcpyDeviceToDevice,
+                                        st));
+        ADJ_CUDA(a, cudaStreamSynchronize(st));
+        *out = k;
+        return LBM_OK;
+    }
+
+    void release(int k) { a->bfree.push_back(k); }
+};
+
+lbm_status restore_state(lbm_adjoint* a, int base)
+{
+    const long long n = a->n;
+    if (base < 0) {
+        ADJ_TRY(a, lbm_load_fields_device(a->fwd, slot(a->init, n, 0), slot(a->init, n, 1), slot(a->init, n, 2),
+                                          slot(a->init, n, 3), slot(a->init, n, 4), slot(a->init, n, 5)),
+                "reload of the initial fields");
+        return LBM_OK;
+    }
+    double* ck = a->bslot[base];
+    const double* m[6];
+    for (int i = 0; i < 6; ++i) m[i] = slot(ck, n, 30 + i);
+    ADJ_TRY(a, fp64_restore(a->fwd, ck, slot(ck, n, 15), m), "checkpoint restore");
+    return LBM_OK;
+}
+
+lbm_status advance(lbm_adjoint* a, int from, int to, uint64_t* counted)
+{
+    for (int k = from; k < to; ++k) {
+        ADJ_TRY(a, lbm_step_replay(a->fwd, 1, &a->sweeps[k], nullptr), "recomputation step");
+        ++*counted;
+    }
+    return LBM_OK;
+}
+
 double ms_since(std::chrono::steady_clock::time_point t0)
 {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -278,10 +445,11 @@ lbm_status lbm_adjoint_create(const lbm_params* p, int device, const lbm_adjoint
         g_adj_create_error = "adjoint runs need periodic_x = 1 (the slip walls are not differentiated)";
         return LBM_ERR_BAD_ARG;
     }
-    if (cfg->checkpoint_interval < 1 || cfg->check_interval < 1 || !(cfg->tolerance > 0.0) ||
+    if ((cfg->binomial_checkpoints == 0 && cfg->checkpoint_interval < 1) || cfg->binomial_checkpoints < 0 ||
+        cfg->check_interval < 1 || !(cfg->tolerance > 0.0) ||
         (cfg->max_sweeps && cfg->max_sweeps % static_cast<uint64_t>(cfg->check_interval) != 0)) {
-        g_adj_create_error = "adjoint settings: checkpoint_interval >= 1, check_interval >= 1, tolerance > 0, "
-                             "max_sweeps a multiple of check_interval";
+        g_adj_create_error = "adjoint settings: checkpoint_interval >= 1 (or binomial_checkpoints > 0), "
+                             "check_interval >= 1, tolerance > 0, max_sweeps a multiple of check_interval";
         return LBM_ERR_BAD_ARG;
     }
     lbm_adjoint* a = new lbm_adjoint();
@@ -303,7 +471,7 @@ lbm_status lbm_adjoint_create(const lbm_params* p, int device, const lbm_adjoint
     }
     const long long n = a->view.geom.n;
     a->n = n;
-    const size_t K = static_cast<size_t>(cfg->checkpoint_interval);
+    const size_t K = cfg->binomial_checkpoints > 0 ? 1 : static_cast<size_t>(cfg->checkpoint_interval);
     cudaError_t e = cudaSuccess;
     struct Req { double** dst; size_t count; };
     const Req reqs[] = {
@@ -365,7 +533,7 @@ lbm_status lbm_adjoint_forward(lbm_adjoint* a, const double* phi, const double* 
     ADJ_CUDA(a, cudaStreamSynchronize(st));
     for (double* c : a->ckpt) cudaFree(c);
     a->ckpt.clear();
-    const int K = a->cfg.checkpoint_interval;
+    const int K = a->cfg.binomial_checkpoints > 0 ? n_steps : a->cfg.checkpoint_interval;
     const int n_ckpt = (n_steps - 1) / K;
     cudaError_t e = cudaSuccess;
     for (int k = 0; k < n_ckpt; ++k) {
@@ -442,12 +610,24 @@ lbm_status lbm_adjoint_backward(lbm_adjoint* a, const double* lam_phi, const dou
         if (lam[i]) ADJ_CUDA(a, cudaMemcpyAsync(slot(a->lmac[cur], n, i), lam[i], fbytes, cudaMemcpyHostToDevice, st));
         else ADJ_CUDA(a, cudaMemsetAsync(slot(a->lmac[cur], n, i), 0, fbytes, st));
     }
-    const int K = a->cfg.checkpoint_interval;
     const int T = a->n_steps;
-    const int n_seg = (T + K - 1) / K;
+    const int K = a->cfg.binomial_checkpoints > 0 ? T : a->cfg.checkpoint_interval;
+    const int n_seg = a->cfg.binomial_checkpoints > 0 ? 0 : (T + K - 1) / K;
     double kf = 0.0;
     uint64_t adj_sweeps = 0, recomputed = 0;
     a->y_warm = -1;
+    if (a->cfg.binomial_checkpoints > 0) {
+        a->bfree.clear();
+        for (int k = static_cast<int>(a->bslot.size()) - 1; k >= 0; --k) a->bfree.push_back(k);
+        GpuOps ops{a};
+        ops.cur = cur;
+        const lbm_status s = revolve(ops, 0, T, a->cfg.binomial_checkpoints, -1);
+        if (s != LBM_OK) return s;
+        cur = ops.cur;
+        kf = ops.kf;
+        adj_sweeps = ops.adj_sweeps;
+        recomputed = ops.recomputed;
+    }
     for (int seg = n_seg - 1; seg >= 0; --seg) {
         const int s0 = seg * K;
         const int s1 = std::min(T, s0 + K);
@@ -481,5 +661,15 @@ lbm_status lbm_adjoint_backward(lbm_adjoint* a, const double* lam_phi, const dou
 }
 
 const char* lbm_adjoint_last_error(const lbm_adjoint* a) { return a ? a->err.c_str() : g_adj_create_error.c_str(); }
+
+lbm_status lbm_adjoint_schedule(int n_steps, int checkpoints, uint64_t* recompute_steps, int* peak_checkpoints)
+{
+    if (n_steps < 1 || checkpoints < 0) return LBM_ERR_BAD_ARG;
+    DryOps ops;
+    revolve(ops, 0, n_steps, checkpoints, -1);
+    if (recompute_steps) *recompute_steps = ops.steps;
+    if (peak_checkpoints) *peak_checkpoints = ops.peak;
+    return LBM_OK;
+}
 
 }  // extern "C"

@@ -155,3 +155,21 @@ def test_adjoint_needs_periodic_x():
     with pytest.raises(L.LBMError) as e:
         L.Adjoint(p)
     assert e.value.status == 4 and "periodic" in str(e.value)
+
+
+@pytest.mark.parametrize("slots", [1, 2])
+def test_binomial_checkpointing_matches_uniform(run, slots):
+    """Binomial checkpointing (revolve) recomputes the same states bitwise and
+    runs the same step adjoints in the same order: the gradient is bitwise the
+    uniform schedule's, and the recomputed steps are the dry schedule's."""
+    p, f, obj, y, sweeps, grads, stats, a = run
+    b = L.Adjoint(p, check_interval=50, tolerance=1e-13, max_sweeps=2000000, binomial_checkpoints=slots)
+    poisson(b)
+    b.forward(f, STEPS)
+    assert b.sweeps() == sweeps
+    g2, s2 = b.backward(obj.adjoint(y))
+    for k in L.FIELDS:
+        assert np.array_equal(g2[k], grads[k]), (slots, k)
+    assert s2["grad_kappa_f"] == stats["grad_kappa_f"]
+    assert s2["recompute_steps"] == L.adjoint_schedule(STEPS, slots)["recompute_steps"]
+    b.close()
