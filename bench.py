@@ -537,7 +537,7 @@ def run_adjoint(args):
     checked against centred finite differences (step 1e-6) of replayed runs."""
     import lbm_b200 as L
     n, K = args.adjoint_size, args.steps
-    tol_f, tol_a = 1e-10, 1e-13
+    tol_f, tol_a = args.adjoint_forward_tol, args.adjoint_tol
     p, f = adjoint_workload(n)
     pt, ft = adjoint_workload(n, e=0.2, kf_scale=1.05)
 
@@ -776,6 +776,9 @@ def main(argv=None):
                     help="batch: the batched droplet oscillation (64 uneven boxes, mixed precision); "
                          "adjoint: the adjoint calibration run (FP64, 64^3), --steps forward steps")
     ap.add_argument("--adjoint-size", type=int, default=64)
+    ap.add_argument("--adjoint-forward-tol", type=float, default=1e-10,
+                    help="forward Poisson exit (relative change) of the adjoint workload")
+    ap.add_argument("--adjoint-tol", type=float, default=1e-13, help="adjoint Poisson exit of the adjoint workload")
     ap.add_argument("--adjoint-directions", type=int, default=2,
                     help="seeded random phi_0 directions checked by finite differences")
     ap.add_argument("--batch-instances", type=int, default=64)

@@ -21,6 +21,7 @@
 #include <math_constants.h>
 
 #include <string>
+#include <type_traits>
 
 #include "../../include/lbm_b200.h"
 #include "adjoint.hpp"
@@ -367,8 +368,10 @@ padj_pi(Geom g, const double* __restrict__ y, double* __restrict__ pi)
 
 // One transposed sweep.  kCheck: also the relative change of
 // pi = sum_q y_q against the copy kept from the previous check (block
-// partials of sum |pi - pi_prev| and sum |pi|), and the new copy.
-template <bool kCheck>
+// partials of sum |pi - pi_prev| and sum |pi|), and the new copy.  The pull
+// from x + c_q uses the forward sweep's wrap table with the directions
+// reversed; kOff32: 32-bit offsets (15 n < 2^31).
+template <bool kCheck, bool kOff32>
 __global__ void __launch_bounds__(256)
 padj_sweep(Geom g, const double* __restrict__ yin, double* __restrict__ yout, const double* __restrict__ rho,
            const double* __restrict__ lp, double* __restrict__ pi_prev, double* __restrict__ part,
@@ -378,22 +381,27 @@ padj_sweep(Geom g, const double* __restrict__ yin, double* __restrict__ yout, co
     const bool active = cell_xyz(g, x, yy, z);
     double red[2] = {0.0, 0.0};
     if (active) {
-        const long long n = g.n;
-        const long long c = cell_of(g, x, yy, z);
+        using I = typename std::conditional<kOff32, unsigned, long long>::type;
+        const I n = static_cast<I>(g.n);
+        const I c = static_cast<I>(cell_of(g, x, yy, z));
+        const Wrap w(g, x, yy, z);
         double m[Q];
         double S = 0.0;
         static_for<0, Q>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
-            m[q] = yin[(long long)q * n + nb(g, x, yy, z, cx(q), cy(q), cz(q))];
+            const I src = (static_cast<I>(pick<cz(q)>(w.zm, z, w.zp)) * static_cast<I>(g.ly) +
+                           static_cast<I>(pick<cy(q)>(w.ym, yy, w.yp))) * static_cast<I>(g.lx) +
+                          static_cast<I>(pick<cx(q)>(w.xm, x, w.xp));
+            m[q] = __ldg(yin + static_cast<I>(q) * n + src);
             S += wE(q) * m[q];
         });
-        const double tau = 1.0 / rho[c] + 0.5;
-        const double a = 1.0 - 1.0 / tau, b = S / tau, l = lp[c];
+        const double tau = 1.0 / __ldg(rho + c) + 0.5;
+        const double a = 1.0 - 1.0 / tau, b = S / tau, l = __ldg(lp + c);
         double pi = 0.0;
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
             const double v = a * m[q] + b + l;
-            yout[(long long)q * n + c] = v;
+            yout[static_cast<I>(q) * n + c] = v;
             pi += v;
         }
         if constexpr (kCheck) {
@@ -510,10 +518,14 @@ void poisson_pi(cudaStream_t st, const Launch& L, const Geom& g, const double* y
 void poisson_sweep(cudaStream_t st, const Launch& L, const Geom& g, bool check, const double* yin, double* yout,
                    const double* rho, const double* lp, double* pi_prev, double* part)
 {
-    if (check)
-        padj_sweep<true><<<L.grid, L.block, 0, st>>>(g, yin, yout, rho, lp, pi_prev, part, L.nblocks);
-    else
-        padj_sweep<false><<<L.grid, L.block, 0, st>>>(g, yin, yout, rho, lp, pi_prev, part, L.nblocks);
+    const bool off32 = 15 * g.n < (1LL << 31);
+    if (check) {
+        if (off32) padj_sweep<true, true><<<L.grid, L.block, 0, st>>>(g, yin, yout, rho, lp, pi_prev, part, L.nblocks);
+        else padj_sweep<true, false><<<L.grid, L.block, 0, st>>>(g, yin, yout, rho, lp, pi_prev, part, L.nblocks);
+    } else {
+        if (off32) padj_sweep<false, true><<<L.grid, L.block, 0, st>>>(g, yin, yout, rho, lp, pi_prev, part, L.nblocks);
+        else padj_sweep<false, false><<<L.grid, L.block, 0, st>>>(g, yin, yout, rho, lp, pi_prev, part, L.nblocks);
+    }
 }
 
 void poisson_final(cudaStream_t st, const Launch& L, const Geom& g, const double* y, const double* h,
