@@ -133,6 +133,8 @@ public:
             fused_boundary_ = o.fused_boundary_;
             scalar_ = o.scalar_;
             scalar_scale_ = o.scalar_scale_;
+            onepass_ = o.onepass_;
+            acc_ = o.acc_;
             diag_ = o.diag_;
             csv_path_ = o.csv_path_;
             if (h_) lbm_set_check_callback(h_, &InamuroCUDA::onCheck, this);
@@ -146,7 +148,9 @@ public:
     void performTimeStepGPU()
     {
         // The reference's own guard (GPU/InamuroCUDA.cu:1846-1856).
-        if ((dual_ || shadow_) && (fused_ || fused_boundary_ || scalar_))
+        if ((dual_ || shadow_) && (fused_ || fused_boundary_ || scalar_ || onepass_ || acc_.anderson_m1 ||
+                                   acc_.two_grid || acc_.source_aware_init || acc_.pressure_relax_scale != 1.0 ||
+                                   acc_.fixed_point_relax != 1.0))
             throw std::runtime_error(
                 "fixed-point residual requires frozen split+split Poisson with unit relaxation and all "
                 "accelerators disabled");
@@ -221,12 +225,62 @@ public:
         scalar_scale_ = scale;
         applyPoissonForm();
     }
-    // The other non-production accelerators are not provided by the library;
-    // enabling one is rejected, disabling is accepted.
-    void setUseOnePassPoisson(bool e) { rejectAccelerator(e, "one-pass Poisson"); }
-    void setUseSourceAwareHHInit(bool e) { rejectAccelerator(e, "source-aware hh init"); }
-    void setUsePoissonAndersonM1(bool e) { rejectAccelerator(e, "Anderson-m1"); }
-    void setUsePoissonTwoGridCorrection(bool e) { rejectAccelerator(e, "two-grid correction"); }
+    // The one-pass form and the accelerators (GPU/InamuroCUDA.cu:780-1328,
+    // 2161-2275): lbm_set_poisson_form / lbm_set_poisson_accel.
+    void setUseOnePassPoisson(bool e)
+    {
+        onepass_ = e;
+        applyPoissonForm();
+    }
+    void setUseSourceAwareHHInit(bool e)
+    {
+        lbm_poisson_accel a = acc_;
+        a.source_aware_init = e ? 1 : 0;
+        applyPoissonAccel(a, "setUseSourceAwareHHInit");
+    }
+    void setSourceAwareHHScale(double v)
+    {
+        lbm_poisson_accel a = acc_;
+        a.source_aware_scale = v;
+        applyPoissonAccel(a, "setSourceAwareHHScale");
+    }
+    void setPressureRelaxScale(double v)
+    {
+        lbm_poisson_accel a = acc_;
+        a.pressure_relax_scale = v;
+        applyPoissonAccel(a, "setPressureRelaxScale");
+    }
+    void setPoissonFixedPointRelax(double v)
+    {
+        lbm_poisson_accel a = acc_;
+        a.fixed_point_relax = v;
+        applyPoissonAccel(a, "setPoissonFixedPointRelax");
+    }
+    void setUsePoissonAndersonM1(bool e)
+    {
+        lbm_poisson_accel a = acc_;
+        a.anderson_m1 = e ? 1 : 0;
+        applyPoissonAccel(a, "setUsePoissonAndersonM1");
+    }
+    void setPoissonAndersonBetaMax(double v)
+    {
+        lbm_poisson_accel a = acc_;
+        a.anderson_beta_max = v;
+        applyPoissonAccel(a, "setPoissonAndersonBetaMax");
+    }
+    void setUsePoissonTwoGridCorrection(bool e)
+    {
+        lbm_poisson_accel a = acc_;
+        a.two_grid = e ? 1 : 0;
+        applyPoissonAccel(a, "setUsePoissonTwoGridCorrection");
+    }
+    void setPoissonTwoGridStrength(double v)
+    {
+        lbm_poisson_accel a = acc_;
+        a.two_grid_strength = v;
+        applyPoissonAccel(a, "setPoissonTwoGridStrength");
+    }
+    // Not provided by the library; enabling it is rejected, disabling is accepted.
     void setUsePoissonSpatialDiagnostics(bool e) { rejectAccelerator(e, "spatial diagnostics"); }
     // Every Poisson segment already runs as a captured CUDA graph.
     void setUsePoissonGraph(bool) {}
@@ -234,25 +288,6 @@ public:
     void setEnablePoissonDetailTiming(bool) {}
     // Reductions are always fixed-order (deterministic).
     void setUsePoissonDeterministicReductions(bool) {}
-    void setSourceAwareHHScale(double) {}
-    void setPressureRelaxScale(double scale)
-    {
-        if (!(scale > 0.0)) throw std::invalid_argument("pressure relaxation scale must be positive");
-        if (scale != 1.0) throw std::invalid_argument("only unit pressure relaxation is supported");
-    }
-    void setPoissonFixedPointRelax(double omega)
-    {
-        if (!(omega > 0.0)) throw std::invalid_argument("Poisson fixed-point relaxation must be positive");
-        if (omega != 1.0) throw std::invalid_argument("only unit fixed-point relaxation is supported");
-    }
-    void setPoissonAndersonBetaMax(double v)
-    {
-        if (!(v >= 0.0)) throw std::invalid_argument("Poisson Anderson beta max must be non-negative");
-    }
-    void setPoissonTwoGridStrength(double v)
-    {
-        if (!(v >= 0.0)) throw std::invalid_argument("Poisson two-grid strength must be non-negative");
-    }
     void setEnablePoissonFixedPointShadow(bool e)
     {
         shadow_ = e;
@@ -358,6 +393,8 @@ private:
     bool fused_boundary_ = false;
     bool scalar_ = false;
     double scalar_scale_ = 2.0;
+    bool onepass_ = false;
+    lbm_poisson_accel acc_{1.0, 1.0, 0, 1.0, 0, 0.5, 0, 1.0};
     PoissonStepDiagnostics diag_;
     std::string csv_path_;
 
@@ -381,15 +418,22 @@ private:
     {
         if (enabled)
             throw std::invalid_argument(std::string(name) +
-                                        ": this experimental Poisson accelerator is not provided by "
-                                        "liblbm_b200 (split, fused and scalar Poisson only)");
+                                        ": not provided by liblbm_b200");
     }
 
     void applyPoissonForm()
     {
         if (!h_) return;
-        check(lbm_set_poisson_form(h_, scalar_ ? LBM_POISSON_SCALAR_JACOBI : LBM_POISSON_KINETIC, scalar_scale_, 0.0),
-              "setUseScalarPoisson");
+        const lbm_poisson_form f =
+            scalar_ ? LBM_POISSON_SCALAR_JACOBI : (onepass_ ? LBM_POISSON_ONEPASS : LBM_POISSON_KINETIC);
+        check(lbm_set_poisson_form(h_, f, scalar_scale_, 0.0), "setPoissonForm");
+    }
+
+    // Invalid values throw as the reference's setters do and leave the settings unchanged.
+    void applyPoissonAccel(const lbm_poisson_accel& a, const char* what)
+    {
+        if (h_) check(lbm_set_poisson_accel(h_, &a), what);
+        acc_ = a;
     }
 
     void applyPoissonConfig()

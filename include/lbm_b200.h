@@ -254,12 +254,35 @@ lbm_status lbm_get_poisson(const lbm_handle* h, lbm_poisson_cfg* cfg);
 typedef enum {
     LBM_POISSON_KINETIC = 0,
     LBM_POISSON_SCALAR_JACOBI = 1,
-    LBM_POISSON_SCALAR_RB = 2
+    LBM_POISSON_SCALAR_RB = 2,
+    LBM_POISSON_ONEPASS = 3      /* the reference's one-pass form (setUseOnePassPoisson,
+                                    GPU/InamuroCUDA.cu:780-844): the kinetic map on the
+                                    pre-collision h with the accelerators of lbm_poisson_accel */
 } lbm_poisson_form;
 lbm_status lbm_set_poisson_form(lbm_handle* h, lbm_poisson_form form, double source_scale, double omega);
 /* Current form, source scale and the relaxation in use (the computed optimum
  * when 0 was set); any pointer may be NULL. */
 lbm_status lbm_get_poisson_form(const lbm_handle* h, lbm_poisson_form* form, double* source_scale, double* omega);
+
+/* The reference's Poisson accelerators (InamuroCUDA setters,
+ * GPU/InamuroCUDA.hpp:67-88; CLI flags of GPU/main.cpp:156-171), FP64.
+ * pressure_relax_scale, fixed_point_relax, Anderson-m1 and two-grid need the
+ * one-pass form (LBM_ERR_BAD_ARG at the next step otherwise); source-aware h
+ * init applies to the kinetic and one-pass forms.  None combines with the
+ * dual residual (the reference refuses that too).  Defaults: 1, 1, off, 1,
+ * off, 0.5, off, 1. */
+typedef struct {
+    double pressure_relax_scale;   /* --pressure-relax-scale: scales (h - E p) / tau_h */
+    double fixed_point_relax;      /* --poisson-fixed-point-relax: h = h_old + omega (T(h) - h_old) */
+    int anderson_m1;               /* --poisson-anderson-m1 */
+    double anderson_beta_max;      /* --poisson-anderson-beta-max: alpha clamped to [-b, 1 + b] */
+    int two_grid;                  /* --poisson-two-grid-correction */
+    double two_grid_strength;      /* --poisson-two-grid-strength */
+    int source_aware_init;         /* --source-aware-hh-init */
+    double source_aware_scale;     /* --source-aware-hh-scale */
+} lbm_poisson_accel;
+lbm_status lbm_set_poisson_accel(lbm_handle* h, const lbm_poisson_accel* a);
+lbm_status lbm_get_poisson_accel(const lbm_handle* h, lbm_poisson_accel* out);
 
 /* Advances n_steps time steps (InamuroCUDA::performTimeStepGPU,
  * GPU/InamuroCUDA.cu:2372-2442).  `stats` (may be NULL) receives n_steps

@@ -111,6 +111,14 @@ class Diagnostics(C.Structure):
         return {k: getattr(self, k).as_dict() for k in self.NAMES}
 
 
+class PoissonAccel(C.Structure):
+    """lbm_poisson_accel: the reference's Poisson accelerator settings."""
+    _fields_ = [("pressure_relax_scale", C.c_double), ("fixed_point_relax", C.c_double),
+                ("anderson_m1", C.c_int), ("anderson_beta_max", C.c_double), ("two_grid", C.c_int),
+                ("two_grid_strength", C.c_double), ("source_aware_init", C.c_int),
+                ("source_aware_scale", C.c_double)]
+
+
 class AdjointCfg(C.Structure):
     """lbm_adjoint_cfg: checkpoint interval and the adjoint Poisson solve's exit."""
     _fields_ = [("checkpoint_interval", C.c_int), ("check_interval", C.c_int), ("tolerance", C.c_double),
@@ -163,6 +171,8 @@ def load_library(path: str = LIB_PATH):
     L.lbm_get_poisson.argtypes = [H, C.POINTER(PoissonCfg)]
     L.lbm_set_poisson_form.argtypes = [H, C.c_int, C.c_double, C.c_double]
     L.lbm_get_poisson_form.argtypes = [H, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.lbm_set_poisson_accel.argtypes = [H, C.POINTER(PoissonAccel)]
+    L.lbm_get_poisson_accel.argtypes = [H, C.POINTER(PoissonAccel)]
     L.lbm_step.argtypes = [H, C.c_int, C.POINTER(StepStats)]
     L.lbm_step_replay.argtypes = [H, C.c_int, C.POINTER(C.c_uint64), C.POINTER(StepStats)]
     L.lbm_download.argtypes = [H, C.c_int, dp]
@@ -410,7 +420,7 @@ class InamuroCUDA:
         cfg = PoissonCfg(check_interval, tolerance, int(dual), max_sweeps, int(fail_on_limit))
         self._check(self._lib.lbm_set_poisson(self._h, C.byref(cfg)), "set_poisson")
 
-    POISSON_FORMS = {"kinetic": 0, "scalar": 1, "scalar-rb": 2}
+    POISSON_FORMS = {"kinetic": 0, "scalar": 1, "scalar-rb": 2, "onepass": 3}
 
     def set_poisson_form(self, form: str = "kinetic", source_scale: float = 2.0, omega: float = 0.0):
         """lbm_set_poisson_form: "kinetic" (the production solve), "scalar"
@@ -418,6 +428,19 @@ class InamuroCUDA:
         the same scalar equation; omega 0 = the optimum for the box)."""
         self._check(self._lib.lbm_set_poisson_form(self._h, self.POISSON_FORMS[form], source_scale, omega),
                     "set_poisson_form")
+
+    def set_poisson_accel(self, **kw):
+        """lbm_set_poisson_accel: the reference's accelerators (pressure_relax_scale,
+        fixed_point_relax, anderson_m1, anderson_beta_max, two_grid,
+        two_grid_strength, source_aware_init, source_aware_scale); unnamed
+        settings keep their current values."""
+        a = PoissonAccel()
+        self._check(self._lib.lbm_get_poisson_accel(self._h, C.byref(a)), "get_poisson_accel")
+        for k, v in kw.items():
+            if not any(k == f for f, _ in PoissonAccel._fields_):
+                raise KeyError(k)
+            setattr(a, k, v)
+        self._check(self._lib.lbm_set_poisson_accel(self._h, C.byref(a)), "set_poisson_accel")
 
     def poisson_form(self) -> Dict[str, float]:
         f, sc, om = C.c_int(), C.c_double(), C.c_double()

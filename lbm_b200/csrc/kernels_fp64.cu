@@ -421,7 +421,8 @@ prep_kernel(Geom g, const DevState* __restrict__ ds, const double* __restrict__ 
 __global__ void __launch_bounds__(256)
 poisson_init_kernel(Geom g, int h_loaded, const double* __restrict__ hload,
                     double* __restrict__ hout, const double* __restrict__ p,
-                    const double* __restrict__ rho, const double* __restrict__ s)
+                    const double* __restrict__ rho, const double* __restrict__ s, int source_aware,
+                    double sa_scale)
 {
     int x, y, z;
     if (!tile_coords(g, x, y, z)) return;
@@ -433,8 +434,10 @@ poisson_init_kernel(Geom g, int h_loaded, const double* __restrict__ hload,
     static_for<0, Q>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
         constexpr double E = wE(q);
-        // h = p * E_q after update_hh (CPU/Inamuro.cpp:835), or the loaded h.
-        const double h0 = h_loaded ? hload[(long long)q * g.n + c] : pv * E;
+        // h = p * E_q after update_hh (CPU/Inamuro.cpp:835), or the loaded h;
+        // source-aware: E_q p - scale tau_h (E_q / 3) s (GPU/InamuroCUDA.cu:903-929).
+        const double h0 = source_aware ? E * pv - sa_scale * tauh * ((E / 3.0) * sv)
+                                       : (h_loaded ? hload[(long long)q * g.n + c] : pv * E);
         const double hequ = E * pv;
         hout[(long long)q * g.n + c] = h0 - div_rn(h0 - hequ, tauh, inv_tauh) - (E / 3.0) * sv;
     });
@@ -790,6 +793,193 @@ scalar_check_kernel(Geom g, int zrun, const double* __restrict__ pin, double* __
     block_sum_store<5>(red, part, nblocks, block_linear());
 }
 
+// ---- the reference's one-pass Poisson form -------------------------------
+// State: the pre-collision h (after stream and bounce) and p = sum_q h, as the
+// reference's Poisson loop keeps them (GPU/InamuroCUDA.cu:2199-2330).
+
+// h0 of a one-pass solve: the loaded h (first step after a load) or E_q p
+// (updateHHKernel, .cu:1377-1396); with source_aware, the reference's
+// sourceAwareHHInitKernel (.cu:903-929): E_q p - scale tau_h (E_q / 3) s.
+__global__ void __launch_bounds__(256)
+onepass_init_kernel(Geom g, int h_loaded, const double* __restrict__ hload, double* __restrict__ hh,
+                    const double* __restrict__ p, const double* __restrict__ rho, const double* __restrict__ s,
+                    int source_aware, double sa_scale)
+{
+    int x, y, z;
+    if (!tile_coords(g, x, y, z)) return;
+    const long long c = cell_of(g, x, y, z);
+    const double pv = p[c];
+    const double tauh = 1.0 / rho[c] + 0.5;
+    const double sv = s[c];
+    static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        constexpr double E = wE(q);
+        double h;
+        if (source_aware) h = E * pv - sa_scale * tauh * ((E / 3.0) * sv);
+        else h = h_loaded ? hload[(long long)q * g.n + c] : pv * E;
+        hh[(long long)q * g.n + c] = h;
+    });
+}
+
+// One one-pass sweep (collisionStreamBoundaryPressureKernel, .cu:780-844):
+// each population collides at its source cell x - c_q with that cell's p,
+// rho and s (relax scales the relaxation term), streams, the x walls
+// overwrite the incoming ones, then h = h_old + omega (h - h_old) against the
+// cell's own previous h, and p = sum_q h.
+__global__ void __launch_bounds__(256)
+onepass_sweep_kernel(Geom g, const double* __restrict__ hin, double* __restrict__ hout,
+                     const double* __restrict__ pin, double* __restrict__ pout, const double* __restrict__ rho,
+                     const double* __restrict__ s, double relax, double omega)
+{
+    int x, y, z;
+    if (!tile_coords(g, x, y, z)) return;
+    const Wrap w(g, x, y, z);
+    double h[Q];
+    static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        constexpr double E = wE(q);
+        const long long src = pull_src<q>(g, w, x, y, z);
+        const double tauh = 1.0 / __ldg(rho + src) + 0.5;
+        const double hequ = E * __ldg(pin + src);
+        const double h_old = __ldg(hin + (long long)q * g.n + src);
+        h[q] = h_old - relax * (h_old - hequ) / tauh - (E / 3.0) * __ldg(s + src);
+    });
+    bounce_regs(h, g, x);
+    const long long c = cell_of(g, x, y, z);
+    double psum = 0.0;
+    static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        const double h_old = hin[(long long)q * g.n + c];
+        const double hv = h_old + omega * (h[q] - h_old);
+        hout[(long long)q * g.n + c] = hv;
+        psum = psum + hv;
+    });
+    pout[c] = psum;
+}
+
+// Anderson-m1 on the one-pass map (.cu:931-1013, 2230-2275).  Residual r =
+// image - old.  First sweep of a solve: keep r and the image.  Later sweeps:
+// partial sums of prev_r (r - prev_r) and (r - prev_r)^2 (the host forms
+// alpha), then image <- (1 - alpha) prev_image + alpha image, history <-
+// this sweep's r and image, p = sum_q of the result.
+__global__ void __launch_bounds__(256)
+anderson_store_kernel(long long count, const double* __restrict__ hold, const double* __restrict__ himg,
+                      double* __restrict__ prev_r, double* __restrict__ prev_img)
+{
+    for (long long i = blockIdx.x * 256LL + threadIdx.x; i < count; i += (long long)gridDim.x * 256) {
+        prev_r[i] = himg[i] - hold[i];
+        prev_img[i] = himg[i];
+    }
+}
+
+__global__ void __launch_bounds__(256)
+anderson_dot_kernel(long long count, const double* __restrict__ hold, const double* __restrict__ himg,
+                    const double* __restrict__ prev_r, double* __restrict__ part)
+{
+    double red[2] = {0.0, 0.0};
+    for (long long i = blockIdx.x * 256LL + threadIdx.x; i < count; i += (long long)gridDim.x * 256) {
+        const double r = himg[i] - hold[i];
+        const double d = r - prev_r[i];
+        red[0] += prev_r[i] * d;
+        red[1] += d * d;
+    }
+    block_sum_store<2>(red, part, gridDim.x, blockIdx.x);
+}
+
+__global__ void __launch_bounds__(256)
+anderson_apply_kernel(Geom g, const double* __restrict__ hold, double* __restrict__ himg,
+                      double* __restrict__ prev_r, double* __restrict__ prev_img, double* __restrict__ pimg,
+                      double alpha)
+{
+    int x, y, z;
+    if (!tile_coords(g, x, y, z)) return;
+    const long long c = cell_of(g, x, y, z);
+    double psum = 0.0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const long long i = (long long)q * g.n + c;
+        const double cur = himg[i];
+        const double acc = (1.0 - alpha) * prev_img[i] + alpha * cur;
+        prev_r[i] = cur - hold[i];
+        prev_img[i] = cur;
+        himg[i] = acc;
+        psum += acc;
+    }
+    pimg[c] = psum;
+}
+
+// Check of the one-pass form: gauge p -= shift, h_q -= E_q shift
+// (applyPressureGaugeKernel, .cu:716-730), relative change (:1015-1103), the
+// results into the parity-0 buffers.  FIN_CHECK layout, dual terms zero.
+__global__ void __launch_bounds__(256)
+onepass_check_kernel(Geom g, int zrun, const double* __restrict__ hin, double* __restrict__ hout,
+                     const double* __restrict__ pin, double* __restrict__ p, double* __restrict__ p_prev,
+                     const DevState* __restrict__ ds, double* __restrict__ part, long long nblocks)
+{
+    int x, y, z0, z1;
+    const bool active = tile_zrun(g, zrun, x, y, z0, z1);
+    double red[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const double shift = ds->sigma;
+    for (int z = z0; active && z < z1; ++z) {
+        const long long c = cell_of(g, x, y, z);
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            hout[(long long)q * g.n + c] = hin[(long long)q * g.n + c] - wE(q) * shift;
+        });
+        const double pv = pin[c] - shift;
+        red[0] += fabs(pv - p_prev[c]);
+        red[1] += fabs(pv);
+        p_prev[c] = pv;
+        p[c] = pv;
+    }
+    block_sum_store<5>(red, part, nblocks, block_linear());
+}
+
+// Two-grid correction (.cu:1198-1255, 1284-1328): per 4 x 4 x 4 block (partial
+// at the far edges) the sum of the check's change p - p_prev (p gauged), one
+// thread per block in a fixed order; after an unconverged check
+// p += strength * block_sum / block_cells, p_prev = p, h_q += E_q times that.
+constexpr int kTwoGridBlock = 4;
+
+__global__ void __launch_bounds__(256)
+twogrid_sums_kernel(Geom g, const double* __restrict__ p, const double* __restrict__ p_prev,
+                    const DevState* __restrict__ ds, double* __restrict__ bsum, int bxn, int byn, int bzn)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= bxn * byn * bzn) return;
+    const int bx = b % bxn, by = (b / bxn) % byn, bz = b / (bxn * byn);
+    const double shift = ds->sigma;
+    double acc = 0.0;
+    for (int z = bz * kTwoGridBlock; z < min(bz * kTwoGridBlock + kTwoGridBlock, g.lz); ++z)
+        for (int y = by * kTwoGridBlock; y < min(by * kTwoGridBlock + kTwoGridBlock, g.ly); ++y)
+            for (int x = bx * kTwoGridBlock; x < min(bx * kTwoGridBlock + kTwoGridBlock, g.lx); ++x) {
+                const long long c = cell_of(g, x, y, z);
+                acc += (p[c] - shift) - p_prev[c];
+            }
+    bsum[b] = acc;
+}
+
+__global__ void __launch_bounds__(256)
+twogrid_correct_kernel(Geom g, double* __restrict__ hh, double* __restrict__ p, double* __restrict__ p_prev,
+                       const double* __restrict__ bsum, int bxn, int byn, double strength)
+{
+    int x, y, z;
+    if (!tile_coords(g, x, y, z)) return;
+    const int bx = x / kTwoGridBlock, by = y / kTwoGridBlock, bz = z / kTwoGridBlock;
+    const int x0 = bx * kTwoGridBlock, y0 = by * kTwoGridBlock, z0 = bz * kTwoGridBlock;
+    const int cells = max(1, (min(x0 + kTwoGridBlock, g.lx) - x0) * (min(y0 + kTwoGridBlock, g.ly) - y0) *
+                                 (min(z0 + kTwoGridBlock, g.lz) - z0));
+    const double corr = strength * bsum[(bz * byn + by) * bxn + bx] / static_cast<double>(cells);
+    const long long c = cell_of(g, x, y, z);
+    const double pc = p[c] + corr;
+    p[c] = pc;
+    p_prev[c] = pc;
+    static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        hh[(long long)q * g.n + c] += wE(q) * corr;
+    });
+}
+
 __global__ void __launch_bounds__(256)
 correct_kernel(Geom g, double* __restrict__ u, double* __restrict__ v, double* __restrict__ w,
                const double* __restrict__ p, const double* __restrict__ rho)
@@ -870,9 +1060,10 @@ void prep(cudaStream_t st, const Launch& L, const Geom& g, const DevState* ds, c
 
 void poisson_init(cudaStream_t st, const Launch& L, const Geom& g, bool h_loaded,
                   const double* hload, double* hout, const double* p, const double* rho,
-                  const double* s)
+                  const double* s, bool source_aware, double sa_scale)
 {
-    poisson_init_kernel<<<L.grid, L.block, 0, st>>>(g, h_loaded ? 1 : 0, hload, hout, p, rho, s);
+    poisson_init_kernel<<<L.grid, L.block, 0, st>>>(g, h_loaded ? 1 : 0, hload, hout, p, rho, s,
+                                                    source_aware ? 1 : 0, sa_scale);
 }
 
 void sweep(cudaStream_t st, const Launch& L, const Geom& g, const double* hin, double* hout,
@@ -953,6 +1144,67 @@ void scalar_check(cudaStream_t st, const Launch& L, const Geom& g, const double*
                   const DevState* ds, double* part)
 {
     scalar_check_kernel<<<L.cgrid, L.block, 0, st>>>(g, L.zrun, pin, p, p_prev, ds, part, L.cnblocks);
+}
+
+void onepass_init(cudaStream_t st, const Launch& L, const Geom& g, bool h_loaded, const double* hload, double* hh,
+                  const double* p, const double* rho, const double* s, bool source_aware, double sa_scale)
+{
+    onepass_init_kernel<<<L.grid, L.block, 0, st>>>(g, h_loaded ? 1 : 0, hload, hh, p, rho, s, source_aware ? 1 : 0,
+                                                    sa_scale);
+}
+
+void onepass_sweep(cudaStream_t st, const Launch& L, const Geom& g, const double* hin, double* hout, const double* pin,
+                   double* pout, const double* rho, const double* s, double relax, double omega)
+{
+    onepass_sweep_kernel<<<L.grid, L.block, 0, st>>>(g, hin, hout, pin, pout, rho, s, relax, omega);
+}
+
+void anderson_store(cudaStream_t st, const Geom& g, const double* hold, const double* himg, double* prev_r,
+                    double* prev_img)
+{
+    anderson_store_kernel<<<kAndersonBlocks, 256, 0, st>>>(15 * g.n, hold, himg, prev_r, prev_img);
+}
+
+void anderson_dot(cudaStream_t st, const Geom& g, const double* hold, const double* himg, const double* prev_r,
+                  double* part)
+{
+    anderson_dot_kernel<<<kAndersonBlocks, 256, 0, st>>>(15 * g.n, hold, himg, prev_r, part);
+}
+
+void anderson_apply(cudaStream_t st, const Launch& L, const Geom& g, const double* hold, double* himg, double* prev_r,
+                    double* prev_img, double* pimg, double alpha)
+{
+    anderson_apply_kernel<<<L.grid, L.block, 0, st>>>(g, hold, himg, prev_r, prev_img, pimg, alpha);
+}
+
+void onepass_check(cudaStream_t st, const Launch& L, const Geom& g, const double* hin, double* hout, const double* pin,
+                   double* p, double* p_prev, const DevState* ds, double* part)
+{
+    onepass_check_kernel<<<L.cgrid, L.block, 0, st>>>(g, L.zrun, hin, hout, pin, p, p_prev, ds, part, L.cnblocks);
+}
+
+int twogrid_blocks(const Geom& g, int* bxn, int* byn, int* bzn)
+{
+    *bxn = (g.lx + kTwoGridBlock - 1) / kTwoGridBlock;
+    *byn = (g.ly + kTwoGridBlock - 1) / kTwoGridBlock;
+    *bzn = (g.lz + kTwoGridBlock - 1) / kTwoGridBlock;
+    return *bxn * *byn * *bzn;
+}
+
+void twogrid_sums(cudaStream_t st, const Geom& g, const double* p, const double* p_prev, const DevState* ds,
+                  double* bsum)
+{
+    int bxn, byn, bzn;
+    const int nb = twogrid_blocks(g, &bxn, &byn, &bzn);
+    twogrid_sums_kernel<<<(nb + 255) / 256, 256, 0, st>>>(g, p, p_prev, ds, bsum, bxn, byn, bzn);
+}
+
+void twogrid_correct(cudaStream_t st, const Launch& L, const Geom& g, double* hh, double* p, double* p_prev,
+                     const double* bsum, double strength)
+{
+    int bxn, byn, bzn;
+    twogrid_blocks(g, &bxn, &byn, &bzn);
+    twogrid_correct_kernel<<<L.grid, L.block, 0, st>>>(g, hh, p, p_prev, bsum, bxn, byn, strength);
 }
 
 void correct(cudaStream_t st, const Launch& L, const Geom& g, double* u, double* v, double* w,

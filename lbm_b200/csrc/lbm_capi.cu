@@ -85,6 +85,12 @@ struct lbm_handle {
     int pform = LBM_POISSON_KINETIC;     // lbm_poisson_form
     double scalar_scale = 2.0;           // scalar forms: source scale (reference default 2.0)
     double sor_omega = 0.0;              // red-black form: relaxation (0: from the box size)
+    lbm_poisson_accel paccel{1.0, 1.0, 0, 1.0, 0, 0.5, 0, 1.0};   // the reference's accelerator settings
+    double* and_r = nullptr;             // Anderson-m1 history: previous residual, previous image (15 n each)
+    double* and_i = nullptr;
+    double* and_part = nullptr;          // 2 x kAndersonBlocks dot partials, and their pinned copy
+    double* and_host = nullptr;
+    double* tg_sum = nullptr;            // two-grid 4^3 block sums
 };
 
 namespace {
@@ -130,6 +136,13 @@ void free_all(lbm_handle* h)
         *p = nullptr;
     }
     mixed_free(h->mb);
+    double** extra[] = {&h->and_r, &h->and_i, &h->and_part, &h->tg_sum};
+    for (double** p : extra) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
+    if (h->and_host) cudaFreeHost(h->and_host);
+    h->and_host = nullptr;
     if (h->stats_part) cudaFree(h->stats_part);
     if (h->stats_dev) cudaFree(h->stats_dev);
     h->stats_part = nullptr;
@@ -321,6 +334,82 @@ void fill_stats(const lbm_handle* h, const DevState& d, lbm_step_stats* s)
 }
 
 // One time step.  replay > 0 forces that many sweeps.
+lbm_status ensure_onepass_buffers(lbm_handle* h)
+{
+    const size_t pop = 15 * static_cast<size_t>(h->geom.n) * sizeof(double);
+    if (h->paccel.anderson_m1 && !h->and_r) {
+        LBM_CUDA(h, cudaMalloc(&h->and_r, pop));
+        LBM_CUDA(h, cudaMalloc(&h->and_i, pop));
+        LBM_CUDA(h, cudaMalloc(&h->and_part, 2 * fp64::kAndersonBlocks * sizeof(double)));
+        LBM_CUDA(h, cudaMallocHost(&h->and_host, 2 * fp64::kAndersonBlocks * sizeof(double)));
+    }
+    if (h->paccel.two_grid && !h->tg_sum) {
+        int bx, by, bz;
+        const int nb = fp64::twogrid_blocks(h->geom, &bx, &by, &bz);
+        LBM_CUDA(h, cudaMalloc(&h->tg_sum, static_cast<size_t>(nb) * sizeof(double)));
+    }
+    return LBM_OK;
+}
+
+// One segment of the one-pass form (check_interval sweeps, the check, the
+// two-grid correction after an unconverged check), launched directly: the
+// Anderson mixing needs its coefficient on the host every sweep, as in the
+// reference (GPU/InamuroCUDA.cu:2199-2275).  h and p start and end in the
+// parity-0 buffers (b.h[0], b.p); *has_history: Anderson history of this solve.
+lbm_status onepass_segment(lbm_handle* h, bool* has_history, uint64_t* launches)
+{
+    cudaStream_t st = h->stream;
+    const Geom& g = h->geom;
+    const Launch& L = h->L;
+    Fp64Buffers& b = h->b;
+    const lbm_poisson_accel& acc = h->paccel;
+    double* H[2] = {b.h[0], b.h[1]};
+    double* P[2] = {b.p, b.p_chk};
+    int c = 0;
+    for (int i = 0; i < h->pcfg.check_interval; ++i) {
+        fp64::onepass_sweep(st, L, g, H[c], H[1 - c], P[c], P[1 - c], b.rho, b.s, acc.pressure_relax_scale,
+                            acc.fixed_point_relax);
+        ++*launches;
+        if (acc.anderson_m1) {
+            if (!*has_history) {
+                fp64::anderson_store(st, g, H[c], H[1 - c], h->and_r, h->and_i);
+                *has_history = true;
+                ++*launches;
+            } else {
+                fp64::anderson_dot(st, g, H[c], H[1 - c], h->and_r, h->and_part);
+                LBM_CUDA(h, cudaMemcpyAsync(h->and_host, h->and_part, 2 * fp64::kAndersonBlocks * sizeof(double),
+                                            cudaMemcpyDeviceToHost, st));
+                LBM_CUDA(h, cudaStreamSynchronize(st));
+                double num = 0.0, den = 0.0;
+                for (int k = 0; k < fp64::kAndersonBlocks; ++k) num += h->and_host[k];
+                for (int k = 0; k < fp64::kAndersonBlocks; ++k) den += h->and_host[fp64::kAndersonBlocks + k];
+                double alpha = 1.0;
+                if (den > 1.0e-300) alpha = -num / den;
+                if (!std::isfinite(alpha)) alpha = 1.0;
+                alpha = std::max(-acc.anderson_beta_max, std::min(1.0 + acc.anderson_beta_max, alpha));
+                fp64::anderson_apply(st, L, g, H[c], H[1 - c], h->and_r, h->and_i, P[1 - c], alpha);
+                *launches += 2;
+            }
+        }
+        c = 1 - c;
+    }
+    fp64::p_sum(st, L, g, P[c], b.part_a);
+    finalize(st, FIN_SIGMA, h->ds, b.part_a, L.cnblocks, nullptr, 0, nullptr, 0);
+    if (acc.two_grid) fp64::twogrid_sums(st, g, P[c], b.p_prev, h->ds, h->tg_sum);
+    fp64::onepass_check(st, L, g, H[c], H[0], P[c], b.p, b.p_prev, h->ds, b.part_b);
+    finalize(st, FIN_CHECK, h->ds, b.part_b, L.cnblocks, nullptr, 0, nullptr, 0);
+    LBM_CUDA(h, cudaMemcpyAsync(h->ds_host, h->ds, sizeof(DevState), cudaMemcpyDeviceToHost, st));
+    LBM_CUDA(h, cudaStreamSynchronize(st));
+    *launches += 4 + (acc.two_grid ? 1 : 0);
+    const DevState& dh = *h->ds_host;
+    if (acc.two_grid && !dh.error && !dh.converged && dh.l1_delta > 0.0) {
+        fp64::twogrid_correct(st, L, g, b.h[0], b.p, b.p_prev, h->tg_sum, acc.two_grid_strength);
+        LBM_CUDA(h, cudaGetLastError());
+        ++*launches;
+    }
+    return LBM_OK;
+}
+
 lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
 {
     cudaStream_t st = h->stream;
@@ -329,9 +418,20 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
     const int ci = h->pcfg.check_interval;
     const int dual = h->pcfg.dual_residual != 0;   // residual kernels run in exit and shadow mode
     const int form = h->pform;
-    if (form != LBM_POISSON_KINETIC && dual)
+    const lbm_poisson_accel& acc = h->paccel;
+    const bool onepass_only = acc.pressure_relax_scale != 1.0 || acc.fixed_point_relax != 1.0 || acc.anderson_m1 ||
+                              acc.two_grid;
+    if (dual && (form != LBM_POISSON_KINETIC || onepass_only || acc.source_aware_init))
         return fail(h, LBM_ERR_BAD_ARG,
-                    "fixed-point residual requires the kinetic (split) Poisson form");
+                    "fixed-point residual requires the kinetic (split) Poisson form with unit relaxation and "
+                    "all accelerators disabled");
+    if (onepass_only && form != LBM_POISSON_ONEPASS)
+        return fail(h, LBM_ERR_BAD_ARG,
+                    "relaxation scales, Anderson-m1 and two-grid correction need the one-pass Poisson form");
+    if (form == LBM_POISSON_ONEPASS) {
+        const lbm_status s = ensure_onepass_buffers(h);
+        if (s != LBM_OK) return s;
+    }
     if (dual) {
         const lbm_status s = ensure_dual_buffer(h);
         if (s != LBM_OK) return s;
@@ -360,7 +460,11 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
         fp64::prep(st, L, g, h->ds, b.dux, b.dvy, b.dwz, b.p, b.s, b.part_prep);
         finalize(st, FIN_PREP, h->ds, b.part_prep, L.nblocks, nullptr, 0, nullptr, 0);
         if (form == LBM_POISSON_KINETIC) {
-            fp64::poisson_init(st, L, g, h->h_loaded, b.h[1], b.h[0], b.p, b.rho, b.s);
+            fp64::poisson_init(st, L, g, h->h_loaded, b.h[1], b.h[0], b.p, b.rho, b.s, acc.source_aware_init != 0,
+                               acc.source_aware_scale);
+        } else if (form == LBM_POISSON_ONEPASS) {
+            fp64::onepass_init(st, L, g, h->h_loaded, b.h[1], b.h[0], b.p, b.rho, b.s, acc.source_aware_init != 0,
+                               acc.source_aware_scale);
         } else if (form == LBM_POISSON_SCALAR_RB) {
             fp64::scalar_rhs_sum(st, L, g, b.rho, b.s, h->scalar_scale, b.part_a);
             finalize(st, FIN_RHS, h->ds, b.part_a, L.cnblocks, nullptr, 0, nullptr, 0);
@@ -385,21 +489,30 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
     if (form == LBM_POISSON_SCALAR_JACOBI) launches = 6;   // no h initialisation
     if (form == LBM_POISSON_SCALAR_RB) launches = 8;       // no h initialisation; right-hand-side mean
     uint64_t fused_sweeps = 0;
+    bool anderson_history = false;
     for (;;) {
         const int n_normal =
             form != LBM_POISSON_KINETIC ? ci : (dual ? (first_seg ? ci - 1 : ci - 2) : ci - 1);
-        SegKey key{hcur, n_normal, dual, form};
-        cudaGraphExec_t ex = nullptr;
-        int end_parity = hcur;
-        const lbm_status gs = get_segment(h, key, &ex, &end_parity);
-        if (gs != LBM_OK) return gs;
-        LBM_CUDA(h, cudaGraphLaunch(ex, st));
-        LBM_CUDA(h, cudaStreamSynchronize(st));
-        hcur = end_parity;
+        if (form == LBM_POISSON_ONEPASS) {
+            const lbm_status os = onepass_segment(h, &anderson_history, &launches);
+            if (os != LBM_OK) return os;
+            hcur = 0;
+        } else {
+            SegKey key{hcur, n_normal, dual, form};
+            cudaGraphExec_t ex = nullptr;
+            int end_parity = hcur;
+            const lbm_status gs = get_segment(h, key, &ex, &end_parity);
+            if (gs != LBM_OK) return gs;
+            LBM_CUDA(h, cudaGraphLaunch(ex, st));
+            LBM_CUDA(h, cudaStreamSynchronize(st));
+            hcur = end_parity;
+        }
         h->h_last = hcur;
         // sweep-equivalents executed (plain, A, B, C) and actual launches
         // (two plain sweeps per launch where the mixed box fuses them)
-        if (form != LBM_POISSON_KINETIC) {
+        if (form == LBM_POISSON_ONEPASS) {
+            kernels += static_cast<uint64_t>(n_normal);   // launches counted by onepass_segment
+        } else if (form != LBM_POISSON_KINETIC) {
             // scalar sweeps (red-black: two launches each), p sum, check, 2 finalize
             kernels += static_cast<uint64_t>(n_normal);
             launches += static_cast<uint64_t>(n_normal) * (form == LBM_POISSON_SCALAR_RB ? 2 : 1) + 4;
@@ -757,10 +870,11 @@ lbm_status lbm_set_poisson(lbm_handle* h, const lbm_poisson_cfg* cfg)
 lbm_status lbm_set_poisson_form(lbm_handle* h, lbm_poisson_form form, double source_scale, double omega)
 {
     if (check_handle(h) != LBM_OK) return LBM_ERR_BAD_ARG;
-    if (form != LBM_POISSON_KINETIC && form != LBM_POISSON_SCALAR_JACOBI && form != LBM_POISSON_SCALAR_RB)
+    if (form != LBM_POISSON_KINETIC && form != LBM_POISSON_SCALAR_JACOBI && form != LBM_POISSON_SCALAR_RB &&
+        form != LBM_POISSON_ONEPASS)
         return fail(h, LBM_ERR_BAD_ARG, "unknown Poisson form");
     if (form != LBM_POISSON_KINETIC && h->precision != LBM_PRECISION_FP64)
-        return fail(h, LBM_ERR_BAD_ARG, "the scalar Poisson forms run in FP64 precision only");
+        return fail(h, LBM_ERR_BAD_ARG, "the scalar and one-pass Poisson forms run in FP64 precision only");
     if (!std::isfinite(source_scale)) return fail(h, LBM_ERR_BAD_ARG, "scalar source scale must be finite");
     if (!(omega == 0.0 || (omega > 0.0 && omega < 2.0)))
         return fail(h, LBM_ERR_BAD_ARG, "SOR relaxation must be 0 (automatic) or in (0, 2)");
@@ -784,6 +898,38 @@ lbm_status lbm_set_poisson_form(lbm_handle* h, lbm_poisson_form form, double sou
     h->pform = form;
     h->scalar_scale = source_scale;
     h->sor_omega = w;
+    return LBM_OK;
+}
+
+lbm_status lbm_set_poisson_accel(lbm_handle* h, const lbm_poisson_accel* a)
+{
+    if (check_handle(h) != LBM_OK || !a) return fail(h, LBM_ERR_BAD_ARG, "null settings");
+    // The reference setters' own checks (GPU/InamuroCUDA.cu:2488-2540).
+    if (!(a->pressure_relax_scale > 0.0)) return fail(h, LBM_ERR_BAD_ARG, "pressure relaxation scale must be positive");
+    if (!(a->fixed_point_relax > 0.0))
+        return fail(h, LBM_ERR_BAD_ARG, "Poisson fixed-point relaxation must be positive");
+    if (!(a->anderson_beta_max >= 0.0))
+        return fail(h, LBM_ERR_BAD_ARG, "Poisson Anderson beta max must be non-negative");
+    if (!(a->two_grid_strength >= 0.0))
+        return fail(h, LBM_ERR_BAD_ARG, "Poisson two-grid strength must be non-negative");
+    if (!std::isfinite(a->source_aware_scale)) return fail(h, LBM_ERR_BAD_ARG, "source-aware scale must be finite");
+    if ((a->pressure_relax_scale != 1.0 || a->fixed_point_relax != 1.0 || a->anderson_m1 || a->two_grid ||
+         a->source_aware_init) && h->precision != LBM_PRECISION_FP64)
+        return fail(h, LBM_ERR_BAD_ARG, "the Poisson accelerators run in FP64 precision only");
+    const bool init_changed = (a->source_aware_init != 0) != (h->paccel.source_aware_init != 0) ||
+                              a->source_aware_scale != h->paccel.source_aware_scale;
+    h->paccel = *a;
+    if (init_changed) {
+        for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second.first);
+        h->graphs.clear();
+    }
+    return LBM_OK;
+}
+
+lbm_status lbm_get_poisson_accel(const lbm_handle* h, lbm_poisson_accel* out)
+{
+    if (!h || !out) return LBM_ERR_BAD_ARG;
+    *out = h->paccel;
     return LBM_OK;
 }
 

@@ -120,7 +120,8 @@ void prep(cudaStream_t st, const Launch& L, const Geom& g, const DevState* ds,
           double* s, double* part);
 void poisson_init(cudaStream_t st, const Launch& L, const Geom& g, bool h_loaded,
                   const double* hload, double* hout, const double* p, const double* rho,
-                  const double* s);
+                  const double* s, bool source_aware = false,
+                  double sa_scale = 1.0);
 void sweep(cudaStream_t st, const Launch& L, const Geom& g, const double* hin, double* hout,
            const double* rho, const double* s);
 // Two sweeps per launch (temporal blocking).  sweep2_prepare returns 1 when
@@ -151,6 +152,29 @@ void scalar_rhs_sum(cudaStream_t st, const Launch& L, const Geom& g, const doubl
 void p_sum(cudaStream_t st, const Launch& L, const Geom& g, const double* p, double* part);
 void scalar_check(cudaStream_t st, const Launch& L, const Geom& g, const double* pin, double* p, double* p_prev,
                   const DevState* ds, double* part);
+// The reference's one-pass form on the pre-collision h: start state, sweep
+// (relaxation scale, fixed-point relaxation), Anderson-m1 (store, dot
+// partials over kAndersonBlocks blocks, apply), the check (gauge of p and h,
+// relative change, results into the parity-0 buffers) and the two-grid
+// correction (4^3 block sums of the change, correction).
+constexpr int kAndersonBlocks = 296;
+void onepass_init(cudaStream_t st, const Launch& L, const Geom& g, bool h_loaded, const double* hload, double* hh,
+                  const double* p, const double* rho, const double* s, bool source_aware, double sa_scale);
+void onepass_sweep(cudaStream_t st, const Launch& L, const Geom& g, const double* hin, double* hout, const double* pin,
+                   double* pout, const double* rho, const double* s, double relax, double omega);
+void anderson_store(cudaStream_t st, const Geom& g, const double* hold, const double* himg, double* prev_r,
+                    double* prev_img);
+void anderson_dot(cudaStream_t st, const Geom& g, const double* hold, const double* himg, const double* prev_r,
+                  double* part);
+void anderson_apply(cudaStream_t st, const Launch& L, const Geom& g, const double* hold, double* himg, double* prev_r,
+                    double* prev_img, double* pimg, double alpha);
+void onepass_check(cudaStream_t st, const Launch& L, const Geom& g, const double* hin, double* hout, const double* pin,
+                   double* p, double* p_prev, const DevState* ds, double* part);
+int twogrid_blocks(const Geom& g, int* bxn, int* byn, int* bzn);
+void twogrid_sums(cudaStream_t st, const Geom& g, const double* p, const double* p_prev, const DevState* ds,
+                  double* bsum);
+void twogrid_correct(cudaStream_t st, const Launch& L, const Geom& g, double* hh, double* p, double* p_prev,
+                     const double* bsum, double strength);
 }  // namespace fp64
 
 // Finalisation kernels (kernels_fp64.cu): reduce block partials in a fixed

@@ -8,9 +8,10 @@
   tolerance on both: fields within 1e-8) in a fraction of the sweeps.
 * oracle/_ref/lbm_gpu_ref, the reference's GPU program compiled from its
   sources, against the reference's GPU/main.cpp over this library
-  (oracle/_ref/lbm_gpu_dropin) on the same params.in with the split and the
-  fused Poisson flags: Tecplot fields to float32 rounding and the same sweep
-  count at every step.
+  (oracle/_ref/lbm_gpu_dropin) on the same params.in with the split, fused
+  and one-pass Poisson flags and the accelerators (source-aware h init,
+  relaxation scales, Anderson-m1, two-grid correction): Tecplot fields to
+  float32 rounding and the same sweep count at every step.
 * With --poisson scalar the reference program does not solve the scalar
   equation: after each Jacobi sweep its loop still runs the split form's
   bounce + computePressure on the unchanged h (the block after the sweep is
@@ -143,7 +144,15 @@ def run_program(exe, d, pf, flags):
 @pytest.mark.skipif(not (os.path.exists(GPU_REF) and os.path.exists(DROPIN)),
                     reason="reference GPU program or drop-in CLI not built (needs the reference sources)")
 @pytest.mark.parametrize("flags", [["--poisson", "split"],
-                                   ["--poisson", "fused", "--pressure-boundary", "fused"]])
+                                   ["--poisson", "fused", "--pressure-boundary", "fused"],
+                                   ["--poisson", "split", "--source-aware-hh-init", "--source-aware-hh-scale", "0.5"],
+                                   ["--poisson", "onepass"],
+                                   ["--poisson", "onepass", "--poisson-fixed-point-relax", "0.8"],
+                                   ["--poisson", "onepass", "--pressure-relax-scale", "0.9"],
+                                   ["--poisson", "onepass", "--source-aware-hh-init"],
+                                   ["--poisson", "onepass", "--poisson-anderson-m1"],
+                                   ["--poisson", "onepass", "--poisson-two-grid-correction",
+                                    "--poisson-two-grid-strength", "0.5"]])
 def test_reference_gpu_program_matches_dropin(tmp_path, flags):
     pf = tmp_path / "params.in"
     pf.write_text(PARAMS)
