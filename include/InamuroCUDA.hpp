@@ -149,7 +149,8 @@ public:
     {
         // The reference's own guard (GPU/InamuroCUDA.cu:1846-1856).
         if ((dual_ || shadow_) && (fused_ || fused_boundary_ || scalar_ || onepass_ || acc_.anderson_m1 ||
-                                   acc_.two_grid || acc_.source_aware_init || acc_.pressure_relax_scale != 1.0 ||
+                                   acc_.two_grid || acc_.source_aware_init || acc_.spatial_diagnostics ||
+                                   acc_.pressure_relax_scale != 1.0 ||
                                    acc_.fixed_point_relax != 1.0))
             throw std::runtime_error(
                 "fixed-point residual requires frozen split+split Poisson with unit relaxation and all "
@@ -280,8 +281,12 @@ public:
         a.two_grid_strength = v;
         applyPoissonAccel(a, "setPoissonTwoGridStrength");
     }
-    // Not provided by the library; enabling it is rejected, disabling is accepted.
-    void setUsePoissonSpatialDiagnostics(bool e) { rejectAccelerator(e, "spatial diagnostics"); }
+    void setUsePoissonSpatialDiagnostics(bool e)
+    {
+        lbm_poisson_accel a = acc_;
+        a.spatial_diagnostics = e ? 1 : 0;
+        applyPoissonAccel(a, "setUsePoissonSpatialDiagnostics");
+    }
     // Every Poisson segment already runs as a captured CUDA graph.
     void setUsePoissonGraph(bool) {}
     // Per-phase device timing is always collected.
@@ -394,7 +399,7 @@ private:
     bool scalar_ = false;
     double scalar_scale_ = 2.0;
     bool onepass_ = false;
-    lbm_poisson_accel acc_{1.0, 1.0, 0, 1.0, 0, 0.5, 0, 1.0};
+    lbm_poisson_accel acc_{1.0, 1.0, 0, 1.0, 0, 0.5, 0, 1.0, 0};
     PoissonStepDiagnostics diag_;
     std::string csv_path_;
 
@@ -414,12 +419,6 @@ private:
         throw std::runtime_error(msg);
     }
 
-    static void rejectAccelerator(bool enabled, const char* name)
-    {
-        if (enabled)
-            throw std::invalid_argument(std::string(name) +
-                                        ": not provided by liblbm_b200");
-    }
 
     void applyPoissonForm()
     {
@@ -464,6 +463,8 @@ private:
             out << ',';
         }
         out << r->fixed_point_evaluated << ',' << r->pressure_converged << ',' << r->fixed_point_converged << ','
-            << r->dual_residual_enabled << ',' << r->converged << ",,0,0\n";
+            << r->dual_residual_enabled << ',' << r->converged << ',';
+        if (std::isfinite(r->block_low_frequency_fraction)) out << r->block_low_frequency_fraction;
+        out << ',' << r->spatial_block_size << ',' << r->spatial_block_count << '\n';
     }
 };

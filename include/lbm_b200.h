@@ -30,7 +30,7 @@ extern "C" {
 
 /* Bumped whenever a struct layout or a signature of this header changes;
    callers compare it with lbm_abi_version() of the loaded library. */
-#define LBM_B200_ABI_VERSION 4
+#define LBM_B200_ABI_VERSION 5
 
 typedef enum {
     LBM_OK = 0,
@@ -181,6 +181,11 @@ typedef struct {
     int dual_residual_enabled;
     int converged;
     int reserved;
+    double block_low_frequency_fraction;   /* spatial diagnostics: sum_b |sum_{cells of b} (p - p_prev)|
+                                              / sum |p - p_prev| over 4^3 blocks b; NaN when off */
+    int spatial_block_size;                /* 4 when block sums are taken (spatial diagnostics or
+                                              two-grid correction), else 0 */
+    int spatial_block_count;
 } lbm_check_record;
 
 typedef void (*lbm_check_callback)(void* user, const lbm_check_record* record);
@@ -266,11 +271,11 @@ lbm_status lbm_get_poisson_form(const lbm_handle* h, lbm_poisson_form* form, dou
 
 /* The reference's Poisson accelerators (InamuroCUDA setters,
  * GPU/InamuroCUDA.hpp:67-88; CLI flags of GPU/main.cpp:156-171), FP64.
- * pressure_relax_scale, fixed_point_relax, Anderson-m1 and two-grid need the
- * one-pass form (LBM_ERR_BAD_ARG at the next step otherwise); source-aware h
- * init applies to the kinetic and one-pass forms.  None combines with the
- * dual residual (the reference refuses that too).  Defaults: 1, 1, off, 1,
- * off, 0.5, off, 1. */
+ * pressure_relax_scale, fixed_point_relax and Anderson-m1 need the one-pass
+ * form (LBM_ERR_BAD_ARG at the next step otherwise); two-grid correction,
+ * source-aware h init and spatial diagnostics apply to the kinetic and
+ * one-pass forms.  None combines with the dual residual (the reference
+ * refuses that too).  Defaults: 1, 1, off, 1, off, 0.5, off, 1, off. */
 typedef struct {
     double pressure_relax_scale;   /* --pressure-relax-scale: scales (h - E p) / tau_h */
     double fixed_point_relax;      /* --poisson-fixed-point-relax: h = h_old + omega (T(h) - h_old) */
@@ -280,6 +285,8 @@ typedef struct {
     double two_grid_strength;      /* --poisson-two-grid-strength */
     int source_aware_init;         /* --source-aware-hh-init */
     double source_aware_scale;     /* --source-aware-hh-scale */
+    int spatial_diagnostics;       /* --poisson-spatial-diagnostics: block_low_frequency_fraction of
+                                      every check record */
 } lbm_poisson_accel;
 lbm_status lbm_set_poisson_accel(lbm_handle* h, const lbm_poisson_accel* a);
 lbm_status lbm_get_poisson_accel(const lbm_handle* h, lbm_poisson_accel* out);

@@ -116,7 +116,7 @@ class PoissonAccel(C.Structure):
     _fields_ = [("pressure_relax_scale", C.c_double), ("fixed_point_relax", C.c_double),
                 ("anderson_m1", C.c_int), ("anderson_beta_max", C.c_double), ("two_grid", C.c_int),
                 ("two_grid_strength", C.c_double), ("source_aware_init", C.c_int),
-                ("source_aware_scale", C.c_double)]
+                ("source_aware_scale", C.c_double), ("spatial_diagnostics", C.c_int)]
 
 
 class AdjointCfg(C.Structure):
@@ -145,7 +145,7 @@ class LBMError(RuntimeError):
 
 _lib = None
 # LBM_B200_ABI_VERSION of include/lbm_b200.h that the structures above mirror.
-ABI_VERSION = 4
+ABI_VERSION = 5
 
 
 def load_library(path: str = LIB_PATH):

@@ -123,6 +123,10 @@ __device__ void finalize_body(int kind, DevState* __restrict__ ds, const double*
         double r[1];
         reduce_partials<1>(part, stride, count, r);
         if (threadIdx.x == 0) ds->mass = r[0];
+    } else if (kind == FIN_BLOCK) {
+        double r[1];
+        reduce_partials<1>(part, stride, count, r);
+        if (threadIdx.x == 0) ds->block_frac = ds->l1_delta > 0.0 ? r[0] / ds->l1_delta : 0.0;
     } else if (kind == FIN_RHS) {
         double r[3];
         reduce_partials<3>(part, stride, count, r);

@@ -959,11 +959,23 @@ twogrid_sums_kernel(Geom g, const double* __restrict__ p, const double* __restri
     bsum[b] = acc;
 }
 
+// Skipped after a converged check or a zero change (read from the device state,
+// so the correction sits in a captured segment without a host decision).
+__global__ void __launch_bounds__(256)
+block_abs_sum_kernel(const double* __restrict__ bsum, int nb, double* __restrict__ part)
+{
+    double red[1] = {0.0};
+    for (int i = blockIdx.x * 256 + threadIdx.x; i < nb; i += gridDim.x * 256) red[0] += fabs(bsum[i]);
+    block_sum_store<1>(red, part, gridDim.x, blockIdx.x);
+}
+
 __global__ void __launch_bounds__(256)
 twogrid_correct_kernel(Geom g, double* __restrict__ hh, double* __restrict__ p, double* __restrict__ p_prev,
-                       const double* __restrict__ bsum, int bxn, int byn, double strength)
+                       const double* __restrict__ bsum, int bxn, int byn, double strength,
+                       const DevState* __restrict__ ds)
 {
     int x, y, z;
+    if (ds->converged || !(ds->l1_delta > 0.0) || ds->error) return;
     if (!tile_coords(g, x, y, z)) return;
     const int bx = x / kTwoGridBlock, by = y / kTwoGridBlock, bz = z / kTwoGridBlock;
     const int x0 = bx * kTwoGridBlock, y0 = by * kTwoGridBlock, z0 = bz * kTwoGridBlock;
@@ -1200,11 +1212,18 @@ void twogrid_sums(cudaStream_t st, const Geom& g, const double* p, const double*
 }
 
 void twogrid_correct(cudaStream_t st, const Launch& L, const Geom& g, double* hh, double* p, double* p_prev,
-                     const double* bsum, double strength)
+                     const double* bsum, double strength, const DevState* ds)
 {
     int bxn, byn, bzn;
     twogrid_blocks(g, &bxn, &byn, &bzn);
-    twogrid_correct_kernel<<<L.grid, L.block, 0, st>>>(g, hh, p, p_prev, bsum, bxn, byn, strength);
+    twogrid_correct_kernel<<<L.grid, L.block, 0, st>>>(g, hh, p, p_prev, bsum, bxn, byn, strength, ds);
+}
+
+void block_abs_sum(cudaStream_t st, const Geom& g, const double* bsum, double* part)
+{
+    int bxn, byn, bzn;
+    const int nb = twogrid_blocks(g, &bxn, &byn, &bzn);
+    block_abs_sum_kernel<<<kAndersonBlocks, 256, 0, st>>>(bsum, nb, part);
 }
 
 void correct(cudaStream_t st, const Launch& L, const Geom& g, double* u, double* v, double* w,

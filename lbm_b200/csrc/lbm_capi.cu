@@ -40,12 +40,14 @@ namespace {
 struct SegKey {
     int start_parity, n_normal, dual;
     int form = 0;   // lbm_poisson_form
+    int accel = 0;  // 1: two-grid correction, 2: spatial diagnostics
     bool operator<(const SegKey& o) const
     {
         if (start_parity != o.start_parity) return start_parity < o.start_parity;
         if (n_normal != o.n_normal) return n_normal < o.n_normal;
         if (dual != o.dual) return dual < o.dual;
-        return form < o.form;
+        if (form != o.form) return form < o.form;
+        return accel < o.accel;
     }
 };
 
@@ -85,12 +87,13 @@ struct lbm_handle {
     int pform = LBM_POISSON_KINETIC;     // lbm_poisson_form
     double scalar_scale = 2.0;           // scalar forms: source scale (reference default 2.0)
     double sor_omega = 0.0;              // red-black form: relaxation (0: from the box size)
-    lbm_poisson_accel paccel{1.0, 1.0, 0, 1.0, 0, 0.5, 0, 1.0};   // the reference's accelerator settings
+    lbm_poisson_accel paccel{1.0, 1.0, 0, 1.0, 0, 0.5, 0, 1.0, 0};   // the reference's accelerator settings
     double* and_r = nullptr;             // Anderson-m1 history: previous residual, previous image (15 n each)
     double* and_i = nullptr;
     double* and_part = nullptr;          // 2 x kAndersonBlocks dot partials, and their pinned copy
     double* and_host = nullptr;
-    double* tg_sum = nullptr;            // two-grid 4^3 block sums
+    double* tg_sum = nullptr;            // two-grid / spatial diagnostics: 4^3 block sums of the change
+    double* blk_part = nullptr;          // spatial diagnostics: partials of sum |block sum|
 };
 
 namespace {
@@ -136,7 +139,7 @@ void free_all(lbm_handle* h)
         *p = nullptr;
     }
     mixed_free(h->mb);
-    double** extra[] = {&h->and_r, &h->and_i, &h->and_part, &h->tg_sum};
+    double** extra[] = {&h->and_r, &h->and_i, &h->and_part, &h->tg_sum, &h->blk_part};
     for (double** p : extra) {
         if (*p) cudaFree(*p);
         *p = nullptr;
@@ -251,6 +254,7 @@ lbm_status build_segment(lbm_handle* h, const SegKey& key, cudaGraphExec_t* out,
         fp64::sweep_check_a(st, L, g, b.h[cur], b.h[1 - cur], b.p_chk, b.part_a);
         cur = 1 - cur;
         finalize(st, FIN_SIGMA, h->ds, b.part_a, L.cnblocks, nullptr, 0, nullptr, 0);
+        if (key.accel) fp64::twogrid_sums(st, g, b.p_chk, b.p_prev, h->ds, h->tg_sum);
         fp64::sweep_check_b(st, L, g, key.dual != 0, b.h[cur], b.h[1 - cur], b.hc, b.p_chk, b.p_prev, b.p,
                             b.rho, b.s, h->ds, b.part_b);
         cur = 1 - cur;
@@ -259,6 +263,16 @@ lbm_status build_segment(lbm_handle* h, const SegKey& key, cudaGraphExec_t* out,
             cur = 1 - cur;
         }
         finalize(st, FIN_CHECK, h->ds, b.part_b, L.cnblocks, b.part_c, L.cnblocks, nullptr, 0);
+        if (key.accel & 2) {
+            fp64::block_abs_sum(st, g, h->tg_sum, h->blk_part);
+            finalize(st, FIN_BLOCK, h->ds, h->blk_part, fp64::kAndersonBlocks, nullptr, 0, nullptr, 0);
+        }
+        // Two-grid correction (GPU/InamuroCUDA.cu:2149-2156): h here is the
+        // next sweep's post-collision h; adding E_q c to it equals colliding the
+        // corrected pre-collision h with the corrected p.
+        if (key.accel & 1)
+            fp64::twogrid_correct(st, L, g, b.h[cur], b.p, b.p_prev, h->tg_sum, h->paccel.two_grid_strength,
+                                  h->ds);
     } else {
         cur = mixed_segment(st, h->mb, L, g, key.start_parity, key.n_normal, key.dual != 0, h->ds);
     }
@@ -334,7 +348,7 @@ void fill_stats(const lbm_handle* h, const DevState& d, lbm_step_stats* s)
 }
 
 // One time step.  replay > 0 forces that many sweeps.
-lbm_status ensure_onepass_buffers(lbm_handle* h)
+lbm_status ensure_accel_buffers(lbm_handle* h)
 {
     const size_t pop = 15 * static_cast<size_t>(h->geom.n) * sizeof(double);
     if (h->paccel.anderson_m1 && !h->and_r) {
@@ -343,11 +357,13 @@ lbm_status ensure_onepass_buffers(lbm_handle* h)
         LBM_CUDA(h, cudaMalloc(&h->and_part, 2 * fp64::kAndersonBlocks * sizeof(double)));
         LBM_CUDA(h, cudaMallocHost(&h->and_host, 2 * fp64::kAndersonBlocks * sizeof(double)));
     }
-    if (h->paccel.two_grid && !h->tg_sum) {
+    if ((h->paccel.two_grid || h->paccel.spatial_diagnostics) && !h->tg_sum) {
         int bx, by, bz;
         const int nb = fp64::twogrid_blocks(h->geom, &bx, &by, &bz);
         LBM_CUDA(h, cudaMalloc(&h->tg_sum, static_cast<size_t>(nb) * sizeof(double)));
     }
+    if (h->paccel.spatial_diagnostics && !h->blk_part)
+        LBM_CUDA(h, cudaMalloc(&h->blk_part, fp64::kAndersonBlocks * sizeof(double)));
     return LBM_OK;
 }
 
@@ -395,18 +411,19 @@ lbm_status onepass_segment(lbm_handle* h, bool* has_history, uint64_t* launches)
     }
     fp64::p_sum(st, L, g, P[c], b.part_a);
     finalize(st, FIN_SIGMA, h->ds, b.part_a, L.cnblocks, nullptr, 0, nullptr, 0);
-    if (acc.two_grid) fp64::twogrid_sums(st, g, P[c], b.p_prev, h->ds, h->tg_sum);
+    const bool sums = acc.two_grid || acc.spatial_diagnostics;
+    if (sums) fp64::twogrid_sums(st, g, P[c], b.p_prev, h->ds, h->tg_sum);
     fp64::onepass_check(st, L, g, H[c], H[0], P[c], b.p, b.p_prev, h->ds, b.part_b);
     finalize(st, FIN_CHECK, h->ds, b.part_b, L.cnblocks, nullptr, 0, nullptr, 0);
+    if (acc.spatial_diagnostics) {
+        fp64::block_abs_sum(st, g, h->tg_sum, h->blk_part);
+        finalize(st, FIN_BLOCK, h->ds, h->blk_part, fp64::kAndersonBlocks, nullptr, 0, nullptr, 0);
+    }
+    // after an unconverged check only (the kernel reads the verdict on the device)
+    if (acc.two_grid) fp64::twogrid_correct(st, L, g, b.h[0], b.p, b.p_prev, h->tg_sum, acc.two_grid_strength, h->ds);
     LBM_CUDA(h, cudaMemcpyAsync(h->ds_host, h->ds, sizeof(DevState), cudaMemcpyDeviceToHost, st));
     LBM_CUDA(h, cudaStreamSynchronize(st));
-    *launches += 4 + (acc.two_grid ? 1 : 0);
-    const DevState& dh = *h->ds_host;
-    if (acc.two_grid && !dh.error && !dh.converged && dh.l1_delta > 0.0) {
-        fp64::twogrid_correct(st, L, g, b.h[0], b.p, b.p_prev, h->tg_sum, acc.two_grid_strength);
-        LBM_CUDA(h, cudaGetLastError());
-        ++*launches;
-    }
+    *launches += 4 + (sums ? 1 : 0) + (acc.spatial_diagnostics ? 2 : 0) + (acc.two_grid ? 1 : 0);
     return LBM_OK;
 }
 
@@ -419,17 +436,19 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
     const int dual = h->pcfg.dual_residual != 0;   // residual kernels run in exit and shadow mode
     const int form = h->pform;
     const lbm_poisson_accel& acc = h->paccel;
-    const bool onepass_only = acc.pressure_relax_scale != 1.0 || acc.fixed_point_relax != 1.0 || acc.anderson_m1 ||
-                              acc.two_grid;
-    if (dual && (form != LBM_POISSON_KINETIC || onepass_only || acc.source_aware_init))
+    const bool onepass_only = acc.pressure_relax_scale != 1.0 || acc.fixed_point_relax != 1.0 || acc.anderson_m1;
+    const bool block_sums = acc.two_grid || acc.spatial_diagnostics;
+    if (dual && (form != LBM_POISSON_KINETIC || onepass_only || block_sums || acc.source_aware_init))
         return fail(h, LBM_ERR_BAD_ARG,
                     "fixed-point residual requires the kinetic (split) Poisson form with unit relaxation and "
                     "all accelerators disabled");
     if (onepass_only && form != LBM_POISSON_ONEPASS)
+        return fail(h, LBM_ERR_BAD_ARG, "relaxation scales and Anderson-m1 need the one-pass Poisson form");
+    if (block_sums && form != LBM_POISSON_ONEPASS && form != LBM_POISSON_KINETIC)
         return fail(h, LBM_ERR_BAD_ARG,
-                    "relaxation scales, Anderson-m1 and two-grid correction need the one-pass Poisson form");
-    if (form == LBM_POISSON_ONEPASS) {
-        const lbm_status s = ensure_onepass_buffers(h);
+                    "two-grid correction and spatial diagnostics need the kinetic or one-pass Poisson form");
+    if (form == LBM_POISSON_ONEPASS || block_sums) {
+        const lbm_status s = ensure_accel_buffers(h);
         if (s != LBM_OK) return s;
     }
     if (dual) {
@@ -498,7 +517,8 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
             if (os != LBM_OK) return os;
             hcur = 0;
         } else {
-            SegKey key{hcur, n_normal, dual, form};
+            const int accel = (acc.two_grid ? 1 : 0) | (acc.spatial_diagnostics ? 2 : 0);
+            SegKey key{hcur, n_normal, dual, form, accel};
             cudaGraphExec_t ex = nullptr;
             int end_parity = hcur;
             const lbm_status gs = get_segment(h, key, &ex, &end_parity);
@@ -552,6 +572,12 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
             rec.fixed_point_converged = tmp.fixed_point_converged;
             rec.dual_residual_enabled = h->pcfg.dual_residual == 1;
             rec.converged = tmp.converged;
+            rec.block_low_frequency_fraction = acc.spatial_diagnostics ? dh.block_frac : std::nan("");
+            if (block_sums) {
+                int bx, by, bz;
+                rec.spatial_block_size = 4;
+                rec.spatial_block_count = fp64::twogrid_blocks(g, &bx, &by, &bz);
+            }
             h->check_cb(h->check_user, &rec);
         }
         if (replay) {
@@ -914,10 +940,11 @@ lbm_status lbm_set_poisson_accel(lbm_handle* h, const lbm_poisson_accel* a)
         return fail(h, LBM_ERR_BAD_ARG, "Poisson two-grid strength must be non-negative");
     if (!std::isfinite(a->source_aware_scale)) return fail(h, LBM_ERR_BAD_ARG, "source-aware scale must be finite");
     if ((a->pressure_relax_scale != 1.0 || a->fixed_point_relax != 1.0 || a->anderson_m1 || a->two_grid ||
-         a->source_aware_init) && h->precision != LBM_PRECISION_FP64)
+         a->source_aware_init || a->spatial_diagnostics) && h->precision != LBM_PRECISION_FP64)
         return fail(h, LBM_ERR_BAD_ARG, "the Poisson accelerators run in FP64 precision only");
     const bool init_changed = (a->source_aware_init != 0) != (h->paccel.source_aware_init != 0) ||
-                              a->source_aware_scale != h->paccel.source_aware_scale;
+                              a->source_aware_scale != h->paccel.source_aware_scale ||
+                              a->two_grid_strength != h->paccel.two_grid_strength;
     h->paccel = *a;
     if (init_changed) {
         for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second.first);

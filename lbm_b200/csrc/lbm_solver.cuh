@@ -52,6 +52,7 @@ struct DevState {
     double n_cells;             // (double)lx * ly * lz
     double rhs_mean;            // scalar red-black form: weighted mean of f = scale rho s (per step)
     double rhs_chk;             // ... and of chi f, chi = (-1)^(x+y+z)
+    double block_frac;          // spatial diagnostics: sum |4^3 block sums of the change| / l1_delta
 };
 
 enum ErrorSite {
@@ -174,12 +175,14 @@ int twogrid_blocks(const Geom& g, int* bxn, int* byn, int* bzn);
 void twogrid_sums(cudaStream_t st, const Geom& g, const double* p, const double* p_prev, const DevState* ds,
                   double* bsum);
 void twogrid_correct(cudaStream_t st, const Launch& L, const Geom& g, double* hh, double* p, double* p_prev,
-                     const double* bsum, double strength);
+                     const double* bsum, double strength, const DevState* ds);
+// Partial sums (kAndersonBlocks blocks) of |bsum| over the 4^3 blocks (FIN_BLOCK).
+void block_abs_sum(cudaStream_t st, const Geom& g, const double* bsum, double* part);
 }  // namespace fp64
 
 // Finalisation kernels (kernels_fp64.cu): reduce block partials in a fixed
 // order and update DevState.
-enum FinKind { FIN_SOURCE = 0, FIN_PREP = 1, FIN_SIGMA = 2, FIN_CHECK = 3, FIN_MASS = 4, FIN_RHS = 5 };
+enum FinKind { FIN_SOURCE = 0, FIN_PREP = 1, FIN_SIGMA = 2, FIN_CHECK = 3, FIN_MASS = 4, FIN_RHS = 5, FIN_BLOCK = 6 };
 void finalize(cudaStream_t st, FinKind kind, DevState* ds, const double* part,
               long long nblocks, const double* part2, long long nblocks2,
               const double* part3, long long nblocks3);

@@ -152,7 +152,11 @@ def run_program(exe, d, pf, flags):
                                    ["--poisson", "onepass", "--source-aware-hh-init"],
                                    ["--poisson", "onepass", "--poisson-anderson-m1"],
                                    ["--poisson", "onepass", "--poisson-two-grid-correction",
-                                    "--poisson-two-grid-strength", "0.5"]])
+                                    "--poisson-two-grid-strength", "0.5"],
+                                   ["--poisson", "split", "--poisson-two-grid-correction"],
+                                   ["--poisson", "split", "--poisson-spatial-diagnostics"],
+                                   ["--poisson", "onepass", "--poisson-spatial-diagnostics",
+                                    "--poisson-two-grid-correction"]])
 def test_reference_gpu_program_matches_dropin(tmp_path, flags):
     pf = tmp_path / "params.in"
     pf.write_text(PARAMS)
@@ -166,6 +170,17 @@ def test_reference_gpu_program_matches_dropin(tmp_path, flags):
         err = float(np.max(np.abs(vo[:, j].astype(np.float64) - vr[:, j])))
         assert err <= 2e-6 * max(scale, 1e-30), (name, err, scale)
     assert final_counts(outs["ours"] / "diag.csv") == final_counts(outs["ref"] / "diag.csv")
+    # the spatial columns of every check row (block fraction to 1e-9: the
+    # reference sums its blocks with atomicAdd)
+    ref_rows = list(csv.DictReader(open(outs["ref"] / "diag.csv")))
+    our_rows = list(csv.DictReader(open(outs["ours"] / "diag.csv")))
+    assert len(ref_rows) == len(our_rows)
+    for a, b in zip(ref_rows, our_rows):
+        assert (a["block_size"], a["block_count"]) == (b["block_size"], b["block_count"])
+        fa, fb = a["block_low_frequency_fraction"], b["block_low_frequency_fraction"]
+        assert (fa == "") == (fb == "")
+        if fa:
+            assert abs(float(fa) - float(fb)) <= 1e-9 * max(abs(float(fa)), 1e-300), (a["iteration"], fa, fb)
 
 
 @pytest.mark.skipif(not os.path.exists(GPU_REF), reason="reference GPU program not built (needs the reference sources)")
