@@ -668,6 +668,49 @@ def run_poisson_forms(args):
     return 0
 
 
+def run_krylov(args):
+    """The kinetic Poisson fixed point to a tight tolerance, by the kinetic
+    sweeps (relative change < tol between checks 100 sweeps apart) and by
+    BiCGSTAB (residual < tol), FP64, the head-on workload at --size with x
+    periodic: W warm-up
+    steps, K timed steps each, device time from the handle's CUDA events;
+    reports sweeps (kinetic-map applications) per step, the Poisson time per
+    step and the two forms' difference after the run."""
+    import lbm_b200 as L
+    n = args.size
+    p = workload_params(n)
+    p.periodic_x = 1   # the Krylov form needs periodic x
+    f = workload_fields(p)
+    tol = args.krylov_tol
+    out, fields = {}, {}
+    for form in ("kinetic", "krylov"):
+        g = L.InamuroCUDA(p, f, precision="fp64")
+        g.set_poisson(check_interval=100, tolerance=tol, max_sweeps=args.max_sweeps, fail_on_limit=True)
+        g.set_poisson_form(form)
+        g.step(args.warmup)
+        g.reset_timing()
+        clk = ClockSampler(0)
+        clk.start()
+        stats = g.step(args.steps)
+        clocks = clk.stop()
+        tm = g.timing()
+        out[form] = {"sweeps_per_step": sum(st["iterations"] for st in stats) / args.steps,
+                     "poisson_ms_per_step": tm["poisson_ms"] / args.steps,
+                     "ms_per_step": sum(st["device_ms"] for st in stats) / args.steps,
+                     "final_relative": stats[-1]["relative_error"], "clocks": clocks}
+        fields[form] = g.download_fields()
+        g.close()
+    diff = {k: float(np.max(np.abs(fields["krylov"][k] - fields["kinetic"][k])) /
+                     max(float(np.max(np.abs(fields["kinetic"][k]))), 1e-300)) for k in L.FIELDS}
+    line = {"metric": "Poisson time per step to the kinetic fixed point, kinetic sweeps vs BiCGSTAB",
+            "value": out["kinetic"]["poisson_ms_per_step"] / out["krylov"]["poisson_ms_per_step"],
+            "unit": "speed-up (x)", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(config_dict(n, "fp64"), tolerance=tol), "forms": out, "rel_diff_krylov_vs_kinetic": diff}
+    print(json.dumps(line))
+    return 0
+
+
 def run_ours(args):
     world, rank, local = dist_setup(args.gpus)
     n = args.size
@@ -772,7 +815,8 @@ def main(argv=None):
     ap.add_argument("--phase-timing", action="store_true",
                     help="time the non-Poisson kernels per step with --phase-sweeps sweeps per step")
     ap.add_argument("--phase-sweeps", type=int, default=100)
-    ap.add_argument("--workload", choices=("headon", "batch", "adjoint", "poisson-forms"), default="headon",
+    ap.add_argument("--krylov-tol", type=float, default=1e-10, help="tolerance of the krylov workload")
+    ap.add_argument("--workload", choices=("headon", "batch", "adjoint", "poisson-forms", "krylov"), default="headon",
                     help="batch: the batched droplet oscillation (64 uneven boxes, mixed precision); "
                          "adjoint: the adjoint calibration run (FP64, 64^3), --steps forward steps")
     ap.add_argument("--adjoint-size", type=int, default=64)
@@ -794,6 +838,8 @@ def main(argv=None):
         return run_adjoint(args)
     if args.workload == "poisson-forms":
         return run_poisson_forms(args)
+    if args.workload == "krylov":
+        return run_krylov(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_ours(args)

@@ -260,9 +260,16 @@ typedef enum {
     LBM_POISSON_KINETIC = 0,
     LBM_POISSON_SCALAR_JACOBI = 1,
     LBM_POISSON_SCALAR_RB = 2,
-    LBM_POISSON_ONEPASS = 3      /* the reference's one-pass form (setUseOnePassPoisson,
+    LBM_POISSON_ONEPASS = 3,     /* the reference's one-pass form (setUseOnePassPoisson,
                                     GPU/InamuroCUDA.cu:780-844): the kinetic map on the
                                     pre-collision h with the accelerators of lbm_poisson_accel */
+    LBM_POISSON_KRYLOV = 4       /* not a reference form: the kinetic form's fixed point solved by
+                                    BiCGSTAB, stopping at ||b - (I - K) h|| < tolerance ||b|| (the
+                                    lbm_poisson_cfg tolerance; max_sweeps caps the applications of
+                                    the kinetic map).  Same fixed point as the kinetic form; FP64,
+                                    periodic x only (with the slip walls' overwrite the singular
+                                    system is inconsistent), no dual residual, no two-grid or
+                                    spatial diagnostics */
 } lbm_poisson_form;
 lbm_status lbm_set_poisson_form(lbm_handle* h, lbm_poisson_form form, double source_scale, double omega);
 /* Current form, source scale and the relaxation in use (the computed optimum

@@ -420,7 +420,7 @@ class InamuroCUDA:
         cfg = PoissonCfg(check_interval, tolerance, int(dual), max_sweeps, int(fail_on_limit))
         self._check(self._lib.lbm_set_poisson(self._h, C.byref(cfg)), "set_poisson")
 
-    POISSON_FORMS = {"kinetic": 0, "scalar": 1, "scalar-rb": 2, "onepass": 3}
+    POISSON_FORMS = {"kinetic": 0, "scalar": 1, "scalar-rb": 2, "onepass": 3, "krylov": 4}
 
     def set_poisson_form(self, form: str = "kinetic", source_scale: float = 2.0, omega: float = 0.0):
         """lbm_set_poisson_form: "kinetic" (the production solve), "scalar"

@@ -1,0 +1,271 @@
+// krylov.cu -- the kinetic Poisson fixed point solved by BiCGSTAB
+// (LBM_POISSON_KRYLOV), FP64.
+//
+// The production solve iterates h <- K h + b to its fixed point (Richardson):
+// K = collide o (pull + x-wall overwrite) without the source,
+// collide: hv -> hv - (hv - E_q sum(hv)) / tau_h, tau_h = 1/rho + 1/2, and
+// b_q = -(E_q / 3) s (CPU/Inamuro.cpp:755-793).  This form solves the same
+// linear system (I - K) h = b by BiCGSTAB (van der Vorst 1992) on the
+// post-collision populations, so it converges to the same fixed point; p is
+// then the sum of the pulled populations, gauged to the step's target mean.
+// (I - K) is singular (constant p) but the system is consistent: the
+// projected source has zero sum.  One iteration is two applications of K
+// (each one pass over the populations, like a sweep) and the vector updates;
+// the five inner products per iteration are fixed-order block partial sums
+// added on the host.  The exit: ||b - (I - K) h||_2 < tolerance ||b||_2.
+#include <cuda_runtime.h>
+
+#include "../../include/lbm_b200.h"
+#include "lbm_solver.cuh"
+
+namespace lbm {
+namespace {
+
+constexpr int kDotBlocks = 296;
+
+__device__ __forceinline__ bool kcell(const Geom& g, int& x, int& y, int& z)
+{
+    x = blockIdx.x * blockDim.x + threadIdx.x;
+    y = blockIdx.y * blockDim.y + threadIdx.y;
+    z = blockIdx.z;
+    return x < g.lx && y < g.ly;
+}
+
+// x slip overwrite of pulled populations (CPU/Inamuro.cpp:589-623).
+__device__ __forceinline__ void kbounce(double (&v)[Q], const Geom& g, int x)
+{
+    if (g.periodic_x) return;
+    if (x == 0) {
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            if constexpr (bounce_left(q) != q) v[q] = v[bounce_left(q)];
+        });
+    }
+    if (x == g.lx - 1) {
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            if constexpr (bounce_right(q) != q) v[q] = v[bounce_right(q)];
+        });
+    }
+}
+
+// out = in - K in (kinds 0, 2), or out = b - (in - K in) with b = -(E/3) s
+// (kind 1, a true residual).  Partial sums: kind 0 dot(w, out) and
+// dot(out, out); kind 1 dot(out, out); kind 2 dot(w, out) and dot(out, out).
+template <int kKind>
+__global__ void __launch_bounds__(256)
+apply_kernel(Geom g, const double* __restrict__ in, double* __restrict__ out, const double* __restrict__ rho,
+             const double* __restrict__ s, const double* __restrict__ w, double* __restrict__ part,
+             long long nblocks)
+{
+    int x, y, z;
+    const bool active = kcell(g, x, y, z);
+    double red[2] = {0.0, 0.0};
+    if (active) {
+        const long long n = g.n;
+        const long long c = cell_of(g, x, y, z);
+        const Wrap wr(g, x, y, z);
+        double hv[Q];
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            hv[q] = __ldg(in + (long long)q * n + pull_src<q>(g, wr, x, y, z));
+        });
+        kbounce(hv, g, x);
+        double p = 0.0;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) p += hv[q];
+        const double inv_tau = 1.0 / (1.0 / __ldg(rho + c) + 0.5);
+        const double sv = (kKind == 1) ? __ldg(s + c) : 0.0;
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            constexpr double E = wE(q);
+            const long long i = (long long)q * n + c;
+            const double kh = hv[q] - (hv[q] - E * p) * inv_tau;
+            double v = __ldg(in + i) - kh;
+            if constexpr (kKind == 1) v = -(E / 3.0) * sv - v;
+            out[i] = v;
+            if constexpr (kKind == 0) {
+                red[0] += __ldg(w + i) * v;
+                red[1] += v * v;
+            }
+            if constexpr (kKind == 2) {
+                red[0] += __ldg(w + i) * v;
+                red[1] += v * v;
+            }
+            if constexpr (kKind == 1) red[0] += v * v;
+        });
+    }
+    block_sum_store<2>(red, part, nblocks, block_linear());
+}
+
+// Grid-stride vector updates over the 15 n populations.
+// op 0: p = r + beta (p - omega v)
+// op 1: s = r - alpha v
+// op 2: x += alpha p + omega s; r = s - omega t; partials of r.r and r0.r
+// op 3: copy (r0 = r, p = r)
+template <int kOp>
+__global__ void __launch_bounds__(256)
+vec_kernel(long long count, double a0, double a1, double* __restrict__ y0, double* __restrict__ y1,
+           const double* __restrict__ x0, const double* __restrict__ x1, const double* __restrict__ x2,
+           const double* __restrict__ x3, double* __restrict__ part)
+{
+    double red[2] = {0.0, 0.0};
+    for (long long i = blockIdx.x * 256LL + threadIdx.x; i < count; i += (long long)gridDim.x * 256) {
+        if constexpr (kOp == 0) {
+            y0[i] = x0[i] + a0 * (y0[i] - a1 * x1[i]);
+        } else if constexpr (kOp == 1) {
+            y0[i] = x0[i] - a0 * x1[i];
+        } else if constexpr (kOp == 2) {
+            // y0 = x (solution), y1 = r; x0 = p, x1 = s, x2 = t, x3 = r0
+            y0[i] = y0[i] + a0 * x0[i] + a1 * x1[i];
+            const double r = x1[i] - a1 * x2[i];
+            y1[i] = r;
+            red[0] += r * r;
+            red[1] += x3[i] * r;
+        } else {
+            y0[i] = x0[i];
+            y1[i] = x0[i];
+        }
+    }
+    if constexpr (kOp == 2) block_sum_store<2>(red, part, gridDim.x, blockIdx.x);
+}
+
+// p = sum of the pulled, bounced populations of the solution (the p a sweep
+// would compute), and its block partial sums for the gauge mean.
+__global__ void __launch_bounds__(256)
+pressure_kernel(Geom g, const double* __restrict__ h, double* __restrict__ p, double* __restrict__ part,
+                long long nblocks)
+{
+    int x, y, z;
+    const bool active = kcell(g, x, y, z);
+    double red[1] = {0.0};
+    if (active) {
+        const Wrap wr(g, x, y, z);
+        double hv[Q];
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            hv[q] = __ldg(h + (long long)q * g.n + pull_src<q>(g, wr, x, y, z));
+        });
+        kbounce(hv, g, x);
+        double pv = 0.0;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) pv += hv[q];
+        p[cell_of(g, x, y, z)] = pv;
+        red[0] = pv;
+    }
+    block_sum_store<1>(red, part, nblocks, block_linear());
+}
+
+__global__ void __launch_bounds__(256)
+shift_kernel(long long n, double* __restrict__ p, double* __restrict__ p_prev, double shift)
+{
+    for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256) {
+        const double v = p[i] - shift;
+        p[i] = v;
+        p_prev[i] = v;
+    }
+}
+
+}  // namespace
+
+namespace krylov {
+
+lbm_status solve(cudaStream_t st, const Launch& L, const Geom& g, const KrylovBuffers& kb, double* h, const double* rho,
+                 const double* s, double* p, double* p_prev, double target, double tol, uint64_t max_matvecs,
+                 KrylovResult* res)
+{
+    const long long cnt = 15 * g.n;
+    auto host_sum = [&](long long blocks, int cols, double* out) -> bool {
+        if (cudaMemcpyAsync(kb.host, kb.part, static_cast<size_t>(cols) * blocks * sizeof(double),
+                            cudaMemcpyDeviceToHost, st) != cudaSuccess)
+            return false;
+        if (cudaStreamSynchronize(st) != cudaSuccess) return false;
+        for (int c = 0; c < cols; ++c) {
+            double acc = 0.0;
+            for (long long b = 0; b < blocks; ++b) acc += kb.host[c * blocks + b];
+            out[c] = acc;
+        }
+        return true;
+    };
+    double d2[2];
+    *res = KrylovResult{};
+    // ||b||: the residual of x = 0 (v is zero, and stays the v_0 = 0 of the method)
+    if (cudaMemsetAsync(kb.v, 0, static_cast<size_t>(cnt) * sizeof(double), st) != cudaSuccess) return LBM_ERR_CUDA;
+    apply_kernel<1><<<L.grid, L.block, 0, st>>>(g, kb.v, kb.t, rho, s, nullptr, kb.part, L.nblocks);
+    if (!host_sum(L.nblocks, 1, d2)) return LBM_ERR_CUDA;
+    const double bnorm = sqrt(d2[0]);
+    // r = b - A x0, r0 = p = r
+    apply_kernel<1><<<L.grid, L.block, 0, st>>>(g, h, kb.r, rho, s, nullptr, kb.part, L.nblocks);
+    if (!host_sum(L.nblocks, 1, d2)) return LBM_ERR_CUDA;
+    double rr = d2[0];
+    vec_kernel<3><<<kDotBlocks, 256, 0, st>>>(cnt, 0.0, 0.0, kb.r0, kb.p, kb.r, nullptr, nullptr, nullptr, nullptr);
+    res->matvecs = 1;
+    double rho_old = 1.0, alpha = 1.0, omega = 1.0, rho_new = rr, r0r0 = rr;
+    bool first = true, budget = false;
+    int since = 0;
+    res->rel_residual = bnorm > 0.0 ? sqrt(rr) / bnorm : 0.0;
+    while (bnorm > 0.0 && res->rel_residual >= tol) {
+        if (max_matvecs && res->matvecs + 3 > max_matvecs) {
+            budget = true;
+            break;
+        }
+        if (!first) {
+            if (rho_old == 0.0 || omega == 0.0) return LBM_ERR_NONFINITE;   // breakdown
+            const double beta = (rho_new / rho_old) * (alpha / omega);
+            vec_kernel<0><<<kDotBlocks, 256, 0, st>>>(cnt, beta, omega, kb.p, nullptr, kb.r, kb.v, nullptr, nullptr,
+                                                       nullptr);
+        }
+        first = false;
+        apply_kernel<0><<<L.grid, L.block, 0, st>>>(g, kb.p, kb.v, rho, nullptr, kb.r0, kb.part, L.nblocks);
+        if (!host_sum(L.nblocks, 2, d2)) return LBM_ERR_CUDA;
+        ++res->matvecs;
+        if (!isfinite(d2[0]) || !isfinite(d2[1])) return LBM_ERR_NONFINITE;
+        // Near-breakdown (r0 . v ~ 0 against |r0| |v|, as at the rounding
+        // floor) or 200 iterations since the last start: restart from the
+        // true residual of the current iterate.
+        if (fabs(d2[0]) <= 1e-12 * sqrt(r0r0 * d2[1]) || since >= 200) {
+            apply_kernel<1><<<L.grid, L.block, 0, st>>>(g, h, kb.r, rho, s, nullptr, kb.part, L.nblocks);
+            if (!host_sum(L.nblocks, 1, d2)) return LBM_ERR_CUDA;
+            ++res->matvecs;
+            rr = d2[0];
+            if (!isfinite(rr)) return LBM_ERR_NONFINITE;
+            vec_kernel<3><<<kDotBlocks, 256, 0, st>>>(cnt, 0.0, 0.0, kb.r0, kb.p, kb.r, nullptr, nullptr, nullptr,
+                                                       nullptr);
+            rho_new = r0r0 = rr;
+            rho_old = alpha = omega = 1.0;
+            first = true;
+            since = 0;
+            ++res->restarts;
+            res->rel_residual = sqrt(rr) / bnorm;
+            continue;
+        }
+        alpha = rho_new / d2[0];
+        vec_kernel<1><<<kDotBlocks, 256, 0, st>>>(cnt, alpha, 0.0, kb.s, nullptr, kb.r, kb.v, nullptr, nullptr, nullptr);
+        apply_kernel<2><<<L.grid, L.block, 0, st>>>(g, kb.s, kb.t, rho, nullptr, kb.s, kb.part, L.nblocks);
+        if (!host_sum(L.nblocks, 2, d2)) return LBM_ERR_CUDA;
+        omega = d2[1] > 0.0 ? d2[0] / d2[1] : 0.0;
+        vec_kernel<2><<<kDotBlocks, 256, 0, st>>>(cnt, alpha, omega, h, kb.r, kb.p, kb.s, kb.t, kb.r0, kb.part);
+        if (!host_sum(kDotBlocks, 2, d2)) return LBM_ERR_CUDA;
+        rr = d2[0];
+        rho_old = rho_new;
+        rho_new = d2[1];
+        ++res->matvecs;
+        ++res->iterations;
+        ++since;
+        if (!isfinite(rr)) return LBM_ERR_NONFINITE;
+        res->rel_residual = sqrt(rr) / bnorm;
+        if (omega == 0.0 && res->rel_residual >= tol) since = 200;   // stagnation: restart next
+    }
+    // p of the solution, gauged to the target mean (p_prev follows, as after a check)
+    pressure_kernel<<<L.grid, L.block, 0, st>>>(g, h, p, kb.part, L.nblocks);
+    if (!host_sum(L.nblocks, 1, d2)) return LBM_ERR_CUDA;
+    const double shift = d2[0] / static_cast<double>(g.n) - target;
+    if (!isfinite(shift)) return LBM_ERR_NONFINITE;
+    shift_kernel<<<kDotBlocks, 256, 0, st>>>(g.n, p, p_prev, shift);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) return LBM_ERR_CUDA;
+    res->gauge_shift = shift;
+    return budget ? LBM_ERR_POISSON_BUDGET : LBM_OK;
+}
+
+}  // namespace krylov
+}  // namespace lbm

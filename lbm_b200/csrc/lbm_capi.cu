@@ -94,6 +94,7 @@ struct lbm_handle {
     double* and_host = nullptr;
     double* tg_sum = nullptr;            // two-grid / spatial diagnostics: 4^3 block sums of the change
     double* blk_part = nullptr;          // spatial diagnostics: partials of sum |block sum|
+    KrylovBuffers kb{};                  // BiCGSTAB work vectors (LBM_POISSON_KRYLOV)
 };
 
 namespace {
@@ -146,6 +147,13 @@ void free_all(lbm_handle* h)
     }
     if (h->and_host) cudaFreeHost(h->and_host);
     h->and_host = nullptr;
+    double** kv[] = {&h->kb.r, &h->kb.r0, &h->kb.p, &h->kb.v, &h->kb.s, &h->kb.t, &h->kb.part};
+    for (double** p : kv) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
+    if (h->kb.host) cudaFreeHost(h->kb.host);
+    h->kb.host = nullptr;
     if (h->stats_part) cudaFree(h->stats_part);
     if (h->stats_dev) cudaFree(h->stats_dev);
     h->stats_part = nullptr;
@@ -451,6 +459,14 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
         const lbm_status s = ensure_accel_buffers(h);
         if (s != LBM_OK) return s;
     }
+    if (form == LBM_POISSON_KRYLOV && !h->kb.r) {
+        const size_t pop = 15 * static_cast<size_t>(g.n) * sizeof(double);
+        double** kv[] = {&h->kb.r, &h->kb.r0, &h->kb.p, &h->kb.v, &h->kb.s, &h->kb.t};
+        for (double** p : kv) LBM_CUDA(h, cudaMalloc(p, pop));
+        const size_t parts = 2 * static_cast<size_t>(std::max<long long>(L.nblocks, 296));
+        LBM_CUDA(h, cudaMalloc(&h->kb.part, parts * sizeof(double)));
+        LBM_CUDA(h, cudaMallocHost(&h->kb.host, parts * sizeof(double)));
+    }
     if (dual) {
         const lbm_status s = ensure_dual_buffer(h);
         if (s != LBM_OK) return s;
@@ -478,7 +494,7 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
         finalize(st, FIN_MASS, h->ds, b.part_mass, L.nblocks, nullptr, 0, nullptr, 0);
         fp64::prep(st, L, g, h->ds, b.dux, b.dvy, b.dwz, b.p, b.s, b.part_prep);
         finalize(st, FIN_PREP, h->ds, b.part_prep, L.nblocks, nullptr, 0, nullptr, 0);
-        if (form == LBM_POISSON_KINETIC) {
+        if (form == LBM_POISSON_KINETIC || form == LBM_POISSON_KRYLOV) {
             fp64::poisson_init(st, L, g, h->h_loaded, b.h[1], b.h[0], b.p, b.rho, b.s, acc.source_aware_init != 0,
                                acc.source_aware_scale);
         } else if (form == LBM_POISSON_ONEPASS) {
@@ -509,7 +525,44 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
     if (form == LBM_POISSON_SCALAR_RB) launches = 8;       // no h initialisation; right-hand-side mean
     uint64_t fused_sweeps = 0;
     bool anderson_history = false;
-    for (;;) {
+    if (form == LBM_POISSON_KRYLOV) {
+        // The step's source and gauge target are on the device (FIN_SOURCE, FIN_PREP).
+        LBM_CUDA(h, cudaMemcpyAsync(h->ds_host, h->ds, sizeof(DevState), cudaMemcpyDeviceToHost, st));
+        LBM_CUDA(h, cudaStreamSynchronize(st));
+        if (dh.error) return fail(h, static_cast<lbm_status>(dh.error), site_text(dh.error_site));
+        KrylovResult kr;
+        Fp64Buffers& b = h->b;
+        const lbm_status ks = krylov::solve(st, L, g, h->kb, b.h[0], b.rho, b.s, b.p, b.p_prev, dh.target,
+                                            h->pcfg.tolerance, h->pcfg.max_sweeps, &kr);
+        if (ks != LBM_OK && ks != LBM_ERR_POISSON_BUDGET)
+            return fail(h, ks, ks == LBM_ERR_NONFINITE ? "Krylov Poisson solve broke down or diverged"
+                                                       : "Krylov Poisson solve failed");
+        if (ks == LBM_ERR_POISSON_BUDGET && h->pcfg.fail_on_limit)
+            return fail(h, LBM_ERR_POISSON_BUDGET, "Poisson sweep limit reached without convergence");
+        iters = kr.matvecs;
+        kernels = kr.matvecs;
+        launches += 4 * kr.iterations + 6;
+        dh.iterations = kr.matvecs;
+        dh.rel = kr.rel_residual;
+        dh.max_shift = std::fabs(kr.gauge_shift);
+        dh.pressure_converged = ks == LBM_OK;
+        dh.converged = ks == LBM_OK;
+        hcur = 0;
+        h->h_last = 0;
+        if (h->check_cb) {
+            lbm_check_record rec{};
+            rec.step = h->steps_done + 1;
+            rec.iteration = iters;
+            rec.relative_error = kr.rel_residual;
+            rec.fixed_point_h_l1 = rec.fixed_point_h_scale = rec.fixed_point_h_relative = std::nan("");
+            rec.fixed_point_p_l1 = rec.fixed_point_p_scale = rec.fixed_point_p_relative = std::nan("");
+            rec.fixed_point_relative = std::nan("");
+            rec.block_low_frequency_fraction = std::nan("");
+            rec.pressure_converged = rec.converged = dh.converged;
+            h->check_cb(h->check_user, &rec);
+        }
+    }
+    for (; form != LBM_POISSON_KRYLOV;) {
         const int n_normal =
             form != LBM_POISSON_KINETIC ? ci : (dual ? (first_seg ? ci - 1 : ci - 2) : ci - 1);
         if (form == LBM_POISSON_ONEPASS) {
@@ -897,14 +950,18 @@ lbm_status lbm_set_poisson_form(lbm_handle* h, lbm_poisson_form form, double sou
 {
     if (check_handle(h) != LBM_OK) return LBM_ERR_BAD_ARG;
     if (form != LBM_POISSON_KINETIC && form != LBM_POISSON_SCALAR_JACOBI && form != LBM_POISSON_SCALAR_RB &&
-        form != LBM_POISSON_ONEPASS)
+        form != LBM_POISSON_ONEPASS && form != LBM_POISSON_KRYLOV)
         return fail(h, LBM_ERR_BAD_ARG, "unknown Poisson form");
     if (form != LBM_POISSON_KINETIC && h->precision != LBM_PRECISION_FP64)
-        return fail(h, LBM_ERR_BAD_ARG, "the scalar and one-pass Poisson forms run in FP64 precision only");
+        return fail(h, LBM_ERR_BAD_ARG, "the scalar, one-pass and Krylov Poisson forms run in FP64 precision only");
     if (!std::isfinite(source_scale)) return fail(h, LBM_ERR_BAD_ARG, "scalar source scale must be finite");
     if (!(omega == 0.0 || (omega > 0.0 && omega < 2.0)))
         return fail(h, LBM_ERR_BAD_ARG, "SOR relaxation must be 0 (automatic) or in (0, 2)");
     const Geom& g = h->geom;
+    if (form == LBM_POISSON_KRYLOV && !g.periodic_x)
+        return fail(h, LBM_ERR_BAD_ARG,
+                    "the Krylov form needs periodic x: the slip walls' overwrite makes the singular system "
+                    "inconsistent, and the sweeps' gauge absorbs what a Krylov solve cannot");
     if (form == LBM_POISSON_SCALAR_RB && (g.ly % 2 || g.lz % 2 || (g.periodic_x && g.lx % 2)))
         return fail(h, LBM_ERR_BAD_ARG, "the red-black form needs even extents along the periodic axes");
     double w = omega;

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 
+#include "../../include/lbm_b200.h"
 #include "lbm_device.cuh"
 
 namespace lbm {
@@ -179,6 +180,30 @@ void twogrid_correct(cudaStream_t st, const Launch& L, const Geom& g, double* hh
 // Partial sums (kAndersonBlocks blocks) of |bsum| over the 4^3 blocks (FIN_BLOCK).
 void block_abs_sum(cudaStream_t st, const Geom& g, const double* bsum, double* part);
 }  // namespace fp64
+
+// BiCGSTAB on the kinetic fixed point (krylov.cu).  Work vectors of 15 n
+// doubles; part/host: at least 2 * max(L.nblocks, 296) doubles (host pinned).
+struct KrylovBuffers {
+    double *r, *r0, *p, *v, *s, *t;
+    double* part;
+    double* host;
+};
+struct KrylovResult {
+    uint64_t matvecs = 0;      // applications of (I - K): two per iteration plus the initial residual
+    uint64_t iterations = 0;
+    uint64_t restarts = 0;     // restarts from the true residual (near-breakdown, every 200 iterations)
+    double rel_residual = 0.0; // ||b - (I - K) h|| / ||b|| at exit (the recurrence's)
+    double gauge_shift = 0.0;
+};
+namespace krylov {
+// h: initial guess in, solution out (post-collision populations); p, p_prev:
+// the solution's p gauged to `target`.  Stops at ||r|| < tol ||b||;
+// LBM_ERR_POISSON_BUDGET past max_matvecs applications (0: no cap),
+// LBM_ERR_NONFINITE on a breakdown or a non-finite residual.
+lbm_status solve(cudaStream_t st, const Launch& L, const Geom& g, const KrylovBuffers& kb, double* h, const double* rho,
+                 const double* s, double* p, double* p_prev, double target, double tol, uint64_t max_matvecs,
+                 KrylovResult* res);
+}  // namespace krylov
 
 // Finalisation kernels (kernels_fp64.cu): reduce block partials in a fixed
 // order and update DevState.

@@ -6,6 +6,8 @@
   order than the oracle's x-outer loops).
 * The red-black SOR form reaches the Jacobi sweeps' fixed point (tight
   tolerance on both: fields within 1e-8) in a fraction of the sweeps.
+* The Krylov form (BiCGSTAB) reaches the kinetic form's fixed point (tight
+  tolerance on both: fields within 1e-8) in a fraction of its applications.
 * oracle/_ref/lbm_gpu_ref, the reference's GPU program compiled from its
   sources, against the reference's GPU/main.cpp over this library
   (oracle/_ref/lbm_gpu_dropin) on the same params.in with the split, fused
@@ -80,6 +82,31 @@ def test_red_black_reaches_the_jacobi_fixed_point():
         assert rel_err(fb[k], fa[k]) <= 1e-8, k
     for k in ("phi", "rho"):
         assert rel_err(fb[k], fa[k]) <= 1e-12, k
+
+
+def test_krylov_reaches_the_kinetic_fixed_point():
+    """BiCGSTAB on (I - K) h = b converges to the kinetic form's fixed point:
+    both run to tight tolerances (relative change 1e-12 between checks;
+    residual 1e-10, near the method's rounding floor of ~1e-11 here) and agree
+    to 1e-8, the Krylov form in a fraction of the kinetic map's
+    applications.  Periodic x only: with the slip walls the singular system
+    is inconsistent (the wall overwrite is not a permutation) and the form is
+    refused."""
+    p, f = case(True)
+    a = gpu_box(p, f, "kinetic", 1e-12, cap=2000000)
+    b = gpu_box(p, f, "krylov", 1e-10, cap=2000000)
+    sa = [s["iterations"] for s in a.step(2)]
+    sb = b.step(2)
+    assert all(s["converged"] == 1 and s["relative_error"] < 1e-10 for s in sb)
+    assert all(y["iterations"] * 4 <= x for x, y in zip(sa, sb)), (sa, [y["iterations"] for y in sb])
+    fa, fb = a.download_fields(), b.download_fields()
+    for k in L.FIELDS:
+        assert rel_err(fb[k], fa[k]) <= 1e-8, k
+    ps, fs = case(False)
+    g = L.InamuroCUDA(ps, fs, precision="fp64")
+    with pytest.raises(L.LBMError) as e:
+        g.set_poisson_form("krylov")
+    assert e.value.status == 4 and "periodic" in str(e.value)
 
 
 def test_scalar_form_rejections():
