@@ -542,7 +542,8 @@ def run_adjoint(args):
     pt, ft = adjoint_workload(n, e=0.2, kf_scale=1.05)
 
     def forward(pp, ff, sweeps=None):
-        a = L.Adjoint(pp, checkpoint_interval=min(100, K), check_interval=100, tolerance=tol_a)
+        a = L.Adjoint(pp, checkpoint_interval=min(100, K), check_interval=100, tolerance=tol_a,
+                      krylov=args.adjoint_krylov, krylov_tolerance=args.adjoint_krylov_tol)
         a.set_poisson(check_interval=100, tolerance=tol_f, max_sweeps=args.max_sweeps, fail_on_limit=1)
         a.forward(ff, K, sweeps)
         return a
@@ -599,7 +600,9 @@ def run_adjoint(args):
             "data": "synthetic (seeded phi noise 1e-4; target from an ellipsoidal drop e=0.2, kappa_f +5%)",
             "config": {"workload": f"adjoint calibration {n}^3 periodic, R={n // 4}, rho_L/rho_G=100, "
                                    f"{K} of 2000 steps (bounded sample), checkpoints every {min(100, K)} steps",
-                       "poisson": {"forward_tolerance": tol_f, "adjoint_tolerance": tol_a, "check_interval": 100},
+                       "poisson": {"forward_tolerance": tol_f, "adjoint_tolerance": tol_a, "check_interval": 100,
+                                   "adjoint_solver": "BiCGSTAB" if args.adjoint_krylov else "transposed sweeps",
+                                   "adjoint_krylov_tolerance": args.adjoint_krylov_tol if args.adjoint_krylov else None},
                        "l2": "per-step state larger than L2" if cells * 288 > 126e6 else "state fits in L2"},
             "forward_mlups": fwd_updates / fwd_s / 1e6, "reverse_mlups": bwd_updates / bwd_s / 1e6,
             "adjoint_forward_time_ratio": bwd_s / fwd_s,
@@ -823,6 +826,9 @@ def main(argv=None):
     ap.add_argument("--adjoint-forward-tol", type=float, default=1e-10,
                     help="forward Poisson exit (relative change) of the adjoint workload")
     ap.add_argument("--adjoint-tol", type=float, default=1e-13, help="adjoint Poisson exit of the adjoint workload")
+    ap.add_argument("--adjoint-krylov", action="store_true",
+                    help="adjoint workload: solve the adjoint Poisson problems by BiCGSTAB")
+    ap.add_argument("--adjoint-krylov-tol", type=float, default=1e-11)
     ap.add_argument("--adjoint-directions", type=int, default=2,
                     help="seeded random phi_0 directions checked by finite differences")
     ap.add_argument("--batch-instances", type=int, default=64)

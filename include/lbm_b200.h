@@ -518,6 +518,11 @@ typedef struct {
                                   binomial checkpointing (Griewank's revolve schedule) with at most
                                   this many stored states besides the loaded one; the forward run
                                   then keeps no states, and the reverse pass keeps one step's */
+    int krylov;                /* 1: solve each step's adjoint Poisson problem by BiCGSTAB (the
+                                  transposed kinetic operator, as LBM_POISSON_KRYLOV does forward)
+                                  to a relative residual of krylov_tolerance, instead of the
+                                  transposed sweeps and their check of tolerance */
+    double krylov_tolerance;   /* 0: 1e-10 */
 } lbm_adjoint_cfg;
 
 typedef struct {

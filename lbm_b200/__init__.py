@@ -122,7 +122,8 @@ class PoissonAccel(C.Structure):
 class AdjointCfg(C.Structure):
     """lbm_adjoint_cfg: checkpoint interval and the adjoint Poisson solve's exit."""
     _fields_ = [("checkpoint_interval", C.c_int), ("check_interval", C.c_int), ("tolerance", C.c_double),
-                ("max_sweeps", C.c_uint64), ("binomial_checkpoints", C.c_int)]
+                ("max_sweeps", C.c_uint64), ("binomial_checkpoints", C.c_int), ("krylov", C.c_int),
+                ("krylov_tolerance", C.c_double)]
 
 
 class AdjointStats(C.Structure):
@@ -671,10 +672,12 @@ class Adjoint:
     dJ/d(loaded fields) and dJ/dk_f for the adjoint lam of the final fields."""
 
     def __init__(self, params: Params, checkpoint_interval: int = 100, check_interval: int = 100,
-                 tolerance: float = 1e-12, max_sweeps: int = 0, binomial_checkpoints: int = 0, device: int = 0):
+                 tolerance: float = 1e-12, max_sweeps: int = 0, binomial_checkpoints: int = 0, krylov: bool = False,
+                 krylov_tolerance: float = 0.0, device: int = 0):
         self._lib = load_library()
         self.params = params
-        self.cfg = AdjointCfg(checkpoint_interval, check_interval, tolerance, max_sweeps, binomial_checkpoints)
+        self.cfg = AdjointCfg(checkpoint_interval, check_interval, tolerance, max_sweeps, binomial_checkpoints,
+                              int(krylov), krylov_tolerance)
         h = C.c_void_p()
         st = self._lib.lbm_adjoint_create(C.byref(params), device, C.byref(self.cfg), C.byref(h))
         if st != 0:

@@ -72,6 +72,7 @@ struct lbm_adjoint {
     int y_warm = -1;                    // y buffer holding the last converged adjoint iterate, -1: none
     std::vector<double*> bslot;         // binomial mode: checkpoint slots (36 n each), allocated on first use
     std::vector<int> bfree;             // free slot indices
+    KrylovBuffers kb{};                 // cfg.krylov: BiCGSTAB work vectors
 };
 
 namespace {
@@ -112,6 +113,10 @@ void free_all(lbm_adjoint* a)
     a->ckpt.clear();
     for (double* p : a->bslot) cudaFree(p);
     a->bslot.clear();
+    double* kv[] = {a->kb.r, a->kb.r0, a->kb.p, a->kb.v, a->kb.s, a->kb.t, a->kb.part};
+    for (double* p : kv) cudaFree(p);
+    if (a->kb.host) cudaFreeHost(a->kb.host);
+    a->kb = KrylovBuffers{};
     double* bufs[] = {a->init, a->final_state, a->seg_macro, a->seg_h, a->lpop[0][0], a->lpop[0][1],
                       a->lpop[1][0], a->lpop[1][1], a->lmac[0], a->lmac[1], a->y[0], a->y[1], a->pi_prev,
                       a->scratch, a->ls, a->lsrc, a->lkf, a->part};
@@ -175,10 +180,20 @@ lbm_status step_adjoint(lbm_adjoint* a, bool first, double* const xn, double* co
     } else {
         adj::poisson_init(st, L, g, LM(5), a->y[0]);
     }
+    uint64_t it = 0;
+    if (a->cfg.krylov) {
+        // BiCGSTAB on (I - B) y = lam_p, B = M^T o pull from x + c_q
+        KrylovResult kr;
+        const double tol = a->cfg.krylov_tolerance > 0.0 ? a->cfg.krylov_tolerance : 1e-10;
+        const lbm_status ks = krylov::solve_adjoint(st, L, g, a->kb, a->y[yc], X1(1), LM(5), tol, a->cfg.max_sweeps, &kr);
+        if (ks == LBM_ERR_POISSON_BUDGET)
+            return afail(a, ks, "adjoint Poisson sweep limit reached without convergence");
+        if (ks != LBM_OK) return afail(a, ks, "adjoint Krylov solve broke down or diverged");
+        it = kr.matvecs;
+    }
     adj::poisson_pi(st, L, g, a->y[yc], a->pi_prev);
     const int ci = a->cfg.check_interval;
-    uint64_t it = 0;
-    for (;;) {
+    for (; !a->cfg.krylov;) {
         for (int i = 0; i < ci; ++i) {
             const bool check = i == ci - 1;
             adj::poisson_sweep(st, L, g, check, a->y[yc], a->y[1 - yc], X1(1), LM(5), a->pi_prev, a->part);
@@ -472,6 +487,21 @@ lbm_status lbm_adjoint_create(const lbm_params* p, int device, const lbm_adjoint
     const long long n = a->view.geom.n;
     a->n = n;
     const size_t K = cfg->binomial_checkpoints > 0 ? 1 : static_cast<size_t>(cfg->checkpoint_interval);
+    if (cfg->krylov) {
+        const size_t parts = 2 * static_cast<size_t>(std::max<long long>(a->view.L.nblocks, 296));
+        double** kv[] = {&a->kb.r, &a->kb.r0, &a->kb.p, &a->kb.v, &a->kb.s, &a->kb.t};
+        cudaError_t ke = cudaSuccess;
+        for (double** p : kv)
+            if (ke == cudaSuccess) *p = dalloc(15 * static_cast<size_t>(n), &ke);
+        if (ke == cudaSuccess) a->kb.part = dalloc(parts, &ke);
+        if (ke == cudaSuccess) ke = cudaMallocHost(&a->kb.host, parts * sizeof(double));
+        if (ke != cudaSuccess) {
+            g_adj_create_error = std::string("Krylov buffers: ") + cudaGetErrorString(ke);
+            free_all(a);
+            delete a;
+            return ke == cudaErrorMemoryAllocation ? LBM_ERR_OOM : LBM_ERR_CUDA;
+        }
+    }
     cudaError_t e = cudaSuccess;
     struct Req { double** dst; size_t count; };
     const Req reqs[] = {

@@ -52,7 +52,10 @@ __device__ __forceinline__ void kbounce(double (&v)[Q], const Geom& g, int x)
 // out = in - K in (kinds 0, 2), or out = b - (in - K in) with b = -(E/3) s
 // (kind 1, a true residual).  Partial sums: kind 0 dot(w, out) and
 // dot(out, out); kind 1 dot(out, out); kind 2 dot(w, out) and dot(out, out).
-template <int kKind>
+// kAdj: the adjoint solve's operator B = M^T o (pull from x + c_q) instead of
+// K (M^T m = (1 - 1/tau) m + (sum_k E_k m_k) / tau per cell; periodic
+// boxes), and b_q = s (the adjoint of p, the same for every q).
+template <int kKind, bool kAdj>
 __global__ void __launch_bounds__(256)
 apply_kernel(Geom g, const double* __restrict__ in, double* __restrict__ out, const double* __restrict__ rho,
              const double* __restrict__ s, const double* __restrict__ w, double* __restrict__ part,
@@ -68,21 +71,28 @@ apply_kernel(Geom g, const double* __restrict__ in, double* __restrict__ out, co
         double hv[Q];
         static_for<0, Q>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
-            hv[q] = __ldg(in + (long long)q * n + pull_src<q>(g, wr, x, y, z));
+            if constexpr (kAdj)
+                hv[q] = __ldg(in + (long long)q * n + cell_of(g, pick<cx(q)>(wr.xm, x, wr.xp),
+                                                              pick<cy(q)>(wr.ym, y, wr.yp),
+                                                              pick<cz(q)>(wr.zm, z, wr.zp)));
+            else
+                hv[q] = __ldg(in + (long long)q * n + pull_src<q>(g, wr, x, y, z));
         });
-        kbounce(hv, g, x);
+        if constexpr (!kAdj) kbounce(hv, g, x);
         double p = 0.0;
-#pragma unroll
-        for (int q = 0; q < Q; ++q) p += hv[q];
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            p += kAdj ? wE(q) * hv[q] : hv[q];
+        });
         const double inv_tau = 1.0 / (1.0 / __ldg(rho + c) + 0.5);
         const double sv = (kKind == 1) ? __ldg(s + c) : 0.0;
         static_for<0, Q>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
             constexpr double E = wE(q);
             const long long i = (long long)q * n + c;
-            const double kh = hv[q] - (hv[q] - E * p) * inv_tau;
+            const double kh = kAdj ? hv[q] - (hv[q] - p) * inv_tau : hv[q] - (hv[q] - E * p) * inv_tau;
             double v = __ldg(in + i) - kh;
-            if constexpr (kKind == 1) v = -(E / 3.0) * sv - v;
+            if constexpr (kKind == 1) v = (kAdj ? sv : -(E / 3.0) * sv) - v;
             out[i] = v;
             if constexpr (kKind == 0) {
                 red[0] += __ldg(w + i) * v;
@@ -169,10 +179,14 @@ shift_kernel(long long n, double* __restrict__ p, double* __restrict__ p_prev, d
 }  // namespace
 
 namespace krylov {
+namespace {
 
-lbm_status solve(cudaStream_t st, const Launch& L, const Geom& g, const KrylovBuffers& kb, double* h, const double* rho,
-                 const double* s, double* p, double* p_prev, double target, double tol, uint64_t max_matvecs,
-                 KrylovResult* res)
+// BiCGSTAB iterations on (I - A_op) h = b from the initial guess in h; the
+// operator and source as apply_kernel<., kAdj>.  *budget: stopped at the cap.
+template <bool kAdj>
+lbm_status bicgstab(cudaStream_t st, const Launch& L, const Geom& g, const KrylovBuffers& kb, double* h,
+                    const double* rho, const double* s, double tol, uint64_t max_matvecs, KrylovResult* res,
+                    bool* budget_out)
 {
     const long long cnt = 15 * g.n;
     auto host_sum = [&](long long blocks, int cols, double* out) -> bool {
@@ -191,11 +205,11 @@ lbm_status solve(cudaStream_t st, const Launch& L, const Geom& g, const KrylovBu
     *res = KrylovResult{};
     // ||b||: the residual of x = 0 (v is zero, and stays the v_0 = 0 of the method)
     if (cudaMemsetAsync(kb.v, 0, static_cast<size_t>(cnt) * sizeof(double), st) != cudaSuccess) return LBM_ERR_CUDA;
-    apply_kernel<1><<<L.grid, L.block, 0, st>>>(g, kb.v, kb.t, rho, s, nullptr, kb.part, L.nblocks);
+    apply_kernel<1, kAdj><<<L.grid, L.block, 0, st>>>(g, kb.v, kb.t, rho, s, nullptr, kb.part, L.nblocks);
     if (!host_sum(L.nblocks, 1, d2)) return LBM_ERR_CUDA;
     const double bnorm = sqrt(d2[0]);
     // r = b - A x0, r0 = p = r
-    apply_kernel<1><<<L.grid, L.block, 0, st>>>(g, h, kb.r, rho, s, nullptr, kb.part, L.nblocks);
+    apply_kernel<1, kAdj><<<L.grid, L.block, 0, st>>>(g, h, kb.r, rho, s, nullptr, kb.part, L.nblocks);
     if (!host_sum(L.nblocks, 1, d2)) return LBM_ERR_CUDA;
     double rr = d2[0];
     vec_kernel<3><<<kDotBlocks, 256, 0, st>>>(cnt, 0.0, 0.0, kb.r0, kb.p, kb.r, nullptr, nullptr, nullptr, nullptr);
@@ -216,7 +230,7 @@ lbm_status solve(cudaStream_t st, const Launch& L, const Geom& g, const KrylovBu
                                                        nullptr);
         }
         first = false;
-        apply_kernel<0><<<L.grid, L.block, 0, st>>>(g, kb.p, kb.v, rho, nullptr, kb.r0, kb.part, L.nblocks);
+        apply_kernel<0, kAdj><<<L.grid, L.block, 0, st>>>(g, kb.p, kb.v, rho, nullptr, kb.r0, kb.part, L.nblocks);
         if (!host_sum(L.nblocks, 2, d2)) return LBM_ERR_CUDA;
         ++res->matvecs;
         if (!isfinite(d2[0]) || !isfinite(d2[1])) return LBM_ERR_NONFINITE;
@@ -224,7 +238,7 @@ lbm_status solve(cudaStream_t st, const Launch& L, const Geom& g, const KrylovBu
         // floor) or 200 iterations since the last start: restart from the
         // true residual of the current iterate.
         if (fabs(d2[0]) <= 1e-12 * sqrt(r0r0 * d2[1]) || since >= 200) {
-            apply_kernel<1><<<L.grid, L.block, 0, st>>>(g, h, kb.r, rho, s, nullptr, kb.part, L.nblocks);
+            apply_kernel<1, kAdj><<<L.grid, L.block, 0, st>>>(g, h, kb.r, rho, s, nullptr, kb.part, L.nblocks);
             if (!host_sum(L.nblocks, 1, d2)) return LBM_ERR_CUDA;
             ++res->matvecs;
             rr = d2[0];
@@ -241,7 +255,7 @@ lbm_status solve(cudaStream_t st, const Launch& L, const Geom& g, const KrylovBu
         }
         alpha = rho_new / d2[0];
         vec_kernel<1><<<kDotBlocks, 256, 0, st>>>(cnt, alpha, 0.0, kb.s, nullptr, kb.r, kb.v, nullptr, nullptr, nullptr);
-        apply_kernel<2><<<L.grid, L.block, 0, st>>>(g, kb.s, kb.t, rho, nullptr, kb.s, kb.part, L.nblocks);
+        apply_kernel<2, kAdj><<<L.grid, L.block, 0, st>>>(g, kb.s, kb.t, rho, nullptr, kb.s, kb.part, L.nblocks);
         if (!host_sum(L.nblocks, 2, d2)) return LBM_ERR_CUDA;
         omega = d2[1] > 0.0 ? d2[0] / d2[1] : 0.0;
         vec_kernel<2><<<kDotBlocks, 256, 0, st>>>(cnt, alpha, omega, h, kb.r, kb.p, kb.s, kb.t, kb.r0, kb.part);
@@ -256,14 +270,40 @@ lbm_status solve(cudaStream_t st, const Launch& L, const Geom& g, const KrylovBu
         res->rel_residual = sqrt(rr) / bnorm;
         if (omega == 0.0 && res->rel_residual >= tol) since = 200;   // stagnation: restart next
     }
+    *budget_out = budget;
+    return LBM_OK;
+}
+
+}  // namespace
+
+lbm_status solve(cudaStream_t st, const Launch& L, const Geom& g, const KrylovBuffers& kb, double* h, const double* rho,
+                 const double* s, double* p, double* p_prev, double target, double tol, uint64_t max_matvecs,
+                 KrylovResult* res)
+{
+    bool budget = false;
+    const lbm_status it = bicgstab<false>(st, L, g, kb, h, rho, s, tol, max_matvecs, res, &budget);
+    if (it != LBM_OK) return it;
     // p of the solution, gauged to the target mean (p_prev follows, as after a check)
     pressure_kernel<<<L.grid, L.block, 0, st>>>(g, h, p, kb.part, L.nblocks);
-    if (!host_sum(L.nblocks, 1, d2)) return LBM_ERR_CUDA;
-    const double shift = d2[0] / static_cast<double>(g.n) - target;
+    if (cudaMemcpyAsync(kb.host, kb.part, L.nblocks * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return LBM_ERR_CUDA;
+    double sum = 0.0;
+    for (long long b = 0; b < L.nblocks; ++b) sum += kb.host[b];
+    const double shift = sum / static_cast<double>(g.n) - target;
     if (!isfinite(shift)) return LBM_ERR_NONFINITE;
     shift_kernel<<<kDotBlocks, 256, 0, st>>>(g.n, p, p_prev, shift);
     if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) return LBM_ERR_CUDA;
     res->gauge_shift = shift;
+    return budget ? LBM_ERR_POISSON_BUDGET : LBM_OK;
+}
+
+lbm_status solve_adjoint(cudaStream_t st, const Launch& L, const Geom& g, const KrylovBuffers& kb, double* y,
+                         const double* rho, const double* lp, double tol, uint64_t max_matvecs, KrylovResult* res)
+{
+    bool budget = false;
+    const lbm_status it = bicgstab<true>(st, L, g, kb, y, rho, lp, tol, max_matvecs, res, &budget);
+    if (it != LBM_OK) return it;
     return budget ? LBM_ERR_POISSON_BUDGET : LBM_OK;
 }
 

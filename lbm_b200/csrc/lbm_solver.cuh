@@ -203,6 +203,10 @@ namespace krylov {
 lbm_status solve(cudaStream_t st, const Launch& L, const Geom& g, const KrylovBuffers& kb, double* h, const double* rho,
                  const double* s, double* p, double* p_prev, double target, double tol, uint64_t max_matvecs,
                  KrylovResult* res);
+// The adjoint Poisson problem y = M^T (pull from x + c_q of y) + lam_p
+// (periodic boxes) by the same method: y initial guess in, solution out.
+lbm_status solve_adjoint(cudaStream_t st, const Launch& L, const Geom& g, const KrylovBuffers& kb, double* y,
+                         const double* rho, const double* lp, double tol, uint64_t max_matvecs, KrylovResult* res);
 }  // namespace krylov
 
 // Finalisation kernels (kernels_fp64.cu): reduce block partials in a fixed

@@ -173,3 +173,21 @@ def test_binomial_checkpointing_matches_uniform(run, slots):
     assert s2["grad_kappa_f"] == stats["grad_kappa_f"]
     assert s2["recompute_steps"] == L.adjoint_schedule(STEPS, slots)["recompute_steps"]
     b.close()
+
+
+def test_krylov_adjoint_solve_matches_the_sweeps(run):
+    """The adjoint Poisson problem solved by BiCGSTAB (krylov=True) gives the
+    gradient of the transposed sweeps (which the finite-difference tests
+    check) to 1e-7, in a fraction of the applications."""
+    p, f, obj, y, sweeps, grads, stats, a = run
+    b = L.Adjoint(p, checkpoint_interval=KINT, check_interval=50, tolerance=1e-13, max_sweeps=2000000,
+                  krylov=True, krylov_tolerance=1e-11)
+    poisson(b)
+    b.forward(f, STEPS)
+    g2, s2 = b.backward(obj.adjoint(y))
+    for k in L.FIELDS:
+        scale = float(np.max(np.abs(grads[k])))
+        assert float(np.max(np.abs(g2[k] - grads[k]))) <= 1e-7 * scale, k
+    assert abs(s2["grad_kappa_f"] - stats["grad_kappa_f"]) <= 1e-7 * abs(stats["grad_kappa_f"])
+    assert s2["adjoint_sweeps"] * 3 <= stats["adjoint_sweeps"], (s2["adjoint_sweeps"], stats["adjoint_sweeps"])
+    b.close()
