@@ -207,7 +207,9 @@ lbm_status bicgstab(cudaStream_t st, const Launch& L, const Geom& g, const Krylo
     if (cudaMemsetAsync(kb.v, 0, static_cast<size_t>(cnt) * sizeof(double), st) != cudaSuccess) return LBM_ERR_CUDA;
     apply_kernel<1, kAdj><<<L.grid, L.block, 0, st>>>(g, kb.v, kb.t, rho, s, nullptr, kb.part, L.nblocks);
     if (!host_sum(L.nblocks, 1, d2)) return LBM_ERR_CUDA;
-    const double bnorm = sqrt(d2[0]);
+    // relative to ||b||; a zero source (absolute criterion) still drives the
+    // iterate to the null-space representative nearest the start
+    const double bnorm = d2[0] > 0.0 ? sqrt(d2[0]) : 1.0;
     // r = b - A x0, r0 = p = r
     apply_kernel<1, kAdj><<<L.grid, L.block, 0, st>>>(g, h, kb.r, rho, s, nullptr, kb.part, L.nblocks);
     if (!host_sum(L.nblocks, 1, d2)) return LBM_ERR_CUDA;
@@ -217,40 +219,53 @@ lbm_status bicgstab(cudaStream_t st, const Launch& L, const Geom& g, const Krylo
     double rho_old = 1.0, alpha = 1.0, omega = 1.0, rho_new = rr, r0r0 = rr;
     bool first = true, budget = false;
     int since = 0;
-    res->rel_residual = bnorm > 0.0 ? sqrt(rr) / bnorm : 0.0;
-    while (bnorm > 0.0 && res->rel_residual >= tol) {
+    // Restart from the true residual of the current iterate: r = b - A h,
+    // r0 = p = r.
+    auto restart = [&]() -> lbm_status {
+        apply_kernel<1, kAdj><<<L.grid, L.block, 0, st>>>(g, h, kb.r, rho, s, nullptr, kb.part, L.nblocks);
+        if (!host_sum(L.nblocks, 1, d2)) return LBM_ERR_CUDA;
+        ++res->matvecs;
+        rr = d2[0];
+        if (!isfinite(rr)) return LBM_ERR_NONFINITE;
+        vec_kernel<3><<<kDotBlocks, 256, 0, st>>>(cnt, 0.0, 0.0, kb.r0, kb.p, kb.r, nullptr, nullptr, nullptr,
+                                                   nullptr);
+        rho_new = r0r0 = rr;
+        rho_old = alpha = omega = 1.0;
+        first = true;
+        since = 0;
+        ++res->restarts;
+        res->rel_residual = sqrt(rr) / bnorm;
+        return LBM_OK;
+    };
+    res->rel_residual = sqrt(rr) / bnorm;
+    while (res->rel_residual >= tol) {
         if (max_matvecs && res->matvecs + 3 > max_matvecs) {
             budget = true;
             break;
         }
+        // a collapsed recurrence (rho or omega zero: breakdown or stagnation)
+        // or 200 iterations since the last start
+        if (!first && (rho_old == 0.0 || omega == 0.0 || since >= 200)) {
+            const lbm_status rs = restart();
+            if (rs != LBM_OK) return rs;
+            continue;
+        }
         if (!first) {
-            if (rho_old == 0.0 || omega == 0.0) return LBM_ERR_NONFINITE;   // breakdown
             const double beta = (rho_new / rho_old) * (alpha / omega);
             vec_kernel<0><<<kDotBlocks, 256, 0, st>>>(cnt, beta, omega, kb.p, nullptr, kb.r, kb.v, nullptr, nullptr,
                                                        nullptr);
         }
+        const bool fresh = first;
         first = false;
         apply_kernel<0, kAdj><<<L.grid, L.block, 0, st>>>(g, kb.p, kb.v, rho, nullptr, kb.r0, kb.part, L.nblocks);
         if (!host_sum(L.nblocks, 2, d2)) return LBM_ERR_CUDA;
         ++res->matvecs;
         if (!isfinite(d2[0]) || !isfinite(d2[1])) return LBM_ERR_NONFINITE;
-        // Near-breakdown (r0 . v ~ 0 against |r0| |v|, as at the rounding
-        // floor) or 200 iterations since the last start: restart from the
-        // true residual of the current iterate.
-        if (fabs(d2[0]) <= 1e-12 * sqrt(r0r0 * d2[1]) || since >= 200) {
-            apply_kernel<1, kAdj><<<L.grid, L.block, 0, st>>>(g, h, kb.r, rho, s, nullptr, kb.part, L.nblocks);
-            if (!host_sum(L.nblocks, 1, d2)) return LBM_ERR_CUDA;
-            ++res->matvecs;
-            rr = d2[0];
-            if (!isfinite(rr)) return LBM_ERR_NONFINITE;
-            vec_kernel<3><<<kDotBlocks, 256, 0, st>>>(cnt, 0.0, 0.0, kb.r0, kb.p, kb.r, nullptr, nullptr, nullptr,
-                                                       nullptr);
-            rho_new = r0r0 = rr;
-            rho_old = alpha = omega = 1.0;
-            first = true;
-            since = 0;
-            ++res->restarts;
-            res->rel_residual = sqrt(rr) / bnorm;
+        // near-breakdown: r0 . v ~ 0 against |r0| |v| (as at the rounding floor)
+        if (fabs(d2[0]) <= 1e-12 * sqrt(r0r0 * d2[1])) {
+            if (fresh) return LBM_ERR_NONFINITE;   // even a fresh start breaks down
+            const lbm_status rs = restart();
+            if (rs != LBM_OK) return rs;
             continue;
         }
         alpha = rho_new / d2[0];
@@ -268,7 +283,6 @@ lbm_status bicgstab(cudaStream_t st, const Launch& L, const Geom& g, const Krylo
         ++since;
         if (!isfinite(rr)) return LBM_ERR_NONFINITE;
         res->rel_residual = sqrt(rr) / bnorm;
-        if (omega == 0.0 && res->rel_residual >= tol) since = 200;   // stagnation: restart next
     }
     *budget_out = budget;
     return LBM_OK;
