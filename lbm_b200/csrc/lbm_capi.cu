@@ -450,6 +450,8 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
         return fail(h, LBM_ERR_BAD_ARG,
                     "fixed-point residual requires the kinetic (split) Poisson form with unit relaxation and "
                     "all accelerators disabled");
+    if (form == LBM_POISSON_KRYLOV && replay)
+        return fail(h, LBM_ERR_BAD_ARG, "the Krylov form stops on its residual: there is no sweep count to replay");
     if (onepass_only && form != LBM_POISSON_ONEPASS)
         return fail(h, LBM_ERR_BAD_ARG, "relaxation scales and Anderson-m1 need the one-pass Poisson form");
     if (block_sums && form != LBM_POISSON_ONEPASS && form != LBM_POISSON_KINETIC)

@@ -107,6 +107,9 @@ def test_krylov_reaches_the_kinetic_fixed_point():
     with pytest.raises(L.LBMError) as e:
         g.set_poisson_form("krylov")
     assert e.value.status == 4 and "periodic" in str(e.value)
+    with pytest.raises(L.LBMError) as e:
+        b.step_replay([100])
+    assert e.value.status == 4 and "replay" in str(e.value)
 
 
 def test_scalar_form_rejections():
