@@ -21,7 +21,7 @@
 namespace lbm {
 namespace {
 
-constexpr int kDotBlocks = 296;
+constexpr int kDotBlocks = kKrylovBlocks;
 
 __device__ __forceinline__ bool kcell(const Geom& g, int& x, int& y, int& z)
 {

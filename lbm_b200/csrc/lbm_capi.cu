@@ -465,7 +465,7 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
         const size_t pop = 15 * static_cast<size_t>(g.n) * sizeof(double);
         double** kv[] = {&h->kb.r, &h->kb.r0, &h->kb.p, &h->kb.v, &h->kb.s, &h->kb.t};
         for (double** p : kv) LBM_CUDA(h, cudaMalloc(p, pop));
-        const size_t parts = 2 * static_cast<size_t>(std::max<long long>(L.nblocks, 296));
+        const size_t parts = 2 * static_cast<size_t>(std::max<long long>(L.nblocks, kKrylovBlocks));
         LBM_CUDA(h, cudaMalloc(&h->kb.part, parts * sizeof(double)));
         LBM_CUDA(h, cudaMallocHost(&h->kb.host, parts * sizeof(double)));
     }
