@@ -112,6 +112,29 @@ def test_krylov_reaches_the_kinetic_fixed_point():
     assert e.value.status == 4 and "replay" in str(e.value)
 
 
+def test_accelerators_through_python():
+    """lbm_set_poisson_accel from Python: the one-pass form with every
+    accelerator converges; the kinetic form refuses the one-pass-only
+    settings at the next step; invalid values are refused by the setter and
+    leave the settings unchanged."""
+    p, f = case(True)
+    g = gpu_box(p, f, "onepass", 1e-3)
+    g.set_poisson_accel(anderson_m1=1, two_grid=1, spatial_diagnostics=1, source_aware_init=1,
+                        fixed_point_relax=0.9)
+    st = g.step(2)
+    assert all(s["converged"] == 1 for s in st)
+    k = gpu_box(p, f, "kinetic", 1e-3)
+    k.set_poisson_accel(anderson_m1=1)
+    with pytest.raises(L.LBMError) as e:
+        k.step(1)
+    assert e.value.status == 4 and "one-pass" in str(e.value)
+    k.set_poisson_accel(anderson_m1=0, two_grid=1)
+    assert k.step(1)[0]["converged"] == 1
+    with pytest.raises(L.LBMError) as e:
+        k.set_poisson_accel(fixed_point_relax=-1.0)
+    assert e.value.status == 4
+
+
 def test_scalar_form_rejections():
     p, f = case(True)
     m = L.InamuroCUDA(p, f, precision="mixed")
