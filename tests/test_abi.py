@@ -58,3 +58,32 @@ def test_header_compiles_as_c():
     r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-fsyntax-only", "-I", inc, "-x", "c", "-"],
                        input=src, text=True, capture_output=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_python_structs_match_the_header_layout(tmp_path):
+    """Every structure the Python bindings mirror has the header's size and
+    field offsets (a C program built from the Python field lists prints them;
+    a field name the header lacks fails to compile)."""
+    pairs = [("lbm_params", L.Params), ("lbm_poisson_cfg", L.PoissonCfg), ("lbm_step_stats", L.StepStats),
+             ("lbm_timing", L.Timing), ("lbm_field_stats", L.FieldStats), ("lbm_diagnostics", L.Diagnostics),
+             ("lbm_batch_tuning", L.BatchTuning), ("lbm_poisson_accel", L.PoissonAccel),
+             ("lbm_adjoint_cfg", L.AdjointCfg), ("lbm_adjoint_stats", L.AdjointStats)]
+    lines = ["#include <stddef.h>", "#include <stdio.h>", "#include \"lbm_b200.h\"", "int main(void) {"]
+    for cname, cls in pairs:
+        lines.append(f'    printf("{cname} %zu\\n", sizeof({cname}));')
+        for f, _ in cls._fields_:
+            lines.append(f'    printf("{cname}.{f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ["    return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    inc = os.path.dirname(L.HEADER_PATH)
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", inc, str(src), "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                       check=True).stdout.splitlines())
+    for cname, cls in pairs:
+        assert int(got[cname]) == ctypes.sizeof(cls), cname
+        for f, _ in cls._fields_:
+            assert int(got[f"{cname}.{f}"]) == getattr(cls, f).offset, (cname, f)
