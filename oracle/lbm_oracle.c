@@ -423,6 +423,188 @@ static int poisson_scalar(orc_state* s, uint64_t replay, orc_step_info* info, do
     return ORC_OK;
 }
 
+/* sourceAwareHHInitKernel (GPU/InamuroCUDA.cu:903-929): the solve's start
+ * h = E_q p - scale tau_h (E_q / 3) s, s the projected u_x + v_y + w_z. */
+static void source_aware_init(orc_state* s)
+{
+    const long N = s->N;
+    for (long c = 0; c < N; ++c) {
+        const double tauh = 1.0 / s->rho[c] + 0.5;
+        const double div = s->d[D_UX][c] + s->d[D_VY][c] + s->d[D_WZ][c];
+        for (int q = 0; q < Q; ++q)
+            s->h[(long)q * N + c] = EI[q] * s->p[c] - s->P.source_aware_scale * tauh * ((EI[q] / 3.0) * div);
+    }
+}
+
+/* The reference's one-pass Poisson form with its accelerators (GPU only
+ * there): collisionStreamBoundaryPressureKernel (GPU/InamuroCUDA.cu:780-844),
+ * Anderson-m1 (:931-1013, 2230-2275), the check with the two-grid
+ * correction (:1198-1255, 1284-1328, 2057-2156).  State: the pre-collision
+ * h and p = sum_q h.  x-outer sums; Anderson's inner products cell-major. */
+static int poisson_onepass(orc_state* s, uint64_t replay, orc_step_info* info, double target)
+{
+    const orc_params* P = &s->P;
+    const int lx = P->lx, ly = P->ly, lz = P->lz;
+    const long N = s->N;
+    const double cell_count = (double)lx * ly * lz;
+    const double relax = P->pressure_relax_scale != 0.0 ? P->pressure_relax_scale : 1.0;
+    const double omega = P->fixed_point_relax != 0.0 ? P->fixed_point_relax : 1.0;
+    double* prev_r = NULL;
+    double* prev_img = NULL;
+    if (P->anderson_m1) {
+        prev_r = (double*)malloc(sizeof(double) * Q * N);
+        prev_img = (double*)malloc(sizeof(double) * Q * N);
+        if (!prev_r || !prev_img) {
+            free(prev_r);
+            free(prev_img);
+            return ORC_ERR_OOM;
+        }
+    }
+    const int bs = 4, bxn = (lx + bs - 1) / bs, byn = (ly + bs - 1) / bs, bzn = (lz + bs - 1) / bs;
+    double* bsum = P->two_grid ? (double*)calloc((size_t)bxn * byn * bzn, sizeof(double)) : NULL;
+    int has_history = 0, status = ORC_OK;
+    uint64_t iter = 0;
+    for (;;) {
+        ++iter;
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int z = 0; z < lz; ++z)
+            for (int y = 0; y < ly; ++y)
+                for (int x = 0; x < lx; ++x) {
+                    double h[Q];
+                    for (int q = 0; q < Q; ++q) {
+                        int xs = x - EX[q], ys = y - EY[q], zs = z - EZ[q];
+                        if (xs < 0) xs += lx; else if (xs >= lx) xs -= lx;
+                        if (ys < 0) ys += ly; else if (ys >= ly) ys -= ly;
+                        if (zs < 0) zs += lz; else if (zs >= lz) zs -= lz;
+                        const long src = idx(s, xs, ys, zs);
+                        const double tauh = 1.0 / s->rho[src] + 0.5;
+                        const double hequ = EI[q] * s->p[src];
+                        const double h_old = s->h[(long)q * N + src];
+                        const double div = s->d[D_UX][src] + s->d[D_VY][src] + s->d[D_WZ][src];
+                        h[q] = h_old - relax * (h_old - hequ) / tauh - (EI[q] / 3.0) * div;
+                    }
+                    if (!P->periodic_x && x == 0) {
+                        h[1] = h[4]; h[7] = h[8]; h[9] = h[14]; h[10] = h[13]; h[12] = h[11];
+                    } else if (!P->periodic_x && x == lx - 1) {
+                        h[4] = h[1]; h[8] = h[7]; h[14] = h[9]; h[13] = h[10]; h[11] = h[12];
+                    }
+                    const long c = idx(s, x, y, z);
+                    double psum = 0.0;
+                    for (int q = 0; q < Q; ++q) {
+                        const double h_old = s->h[(long)q * N + c];
+                        const double hv = h_old + omega * (h[q] - h_old);
+                        s->img[(long)q * N + c] = hv;
+                        psum += hv;
+                    }
+                    s->pf[c] = psum;
+                }
+        if (P->anderson_m1) {
+            if (!has_history) {
+                for (long i = 0; i < (long)Q * N; ++i) {
+                    prev_r[i] = s->img[i] - s->h[i];
+                    prev_img[i] = s->img[i];
+                }
+                has_history = 1;
+            } else {
+                double num = 0.0, den = 0.0;
+                for (long c = 0; c < N; ++c)
+                    for (int q = 0; q < Q; ++q) {
+                        const long i = (long)q * N + c;
+                        const double r = s->img[i] - s->h[i];
+                        const double dl = r - prev_r[i];
+                        num += prev_r[i] * dl;
+                        den += dl * dl;
+                    }
+                double alpha = 1.0;
+                if (den > 1.0e-300) alpha = -num / den;
+                if (!isfinite(alpha)) alpha = 1.0;
+                const double lo = -P->anderson_beta_max, hi = 1.0 + P->anderson_beta_max;
+                alpha = alpha < lo ? lo : (alpha > hi ? hi : alpha);
+                for (long c = 0; c < N; ++c) {
+                    double psum = 0.0;
+                    for (int q = 0; q < Q; ++q) {
+                        const long i = (long)q * N + c;
+                        const double cur = s->img[i];
+                        const double acc = (1.0 - alpha) * prev_img[i] + alpha * cur;
+                        prev_r[i] = cur - s->h[i];
+                        prev_img[i] = cur;
+                        s->img[i] = acc;
+                        psum += acc;
+                    }
+                    s->pf[c] = psum;
+                }
+            }
+        }
+        double* t = s->h;
+        s->h = s->img;
+        s->img = t;
+        memcpy(s->p, s->pf, sizeof(double) * N);
+        int converged = 0;
+        if (iter % (uint64_t)P->check_interval == 0) {
+            const double shift = sum_xouter(s, s->p) / cell_count - target;
+            if (!isfinite(shift)) { status = ORC_ERR_NONFINITE; break; }
+            if (fabs(shift) > info->gauge_max_shift) info->gauge_max_shift = fabs(shift);
+            for (long c = 0; c < N; ++c) {
+                s->p[c] -= shift;
+                for (int q = 0; q < Q; ++q) s->h[(long)q * N + c] -= EI[q] * shift;
+            }
+            if (bsum) {
+                memset(bsum, 0, sizeof(double) * bxn * byn * bzn);
+                for (int z = 0; z < lz; ++z)
+                    for (int y = 0; y < ly; ++y)
+                        for (int x = 0; x < lx; ++x) {
+                            const long c = idx(s, x, y, z);
+                            bsum[((z / bs) * byn + y / bs) * bxn + x / bs] += s->p[c] - s->p_prev[c];
+                        }
+            }
+            double err1 = 0.0, err2 = 0.0;
+            for (int x = 0; x < lx; ++x)
+                for (int y = 0; y < ly; ++y)
+                    for (int z = 0; z < lz; ++z) {
+                        const long c = idx(s, x, y, z);
+                        err1 += fabs(s->p[c] - s->p_prev[c]);
+                        err2 += fabs(s->p[c]);
+                        s->p_prev[c] = s->p[c];
+                    }
+            if (!isfinite(err1) || !isfinite(err2)) { status = ORC_ERR_NONFINITE; break; }
+            info->pressure_l1_delta = err1;
+            info->pressure_l1_norm = err2;
+            info->relative_error = relative(err1, err2);
+            converged = info->relative_error < P->tol;
+            if (bsum && !converged && err1 > 0.0) {
+                for (int z = 0; z < lz; ++z)
+                    for (int y = 0; y < ly; ++y)
+                        for (int x = 0; x < lx; ++x) {
+                            const int bx = x / bs, by = y / bs, bz = z / bs;
+                            const int x1 = (bx + 1) * bs < lx ? (bx + 1) * bs : lx;
+                            const int y1 = (by + 1) * bs < ly ? (by + 1) * bs : ly;
+                            const int z1 = (bz + 1) * bs < lz ? (bz + 1) * bs : lz;
+                            const int cells = (x1 - bx * bs) * (y1 - by * bs) * (z1 - bz * bs);
+                            const double corr = P->two_grid_strength * bsum[(bz * byn + by) * bxn + bx] / (double)cells;
+                            const long c = idx(s, x, y, z);
+                            s->p[c] += corr;
+                            s->p_prev[c] = s->p[c];
+                            for (int q = 0; q < Q; ++q) s->h[(long)q * N + c] += EI[q] * corr;
+                        }
+            }
+        }
+        if (replay) {
+            if (iter == replay) break;
+        } else if (converged) {
+            break;
+        }
+        if (!replay && P->max_sweeps && iter >= P->max_sweeps) {
+            status = ORC_ERR_BUDGET;
+            break;
+        }
+    }
+    free(prev_r);
+    free(prev_img);
+    free(bsum);
+    info->sweeps = iter;
+    return status;
+}
+
 /* solvePressurePoisson: CPU/Inamuro.cpp:624-724 */
 static int poisson(orc_state* s, uint64_t replay, orc_step_info* info)
 {
@@ -448,6 +630,8 @@ static int poisson(orc_state* s, uint64_t replay, orc_step_info* info)
     info->gauge_target = target;
     info->gauge_max_shift = 0.0;
     if (P->poisson_form == 1) return poisson_scalar(s, replay, info, target);
+    if (P->source_aware_init) source_aware_init(s);
+    if (P->poisson_form == 2) return poisson_onepass(s, replay, info, target);
 
     uint64_t iter = 0;
     for (;;) {
@@ -560,7 +744,7 @@ orc_state* orc_create(const orc_params* prm,
                       const double* p)
 {
     if (!prm || prm->lx < 2 || prm->ly < 1 || prm->lz < 1 || prm->check_interval <= 0) return NULL;
-    if (prm->poisson_form < 0 || prm->poisson_form > 1 || (prm->poisson_form == 1 && prm->dual)) return NULL;
+    if (prm->poisson_form < 0 || prm->poisson_form > 2 || (prm->poisson_form != 0 && prm->dual)) return NULL;
     orc_state* s = (orc_state*)calloc(1, sizeof(orc_state));
     if (!s) return NULL;
     s->P = *prm;

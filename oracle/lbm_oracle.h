@@ -49,8 +49,19 @@ typedef struct {
     int dual;                /* 1: also require the kinetic fixed-point residual < tol */
     uint64_t max_sweeps;     /* 0 = unbounded (reference contract); else error when hit */
     int periodic_x;          /* 1: periodic x (no slip walls) -- not a reference mode */
-    int poisson_form;        /* 0: kinetic (production); 1: the reference's scalar Jacobi form */
+    int poisson_form;        /* 0: kinetic (production); 1: the reference's scalar Jacobi form;
+                                2: the reference's one-pass form */
     double scalar_source_scale;  /* scalar form: --scalar-source-scale (reference default 2.0) */
+    /* the reference's accelerators (GPU/main.cpp flags); a zero-initialised
+       block means: relaxations 1 (0 is read as 1), all off */
+    double pressure_relax_scale;     /* one-pass: --pressure-relax-scale */
+    double fixed_point_relax;        /* one-pass: --poisson-fixed-point-relax */
+    int anderson_m1;                 /* one-pass: --poisson-anderson-m1 */
+    double anderson_beta_max;        /* --poisson-anderson-beta-max */
+    int two_grid;                    /* one-pass: --poisson-two-grid-correction */
+    double two_grid_strength;        /* --poisson-two-grid-strength */
+    int source_aware_init;           /* kinetic and one-pass: --source-aware-hh-init */
+    double source_aware_scale;       /* --source-aware-hh-scale */
 } orc_params;
 
 typedef struct {

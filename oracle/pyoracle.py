@@ -28,7 +28,10 @@ class OrcParams(C.Structure):
         [(k, C.c_double) for k in PARAM_KEYS] + \
         [("check_interval", C.c_int), ("tol", C.c_double), ("dual", C.c_int),
          ("max_sweeps", C.c_uint64), ("periodic_x", C.c_int), ("poisson_form", C.c_int),
-         ("scalar_source_scale", C.c_double)]
+         ("scalar_source_scale", C.c_double), ("pressure_relax_scale", C.c_double),
+         ("fixed_point_relax", C.c_double), ("anderson_m1", C.c_int), ("anderson_beta_max", C.c_double),
+         ("two_grid", C.c_int), ("two_grid_strength", C.c_double), ("source_aware_init", C.c_int),
+         ("source_aware_scale", C.c_double)]
 
 
 class OrcStepInfo(C.Structure):
@@ -90,12 +93,14 @@ class Oracle:
     def __init__(self, shape, params: Dict[str, float], fields: Dict[str, np.ndarray],
                  check_interval: int = 100, tol: float = 1e-3, dual: bool = False,
                  max_sweeps: int = 0, periodic_x: bool = False, poisson_form: int = 0,
-                 scalar_source_scale: float = 2.0):
+                 scalar_source_scale: float = 2.0, accel: Dict[str, float] = None):
         lx, ly, lz = shape
         self.shape = (lz, ly, lx)
         prm = OrcParams(lx=lx, ly=ly, lz=lz, check_interval=check_interval, tol=tol,
                         dual=int(dual), max_sweeps=max_sweeps, periodic_x=int(periodic_x),
                         poisson_form=int(poisson_form), scalar_source_scale=float(scalar_source_scale),
+                        **dict({"pressure_relax_scale": 1.0, "fixed_point_relax": 1.0, "anderson_beta_max": 1.0,
+                                "two_grid_strength": 0.5, "source_aware_scale": 1.0}, **(accel or {})),
                         **{k: float(params[k]) for k in PARAM_KEYS})
         arrs = [np.ascontiguousarray(fields[k], dtype=np.float64).reshape(self.shape)
                 for k in ("phi", "rho", "u", "v", "w")]

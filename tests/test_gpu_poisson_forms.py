@@ -6,6 +6,9 @@
   order than the oracle's x-outer loops).
 * The red-black SOR form reaches the Jacobi sweeps' fixed point (tight
   tolerance on both: fields within 1e-8) in a fraction of the sweeps.
+* The one-pass form with each accelerator, and source-aware init on the
+  kinetic form, against the oracle's FP64 restatements (sweep counts and
+  fields to the FP64 bar).
 * The Krylov form (BiCGSTAB) reaches the kinetic form's fixed point (tight
   tolerance on both: fields within 1e-8) in a fraction of its applications.
 * oracle/_ref/lbm_gpu_ref, the reference's GPU program compiled from its
@@ -64,6 +67,44 @@ def test_scalar_form_matches_oracle(periodic):
         got = g.step(1)[0]
         assert got["iterations"] == want["sweeps"], step
         assert got["converged"] == 1
+    of, gf = o.fields(), g.download_fields()
+    for k in L.FIELDS:
+        assert rel_err(gf[k], of[k]) <= 1e-10, k
+
+
+ACCELS = [{}, {"fixed_point_relax": 0.8}, {"pressure_relax_scale": 0.9}, {"anderson_m1": 1}, {"two_grid": 1},
+          {"source_aware_init": 1, "source_aware_scale": 0.5}]
+
+
+@pytest.mark.parametrize("periodic", [False, True])
+@pytest.mark.parametrize("accel", ACCELS, ids=["plain", "omega", "relax", "anderson", "twogrid", "source"])
+def test_onepass_matches_oracle(periodic, accel):
+    """The one-pass form and each accelerator against the oracle's FP64
+    restatement (poisson_onepass in oracle/lbm_oracle.c): the same sweep
+    count at every natural exit and fields within the FP64 bar (1e-10;
+    Anderson 1e-9: its mixing coefficient comes from sums in another order)."""
+    p, f = case(periodic)
+    g = gpu_box(p, f, "onepass", 1e-3)
+    g.set_poisson_accel(**accel)
+    o = pyoracle.Oracle(SHAPE, oracle_params(p), f, tol=1e-3, periodic_x=periodic, poisson_form=2, accel=accel)
+    for step in range(3):
+        want = o.step()
+        got = g.step(1)[0]
+        assert got["iterations"] == want["sweeps"], step
+    of, gf = o.fields(), g.download_fields()
+    tol = 1e-9 if accel.get("anderson_m1") else 1e-10
+    for k in L.FIELDS:
+        assert rel_err(gf[k], of[k]) <= tol, k
+
+
+def test_kinetic_source_aware_init_matches_oracle():
+    p, f = case(False)
+    g = gpu_box(p, f, "kinetic", 1e-3)
+    g.set_poisson_accel(source_aware_init=1, source_aware_scale=0.5)
+    acc = {"source_aware_init": 1, "source_aware_scale": 0.5}
+    o = pyoracle.Oracle(SHAPE, oracle_params(p), f, tol=1e-3, accel=acc)
+    for step in range(3):
+        assert g.step(1)[0]["iterations"] == o.step()["sweeps"], step
     of, gf = o.fields(), g.download_fields()
     for k in L.FIELDS:
         assert rel_err(gf[k], of[k]) <= 1e-10, k
