@@ -42,3 +42,25 @@ def test_revolve_bounds(n, c):
 def test_schedule_rejects_bad_arguments():
     with pytest.raises(L.LBMError):
         L.adjoint_schedule(0, 3)
+
+
+def fewest_recomputations(n, c):
+    """Exhaustive search over every split of the recursive schedule (the
+    fewest forward steps it can recompute)."""
+    import functools
+
+    @functools.lru_cache(maxsize=None)
+    def best(l, k):
+        if l == 1:
+            return 1
+        if k == 0:
+            return l * (l + 1) // 2
+        return min(l1 + best(l - l1, k - 1) + best(l1, k) for l1 in range(1, l))
+    return best(n, c)
+
+
+@pytest.mark.parametrize("n,c", [(20, 1), (60, 2), (100, 3), (120, 5), (150, 10)])
+def test_schedule_is_near_the_fewest_recomputations(n, c):
+    got = L.adjoint_schedule(n, c)["recompute_steps"]
+    want = fewest_recomputations(n, c)
+    assert want <= got <= 1.05 * want, (got, want)
