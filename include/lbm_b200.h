@@ -249,9 +249,14 @@ lbm_status lbm_get_poisson(const lbm_handle* h, lbm_poisson_cfg* cfg);
  * lap p = (sum_nb p - 14 p)/5 solved for lap p = source_scale rho s, with the
  * same gauge and relative-change exit; its result differs from the kinetic
  * form's (another equation).  LBM_POISSON_SCALAR_JACOBI sweeps as the
- * reference does (Jacobi); LBM_POISSON_SCALAR_RB solves the same equation by
- * red-black SOR (its right-hand side's mean removed, which the gauge makes
- * immaterial), reaching the Jacobi sweeps' fixed point in far fewer sweeps.
+ * kernel of the reference's option states (its own loop overwrites p from
+ * the unchanged h after every sweep, GPU/InamuroCUDA.cu:2307-2329, so its
+ * option leaves p at its start value); LBM_POISSON_SCALAR_RB solves the same
+ * equation by red-black SOR with the right-hand side's constant and
+ * checkerboard components removed (the components the Jacobi sweeps never
+ * take up at their even check counts; projected with weight 1/2 on the
+ * slip-wall planes), reaching the Jacobi sweeps' gauged limit in far fewer
+ * sweeps.
  * Scalar forms: FP64 only, no dual residual; red-black needs even ly, lz
  * (and lx with periodic_x).  source_scale: the reference's
  * --scalar-source-scale (default 2.0); omega: SOR relaxation in (0, 2), 0 =
@@ -269,7 +274,8 @@ typedef enum {
                                     the kinetic map).  Same fixed point as the kinetic form; FP64,
                                     periodic x only (with the slip walls' overwrite the singular
                                     system is inconsistent), no dual residual, no two-grid or
-                                    spatial diagnostics */
+                                    spatial diagnostics, no lbm_step_replay (it has no sweep count
+                                    to replay) */
 } lbm_poisson_form;
 lbm_status lbm_set_poisson_form(lbm_handle* h, lbm_poisson_form form, double source_scale, double omega);
 /* Current form, source scale and the relaxation in use (the computed optimum
