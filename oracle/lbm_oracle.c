@@ -656,6 +656,20 @@ static int poisson(orc_state* s, uint64_t replay, orc_step_info* info)
                 if (st != ORC_OK) return st;
                 fp_ok = info->fp_rel < P->tol;
             }
+            /* two-grid correction (GPU/InamuroCUDA.cu:1198-1255, 1284-1328,
+               2149-2156): 4^3 block sums of the change before p_prev moves */
+            const int bs = 4, bxn = (P->lx + bs - 1) / bs, byn = (P->ly + bs - 1) / bs, bzn = (P->lz + bs - 1) / bs;
+            double* bsum = NULL;
+            if (P->two_grid) {
+                bsum = (double*)calloc((size_t)bxn * byn * bzn, sizeof(double));
+                if (!bsum) return ORC_ERR_OOM;
+                for (int z = 0; z < P->lz; ++z)
+                    for (int y = 0; y < P->ly; ++y)
+                        for (int x = 0; x < P->lx; ++x) {
+                            const long c = idx(s, x, y, z);
+                            bsum[((z / bs) * byn + y / bs) * bxn + x / bs] += s->p[c] - s->p_prev[c];
+                        }
+            }
             /* getError: CPU/Inamuro.cpp:726-753 */
             double err1 = 0.0, err2 = 0.0;
             for (int x = 0; x < P->lx; ++x)
@@ -672,6 +686,23 @@ static int poisson(orc_state* s, uint64_t replay, orc_step_info* info)
             info->pressure_l1_norm = err2;
             info->relative_error = error;
             converged = (error < P->tol) && fp_ok;
+            if (bsum && !converged && err1 > 0.0) {
+                for (int z = 0; z < P->lz; ++z)
+                    for (int y = 0; y < P->ly; ++y)
+                        for (int x = 0; x < P->lx; ++x) {
+                            const int bx = x / bs, by = y / bs, bz = z / bs;
+                            const int x1 = (bx + 1) * bs < P->lx ? (bx + 1) * bs : P->lx;
+                            const int y1 = (by + 1) * bs < P->ly ? (by + 1) * bs : P->ly;
+                            const int z1 = (bz + 1) * bs < P->lz ? (bz + 1) * bs : P->lz;
+                            const int cells = (x1 - bx * bs) * (y1 - by * bs) * (z1 - bz * bs);
+                            const double corr = P->two_grid_strength * bsum[(bz * byn + by) * bxn + bx] / (double)cells;
+                            const long c = idx(s, x, y, z);
+                            s->p[c] += corr;
+                            s->p_prev[c] = s->p[c];
+                            for (int q = 0; q < Q; ++q) s->h[(long)q * N + c] += EI[q] * corr;
+                        }
+            }
+            free(bsum);
         }
         if (replay) {
             if (iter == replay) break;

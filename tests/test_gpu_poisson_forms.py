@@ -97,12 +97,17 @@ def test_onepass_matches_oracle(periodic, accel):
         assert rel_err(gf[k], of[k]) <= tol, k
 
 
-def test_kinetic_source_aware_init_matches_oracle():
-    p, f = case(False)
+@pytest.mark.parametrize("periodic", [False, True])
+@pytest.mark.parametrize("acc", [{"source_aware_init": 1, "source_aware_scale": 0.5}, {"two_grid": 1}],
+                         ids=["source", "twogrid"])
+def test_kinetic_accelerators_match_oracle(periodic, acc):
+    """Source-aware init and two-grid correction on the kinetic form against
+    the oracle (the correction adds E_q c to the next sweep's post-collision
+    h here and to the pre-collision h there: equal up to rounding)."""
+    p, f = case(periodic)
     g = gpu_box(p, f, "kinetic", 1e-3)
-    g.set_poisson_accel(source_aware_init=1, source_aware_scale=0.5)
-    acc = {"source_aware_init": 1, "source_aware_scale": 0.5}
-    o = pyoracle.Oracle(SHAPE, oracle_params(p), f, tol=1e-3, accel=acc)
+    g.set_poisson_accel(**acc)
+    o = pyoracle.Oracle(SHAPE, oracle_params(p), f, tol=1e-3, periodic_x=periodic, accel=acc)
     for step in range(3):
         assert g.step(1)[0]["iterations"] == o.step()["sweeps"], step
     of, gf = o.fields(), g.download_fields()
