@@ -54,17 +54,70 @@ COMPULSORY_BYTES = {"fp64": 256.0, "mixed": 128.0}
 PHASE_BYTES = {"collide_ms": {"fp64": 528.0, "mixed": 264.0},
                "moments_ms": {"fp64": 280.0, "mixed": 140.0},
                "correct_ms": {"fp64": 64.0, "mixed": 36.0}}
-# Mean sweeps per step of this workload (measured on B200 with this bench);
-# the CPU sample is extrapolated to it when no GPU run preceded it.
-DEFAULT_SWEEPS_PER_STEP = 1000.0
+# Mean sweeps per step of the 256^3 head-on workload, FP64, steps 6-25 of the
+# default run (measured on B200 with this bench: 3655); the reference arm's
+# CPU sample is extrapolated to it (the reference needs ~2.3 s per sweep on
+# one core, so a full step of ~3655 sweeps is not run).
+DEFAULT_SWEEPS_PER_STEP = 3655.0
+# The head-on workload as the reference's own params.in (GPU-tree grammar,
+# GPU/Inamuro.cpp:24-115): 14 positional entries, then the initial-condition
+# keys.  Written from constants so that the reference arm needs nothing of
+# this repository's library.
+WORKLOAD = {"rho_L": 100.0, "rho_G": 1.0, "tauf": 1.0, "taug": 1.0, "mu_L": 10.0, "mu_G": 0.1,
+            "k_f": 0.06, "k_g": 6e-6, "T": 0.035, "a": 1.0, "b": 6.7, "fei_max": 0.09714,
+            "fei_min": 0.01134, "fei_L": 0.092, "fei_G": 0.015, "DD": 64.0}
 
 
 def workload_params(n=N_SIDE):
     import lbm_b200 as L
-    return L.make_params(lx=n, ly=n, lz=n, rho_L=100.0, rho_G=1.0, mu_L=10.0, mu_G=0.1, tauf=1.0,
-                         taug=1.0, k_f=0.06, k_g=6e-6, T=0.035, a=1.0, b=6.7, DD=64.0,
-                         init_single_droplet=0, init_tanh=1, interface_width=2.0,
-                         init_velocity=0.02, init_center_x=n / 2.0, init_separation=48.0)
+    w = WORKLOAD
+    p = L.make_params(lx=n, ly=n, lz=n, rho_L=w["rho_L"], rho_G=w["rho_G"], mu_L=w["mu_L"], mu_G=w["mu_G"],
+                      tauf=w["tauf"], taug=w["taug"], k_f=w["k_f"], k_g=w["k_g"], T=w["T"], a=w["a"], b=w["b"],
+                      DD=w["DD"], init_single_droplet=0, init_tanh=1, interface_width=2.0,
+                      init_velocity=0.02, init_center_x=n / 2.0, init_separation=48.0)
+    assert (p.fei_max, p.fei_min, p.fei_L, p.fei_G) == (w["fei_max"], w["fei_min"], w["fei_L"], w["fei_G"])
+    return p
+
+
+def workload_params_text(n=N_SIDE, init_keys=True):
+    """The head-on workload as a params.in of the reference (positional
+    entries of CPU/Inamuro.cpp:38-53; with init_keys the GPU tree's
+    initial-condition tokens, GPU/Inamuro.cpp:56-103)."""
+    w = WORKLOAD
+    text = (f"{n} {n} {n}\n1\n20\n20\n{w['rho_L']!r} {w['rho_G']!r}\n{w['tauf']!r} {w['taug']!r}\n"
+            f"{w['mu_L']!r} {w['mu_G']!r}\n{w['k_f']!r} {w['k_g']!r}\n{w['T']!r}\n{w['a']!r}\n{w['b']!r}\n"
+            f"{w['fei_max']!r} {w['fei_min']!r}\n{w['fei_L']!r} {w['fei_G']!r}\n{w['DD']!r}\n")
+    if init_keys:
+        text += (f"init_mode=two_droplets init_profile=tanh init_velocity=0.02 interface_width=2.0 "
+                 f"init_center_x={n / 2.0!r} init_separation=48.0\n")
+    return text
+
+
+def reference_inputs(n, tmp, seed=1234):
+    """Inputs of the reference arm without this repository's library: the
+    reference's own GPU-tree initial condition (oracle/_ref/ref_init_harness,
+    GPU/Inamuro.cpp:491-566 compiled from its sources) plus the workload's
+    seeded phi noise.  Returns (params path, init path)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_init_harness")
+    if not os.path.exists(exe):
+        raise FileNotFoundError("reference init harness not built (oracle/_ref missing)")
+    gpf = os.path.join(tmp, "params_gpu_tree.in")
+    with open(gpf, "w") as fh:
+        fh.write(workload_params_text(n, init_keys=True))
+    pf = os.path.join(tmp, "params.in")
+    with open(pf, "w") as fh:
+        fh.write(workload_params_text(n, init_keys=False))
+    raw = os.path.join(tmp, "ref_init.bin")
+    r = subprocess.run([exe, gpf, raw], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"reference init harness failed: {r.stderr[-300:]}")
+    cells = n * n * n
+    fields = np.fromfile(raw, dtype=np.float64, count=6 * cells).reshape(6, n, n, n)
+    rng = np.random.default_rng(seed)
+    fields[0] += rng.uniform(-1e-4, 1e-4, size=(n, n, n))
+    ib = os.path.join(tmp, "init.bin")
+    fields.tofile(ib)
+    return pf, ib
 
 
 def workload_fields(p, seed=1234):
@@ -113,6 +166,46 @@ def batch_workload(n_instances=64, seed=2024, noise=1e-4):
         params.append(p)
         fields.append({"phi": phi, "rho": rho, "u": zero, "v": zero, "w": zero, "p": zero})
     return params, fields
+
+
+def coalescence_workload(n=256, R=28.0, side=60.0, speed=0.01, ratio=1000.0, kf=0.06, seed=4242, noise=1e-4):
+    """Three-droplet coalescence: an n^3 periodic box, three drops of radius R
+    centred on an equilateral triangle of side `side` in the plane z = n/2
+    (centroid at the box centre), each moving towards the centroid at
+    `speed`; rho_L/rho_G = ratio (rho_G = 1), mu = 0.1 rho, kappa_f = kf,
+    otherwise the Laplace-test physics (a = 1, b = 6.7, T = 0.035,
+    kappa_g = 6e-6, tau = 1, tanh interfaces W = 4, seeded phi noise).  Each
+    drop's profile is phi = phi_min + (phi_max - phi_min) * 0.5 (1 - tanh(2 (r
+    - R) / W)); where profiles overlap the largest is kept, and the velocity is
+    that of the drop whose profile is kept, scaled by it.  Built here: the
+    reference's initializer makes one or two drops on the z axis.  Returns
+    (params, fields)."""
+    import lbm_b200 as L
+    p = L.make_params(lx=n, ly=n, lz=n, rho_L=ratio, rho_G=1.0, mu_L=0.1 * ratio, mu_G=0.1, tauf=1.0, taug=1.0,
+                      k_f=kf, k_g=6e-6, T=0.035, a=1.0, b=6.7, DD=2.0 * R, init_single_droplet=1, init_tanh=1,
+                      interface_width=2.0, init_velocity=0.0, periodic_x=1)
+    c = (n - 1) / 2.0
+    rc = side / np.sqrt(3.0)             # centroid-to-vertex distance
+    centres = [(c + rc * np.cos(a), c + rc * np.sin(a), c) for a in (np.pi / 2, np.pi / 2 + 2 * np.pi / 3,
+                                                                        np.pi / 2 + 4 * np.pi / 3)]
+    z, y, x = np.meshgrid(np.arange(n, dtype=np.float64), np.arange(n, dtype=np.float64),
+                          np.arange(n, dtype=np.float64), indexing="ij")
+    frac = np.zeros((n, n, n))
+    u = np.zeros((n, n, n))
+    v = np.zeros((n, n, n))
+    for cx_, cy_, cz_ in centres:
+        r = np.sqrt((x - cx_) ** 2 + (y - cy_) ** 2 + (z - cz_) ** 2)
+        fr = 0.5 * (1.0 - np.tanh(2.0 * (r - R) / 4.0))
+        take = fr > frac
+        dx, dy = c - cx_, c - cy_
+        norm = np.hypot(dx, dy)
+        u = np.where(take, speed * dx / norm * fr, u)
+        v = np.where(take, speed * dy / norm * fr, v)
+        frac = np.maximum(frac, fr)
+    rng = np.random.default_rng(seed)
+    phi = p.fei_min + frac * (p.fei_max - p.fei_min) + rng.uniform(-noise, noise, size=frac.shape)
+    rho = p.rho_G + frac * (p.rho_L - p.rho_G)
+    return p, {"phi": phi, "rho": rho, "u": u, "v": v, "w": np.zeros_like(phi), "p": np.zeros_like(phi)}
 
 
 def adjoint_workload(n=64, e=0.0, kf_scale=1.0, seed=31, noise=1e-4):
@@ -201,29 +294,25 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- CPU sample
-def reference_cpu_samples(n, sample_sweeps=1, reps=1):
+def reference_cpu_samples(n, sample_sweeps=3, reps=1, nonpoisson_reps=None):
     """Runs the reference CPU solver (oracle/_ref/ref_cpu_harness, built from
-    the unmodified reference sources) on the n^3 workload: `reps` times one
-    non-Poisson step part + `sample_sweeps` kinetic sweeps.  Returns
-    ([(seconds_nonpoisson, seconds_per_sweep), ...], cells, wall_s) or raises."""
+    the unmodified reference sources) on the n^3 workload, inputs from the
+    reference's own initial condition (reference_inputs): `reps` times
+    `sample_sweeps` kinetic sweeps, the first `nonpoisson_reps` (default all)
+    preceded by one non-Poisson step part.  Returns
+    ([(seconds_nonpoisson or None, seconds_per_sweep), ...], cells, wall_s)
+    or raises."""
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_cpu_harness")
     if not os.path.exists(exe):
         raise FileNotFoundError("reference harness not built (oracle/_ref missing)")
-    import lbm_b200 as L
-    p = workload_params(n)
-    f = workload_fields(p)
     with tempfile.TemporaryDirectory() as tmp:
-        pf = os.path.join(tmp, "params.in")
-        with open(pf, "w") as fh:
-            fh.write(f"{n} {n} {n}\n1\n20\n20\n{p.rho_L!r} {p.rho_G!r}\n{p.tauf!r} {p.taug!r}\n"
-                     f"{p.mu_L!r} {p.mu_G!r}\n{p.k_f!r} {p.k_g!r}\n{p.T!r}\n{p.a!r}\n{p.b!r}\n"
-                     f"{p.fei_max!r} {p.fei_min!r}\n{p.fei_L!r} {p.fei_G!r}\n{p.DD!r}\n")
-        ib = os.path.join(tmp, "init.bin")
-        np.concatenate([f[k].ravel() for k in L.FIELDS]).tofile(ib)
-        del f
+        pf, ib = reference_inputs(n, tmp)
+        cmd = [exe, "--params", pf, "--sample-sweeps", str(sample_sweeps), "--out", tmp, "--init", ib,
+               "--sample-reps", str(reps)]
+        if nonpoisson_reps is not None:
+            cmd += ["--nonpoisson-reps", str(nonpoisson_reps)]
         t0 = time.perf_counter()
-        r = subprocess.run([exe, "--params", pf, "--sample-sweeps", str(sample_sweeps), "--out", tmp,
-                            "--init", ib, "--sample-reps", str(reps)], capture_output=True, text=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
         wall = time.perf_counter() - t0
         if r.returncode != 0:
             raise RuntimeError(f"reference harness failed: {r.stderr[-300:]}")
@@ -233,7 +322,8 @@ def reference_cpu_samples(n, sample_sweeps=1, reps=1):
             if parts[0] == "cells":
                 cells = float(parts[1])
             elif parts[0] == "rep":
-                reps_out.append((float(parts[2]) / 1e3, float(parts[3]) / 1e3 / max(sample_sweeps, 1)))
+                t_np = float(parts[2]) / 1e3
+                reps_out.append((t_np if t_np >= 0 else None, float(parts[3]) / 1e3 / max(sample_sweeps, 1)))
     return reps_out, cells, wall
 
 
@@ -243,15 +333,78 @@ def cpu_value(cells, t_np, t_sw, sweeps_per_step):
 
 
 def cpu_baseline_entry(n, reps_out, cells, wall, sweeps_per_step, sample_sweeps, value=None):
-    t_np = statistics.median(r[0] for r in reps_out)
+    nps = [r[0] for r in reps_out if r[0] is not None]
+    t_np = statistics.median(nps)
     t_sw = statistics.median(r[1] for r in reps_out)
     v = cpu_value(cells, t_np, t_sw, sweeps_per_step) if value is None else value
     sample = (f"reference CPU solver (CPU/Inamuro.cpp, g++ -O3, single-threaded) on the {n}^3 "
-              f"workload, {len(reps_out)} rep(s) of 1 non-Poisson step part ({t_np:.2f} s) + "
-              f"{sample_sweeps} kinetic sweep(s) ({t_sw:.2f} s each), extrapolated to "
-              f"{sweeps_per_step:.0f} sweeps/step; harness wall {wall:.1f} s incl. setup")
+              f"workload (inputs from the reference's own init + seeded noise), {len(reps_out)} rep(s) of "
+              f"{sample_sweeps} kinetic sweeps ({t_sw:.2f} s each) and {len(nps)} non-Poisson step part(s) "
+              f"({t_np:.2f} s), extrapolated to {sweeps_per_step:.0f} sweeps/step (B200 FP64 measurement of "
+              f"this workload); harness wall {wall:.1f} s incl. setup")
     return {"value": v, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample,
-            "seconds_per_sweep": t_sw, "seconds_nonpoisson": t_np}
+            "seconds_per_sweep": t_sw, "seconds_nonpoisson": t_np, "extrapolated": True,
+            "sweeps_per_step_extrapolated_to": sweeps_per_step, "sweeps_timed_per_rep": sample_sweeps}
+
+
+# ---------------------------------------------------------------- reference GPU
+def _program_run(exe, d, pf, steps, limit, timeout):
+    """One run of a GPU/main.cpp front end (the reference's own program or the
+    same main.cpp over this library): wall ms of its step loop (its
+    wall_total_ms) and the sweeps of each step (its Poisson CSV)."""
+    os.makedirs(d)
+    cmd = [exe, "--mode", "gpu", "--params", pf, "--steps", str(steps), "--poisson", "split",
+           "--poisson-check-interval", "100", "--poisson-tolerance", "1e-3",
+           "--poisson-iteration-limit", str(limit), "--poisson-diagnostics", "diag.csv", "--no-roofline"]
+    r = subprocess.run(cmd, cwd=d, capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError(f"{os.path.basename(exe)} exited {r.returncode}: {(r.stdout + r.stderr)[-300:]}")
+    ms = None
+    for tok in r.stdout.split():
+        if tok.startswith("wall_total_ms="):
+            ms = float(tok.split("=", 1)[1])
+    if ms is None:
+        raise RuntimeError(f"{os.path.basename(exe)}: no wall_total_ms in its output")
+    import csv
+    sweeps = {}
+    for row in csv.DictReader(open(os.path.join(d, "diag.csv"))):
+        s = int(row["step"])
+        sweeps[s] = max(sweeps.get(s, 0), int(row["iteration"]))
+    return ms, [sweeps[s] for s in sorted(sweeps)]
+
+
+def reference_gpu_leg(n=N_SIDE, steps=3, limit=3000, timeout=900):
+    """The reference's own FP64 GPU step (GPU/InamuroCUDA.cu, compiled from its
+    unmodified sources for sm_100a: oracle/_ref/lbm_gpu_ref) beside this
+    library behind the same front end (the reference's GPU/main.cpp over
+    include/InamuroCUDA.hpp: oracle/_ref/lbm_gpu_dropin), on the same
+    noise-free head-on params.in (the reference's own initial condition), the
+    split kinetic Poisson form, check 100, tolerance 1e-3.  The first steps of
+    this workload need ~40-50 thousand sweeps; both programs run `steps` steps
+    with the reference's poisson_iteration_limit at `limit` sweeps (the same
+    sweeps in both, the step finished unconverged at the limit), so the
+    comparison is bounded.  Host wall clock of each program's step loop.
+    MLUPS with sweeps counted = cells (steps + sweeps) / wall."""
+    ref = os.path.join(ROOT, "oracle", "_ref", "lbm_gpu_ref")
+    ours = os.path.join(ROOT, "oracle", "_ref", "lbm_gpu_dropin")
+    missing = [os.path.basename(x) for x in (ref, ours) if not os.path.exists(x)]
+    if missing:
+        return {"unavailable": "not built: " + ", ".join(missing)}
+    cells = float(n) ** 3
+    out = {"box": [n, n, n], "steps": steps, "poisson_iteration_limit": limit,
+           "config": "head-on 256^3 params.in without noise, --poisson split, check 100, tolerance 1e-3"}
+    with tempfile.TemporaryDirectory() as tmp:
+        pf = os.path.join(tmp, "params.in")
+        with open(pf, "w") as fh:
+            fh.write(workload_params_text(n, init_keys=True))
+        for name, exe in (("reference", ref), ("ours", ours)):
+            ms, sw = _program_run(exe, os.path.join(tmp, name), pf, steps, limit, timeout)
+            out[name] = {"wall_ms": ms, "sweeps_per_step": sw,
+                         "mlups": cells * (steps + sum(sw)) / (ms / 1e3) / 1e6,
+                         "mlups_reference_definition": cells * steps / (ms / 1e3) / 1e6}
+    out["sweeps_equal"] = out["reference"]["sweeps_per_step"] == out["ours"]["sweeps_per_step"]
+    out["ratio"] = out["ours"]["mlups"] / out["reference"]["mlups"]
+    return out
 
 
 # ---------------------------------------------------------------- helpers
@@ -328,20 +481,26 @@ def run_reference_arm(args):
         return 0
     n = args.size
     try:
-        reps_out, cells, wall = reference_cpu_samples(n, args.sample_sweeps, args.warmup + args.steps)
+        # the non-Poisson part (~11 s on one core) is timed in the first two
+        # reps only, so the W + K reps of sweeps fit a few minutes
+        reps_out, cells, wall = reference_cpu_samples(n, args.sample_sweeps, args.warmup + args.steps,
+                                                      nonpoisson_reps=2)
     except Exception as e:  # harness missing or failed: report, do not crash the driver
         print(json.dumps({"impl": "reference", "unavailable": str(e)[:200]}))
         return 0
+    t_np = statistics.median(r[0] for r in reps_out if r[0] is not None)
     timed = reps_out[args.warmup:] or reps_out
-    vals = [cpu_value(cells, t_np, t_sw, args.sweeps_per_step) for t_np, t_sw in timed]
+    vals = [cpu_value(cells, t_np, t_sw, args.sweeps_per_step) for _, t_sw in timed]
     value = statistics.median(vals)
-    step_s = statistics.median(t_np + args.sweeps_per_step * t_sw for t_np, t_sw in timed)
+    step_s = statistics.median(t_np + args.sweeps_per_step * t_sw for _, t_sw in timed)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": config_dict(n, "fp64"), "impl": "reference",
-            "cpu_baseline": cpu_baseline_entry(n, timed, cells, wall, args.sweeps_per_step,
+            "cpu_baseline": cpu_baseline_entry(n, reps_out, cells, wall, args.sweeps_per_step,
                                                args.sample_sweeps, value=value),
+            "timing": "ms_per_step is extrapolated: per rep, sample_sweeps sweeps are timed and a step is "
+                      "t_nonpoisson + sweeps_per_step x t_sweep (not run in full: ~2.3 s per sweep)",
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -472,10 +631,18 @@ def accuracy_probe(n, steps, sweeps):
 
 
 def run_batch(args):
+    print(json.dumps(batch_measure(args)))
+    return 0
+
+
+def batch_measure(args):
     """The batched droplet oscillation (64 uneven periodic boxes, mixed
     precision): autotune the batched kernels, W warm-up steps, K timed steps
     (natural Poisson exits per instance), device time from the batch's CUDA
-    events.  MLUPS with sweeps counted = sum_i cells_i (steps + sweeps_i) / t."""
+    events.  MLUPS with sweeps counted = sum_i cells_i (steps + sweeps_i) / t.
+    Roofline: the sweep-equivalent bytes (144 B per cell and sweep) and the
+    bytes the launches must move (128 B for a single sweep, 64 B per sweep in
+    a two-sweep pass) over the Poisson device time."""
     import lbm_b200 as L
     params, fields = batch_workload(args.batch_instances, seed=args.batch_seed)
     cells = [p.lx * p.ly * p.lz for p in params]
@@ -500,6 +667,9 @@ def run_batch(args):
     value = updates / (dev_ms / 1e3) / 1e6
     peak, kind = measured_peaks()
     sweep_gbs = SWEEP_BYTES["mixed"] * swept / (t["poisson_ms"] / 1e3) / 1e9
+    fused = t["fused_sweeps"] / max(t["sweep_kernels"], 1)
+    compulsory = COMPULSORY_BYTES["mixed"] * (1.0 - 0.5 * fused)
+    comp_gbs = compulsory * swept / (t["poisson_ms"] / 1e3) / 1e9
     line = {"metric": "MLUPS (Poisson sweeps counted) of the batched droplet oscillation", "value": value,
             "unit": "MLUPS", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -517,16 +687,23 @@ def run_batch(args):
             "roofline": {"bound": "hbm", "kernel": "batched sweep (mixed)", "achieved": sweep_gbs, "peak": peak,
                          "unit": "GB/s", "frac": sweep_gbs / peak, "peak_kind": kind,
                          "bytes_per_cell": SWEEP_BYTES["mixed"],
+                         "fraction_of_sweeps_in_two_sweep_passes": fused,
+                         "compulsory_bytes_per_cell_per_sweep": compulsory, "frac_compulsory": comp_gbs / peak,
                          "note": "sweep-equivalent bytes of the instances' own sweeps over the Poisson device "
-                                 "time, checks and finalisations included"},
+                                 "time, checks and finalisations included; frac_compulsory against what the "
+                                 "launches must move"},
             "gpu_launches": t["kernel_launches"], "clocks": clocks, "wall_s": wall,
             "converged": all(st["converged"] for st in stats[-1])}
-    print(json.dumps(line))
     b.close()
-    return 0
+    return line
 
 
 def run_adjoint(args):
+    print(json.dumps(adjoint_measure(args)))
+    return 0
+
+
+def adjoint_measure(args):
     """Adjoint calibration (FP64, periodic n^3, bounded sample of the
     2000-step run): J = 0.5 sum (phi_T - phi_target)^2, phi_target the final
     phi of a run from an ellipsoidal drop (e = 0.2) with kappa_f + 5 %.  W
@@ -610,9 +787,8 @@ def run_adjoint(args):
             "sweeps_per_step": {"forward": st["forward_sweeps"] / K, "adjoint": st["adjoint_sweeps"] / K},
             "objective": J, "gradient_checks": checks,
             "max_rel_err": max(c["rel_err"] for c in checks), "clocks": clocks}
-    print(json.dumps(line))
     a.close()
-    return 0
+    return line
 
 
 def run_poisson_forms(args):
@@ -760,11 +936,43 @@ def run_ours(args):
                     line["mixed"]["accuracy"] = accuracy_probe(n, 3, 1000)
                 except Exception as e:
                     line["mixed"]["accuracy"] = {"unavailable": str(e)[:200]}
+        if world == 1 and not args.no_extras:
+            extra_legs(args, line)
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0
+
+
+def extra_legs(args, line):
+    """Bounded samples of the other measurements, in the default line: the
+    reference's own GPU step beside this library's (reference_gpu), the
+    adjoint calibration run with its adjoint/forward cost and finite-difference
+    checks (adjoint), and the batched droplet oscillation (batch)."""
+    import copy
+    try:
+        line["reference_gpu"] = reference_gpu_leg(args.size)
+    except Exception as e:
+        line["reference_gpu"] = {"unavailable": str(e)[:300]}
+    try:
+        a = copy.copy(args)
+        a.steps, a.warmup, a.adjoint_krylov = 2, 1, True
+        r = adjoint_measure(a)
+        line["adjoint"] = {k: r[k] for k in ("value", "unit", "steps", "forward_mlups", "reverse_mlups",
+                                             "adjoint_forward_time_ratio", "forward_ms", "backward_ms",
+                                             "sweeps_per_step", "gradient_checks", "max_rel_err", "config")}
+        line["adjoint"]["sample"] = "2 of the 2000 steps of the 64^3 calibration run, BiCGSTAB adjoint solve"
+    except Exception as e:
+        line["adjoint"] = {"unavailable": str(e)[:300]}
+    try:
+        b = copy.copy(args)
+        b.steps, b.warmup = 2, 1
+        r = batch_measure(b)
+        line["batch"] = {k: r[k] for k in ("value", "unit", "steps", "ms_per_step", "sweeps_per_step_mean",
+                                           "roofline", "tuning", "gpu_launches", "converged", "config")}
+    except Exception as e:
+        line["batch"] = {"unavailable": str(e)[:300]}
 
 
 def run_phase_timing(args):
@@ -813,7 +1021,9 @@ def main(argv=None):
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the mixed-vs-FP64 error and mass-drift probe")
-    ap.add_argument("--sample-sweeps", type=int, default=1)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the reference-GPU, adjoint and batch samples of the default line")
+    ap.add_argument("--sample-sweeps", type=int, default=3)
     ap.add_argument("--sweeps-per-step", type=float, default=DEFAULT_SWEEPS_PER_STEP)
     ap.add_argument("--phase-timing", action="store_true",
                     help="time the non-Poisson kernels per step with --phase-sweeps sweeps per step")

@@ -268,14 +268,29 @@ typedef enum {
     LBM_POISSON_ONEPASS = 3,     /* the reference's one-pass form (setUseOnePassPoisson,
                                     GPU/InamuroCUDA.cu:780-844): the kinetic map on the
                                     pre-collision h with the accelerators of lbm_poisson_accel */
-    LBM_POISSON_KRYLOV = 4       /* not a reference form: the kinetic form's fixed point solved by
+    LBM_POISSON_KRYLOV = 4,      /* not a reference form: the kinetic form's fixed point solved by
                                     BiCGSTAB, stopping at ||b - (I - K) h|| < tolerance ||b|| (the
                                     lbm_poisson_cfg tolerance; max_sweeps caps the applications of
                                     the kinetic map).  Same fixed point as the kinetic form; FP64,
                                     periodic x only (with the slip walls' overwrite the singular
                                     system is inconsistent), no dual residual, no two-grid or
                                     spatial diagnostics, no lbm_step_replay (it has no sweep count
-                                    to replay) */
+                                    to replay).  A NaN/Inf source or start iterate returns
+                                    LBM_ERR_NONFINITE; five restarts in a row that do not lower
+                                    the true residual (a tolerance below the rounding floor)
+                                    stop the solve with LBM_ERR_POISSON_BUDGET */
+    LBM_POISSON_VARCOEF_RB = 5   /* not a reference form: div((1/rho) grad p) = s, the continuum
+                                    limit of the kinetic form (diffusivity 1/(3 rho), source
+                                    -s/3), on the D3Q15 neighbours with arithmetic face means
+                                    of 1/rho (x mirrored at the slip walls), solved by red-black
+                                    SOR (omega as for LBM_POISSON_SCALAR_RB).  Each check gauges
+                                    p, takes the relative change and the operator residual
+                                    ||A p - s|| / max(||s||, ||A p||) (reported in the
+                                    fixed-point fields of lbm_step_stats); the exit needs both
+                                    below the tolerance.  Another discretisation than the
+                                    kinetic form's: its p differs at the interface.  FP64, even
+                                    ly, lz (and lx with periodic_x), no lbm_poisson_cfg dual
+                                    residual, no accelerators */
 } lbm_poisson_form;
 lbm_status lbm_set_poisson_form(lbm_handle* h, lbm_poisson_form form, double source_scale, double omega);
 /* Current form, source scale and the relaxation in use (the computed optimum
@@ -366,8 +381,11 @@ lbm_status lbm_diagnostics_snapshot(lbm_handle* h, lbm_diagnostics* out);
  *     start at zero (each block writes its own slot before the final pass reads
  *     it).  Calls whose GPU work overlaps (other threads or streams) race on
  *     it: serialise them.
- *   - The first call on each device looks up the array's device address with
- *     that device current; make that first call before any stream capture.
+ *   - Every call looks up the array's device address with the calling
+ *     thread's current device (the lookup allocates nothing), so a device
+ *     reset between calls is followed.  The first call on a device may also
+ *     load the library's device code there (CUDA's lazy module loading);
+ *     make that first call before any stream capture.
  *   - Returns LBM_ERR_BAD_ARG for a null pointer, n_cells == 0 or
  *     n_cells > LBM_NOALLOC_MAX_CELLS, LBM_ERR_CUDA on a CUDA failure. */
 lbm_status lbm_field_statistics_noalloc(const double* field, uint64_t n_cells, void* stream,
@@ -527,7 +545,9 @@ typedef struct {
     int krylov;                /* 1: solve each step's adjoint Poisson problem by BiCGSTAB (the
                                   transposed kinetic operator, as LBM_POISSON_KRYLOV does forward)
                                   to a relative residual of krylov_tolerance, instead of the
-                                  transposed sweeps and their check of tolerance */
+                                  transposed sweeps and their check of tolerance; a NaN/Inf
+                                  adjoint right-hand side returns LBM_ERR_NONFINITE, restarts
+                                  without progress LBM_ERR_POISSON_BUDGET as in the forward form */
     double krylov_tolerance;   /* 0: 1e-10 */
 } lbm_adjoint_cfg;
 

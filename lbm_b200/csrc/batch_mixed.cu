@@ -60,6 +60,7 @@ struct BCtl {
 
 struct BPool {
     float *f[2], *g[2], *h[2];
+    double* f0;         // rest populations in FP64 (pooled like the macro fields)
     float *phi, *rho, *u, *v, *w, *div, *s, *omega;
     double *p, *p_prev, *p_chk;
 };
@@ -94,7 +95,8 @@ b_collide(const BItem* __restrict__ items, int n_items, const BInst* __restrict_
         double red[3] = {0.0, 0.0, 0.0};
         if (x < I.g.lx && y < I.g.ly)
             for (int z = w.z0; z < w.z1; ++z)
-                mixc_collide<kFirst>(I.g, I.M, fin + I.pop, fout + I.pop, gin + I.pop, gout + I.pop, B.phi + I.fld,
+                mixc_collide<kFirst>(I.g, I.M, fin + I.pop, fout + I.pop, B.f0 + I.fld, gin + I.pop, gout + I.pop,
+                                     B.phi + I.fld,
                                      B.rho + I.fld, B.u + I.fld, B.v + I.fld, B.w + I.fld, B.div + I.fld, x, y, z,
                                      red);
         item_sum<3>(red, part, n_items, it);
@@ -113,7 +115,7 @@ b_moments(const BItem* __restrict__ items, int n_items, const BInst* __restrict_
         double red[1] = {0.0};
         if (x < I.g.lx && y < I.g.ly)
             for (int z = w.z0; z < w.z1; ++z)
-                mixc_moments(I.g, I.mom, f + I.pop, gp + I.pop, B.phi + I.fld, B.rho + I.fld, B.u + I.fld,
+                mixc_moments(I.g, I.mom, f + I.pop, B.f0 + I.fld, gp + I.pop, B.phi + I.fld, B.rho + I.fld, B.u + I.fld,
                              B.v + I.fld, B.w + I.fld, x, y, z, red);
         item_sum<1>(red, part, n_items, it);
     }
@@ -320,6 +322,14 @@ __global__ void b_fill(float* __restrict__ dst, long long n, float v)
         dst[i] = v;
 }
 
+// f0 = phi - phi_G from the loaded phi (or the uniform fill when none is given).
+__global__ void b_rest_from_phi(const double* __restrict__ phi, double fill, double* __restrict__ f0, double fei_G,
+                                long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        f0[i] = (phi ? phi[i] : fill) - fei_G;
+}
+
 thread_local std::string g_batch_create_error;
 
 const char* site_message(int site)
@@ -464,7 +474,7 @@ void free_batch(lbm_batch* b)
         if (*p) cudaFree(*p);
         *p = nullptr;
     }
-    double** db[] = {&b->pool.p, &b->pool.p_prev, &b->pool.p_chk, &b->part_src, &b->part_mass, &b->part_prep,
+    double** db[] = {&b->pool.p, &b->pool.p_prev, &b->pool.p_chk, &b->pool.f0, &b->part_src, &b->part_mass, &b->part_prep,
                      &b->part_a, &b->part_b, &b->scratch};
     for (double** p : db) {
         if (*p) cudaFree(*p);
@@ -506,6 +516,9 @@ lbm_status load_instance(lbm_batch* b, int i, const double* const src[6])
         } else {
             b_fill<<<592, 256, 0, st>>>(dst[f], n, bg[f]);
         }
+        // the rest population holds phi - phi_G until the first collision
+        if (f == 0) b_rest_from_phi<<<592, 256, 0, st>>>(src[0] ? b->scratch : nullptr, p.fei_min,
+                                                         b->pool.f0 + I.fld, I.mom.fei_G, n);
     }
     if (src[5])
         BCUDA(b, cudaMemcpyAsync(b->pool.p + I.fld, src[5], n * sizeof(double), cudaMemcpyHostToDevice, st));
@@ -757,7 +770,7 @@ lbm_status lbm_batch_create(const lbm_params* params, int n_instances, int devic
         ok = okf(&b->pool.f[k], pop) && okf(&b->pool.g[k], pop) && okf(&b->pool.h[k], pop);
     ok = ok && okf(&b->pool.phi, fld) && okf(&b->pool.rho, fld) && okf(&b->pool.u, fld) && okf(&b->pool.v, fld) &&
          okf(&b->pool.w, fld) && okf(&b->pool.div, fld) && okf(&b->pool.s, fld) && okf(&b->pool.omega, fld);
-    ok = ok && okd(&b->pool.p, fld) && okd(&b->pool.p_prev, fld) && okd(&b->pool.p_chk, fld) &&
+    ok = ok && okd(&b->pool.p, fld) && okd(&b->pool.p_prev, fld) && okd(&b->pool.p_chk, fld) && okd(&b->pool.f0, fld) &&
          okd(&b->scratch, b->max_cells);
     const long long cap = b->item_capacity;
     ok = ok && okd(&b->part_src, 3 * cap) && okd(&b->part_mass, cap) && okd(&b->part_prep, 3 * cap) &&

@@ -12,7 +12,6 @@
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
-#include <mutex>
 
 #include "../../include/lbm_b200.h"
 #include "field_stats.cuh"
@@ -185,32 +184,20 @@ struct NoAllocScratch {
 // One instance per device that loads the library, reserved until exit.
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 
-// In host code `g_noalloc_scratch` names a host-side shadow, not device memory:
-// its device address is looked up once per device (with that device current)
-// and cached here.
-constexpr int kMaxDevices = 64;
-std::mutex g_noalloc_mutex;
-NoAllocScratch* g_noalloc_addr[kMaxDevices] = {};
-
 }  // namespace
 
+// In host code `g_noalloc_scratch` names a host-side shadow, not device
+// memory.  Its device address is looked up on every call, with the caller's
+// device current: the lookup allocates nothing, and a cached address would go
+// stale if the caller reset the device (a new primary context reloads the
+// module at another address).
 extern "C" lbm_status lbm_field_statistics_noalloc(const double* field, uint64_t n_cells, void* stream,
                                                    lbm_field_stats* out)
 {
     if (!field || !out || n_cells == 0 || n_cells > LBM_NOALLOC_MAX_CELLS) return LBM_ERR_BAD_ARG;
-    int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return LBM_ERR_CUDA;
-    NoAllocScratch* scratch = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-        if (!g_noalloc_addr[dev]) {
-            void* addr = nullptr;
-            if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || !addr)
-                return LBM_ERR_CUDA;
-            g_noalloc_addr[dev] = static_cast<NoAllocScratch*>(addr);
-        }
-        scratch = g_noalloc_addr[dev];
-    }
+    void* addr = nullptr;
+    if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || !addr) return LBM_ERR_CUDA;
+    NoAllocScratch* scratch = static_cast<NoAllocScratch*>(addr);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (lbm::field_stats<double>(st, field, static_cast<long long>(n_cells), scratch->partials,
                                  &scratch->result) != cudaSuccess)

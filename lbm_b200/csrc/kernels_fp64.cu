@@ -736,10 +736,84 @@ rb_sor_kernel(Geom g, double* __restrict__ p, const double* __restrict__ rho, co
     p[c] = pv + omega * (pj - pv);
 }
 
+// ---- variable-coefficient red-black form -------------------------------
+// div((1/rho) grad p) = s: the continuum limit of the kinetic scheme (its
+// diffusivity c_s^2 (tau_h - 1/2) = 1/(3 rho), its source -s/3 per sweep),
+// discretised on the D3Q15 neighbours (6 sum_q E_q (p(x + c_q) - p(x)) is the
+// isotropic laplacian, sum_q E_q c_q c_q = I/3):
+//   (A p)(x) = 6 sum_{q>=1} E_q k_q(x) (p(x + c_q) - p(x)),
+//   k_q(x) = (1/rho(x) + 1/rho(x + c_q)) / 2   (arithmetic face mean),
+// x neighbours mirrored at the slip walls as in the stencils.  A is symmetric
+// under the weights W (1/2 on the wall planes), so the right-hand side's
+// W-mean is removed (ds->rhs_mean).  Not a reference form: a scalar
+// discretisation whose fixed point differs from the kinetic scheme's at the
+// interface (the error is measured, not claimed).
+
+// sum_q a_q p(x + c_q) and sum_q a_q, a_q = 6 E_q k_q.
+__device__ __forceinline__ void varcoef_terms(const double* __restrict__ p, const double* __restrict__ rho,
+                                              const Geom& g, const Mirror& m, int x, int y, int z, double inv_rho,
+                                              double& num, double& den)
+{
+    num = 0.0;
+    den = 0.0;
+    static_for<1, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        const long long nb = cell_of(g, pick<cx(q)>(m.xm, x, m.xp), pick<cy(q)>(m.ym, y, m.yp),
+                                     pick<cz(q)>(m.zm, z, m.zp));
+        const double a = 6.0 * wE(q) * 0.5 * (inv_rho + 1.0 / __ldg(rho + nb));
+        num += a * p[nb];
+        den += a;
+    });
+}
+
+// One colour of a red-black SOR sweep of A p = s - mean_W(s), in place.
+__global__ void __launch_bounds__(256)
+rb_varcoef_kernel(Geom g, double* __restrict__ p, const double* __restrict__ rho, const double* __restrict__ s,
+                  double omega, int color, const DevState* __restrict__ ds)
+{
+    int x, y, z;
+    if (!tile_coords(g, x, y, z) || ((x + y + z) & 1) != color) return;
+    const Mirror m(g, x, y, z);
+    const long long c = cell_of(g, x, y, z);
+    double num, den;
+    varcoef_terms(p, rho, g, m, x, y, z, 1.0 / __ldg(rho + c), num, den);
+    const double rhs = __ldg(s + c) - ds->rhs_mean;
+    const double pv = p[c];
+    p[c] = pv + omega * ((num - rhs) / den - pv);
+}
+
+// Operator residual terms at a check (after the gauge: A ignores constants):
+// sum W |A p - rhs|, sum W |rhs|, sum W |A p| -- the "h" terms of the
+// fixed-point test (its "p" terms stay zero), so the check's dual exit reads
+// ||A p - rhs|| / max(||rhs||, ||A p||) < tolerance.
+__global__ void __launch_bounds__(256)
+varcoef_residual_kernel(Geom g, int zrun, const double* __restrict__ p, const double* __restrict__ rho,
+                        const double* __restrict__ s, const DevState* __restrict__ ds, double* __restrict__ part,
+                        long long nblocks)
+{
+    int x, y, z0, z1;
+    const bool active = tile_zrun(g, zrun, x, y, z0, z1);
+    double red[3] = {0.0, 0.0, 0.0};
+    const double w = (!g.periodic_x && (x == 0 || x == g.lx - 1)) ? 0.5 : 1.0;
+    for (int z = z0; active && z < z1; ++z) {
+        const Mirror m(g, x, y, z);
+        const long long c = cell_of(g, x, y, z);
+        double num, den;
+        varcoef_terms(p, rho, g, m, x, y, z, 1.0 / __ldg(rho + c), num, den);
+        const double ap = num - den * p[c];
+        const double rhs = __ldg(s + c) - ds->rhs_mean;
+        red[0] += w * fabs(ap - rhs);
+        red[1] += w * fabs(rhs);
+        red[2] += w * fabs(ap);
+    }
+    block_sum_store<3>(red, part, nblocks, block_linear());
+}
+
 // Block partial sums of w f, w chi f and w, f = scale rho s: the constant and
 // checkerboard components the red-black form removes, projected with the
 // weights w under which the mirrored stencil is symmetric (1/2 on the two
 // slip-wall planes, whose cells see their inner neighbours twice; 1 elsewhere).
+// (rho == nullptr: f = s, the variable-coefficient form's right-hand side.)
 __global__ void __launch_bounds__(256)
 scalar_rhs_sum_kernel(Geom g, int zrun, const double* __restrict__ rho, const double* __restrict__ s,
                       double scale, double* __restrict__ part, long long nblocks)
@@ -750,7 +824,7 @@ scalar_rhs_sum_kernel(Geom g, int zrun, const double* __restrict__ rho, const do
     const double w = (!g.periodic_x && (x == 0 || x == g.lx - 1)) ? 0.5 : 1.0;
     for (int z = z0; active && z < z1; ++z) {
         const long long c = cell_of(g, x, y, z);
-        const double f = w * (scale * __ldg(rho + c) * __ldg(s + c));
+        const double f = w * (rho ? scale * __ldg(rho + c) * __ldg(s + c) : __ldg(s + c));
         red[0] += f;
         red[1] += ((x + y + z) & 1) ? -f : f;
         red[2] += w;
@@ -1145,6 +1219,19 @@ void scalar_rhs_sum(cudaStream_t st, const Launch& L, const Geom& g, const doubl
                     double scale, double* part)
 {
     scalar_rhs_sum_kernel<<<L.cgrid, L.block, 0, st>>>(g, L.zrun, rho, s, scale, part, L.cnblocks);
+}
+
+void rb_varcoef(cudaStream_t st, const Launch& L, const Geom& g, double* p, const double* rho, const double* s,
+                double omega, const DevState* ds)
+{
+    rb_varcoef_kernel<<<L.grid, L.block, 0, st>>>(g, p, rho, s, omega, 0, ds);
+    rb_varcoef_kernel<<<L.grid, L.block, 0, st>>>(g, p, rho, s, omega, 1, ds);
+}
+
+void varcoef_residual(cudaStream_t st, const Launch& L, const Geom& g, const double* p, const double* rho,
+                      const double* s, const DevState* ds, double* part)
+{
+    varcoef_residual_kernel<<<L.cgrid, L.block, 0, st>>>(g, L.zrun, p, rho, s, ds, part, L.cnblocks);
 }
 
 void p_sum(cudaStream_t st, const Launch& L, const Geom& g, const double* p, double* part)

@@ -51,7 +51,7 @@ __device__ __forceinline__ bool tile_coords(const Geom& g, int& x, int& y, int& 
 template <bool kFirst>
 __global__ void __launch_bounds__(256)
 collide_kernel(Geom g, MixPhys P, const float* __restrict__ fin, float* __restrict__ fout,
-               const float* __restrict__ gin, float* __restrict__ gout,
+               double* __restrict__ f0, const float* __restrict__ gin, float* __restrict__ gout,
                const float* __restrict__ phi, const float* __restrict__ rho,
                const float* __restrict__ u, const float* __restrict__ v,
                const float* __restrict__ w, float* __restrict__ div_out,
@@ -59,7 +59,7 @@ collide_kernel(Geom g, MixPhys P, const float* __restrict__ fin, float* __restri
 {
     int x, y, z;
     double red[3] = {0.0, 0.0, 0.0};
-    if (tile_coords(g, x, y, z)) mixc_collide<kFirst>(g, P, fin, fout, gin, gout, phi, rho, u, v, w, div_out, x, y, z, red);
+    if (tile_coords(g, x, y, z)) mixc_collide<kFirst>(g, P, fin, fout, f0, gin, gout, phi, rho, u, v, w, div_out, x, y, z, red);
     block_sum_store<3>(red, part, nblocks, block_linear());
 }
 
@@ -70,7 +70,7 @@ collide_kernel(Geom g, MixPhys P, const float* __restrict__ fin, float* __restri
 template <bool kFirst>
 __global__ void __launch_bounds__(ZM_THREADS, 2)
 collide_zm_kernel(Geom g, MixPhys P, int zlen, const float* __restrict__ fin, float* __restrict__ fout,
-                  const float* __restrict__ gin, float* __restrict__ gout,
+                  double* __restrict__ f0, const float* __restrict__ gin, float* __restrict__ gout,
                   const float* __restrict__ phi, const float* __restrict__ rho,
                   const float* __restrict__ u, const float* __restrict__ v,
                   const float* __restrict__ w, float* __restrict__ div_out,
@@ -94,14 +94,15 @@ collide_zm_kernel(Geom g, MixPhys P, int zlen, const float* __restrict__ fin, fl
         // Both population sets are requested before the plane barrier, so
         // their latency overlaps the wait and the stencil arithmetic.
         float gv[Q], fv[Q];
+        const unsigned c = static_cast<unsigned>((z * g.ly + y) * g.lx + x);
+        const double f0_in = f0[c];
         if constexpr (!kFirst) {
             pull_regs32(gv, gin, n, g, x, y, z);
-            pull_regs32(fv, fin, n, g, x, y, z);
+            pull_regs32<1>(fv, fin, n, g, x, y, z);
         }
         cp_async_wait_all();
         __syncthreads();
         if (z + 2 <= z1) ring.issue(z + 2);
-        const unsigned c = static_cast<unsigned>((z * g.ly + y) * g.lx + x);
         CellDeriv<float> d;
         MixCell k;
         // g first: the phi stencil is only live for the f half.
@@ -118,19 +119,14 @@ collide_zm_kernel(Geom g, MixPhys P, int zlen, const float* __restrict__ fin, fl
         zm_derivs_f(ring, z, t, d);
         mix_cell_f(P, d, k);
         if constexpr (!kFirst) bounce_regs(fv, g, x);
-        static_for<0, Q>([&](auto qc) {
-            constexpr int q = decltype(qc)::value;
-            float in = 0.f;
-            if constexpr (!kFirst) in = fv[q];
-            fout[q * static_cast<unsigned>(n) + c] = mix_f_post<q, kFirst>(P, d, k, in);
-        });
+        store_f_post<kFirst>(P, d, k, fv, f0_in, fout, f0, static_cast<unsigned>(n), c);
     }
     block_sum_store<3>(red, part, nblocks, block_linear());
 }
 
 __global__ void __launch_bounds__(256)
 moments_kernel(Geom g, double fei_G, double fei_L, double rho_G, double rho_L, double fei_avg,
-               double dfei, double half_drho, const float* __restrict__ f,
+               double dfei, double half_drho, const float* __restrict__ f, const double* __restrict__ f0,
                const float* __restrict__ gp, float* __restrict__ phi, float* __restrict__ rho,
                float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
                double* __restrict__ part, long long nblocks)
@@ -138,7 +134,7 @@ moments_kernel(Geom g, double fei_G, double fei_L, double rho_G, double rho_L, d
     int x, y, z;
     double red[1] = {0.0};
     const MixMoments M{fei_G, fei_L, rho_G, rho_L, fei_avg, dfei, half_drho};
-    if (tile_coords(g, x, y, z)) mixc_moments(g, M, f, gp, phi, rho, u, v, w, x, y, z, red);
+    if (tile_coords(g, x, y, z)) mixc_moments(g, M, f, f0, gp, phi, rho, u, v, w, x, y, z, red);
     block_sum_store<1>(red, part, nblocks, block_linear());
 }
 
@@ -278,6 +274,16 @@ __global__ void to_float_kernel(const double* __restrict__ src, float* __restric
         dst[i] = (float)src[i];
 }
 
+// f0 = phi - phi_G: a loaded state keeps all of phi's deviation in the rest
+// population until the first collision (which does not read the others).
+__global__ void rest_from_phi_kernel(const double* __restrict__ phi, double* __restrict__ f0, double fei_G,
+                                     long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        f0[i] = (phi ? phi[i] : 0.0) - fei_G;
+}
+
 __global__ void to_double_kernel(const float* __restrict__ src, double* __restrict__ dst, long long n)
 {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -308,7 +314,7 @@ lbm_status mixed_alloc(MixedBuffers& mb, const Geom& g, const Launch& L)
     for (int i = 0; i < 2; ++i) ok = ok && okf(&mb.f[i], 15 * n) && okf(&mb.g[i], 15 * n) && okf(&mb.h[i], 15 * n);
     ok = ok && okf(&mb.phi, n) && okf(&mb.rho, n) && okf(&mb.u, n) && okf(&mb.v, n) && okf(&mb.w, n) &&
          okf(&mb.s, n) && okf(&mb.dux, n) && okf(&mb.dvy, n);
-    ok = ok && okd(&mb.p, n) && okd(&mb.p_prev, n) && okd(&mb.p_chk, n) && okd(&mb.scratch, n);
+    ok = ok && okd(&mb.p, n) && okd(&mb.p_prev, n) && okd(&mb.p_chk, n) && okd(&mb.scratch, n) && okd(&mb.f0, n);
     const size_t nb = static_cast<size_t>(L.nblocks);
     ok = ok && okd(&mb.part_src, 3 * nb) && okd(&mb.part_prep, 3 * nb) && okd(&mb.part_a, nb) &&
          okd(&mb.part_b, 5 * nb) && okd(&mb.part_c, 3 * nb) && okd(&mb.part_mass, nb);
@@ -348,7 +354,7 @@ void mixed_free(MixedBuffers& mb)
         if (*p) cudaFree(*p);
         *p = nullptr;
     }
-    double** db[] = {&mb.p, &mb.p_prev, &mb.p_chk, &mb.scratch, &mb.part_src, &mb.part_prep, &mb.part_a,
+    double** db[] = {&mb.p, &mb.p_prev, &mb.p_chk, &mb.scratch, &mb.f0, &mb.part_src, &mb.part_prep, &mb.part_a,
                      &mb.part_b, &mb.part_c, &mb.part_mass};
     for (double** p : db) {
         if (*p) cudaFree(*p);
@@ -357,7 +363,7 @@ void mixed_free(MixedBuffers& mb)
     mb.allocated = false;
 }
 
-lbm_status mixed_load(cudaStream_t st, MixedBuffers& mb, const Geom& g, const Phys&,
+lbm_status mixed_load(cudaStream_t st, MixedBuffers& mb, const Geom& g, const Phys& P,
                       const double* const src[6], cudaMemcpyKind kind)
 {
     const size_t n = static_cast<size_t>(g.n);
@@ -370,6 +376,7 @@ lbm_status mixed_load(cudaStream_t st, MixedBuffers& mb, const Geom& g, const Ph
         } else if (cudaMemsetAsync(dst, 0, n * sizeof(float), st) != cudaSuccess) {
             return LBM_ERR_CUDA;
         }
+        if (i == 0) rest_from_phi_kernel<<<blocks, 256, 0, st>>>(src[0] ? mb.scratch : nullptr, mb.f0, P.fei_G, g.n);
     }
     if (src[5]) {
         if (cudaMemcpyAsync(mb.p, src[5], n * sizeof(double), kind, st) != cudaSuccess) return LBM_ERR_CUDA;
@@ -410,20 +417,21 @@ lbm_status mixed_prologue(cudaStream_t st, MixedBuffers& mb, const Launch& L, co
         src_blocks = static_cast<long long>(grid.x) * grid.y * grid.z;
         constexpr int smem = zm_ring_bytes<float>();
         auto kern = first ? collide_zm_kernel<true> : collide_zm_kernel<false>;
-        kern<<<grid, ZM_THREADS, smem, st>>>(g, M, mb.collide_zlen, mb.f[fin], mb.f[fout], mb.g[fin], mb.g[fout],
+        kern<<<grid, ZM_THREADS, smem, st>>>(g, M, mb.collide_zlen, mb.f[fin], mb.f[fout], mb.f0, mb.g[fin],
+                                             mb.g[fout],
                                              mb.phi, mb.rho, mb.u, mb.v, mb.w, div, mb.part_src, src_blocks);
     } else if (first) {
-        collide_kernel<true><<<L.grid, L.block, 0, st>>>(g, M, mb.f[fin], mb.f[fout], mb.g[fin], mb.g[fout],
+        collide_kernel<true><<<L.grid, L.block, 0, st>>>(g, M, mb.f[fin], mb.f[fout], mb.f0, mb.g[fin], mb.g[fout],
                                                          mb.phi, mb.rho, mb.u, mb.v, mb.w, div,
                                                          mb.part_src, L.nblocks);
     } else {
-        collide_kernel<false><<<L.grid, L.block, 0, st>>>(g, M, mb.f[fin], mb.f[fout], mb.g[fin], mb.g[fout],
+        collide_kernel<false><<<L.grid, L.block, 0, st>>>(g, M, mb.f[fin], mb.f[fout], mb.f0, mb.g[fin], mb.g[fout],
                                                           mb.phi, mb.rho, mb.u, mb.v, mb.w, div,
                                                           mb.part_src, L.nblocks);
     }
     if (ev) cudaEventRecord(ev[1], st);
     moments_kernel<<<L.grid, L.block, 0, st>>>(g, P.fei_G, P.fei_L, P.rho_G, P.rho_L, P.fei_avg, P.dfei,
-                                               P.half_drho, mb.f[fout], mb.g[fout], mb.phi, mb.rho, mb.u,
+                                               P.half_drho, mb.f[fout], mb.f0, mb.g[fout], mb.phi, mb.rho, mb.u,
                                                mb.v, mb.w, mb.part_mass, L.nblocks);
     if (ev) cudaEventRecord(ev[2], st);
     finalize(st, FIN_SOURCE, ds, mb.part_src, src_blocks, nullptr, 0, nullptr, 0);

@@ -207,6 +207,8 @@ lbm_status bicgstab(cudaStream_t st, const Launch& L, const Geom& g, const Krylo
     if (cudaMemsetAsync(kb.v, 0, static_cast<size_t>(cnt) * sizeof(double), st) != cudaSuccess) return LBM_ERR_CUDA;
     apply_kernel<1, kAdj><<<L.grid, L.block, 0, st>>>(g, kb.v, kb.t, rho, s, nullptr, kb.part, L.nblocks);
     if (!host_sum(L.nblocks, 1, d2)) return LBM_ERR_CUDA;
+    // a NaN/Inf source or right-hand side: NaN norms would skip the loop below
+    if (!isfinite(d2[0])) return LBM_ERR_NONFINITE;
     // relative to ||b||; a zero source (absolute criterion) still drives the
     // iterate to the null-space representative nearest the start
     const double bnorm = d2[0] > 0.0 ? sqrt(d2[0]) : 1.0;
@@ -214,11 +216,20 @@ lbm_status bicgstab(cudaStream_t st, const Launch& L, const Geom& g, const Krylo
     apply_kernel<1, kAdj><<<L.grid, L.block, 0, st>>>(g, h, kb.r, rho, s, nullptr, kb.part, L.nblocks);
     if (!host_sum(L.nblocks, 1, d2)) return LBM_ERR_CUDA;
     double rr = d2[0];
+    if (!isfinite(rr)) return LBM_ERR_NONFINITE;   // a NaN/Inf start iterate
     vec_kernel<3><<<kDotBlocks, 256, 0, st>>>(cnt, 0.0, 0.0, kb.r0, kb.p, kb.r, nullptr, nullptr, nullptr, nullptr);
     res->matvecs = 1;
     double rho_old = 1.0, alpha = 1.0, omega = 1.0, rho_new = rr, r0r0 = rr;
     bool first = true, budget = false;
     int since = 0;
+    // Restarts whose true residual is not below the best true residual of
+    // the earlier starts: a tolerance below
+    // the attainable rounding floor would otherwise restart forever when no
+    // matvec budget is set.  After kStalledRestarts of them the solve stops
+    // with LBM_ERR_POISSON_BUDGET (the iterate is the last one).
+    constexpr int kStalledRestarts = 5;
+    double best = rr;
+    int stalled = 0;
     // Restart from the true residual of the current iterate: r = b - A h,
     // r0 = p = r.
     auto restart = [&]() -> lbm_status {
@@ -235,6 +246,12 @@ lbm_status bicgstab(cudaStream_t st, const Launch& L, const Geom& g, const Krylo
         since = 0;
         ++res->restarts;
         res->rel_residual = sqrt(rr) / bnorm;
+        if (rr < best) {
+            best = rr;
+            stalled = 0;
+        } else if (++stalled >= kStalledRestarts) {
+            budget = true;
+        }
         return LBM_OK;
     };
     res->rel_residual = sqrt(rr) / bnorm;
@@ -248,6 +265,7 @@ lbm_status bicgstab(cudaStream_t st, const Launch& L, const Geom& g, const Krylo
         if (!first && (rho_old == 0.0 || omega == 0.0 || since >= 200)) {
             const lbm_status rs = restart();
             if (rs != LBM_OK) return rs;
+            if (budget) break;
             continue;
         }
         if (!first) {
@@ -266,6 +284,7 @@ lbm_status bicgstab(cudaStream_t st, const Launch& L, const Geom& g, const Krylo
             if (fresh) return LBM_ERR_NONFINITE;   // even a fresh start breaks down
             const lbm_status rs = restart();
             if (rs != LBM_OK) return rs;
+            if (budget) break;
             continue;
         }
         alpha = rho_new / d2[0];

@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "../../include/lbm_b200.h"
+#include "alloc_set.hpp"
 #include "field_stats.cuh"
 #include "handle_internal.hpp"
 #include "lbm_solver.cuh"
@@ -213,7 +214,7 @@ void upload_state_config(lbm_handle* h)
 {
     h->ds_host->check_interval = h->pcfg.check_interval;
     h->ds_host->tolerance = h->pcfg.tolerance;
-    h->ds_host->dual = h->pcfg.dual_residual;
+    h->ds_host->dual = h->pform == LBM_POISSON_VARCOEF_RB ? 1 : h->pcfg.dual_residual;
     h->ds_host->n_cells = static_cast<double>(h->geom.lx) * h->geom.ly * h->geom.lz;
 }
 
@@ -237,6 +238,8 @@ lbm_status build_segment(lbm_handle* h, const SegKey& key, cudaGraphExec_t* out,
             if (key.form == LBM_POISSON_SCALAR_JACOBI) {
                 fp64::scalar_jacobi(st, L, g, P[pc], P[1 - pc], b.rho, b.s, h->scalar_scale);
                 pc = 1 - pc;
+            } else if (key.form == LBM_POISSON_VARCOEF_RB) {
+                fp64::rb_varcoef(st, L, g, b.p, b.rho, b.s, h->sor_omega, h->ds);
             } else {
                 fp64::rb_sor(st, L, g, b.p, b.rho, b.s, h->scalar_scale, h->sor_omega, h->ds);
             }
@@ -244,7 +247,10 @@ lbm_status build_segment(lbm_handle* h, const SegKey& key, cudaGraphExec_t* out,
         fp64::p_sum(st, L, g, P[pc], b.part_a);
         finalize(st, FIN_SIGMA, h->ds, b.part_a, L.cnblocks, nullptr, 0, nullptr, 0);
         fp64::scalar_check(st, L, g, P[pc], b.p, b.p_prev, h->ds, b.part_b);
-        finalize(st, FIN_CHECK, h->ds, b.part_b, L.cnblocks, nullptr, 0, nullptr, 0);
+        // the variable-coefficient form's operator residual rides on the
+        // fixed-point terms of the check (DevState.dual is 1 for it)
+        if (key.form == LBM_POISSON_VARCOEF_RB) fp64::varcoef_residual(st, L, g, b.p, b.rho, b.s, h->ds, b.part_c);
+        finalize(st, FIN_CHECK, h->ds, b.part_b, L.cnblocks, b.part_c, L.cnblocks, nullptr, 0);
     } else if (h->precision == LBM_PRECISION_FP64) {
         Fp64Buffers& b = h->b;
         int n_single = key.n_normal;
@@ -355,15 +361,35 @@ void fill_stats(const lbm_handle* h, const DevState& d, lbm_step_stats* s)
     s->converged = d.converged;
 }
 
-// One time step.  replay > 0 forces that many sweeps.
+// A buffer set allocated whole or not at all (alloc_set.hpp): kind 0 device
+// memory, kind 1 pinned host memory.  On failure no slot changes, so the
+// set's "allocated" test (its first pointer) stays false and a retry
+// allocates again.
+lbm_status alloc_buffers(lbm_handle* h, const AllocSlot* slots, int n, const char* what)
+{
+    auto alloc = [](int kind, void** p, size_t bytes) {
+        return (kind == 0 ? cudaMalloc(p, bytes) : cudaMallocHost(p, bytes)) == cudaSuccess;
+    };
+    auto release = [](int kind, void* p) {
+        if (kind == 0) cudaFree(p);
+        else cudaFreeHost(p);
+    };
+    if (alloc_set(slots, n, alloc, release)) return LBM_OK;
+    cudaGetLastError();
+    return fail(h, LBM_ERR_OOM, what);
+}
+
 lbm_status ensure_accel_buffers(lbm_handle* h)
 {
     const size_t pop = 15 * static_cast<size_t>(h->geom.n) * sizeof(double);
     if (h->paccel.anderson_m1 && !h->and_r) {
-        LBM_CUDA(h, cudaMalloc(&h->and_r, pop));
-        LBM_CUDA(h, cudaMalloc(&h->and_i, pop));
-        LBM_CUDA(h, cudaMalloc(&h->and_part, 2 * fp64::kAndersonBlocks * sizeof(double)));
-        LBM_CUDA(h, cudaMallocHost(&h->and_host, 2 * fp64::kAndersonBlocks * sizeof(double)));
+        const size_t part = 2 * fp64::kAndersonBlocks * sizeof(double);
+        const AllocSlot set[] = {{reinterpret_cast<void**>(&h->and_r), pop, 0},
+                                 {reinterpret_cast<void**>(&h->and_i), pop, 0},
+                                 {reinterpret_cast<void**>(&h->and_part), part, 0},
+                                 {reinterpret_cast<void**>(&h->and_host), part, 1}};
+        const lbm_status s = alloc_buffers(h, set, 4, "Anderson-m1 buffers: device allocation failed");
+        if (s != LBM_OK) return s;
     }
     if ((h->paccel.two_grid || h->paccel.spatial_diagnostics) && !h->tg_sum) {
         int bx, by, bz;
@@ -463,11 +489,19 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
     }
     if (form == LBM_POISSON_KRYLOV && !h->kb.r) {
         const size_t pop = 15 * static_cast<size_t>(g.n) * sizeof(double);
-        double** kv[] = {&h->kb.r, &h->kb.r0, &h->kb.p, &h->kb.v, &h->kb.s, &h->kb.t};
-        for (double** p : kv) LBM_CUDA(h, cudaMalloc(p, pop));
-        const size_t parts = 2 * static_cast<size_t>(std::max<long long>(L.nblocks, kKrylovBlocks));
-        LBM_CUDA(h, cudaMalloc(&h->kb.part, parts * sizeof(double)));
-        LBM_CUDA(h, cudaMallocHost(&h->kb.host, parts * sizeof(double)));
+        const size_t parts = 2 * static_cast<size_t>(std::max<long long>(L.nblocks, kKrylovBlocks)) * sizeof(double);
+        // kb.r doubles as the set's "allocated" flag: alloc_set stores it
+        // only with all the others
+        const AllocSlot set[] = {{reinterpret_cast<void**>(&h->kb.r0), pop, 0},
+                                 {reinterpret_cast<void**>(&h->kb.p), pop, 0},
+                                 {reinterpret_cast<void**>(&h->kb.v), pop, 0},
+                                 {reinterpret_cast<void**>(&h->kb.s), pop, 0},
+                                 {reinterpret_cast<void**>(&h->kb.t), pop, 0},
+                                 {reinterpret_cast<void**>(&h->kb.part), parts, 0},
+                                 {reinterpret_cast<void**>(&h->kb.host), parts, 1},
+                                 {reinterpret_cast<void**>(&h->kb.r), pop, 0}};
+        const lbm_status s = alloc_buffers(h, set, 8, "Krylov work vectors: device allocation failed");
+        if (s != LBM_OK) return s;
     }
     if (dual) {
         const lbm_status s = ensure_dual_buffer(h);
@@ -502,8 +536,9 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
         } else if (form == LBM_POISSON_ONEPASS) {
             fp64::onepass_init(st, L, g, h->h_loaded, b.h[1], b.h[0], b.p, b.rho, b.s, acc.source_aware_init != 0,
                                acc.source_aware_scale);
-        } else if (form == LBM_POISSON_SCALAR_RB) {
-            fp64::scalar_rhs_sum(st, L, g, b.rho, b.s, h->scalar_scale, b.part_a);
+        } else if (form == LBM_POISSON_SCALAR_RB || form == LBM_POISSON_VARCOEF_RB) {
+            fp64::scalar_rhs_sum(st, L, g, form == LBM_POISSON_SCALAR_RB ? b.rho : nullptr, b.s, h->scalar_scale,
+                                 b.part_a);
             finalize(st, FIN_RHS, h->ds, b.part_a, L.cnblocks, nullptr, 0, nullptr, 0);
         }
     } else {
@@ -524,7 +559,8 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
     // collide, moments, 2 finalize, prep, finalize, poisson_init (+ correct below)
     uint64_t launches = 7;
     if (form == LBM_POISSON_SCALAR_JACOBI) launches = 6;   // no h initialisation
-    if (form == LBM_POISSON_SCALAR_RB) launches = 8;       // no h initialisation; right-hand-side mean
+    if (form == LBM_POISSON_SCALAR_RB || form == LBM_POISSON_VARCOEF_RB)
+        launches = 8;   // no h initialisation; right-hand-side mean
     uint64_t fused_sweeps = 0;
     bool anderson_history = false;
     if (form == LBM_POISSON_KRYLOV) {
@@ -589,8 +625,10 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
             kernels += static_cast<uint64_t>(n_normal);   // launches counted by onepass_segment
         } else if (form != LBM_POISSON_KINETIC) {
             // scalar sweeps (red-black: two launches each), p sum, check, 2 finalize
+            // (+ the operator residual of the variable-coefficient form)
+            const bool rb = form == LBM_POISSON_SCALAR_RB || form == LBM_POISSON_VARCOEF_RB;
             kernels += static_cast<uint64_t>(n_normal);
-            launches += static_cast<uint64_t>(n_normal) * (form == LBM_POISSON_SCALAR_RB ? 2 : 1) + 4;
+            launches += static_cast<uint64_t>(n_normal) * (rb ? 2 : 1) + 4 + (form == LBM_POISSON_VARCOEF_RB ? 1 : 0);
         } else {
             kernels += static_cast<uint64_t>(n_normal) + 2 + (dual ? 1 : 0);
             const bool fused = h->precision == LBM_PRECISION_MIXED ? h->mb.fuse_zlen > 0 : h->fuse_zlen > 0;
@@ -952,7 +990,7 @@ lbm_status lbm_set_poisson_form(lbm_handle* h, lbm_poisson_form form, double sou
 {
     if (check_handle(h) != LBM_OK) return LBM_ERR_BAD_ARG;
     if (form != LBM_POISSON_KINETIC && form != LBM_POISSON_SCALAR_JACOBI && form != LBM_POISSON_SCALAR_RB &&
-        form != LBM_POISSON_ONEPASS && form != LBM_POISSON_KRYLOV)
+        form != LBM_POISSON_ONEPASS && form != LBM_POISSON_KRYLOV && form != LBM_POISSON_VARCOEF_RB)
         return fail(h, LBM_ERR_BAD_ARG, "unknown Poisson form");
     if (form != LBM_POISSON_KINETIC && h->precision != LBM_PRECISION_FP64)
         return fail(h, LBM_ERR_BAD_ARG, "the scalar, one-pass and Krylov Poisson forms run in FP64 precision only");
@@ -964,10 +1002,11 @@ lbm_status lbm_set_poisson_form(lbm_handle* h, lbm_poisson_form form, double sou
         return fail(h, LBM_ERR_BAD_ARG,
                     "the Krylov form needs periodic x: the slip walls' overwrite makes the singular system "
                     "inconsistent, and the sweeps' gauge absorbs what a Krylov solve cannot");
-    if (form == LBM_POISSON_SCALAR_RB && (g.ly % 2 || g.lz % 2 || (g.periodic_x && g.lx % 2)))
-        return fail(h, LBM_ERR_BAD_ARG, "the red-black form needs even extents along the periodic axes");
+    const bool rb = form == LBM_POISSON_SCALAR_RB || form == LBM_POISSON_VARCOEF_RB;
+    if (rb && (g.ly % 2 || g.lz % 2 || (g.periodic_x && g.lx % 2)))
+        return fail(h, LBM_ERR_BAD_ARG, "the red-black forms need even extents along the periodic axes");
     double w = omega;
-    if (form == LBM_POISSON_SCALAR_RB && w == 0.0) {
+    if (rb && w == 0.0) {
         // Optimal SOR for the Jacobi iteration of the 14-neighbour stencil:
         // its slowest mode (wave number k) has rho_J = (10 cos k + 4) / 14.
         const double pi = 3.14159265358979323846;

@@ -174,14 +174,15 @@ __device__ __forceinline__ T pick_t(T m, T c, T p)
     else return c;
 }
 
-// Pull stream of all 15 populations into (x, y, z) with 32-bit offsets: the
+// Pull stream of populations Q0..14 into (x, y, z) with 32-bit offsets: the
 // caller guarantees 15 * n < 2^31 (the 64-bit form is pull_src + cell_of).
-template <class T>
+// Q0 = 1 leaves out the rest population (it does not move).
+template <int Q0 = 0, class T>
 __device__ __forceinline__ void pull_regs32(T (&v)[Q], const T* __restrict__ src, int n,
                                             const Geom& g, int x, int y, int z)
 {
     const Wrap w(g, x, y, z);
-    static_for<0, Q>([&](auto qc) {
+    static_for<Q0, Q>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
         const int idx = (pick<-cz(q)>(w.zm, z, w.zp) * g.ly + pick<-cy(q)>(w.ym, y, w.yp)) * g.lx +
                         pick<-cx(q)>(w.xm, x, w.xp);

@@ -11,7 +11,8 @@
 namespace lbm {
 
 struct MixedBuffers {
-    float* f[2] = {nullptr, nullptr};
+    float* f[2] = {nullptr, nullptr};   // moving populations q >= 1 (slot q = 0 unused)
+    double* f0 = nullptr;               // rest population f_0 - f_rest,0 in FP64 (updated in place)
     float* g[2] = {nullptr, nullptr};
     float* h[2] = {nullptr, nullptr};
     float* hc = nullptr;

@@ -147,6 +147,12 @@ void correct(cudaStream_t st, const Launch& L, const Geom& g, double* u, double*
 // (gauge, relative change; FIN_CHECK layout).
 void scalar_jacobi(cudaStream_t st, const Launch& L, const Geom& g, const double* pin, double* pout,
                    const double* rho, const double* s, double scale);
+// Variable-coefficient form: one red-black SOR sweep of div((1/rho) grad p) = s
+// (two launches) and the operator residual terms of a check (3 columns).
+void rb_varcoef(cudaStream_t st, const Launch& L, const Geom& g, double* p, const double* rho, const double* s,
+                double omega, const DevState* ds);
+void varcoef_residual(cudaStream_t st, const Launch& L, const Geom& g, const double* p, const double* rho,
+                      const double* s, const DevState* ds, double* part);
 void rb_sor(cudaStream_t st, const Launch& L, const Geom& g, double* p, const double* rho, const double* s,
             double scale, double omega, const DevState* ds);
 void scalar_rhs_sum(cudaStream_t st, const Launch& L, const Geom& g, const double* rho, const double* s,

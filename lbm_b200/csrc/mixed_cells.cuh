@@ -31,11 +31,12 @@ __device__ __forceinline__ void bounce_regs(T (&v)[Q], const Geom& g, int x)
     }
 }
 
+template <int Q0 = 0>
 __device__ __forceinline__ void pull_regs(float (&v)[Q], const float* __restrict__ src, const Geom& g,
                                           int x, int y, int z)
 {
     const Wrap w(g, x, y, z);
-    static_for<0, Q>([&](auto qc) {
+    static_for<Q0, Q>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
         v[q] = __ldg(src + (long long)q * g.n + pull_src<q>(g, w, x, y, z));
     });
@@ -192,10 +193,48 @@ __device__ __forceinline__ void collide_h_store32(const float (&hv)[Q], float p3
 // single-box kernels and the batched kernels call these, so a cell is
 // evaluated the same way in both.  Reduction terms are added to red.
 
+// phi - phi_G in FP64: the rest population f0 (FP64, it does not move) plus
+// the pulled moving populations f_1..f_14 (FP32 deviations), in q order.  The
+// moments and the next collision evaluate it from the same values in the same
+// order, so both see the same phi.
+__device__ __forceinline__ double phi_dev(double f0, const float (&fv)[Q])
+{
+    double acc = f0;
+    static_for<1, Q>([&](auto qc) { acc += (double)fv[decltype(qc)::value]; });
+    return acc;
+}
+
+// Post-collision f: the moving populations in FP32 (fout, q >= 1), the rest
+// population in FP64 as what remains of phi once the stored moving
+// populations are taken out.  The collision conserves phi (sum_q f_eq = phi),
+// so this is f0's own BGK value; and since the stream moves the stored FP32
+// values unchanged (a permutation under periodic boundaries), sum(phi) over
+// the box is carried from step to step to FP64 rounding.
+template <bool kFirst, class Idx>
+__device__ __forceinline__ void store_f_post(const MixPhys& P, const CellDeriv<float>& d, const MixCell& k,
+                                             const float (&fv)[Q], double f0_in, float* __restrict__ fout,
+                                             double* __restrict__ f0, Idx n, Idx c)
+{
+    // before the first collision f0 holds phi - phi_G (the load), the moving
+    // populations nothing
+    const double dev = kFirst ? f0_in : phi_dev(f0_in, fv);
+    double moved = 0.0;
+    static_for<1, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        float in = 0.f;
+        if constexpr (!kFirst) in = fv[q];
+        const float out = mix_f_post<q, kFirst>(P, d, k, in);
+        fout[q * n + c] = out;
+        moved += (double)out;
+    });
+    f0[c] = dev - moved;
+}
+
 // Plane collide: stencils gathered from global memory (CPU/Inamuro.cpp:134-250).
 template <bool kFirst>
 __device__ __forceinline__ void mixc_collide(const Geom& g, const MixPhys& P, const float* __restrict__ fin,
-                                             float* __restrict__ fout, const float* __restrict__ gin,
+                                             float* __restrict__ fout, double* __restrict__ f0,
+                                             const float* __restrict__ gin,
                                              float* __restrict__ gout, const float* __restrict__ phi,
                                              const float* __restrict__ rho, const float* __restrict__ u,
                                              const float* __restrict__ v, const float* __restrict__ w,
@@ -222,15 +261,10 @@ __device__ __forceinline__ void mixc_collide(const Geom& g, const MixPhys& P, co
     mix_cell_f(P, d, k);
     float fv[Q];
     if constexpr (!kFirst) {
-        pull_regs(fv, fin, g, x, y, z);
+        pull_regs<1>(fv, fin, g, x, y, z);
         bounce_regs(fv, g, x);
     }
-    static_for<0, Q>([&](auto qc) {
-        constexpr int q = decltype(qc)::value;
-        float in = 0.f;
-        if constexpr (!kFirst) in = fv[q];
-        fout[(long long)q * g.n + c] = mix_f_post<q, kFirst>(P, d, k, in);
-    });
+    store_f_post<kFirst>(P, d, k, fv, f0[c], fout, f0, g.n, c);
     float gv[Q];
     if constexpr (!kFirst) {
         pull_regs(gv, gin, g, x, y, z);
@@ -244,13 +278,14 @@ __device__ __forceinline__ void mixc_collide(const Geom& g, const MixPhys& P, co
     });
 }
 
-// Moments (CPU/Inamuro.cpp:294-346): phi = phi_G + sum f_dev (FP64), rho(phi),
-// u* = sum c g; red[0] += phi.
+// Moments (CPU/Inamuro.cpp:294-346): phi = phi_G + f0 + sum_{q>=1} f_dev
+// (FP64), rho(phi), u* = sum c g; red[0] += phi.
 struct MixMoments {
     double fei_G, fei_L, rho_G, rho_L, fei_avg, dfei, half_drho;
 };
 
 __device__ __forceinline__ void mixc_moments(const Geom& g, const MixMoments& M, const float* __restrict__ f,
+                                             const double* __restrict__ f0,
                                              const float* __restrict__ gp, float* __restrict__ phi,
                                              float* __restrict__ rho, float* __restrict__ u,
                                              float* __restrict__ v, float* __restrict__ w, int x, int y, int z,
@@ -258,11 +293,9 @@ __device__ __forceinline__ void mixc_moments(const Geom& g, const MixMoments& M,
 {
     const long long c = cell_of(g, x, y, z);
     float fv[Q];
-    pull_regs(fv, f, g, x, y, z);
+    pull_regs<1>(fv, f, g, x, y, z);
     bounce_regs(fv, g, x);
-    double dev = 0.0;
-    static_for<0, Q>([&](auto qc) { dev += (double)fv[decltype(qc)::value]; });
-    const double fei = M.fei_G + dev;
+    const double fei = M.fei_G + phi_dev(f0[c], fv);
     double density;
     if (fei <= M.fei_G) density = M.rho_G;
     else if (fei >= M.fei_L) density = M.rho_L;

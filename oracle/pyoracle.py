@@ -44,12 +44,18 @@ class OrcStepInfo(C.Structure):
 _lib = None
 
 
+# Where the reference checkout is read from when LBM_REFERENCE_DIR is unset
+# (the build container's read-only copy; absent on machines without it).
+DEFAULT_REFERENCE_DIR = "/root/reference"
+
+
 def build() -> None:
     """Compiles the restatement (and, where the reference checkout exists, the
     reference harnesses) with oracle/Makefile."""
     env = dict(os.environ)
     env["CC"] = "gcc"   # the system gcc ships libgomp
     env["CXX"] = "g++"
+    env.setdefault("LBM_REFERENCE_DIR", DEFAULT_REFERENCE_DIR)
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True, env=env)
 
 

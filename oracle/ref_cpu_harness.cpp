@@ -15,10 +15,12 @@
 //           each, x fastest, no ghost layers) and DIR/summary.txt
 //           ("step sweeps ms" per line).
 //   sample: --params F --sample-sweeps K --out DIR [--init FIELDS.bin] [--sample-reps R]
+//           [--nonpoisson-reps M]
 //           R times (default 1): times one non-Poisson step part (collision,
-//           stream, bounce, moments) and K kinetic Poisson sweeps
-//           (collision_p, stream, bounce, getp) on the box of F; writes
-//           DIR/sample.txt ("cells N", then "rep i nonpoisson_ms sweeps_ms").
+//           stream, bounce, moments; only in the first M reps, default all)
+//           and K kinetic Poisson sweeps (collision_p, stream, bounce, getp)
+//           on the box of F; writes DIR/sample.txt ("cells N", then
+//           "rep i nonpoisson_ms sweeps_ms", nonpoisson_ms -1 where skipped).
 #include <chrono>
 #include <cstdint>
 #include <cstdio>
@@ -132,6 +134,7 @@ int main(int argc, char** argv)
     int steps = 0;
     long sample_sweeps = -1;
     int sample_reps = 1;
+    int nonpoisson_reps = -1;
     bool dump_h = false;
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
@@ -145,6 +148,7 @@ int main(int argc, char** argv)
         else if (a == "--init") init = val();
         else if (a == "--sample-sweeps") sample_sweeps = std::stol(val());
         else if (a == "--sample-reps") sample_reps = std::stoi(val());
+        else if (a == "--nonpoisson-reps") nonpoisson_reps = std::stoi(val());
         else if (a == "--dump-h") dump_h = true;
         else {
             std::cerr << "unknown argument " << a << "\n";
@@ -164,13 +168,14 @@ int main(int argc, char** argv)
             s.precision(17);
             s << "cells " << h.cells() << "\n";
             for (int r = 0; r < sample_reps; ++r) {
+                const bool np = nonpoisson_reps < 0 || r < nonpoisson_reps;
                 const auto t0 = clk::now();
-                h.nonPoissonPart();
+                if (np) h.nonPoissonPart();
                 const auto t1 = clk::now();
                 for (long k = 0; k < sample_sweeps; ++k) h.sweep();
                 const auto t2 = clk::now();
                 s << "rep " << r << " "
-                  << std::chrono::duration<double, std::milli>(t1 - t0).count() << " "
+                  << (np ? std::chrono::duration<double, std::milli>(t1 - t0).count() : -1.0) << " "
                   << std::chrono::duration<double, std::milli>(t2 - t1).count() << "\n";
                 s.flush();
             }

@@ -191,3 +191,20 @@ def test_krylov_adjoint_solve_matches_the_sweeps(run):
     assert abs(s2["grad_kappa_f"] - stats["grad_kappa_f"]) <= 1e-7 * abs(stats["grad_kappa_f"])
     assert s2["adjoint_sweeps"] * 3 <= stats["adjoint_sweeps"], (s2["adjoint_sweeps"], stats["adjoint_sweeps"])
     b.close()
+
+
+@pytest.mark.parametrize("krylov", [False, True])
+def test_nonfinite_adjoint_rhs_is_an_error(krylov):
+    """A NaN in the final fields' adjoint reaches the adjoint Poisson problem's
+    right-hand side: both the transposed sweeps and BiCGSTAB report
+    LBM_ERR_NONFINITE instead of returning a NaN gradient as a success."""
+    p, f = setup_case()
+    a = L.Adjoint(p, checkpoint_interval=KINT, krylov=krylov)
+    poisson(a)
+    a.forward(f, 2)
+    lam_p = np.zeros(f["phi"].shape)
+    lam_p[1, 2, 3] = np.nan
+    with pytest.raises(L.LBMError) as e:
+        a.backward({"p": lam_p})
+    assert e.value.status == 2, str(e.value)
+    a.close()

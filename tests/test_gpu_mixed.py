@@ -28,7 +28,9 @@ def mixed_vs_oracle(p, f, steps, dual=False):
         assert st["iterations"] == info["sweeps"]
         gf, of = g.download_fields(), o.fields()
         errs.append({k: rel_err(gf[k], of[k]) for k in L.FIELDS})
-        assert abs(st["mass"] - info["mass"]) <= 1e-6 * abs(info["mass"])
+        # the FP64 rest population carries sum(phi) exactly; what differs is
+        # the FP32 populations' share of the flux through the slip walls
+        assert abs(st["mass"] - info["mass"]) <= 1e-9 * abs(info["mass"])
     g.close()
     return errs
 
@@ -146,8 +148,9 @@ def test_zmarch_collide_matches_plane_collide(zlen, periodic, monkeypatch):
 
 def test_mixed_periodic_x_against_periodic_oracle():
     """Periodic x (not a reference mode): the mixed box against the FP64
-    oracle run with periodic x, equal sweep counts; phi sum conserved to FP32
-    storage rounding (coherent over uniform regions: ~1e-8 per step)."""
+    oracle run with periodic x, equal sweep counts; sum(phi) conserved to
+    1e-12 of the loaded phi's FP64 sum (FP64 rest population, the stream a
+    permutation of the stored FP32 moving populations)."""
     p, f = laplace_case((32, 24, 16), DD=8.0, noise=1e-4)
     p.periodic_x = 1
     f["u"] = 0.01 * np.sin(2 * np.pi * np.arange(24) / 24)[None, :, None] * np.ones_like(f["u"])
@@ -167,4 +170,5 @@ def test_mixed_periodic_x_against_periodic_oracle():
     vscale = max(float(np.max(np.abs(of[k]))) for k in ("u", "v", "w"))
     for k in ("u", "v", "w"):
         assert float(np.max(np.abs(gf[k] - of[k]))) <= 1e-5 * vscale, k
-    assert max(abs(m - masses[0]) for m in masses) <= 1e-6 * abs(masses[0])
+    m0 = float(np.sum(f["phi"]))
+    assert max(abs(m - m0) for m in masses) <= 1e-12 * abs(m0)

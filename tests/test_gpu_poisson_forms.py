@@ -290,3 +290,80 @@ def test_reference_scalar_option_keeps_its_start_pressure(tmp_path):
     _, v = tecplot_points(d / "out" / "3D000000003.plt", 16 * 32 * 32)
     assert np.all(v[:, 5] == 0.0)
     assert final_counts(d / "diag.csv") == {1: 100, 2: 100, 3: 100}
+
+
+def varcoef_residual_np(pv, rho, s, periodic):
+    """numpy restatement of the variable-coefficient operator of the
+    "varcoef-rb" form: r = A p - (s - mean_W s), A p = 6 sum_q E_q k_q
+    (p(x + c_q) - p(x)), k_q the mean of 1/rho at x and x + c_q, x mirrored at
+    slip walls (x = -1 -> 1, x = lx -> lx - 2), y and z periodic; W = 1/2 on
+    the wall planes.  Arrays (lz, ly, lx).  Returns (r, W)."""
+    lz, ly, lx = pv.shape
+    xs = np.arange(lx)
+
+    def shift(a, cx, cy, cz):
+        ix = xs + cx
+        if periodic:
+            ix %= lx
+        else:
+            ix = np.where(ix < 0, 1, np.where(ix >= lx, lx - 2, ix))
+        a = a[:, :, ix]
+        return np.roll(np.roll(a, -cy, axis=1), -cz, axis=0)
+
+    W = np.ones_like(pv)
+    if not periodic:
+        W[:, :, 0] = W[:, :, -1] = 0.5
+    rhs = s - np.sum(W * s) / np.sum(W)
+    inv = 1.0 / rho
+    ap = np.zeros_like(pv)
+    dirs = [(1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)]
+    dirs += [(a, b, c) for a in (1, -1) for b in (1, -1) for c in (1, -1)]
+    for cx_, cy_, cz_ in dirs:
+        e = 1.0 / 9.0 if abs(cx_) + abs(cy_) + abs(cz_) == 1 else 1.0 / 72.0
+        k = 0.5 * (inv + shift(inv, cx_, cy_, cz_))
+        ap += 6.0 * e * k * (shift(pv, cx_, cy_, cz_) - pv)
+    return ap - rhs, W, rhs
+
+
+@pytest.mark.parametrize("periodic", [False, True])
+def test_varcoef_rb_solves_its_equation(periodic):
+    """The variable-coefficient red-black form solves div((1/rho) grad p) = s
+    on the step's own source (the oracle's projected source of the same
+    collision) to its residual tolerance, p gauged to the step's target."""
+    p, f = case(periodic)
+    f["u"] = 0.01 * np.sin(2 * np.pi * np.arange(SHAPE[0]) / SHAPE[0])[None, None, :] * np.ones_like(f["u"])
+    o = pyoracle.Oracle(p.shape, oracle_params(p), f, tol=1e-12, max_sweeps=400000, periodic_x=periodic)
+    o.step()
+    s = o.derivatives()[6]
+    rho_o = o.fields()["rho"]
+    g = gpu_box(p, f, "varcoef-rb", 1e-12)
+    st = g.step(1)[0]
+    assert st["converged"] == 1 and st["fixed_point_evaluated"] == 1
+    assert st["fixed_point_h_relative"] < 1e-12
+    got = g.download_fields()
+    assert rel_err(got["rho"], rho_o) <= 1e-13
+    r, W, rhs = varcoef_residual_np(got["p"], got["rho"], s, periodic)
+    assert float(np.sum(W * np.abs(r))) <= 1e-10 * float(np.sum(W * np.abs(rhs)))
+    assert abs(float(np.mean(got["p"])) - float(np.mean(f["p"]))) <= 1e-12
+    g.close()
+
+
+@pytest.mark.parametrize("periodic", [False, True])
+def test_varcoef_rb_error_against_kinetic_fixed_point(periodic, capsys):
+    """Reported, not claimed: the variable-coefficient scalar form against the
+    kinetic form's fixed point (both converged to 1e-12 from the same state,
+    one step).  The test records the errors in p and u and checks only that
+    the form tracks the kinetic solution's scale (error below 1)."""
+    p, f = case(periodic)
+    f["u"] = 0.01 * np.sin(2 * np.pi * np.arange(SHAPE[0]) / SHAPE[0])[None, None, :] * np.ones_like(f["u"])
+    out = {}
+    for form in ("kinetic", "varcoef-rb"):
+        g = gpu_box(p, f, form, 1e-12)
+        g.step(1)
+        out[form] = g.download_fields()
+        g.close()
+    errs = {k: rel_err(out["varcoef-rb"][k], out["kinetic"][k]) for k in ("p", "u", "v", "w")}
+    with capsys.disabled():
+        print(f"\nvarcoef-rb vs kinetic fixed point (periodic_x={int(periodic)}): " +
+              ", ".join(f"{k} {v:.3e}" for k, v in errs.items()))
+    assert all(np.isfinite(v) and v < 1.0 for v in errs.values()), errs
