@@ -187,7 +187,7 @@ b_sweep(const BItem* __restrict__ items, int n_items, const BInst* __restrict__ 
 // blocking (sweep2_run).
 constexpr int B2_TX = 16, B2_TY = 8;
 constexpr int B2_THREADS = sweep2_threads(B2_TX, B2_TY);   // 192
-constexpr int B2_SMEM = sweep2_smem(B2_TX, B2_TY);         // 43,200 B
+constexpr int B2_SMEM = sweep2_smem(B2_TX, B2_TY);         // 32,400 B
 constexpr int B2_CTAS_PER_SM = 4;
 
 __global__ void __launch_bounds__(B2_THREADS, B2_CTAS_PER_SM)

@@ -495,26 +495,25 @@ sweep_kernel(Geom g, const double* __restrict__ hin, double* __restrict__ hout,
 // Two sweeps in one pass (temporal blocking; same scheme as the mixed box).
 // A CTA owns a TX x TY xy tile and a run of `zlen` planes; marching in z it
 // computes sweep k on the tile plus a one-cell halo (wrapped coordinates,
-// pulled from global memory) into a ring of shared-memory planes, then sweep
-// k+1 on the tile from that ring.  Every cell's arithmetic is
-// collide_h_store's expression, so (without FMA contraction in this file) the
-// result is bitwise that of two sweep_kernel launches.  Each thread owns one
-// halo-region cell for the whole march and keeps the next plane's global
-// pulls in flight while the CTA works through the shared-memory phase.
-// Four ring slots make one barrier per plane enough (the slot written at
-// iteration z+1 was last read at z-1).  lx % TX == 0, ly % TY == 0 and
-// 15 n < 2^31 are required (checked by the launcher).
-constexpr int F2_TX = 32, F2_TY = 4;
+// pulled from global memory) into the z-grouped plane ring of lbm_device.cuh
+// (45 population planes), then sweep k+1 on the tile from that ring.  Every
+// cell's arithmetic is collide_h_store's expression, so (without FMA
+// contraction in this file) the result is bitwise that of two sweep_kernel
+// launches.  Each thread owns one halo-region cell for the whole march and
+// keeps the next plane's global pulls in flight while the CTA works through
+// the shared-memory phase; one barrier per plane.  lx % TX == 0,
+// ly % TY == 0 and 15 n < 2^31 are required (checked by the launcher).
+constexpr int F2_TX = 16, F2_TY = 8;
 constexpr int F2_RX = F2_TX + 2, F2_RY = F2_TY + 2, F2_RC = F2_RX * F2_RY;
-constexpr int F2_THREADS = (F2_RC + 31) / 32 * 32;   // 224: one thread per region cell
-constexpr int F2_SLOTS = 4;
-constexpr int F2_SMEM = F2_SLOTS * Q * F2_RC * (int)sizeof(double);
+constexpr int F2_THREADS = (F2_RC + 31) / 32 * 32;   // 192: one thread per region cell
+constexpr int F2_SMEM = ring_planes() * F2_RC * (int)sizeof(double);   // 64,800 B
+constexpr int F2_CTAS = 2;
 
-__global__ void __launch_bounds__(F2_THREADS, 2)
+__global__ void __launch_bounds__(F2_THREADS, F2_CTAS)
 sweep2_kernel(Geom g, int zlen, const double* __restrict__ hin, double* __restrict__ hout,
               const double* __restrict__ rho, const double* __restrict__ s)
 {
-    extern __shared__ double ring2[];   // [F2_SLOTS][Q][F2_RC]
+    extern __shared__ double ring2[];   // [ring_planes()][F2_RC]
     const int t = threadIdx.x;
     const int n = (int)g.n;
     const int x0 = blockIdx.x * F2_TX, y0 = blockIdx.y * F2_TY;
@@ -523,7 +522,6 @@ sweep2_kernel(Geom g, int zlen, const double* __restrict__ hin, double* __restri
     const bool owner = t < F2_RC;
     const int xw = (x0 - 1 + t % F2_RX + g.lx) % g.lx;
     const int yw = (y0 - 1 + t / F2_RX + g.ly) % g.ly;
-    auto slot_of = [&](int zz) { return ring2 + ((zz + F2_SLOTS) & (F2_SLOTS - 1)) * (Q * F2_RC); };
 
     double a[Q];
     double a_rho = 1.0, a_s = 0.0;
@@ -540,8 +538,14 @@ sweep2_kernel(Geom g, int zlen, const double* __restrict__ hin, double* __restri
         bounce_regs(a, g, xw);
         const double pv = sum_q(a);
         const double tauh = 1.0 / a_rho + 0.5;
-        // collide_h_store into the ring (n = F2_RC, cell = t)
-        collide_h_store(a, pv, tauh, a_s, slot_of(zz), F2_RC, t);
+        // collide_h_store's expression, each population into its ring plane
+        const double inv_tauh = 1.0 / tauh;
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            constexpr double E = wE(q);
+            const double hequ = E * pv;
+            ring2[ring_plane<q>(zz) * F2_RC + t] = a[q] - div_rn(a[q] - hequ, tauh, inv_tauh) - (E / 3.0) * a_s;
+        });
     };
 
     prefetch(z0 - 1);
@@ -557,14 +561,10 @@ sweep2_kernel(Geom g, int zlen, const double* __restrict__ hin, double* __restri
         if (z + 1 < z1) prefetch(z + 2);
         __syncthreads();
         if (t < F2_TX * F2_TY) {
-            const double* sm = slot_of(z - 1);
-            const double* s0 = slot_of(z);
-            const double* sp = slot_of(z + 1);
             double hv[Q];
             static_for<0, Q>([&](auto qc) {
                 constexpr int q = decltype(qc)::value;
-                const double* slot = pick_t<-cz(q)>(sm, s0, sp);
-                hv[q] = slot[q * F2_RC + rc - cy(q) * F2_RX - cx(q)];
+                hv[q] = ring2[ring_plane<q>(z - cz(q)) * F2_RC + rc - cy(q) * F2_RX - cx(q)];
             });
             bounce_regs(hv, g, x);
             const int c = (z * g.ly + y) * g.lx + x;

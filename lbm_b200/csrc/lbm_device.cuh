@@ -190,6 +190,35 @@ __device__ __forceinline__ void pull_regs32(T (&v)[Q], const T* __restrict__ src
     });
 }
 
+// ---- plane ring of the two-sweep passes --------------------------------
+// A two-sweep pass marches a tile in z: at iteration z it writes sweep k's
+// populations of plane z+1 into a shared-memory ring (before the iteration's
+// barrier) and, after the barrier, pulls sweep k+1's populations of plane z
+// from it -- population q from plane z - cz(q).  So plane P's population q is
+// read at iteration P-1 (cz = -1), P (cz = 0) or P+1 (cz = +1), and a slot may
+// be rewritten only after every thread has passed the barrier that follows
+// its last read: the three groups of five populations (by cz) need 2, 3 and 4
+// plane slots, 45 population planes in all (4 x 15 without the grouping).
+__host__ __device__ constexpr int ring_group_slots(int g) { return g + 2; }   // g = cz + 1
+__host__ __device__ constexpr int ring_group_base(int g) { return g == 0 ? 0 : (g == 1 ? 10 : 25); }
+__host__ __device__ constexpr int ring_planes() { return 45; }   // population planes
+// Rank of q among the populations with the same cz.
+__host__ __device__ constexpr int ring_rank(int q)
+{
+    int r = 0;
+    for (int k = 0; k < q; ++k) r += (cz(k) == cz(q)) ? 1 : 0;
+    return r;
+}
+// Population plane of (q, plane zz) in the ring.
+template <int q>
+__device__ __forceinline__ int ring_plane(int zz)
+{
+    constexpr int gq = cz(q) + 1;
+    constexpr int S = ring_group_slots(gq);
+    const int slot = ((zz % S) + S) % S;
+    return ring_group_base(gq) + slot * 5 + ring_rank(q);
+}
+
 // Stencil neighbour x + c_k.
 template <int k>
 __device__ __forceinline__ long long stencil_nb(const Geom& g, const Mirror& m, int x, int y, int z)

@@ -431,19 +431,19 @@ __device__ __forceinline__ void mixc_correct(const Geom& g, float* __restrict__ 
 // Two kinetic sweeps of the z run [z0, z1) of the TX x TY column at (x0, y0)
 // (temporal blocking; the single box's sweep2_kernel and the batched
 // b_sweep2 run this body).  Threads: one per cell of the tile plus its
-// one-cell halo, (TX+2)(TY+2) rounded up to whole warps; ring: 4 plane slots
-// of 15 populations per region cell in shared memory.  Each thread owns one
+// one-cell halo, (TX+2)(TY+2) rounded up to whole warps.  Each thread owns one
 // region cell for the whole march and keeps the global pulls of the NEXT
 // plane in flight (registers) while the CTA works through the shared-memory
-// phase of the current one; one barrier per plane (the slot written at
-// iteration z+1 was last read at iteration z-1).  Region cells use wrapped
+// phase of the current one; one barrier per plane.  Region cells use wrapped
 // coordinates, so the periodic stream and the x slip overwrite are those of
 // two single sweeps; tile cells outside the box (partial tiles) store
-// nothing.  Cell arithmetic: mixc_sweep32's (collide_h, sum_q32).
+// nothing.  Cell arithmetic: mixc_sweep32's (collide_h, sum_q32).  The ring
+// is the z-direction-grouped one of lbm_device.cuh (ring_plane, 45 population
+// planes).
 __host__ __device__ constexpr int sweep2_threads(int tx, int ty) { return ((tx + 2) * (ty + 2) + 31) / 32 * 32; }
 __host__ __device__ constexpr int sweep2_smem(int tx, int ty)
 {
-    return 4 * Q * (tx + 2) * (ty + 2) * static_cast<int>(sizeof(float));
+    return ring_planes() * (tx + 2) * (ty + 2) * static_cast<int>(sizeof(float));
 }
 
 template <int TX, int TY>
@@ -452,14 +452,13 @@ __device__ __forceinline__ void sweep2_run(const Geom& g, int x0, int y0, int z0
                                            const float* __restrict__ omega, const float* __restrict__ s,
                                            float* __restrict__ ring)
 {
-    constexpr int RX = TX + 2, RC = RX * (TY + 2), SLOTS = 4;
+    constexpr int RX = TX + 2, RC = RX * (TY + 2);
     const int t = threadIdx.x;
     const int n = (int)g.n;
     // this thread's halo-region cell (wrapped coordinates)
     const bool owner = t < RC;
     const int xw = (x0 - 1 + t % RX + g.lx) % g.lx;
     const int yw = (y0 - 1 + t / RX + g.ly) % g.ly;
-    auto slot_of = [&](int zz) { return ring + ((zz + SLOTS) & (SLOTS - 1)) * (Q * RC); };
 
     float a[Q];
     float a_om = 0.f, a_s = 0.f;
@@ -471,14 +470,13 @@ __device__ __forceinline__ void sweep2_run(const Geom& g, int x0, int y0, int z0
         a_om = __ldg(omega + c);
         a_s = __ldg(s + c);
     };
-    auto finish = [&](int zz) {          // complete sweep k on plane zz into its ring slot
+    auto finish = [&](int zz) {          // complete sweep k on plane zz into the ring
         if (!owner) return;
         bounce_regs(a, g, xw);
         const float p32 = sum_q32(a);
-        float* slot = slot_of(zz);
         static_for<0, Q>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
-            slot[q * RC + t] = collide_h<q>(a[q], p32, a_om, a_s);
+            ring[ring_plane<q>(zz) * RC + t] = collide_h<q>(a[q], p32, a_om, a_s);
         });
     };
 
@@ -496,15 +494,11 @@ __device__ __forceinline__ void sweep2_run(const Geom& g, int x0, int y0, int z0
         if (z + 1 < z1) prefetch(z + 2);
         __syncthreads();
         if (inner) {
-            // sweep k+1 at (x, y, z): pull from the ring (planes z-1, z, z+1)
-            const float* sm = slot_of(z - 1);
-            const float* s0 = slot_of(z);
-            const float* sp = slot_of(z + 1);
+            // sweep k+1 at (x, y, z): pull q from plane z - cz(q) of the ring
             float hv[Q];
             static_for<0, Q>([&](auto qc) {
                 constexpr int q = decltype(qc)::value;
-                const float* slot = pick_t<-cz(q)>(sm, s0, sp);
-                hv[q] = slot[q * RC + rc - cy(q) * RX - cx(q)];
+                hv[q] = ring[ring_plane<q>(z - cz(q)) * RC + rc - cy(q) * RX - cx(q)];
             });
             bounce_regs(hv, g, x);
             const int c = (z * g.ly + y) * g.lx + x;
