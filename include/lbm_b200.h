@@ -30,7 +30,7 @@ extern "C" {
 
 /* Bumped whenever a struct layout or a signature of this header changes;
    callers compare it with lbm_abi_version() of the loaded library. */
-#define LBM_B200_ABI_VERSION 5
+#define LBM_B200_ABI_VERSION 6
 
 typedef enum {
     LBM_OK = 0,
@@ -526,7 +526,7 @@ lbm_status lbm_correct_backward(const lbm_params* p, const double* press, const 
  * state every checkpoint_interval steps; the reverse pass recomputes each
  * interval from its checkpoint (replaying the forward's sweep counts, so the
  * recomputed states are bitwise the forward's) and walks it backwards.
- * Device memory: about 288 B/cell per checkpoint plus 168 B/cell per step of
+ * Device memory: about 288 B/cell per checkpoint (156 with the mixed forward box) plus 168 B/cell per step of
  * one interval (uniform) or of one step (binomial) plus about 1 kB/cell of
  * adjoint buffers.  The reference has no derivatives. */
 typedef struct lbm_adjoint lbm_adjoint;
@@ -549,6 +549,13 @@ typedef struct {
                                   adjoint right-hand side returns LBM_ERR_NONFINITE, restarts
                                   without progress LBM_ERR_POISSON_BUDGET as in the forward form */
     double krylov_tolerance;   /* 0: 1e-10 */
+    int precision;             /* 0: the forward box is FP64.  1: the forward box is the mixed box
+                                  (FP32 populations and fields, FP64 rest population, pressure and
+                                  reductions); its checkpoints take 156 B/cell instead of 288, and
+                                  the reverse pass differentiates the FP64 step at the mixed
+                                  forward's states (fields converted to FP64), so the gradient
+                                  carries the mixed forward's error (not bitwise reproducible
+                                  against an FP64 forward) */
 } lbm_adjoint_cfg;
 
 typedef struct {

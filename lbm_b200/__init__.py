@@ -123,7 +123,7 @@ class AdjointCfg(C.Structure):
     """lbm_adjoint_cfg: checkpoint interval and the adjoint Poisson solve's exit."""
     _fields_ = [("checkpoint_interval", C.c_int), ("check_interval", C.c_int), ("tolerance", C.c_double),
                 ("max_sweeps", C.c_uint64), ("binomial_checkpoints", C.c_int), ("krylov", C.c_int),
-                ("krylov_tolerance", C.c_double)]
+                ("krylov_tolerance", C.c_double), ("precision", C.c_int)]
 
 
 class AdjointStats(C.Structure):
@@ -146,7 +146,7 @@ class LBMError(RuntimeError):
 
 _lib = None
 # LBM_B200_ABI_VERSION of include/lbm_b200.h that the structures above mirror.
-ABI_VERSION = 5
+ABI_VERSION = 6
 
 
 def load_library(path: str = LIB_PATH):
@@ -676,11 +676,11 @@ class Adjoint:
 
     def __init__(self, params: Params, checkpoint_interval: int = 100, check_interval: int = 100,
                  tolerance: float = 1e-12, max_sweeps: int = 0, binomial_checkpoints: int = 0, krylov: bool = False,
-                 krylov_tolerance: float = 0.0, device: int = 0):
+                 krylov_tolerance: float = 0.0, device: int = 0, precision: str = "fp64"):
         self._lib = load_library()
         self.params = params
         self.cfg = AdjointCfg(checkpoint_interval, check_interval, tolerance, max_sweeps, binomial_checkpoints,
-                              int(krylov), krylov_tolerance)
+                              int(krylov), krylov_tolerance, {"fp64": 0, "mixed": 1}[precision])
         h = C.c_void_p()
         st = self._lib.lbm_adjoint_create(C.byref(params), device, C.byref(self.cfg), C.byref(h))
         if st != 0:

@@ -46,13 +46,14 @@ struct lbm_adjoint {
     lbm_adjoint_cfg cfg{};
     int device = 0;
     lbm_handle* fwd = nullptr;
-    Fp64View view{};
+    BoxInfo view{};                     // geometry, physics, launch shape, stream of the forward box
+    size_t state_bytes = 0;             // one saved forward state (box_state_bytes)
     long long n = 0;
     std::string err;
     int n_steps = 0;
     bool have_forward = false;
     std::vector<uint64_t> sweeps;       // per forward step
-    std::vector<double*> ckpt;          // ckpt[k]: state after step k * interval (k >= 1): f, g, 6 macro
+    std::vector<double*> ckpt;          // ckpt[k]: state after step k * interval (k >= 1), box_save_state
     double* init = nullptr;             // loaded macro fields (6 n)
     double* final_state = nullptr;      // macro fields after the last step (6 n)
     double* seg_macro = nullptr;        // (interval + 1) x 6 n
@@ -71,7 +72,7 @@ struct lbm_adjoint {
     double forward_ms = 0.0;
     uint64_t forward_sweeps = 0;
     int y_warm = -1;                    // y buffer holding the last converged adjoint iterate, -1: none
-    std::vector<double*> bslot;         // binomial mode: checkpoint slots (36 n each), allocated on first use
+    std::vector<double*> bslot;         // binomial mode: checkpoint slots (state_bytes each), allocated on first use
     std::vector<int> bfree;             // free slot indices
     KrylovBuffers kb{};                 // cfg.krylov: BiCGSTAB work vectors
 };
@@ -250,28 +251,19 @@ lbm_status recompute(lbm_adjoint* a, int s0, int s1)
     const long long n = a->n;
     const size_t fbytes = static_cast<size_t>(n) * sizeof(double);
     cudaStream_t st = a->view.stream;
-    const double* src_macro = nullptr;
     if (s0 == 0) {
         ADJ_TRY(a, lbm_load_fields_device(a->fwd, slot(a->init, n, 0), slot(a->init, n, 1), slot(a->init, n, 2),
                                           slot(a->init, n, 3), slot(a->init, n, 4), slot(a->init, n, 5)),
                 "reload of the initial fields");
-        src_macro = a->init;
+        ADJ_CUDA(a, cudaMemcpyAsync(a->seg_macro, a->init, 6 * fbytes, cudaMemcpyDeviceToDevice, st));
     } else {
-        double* ck = a->ckpt[s0 / a->cfg.checkpoint_interval - 1];
-        const double* m[6];
-        for (int i = 0; i < 6; ++i) m[i] = slot(ck, n, 30 + i);
-        ADJ_TRY(a, fp64_restore(a->fwd, ck, slot(ck, n, 15), m), "checkpoint restore");
-        src_macro = slot(ck, n, 30);
+        ADJ_TRY(a, box_restore_state(a->fwd, a->ckpt[s0 / a->cfg.checkpoint_interval - 1]), "checkpoint restore");
+        ADJ_TRY(a, box_export(a->fwd, a->seg_macro, nullptr), "state export");
     }
-    ADJ_CUDA(a, cudaMemcpyAsync(a->seg_macro, src_macro, 6 * fbytes, cudaMemcpyDeviceToDevice, st));
     for (int k = s0; k < s1; ++k) {
         ADJ_TRY(a, lbm_step_replay(a->fwd, 1, &a->sweeps[k], nullptr), "recomputation step");
-        ADJ_TRY(a, fp64_view(a->fwd, &a->view), "state view");
-        double* dst = slot(a->seg_macro, 6 * n, k - s0 + 1);
-        for (int i = 0; i < 6; ++i)
-            ADJ_CUDA(a, cudaMemcpyAsync(slot(dst, n, i), a->view.macro[i], fbytes, cudaMemcpyDeviceToDevice, st));
-        ADJ_CUDA(a, cudaMemcpyAsync(slot(a->seg_h, 15 * n, k - s0), a->view.h_last, 15 * fbytes,
-                                    cudaMemcpyDeviceToDevice, st));
+        ADJ_TRY(a, box_export(a->fwd, slot(a->seg_macro, 6 * n, k - s0 + 1), slot(a->seg_h, 15 * n, k - s0)),
+                "state export");
     }
     ADJ_CUDA(a, cudaStreamSynchronize(st));
     return LBM_OK;
@@ -415,19 +407,11 @@ struct GpuOps {
     lbm_status recompute_from_current(int n)
     {
         const long long nn = a->n;
-        const size_t fbytes = static_cast<size_t>(nn) * sizeof(double);
         cudaStream_t st = a->view.stream;
-        ADJ_TRY(a, fp64_view(a->fwd, &a->view), "state view");
-        for (int i = 0; i < 6; ++i)
-            ADJ_CUDA(a, cudaMemcpyAsync(slot(a->seg_macro, nn, i), a->view.macro[i], fbytes,
-                                        cudaMemcpyDeviceToDevice, st));
+        ADJ_TRY(a, box_export(a->fwd, a->seg_macro, nullptr), "state export");
         ADJ_TRY(a, lbm_step_replay(a->fwd, 1, &a->sweeps[n], nullptr), "recomputation step");
         ++recomputed;
-        ADJ_TRY(a, fp64_view(a->fwd, &a->view), "state view");
-        double* dst = slot(a->seg_macro, 6 * nn, 1);
-        for (int i = 0; i < 6; ++i)
-            ADJ_CUDA(a, cudaMemcpyAsync(slot(dst, nn, i), a->view.macro[i], fbytes, cudaMemcpyDeviceToDevice, st));
-        ADJ_CUDA(a, cudaMemcpyAsync(a->seg_h, a->view.h_last, 15 * fbytes, cudaMemcpyDeviceToDevice, st));
+        ADJ_TRY(a, box_export(a->fwd, slot(a->seg_macro, 6 * nn, 1), a->seg_h), "state export");
         ADJ_CUDA(a, cudaStreamSynchronize(st));
         return LBM_OK;
     }
@@ -444,20 +428,13 @@ struct GpuOps {
             a->bfree.pop_back();
         } else {
             cudaError_t e = cudaSuccess;
-            double* buf = dalloc(36 * static_cast<size_t>(a->n), &e);
+            double* buf = dalloc(a->state_bytes / sizeof(double), &e);
             if (e != cudaSuccess) return afail(a, LBM_ERR_OOM, "binomial checkpoint allocation failed");
             a->bslot.push_back(buf);
             k = static_cast<int>(a->bslot.size()) - 1;
         }
-        const size_t fbytes = static_cast<size_t>(a->n) * sizeof(double);
         cudaStream_t st = a->view.stream;
-        double* c = a->bslot[k];
-        ADJ_TRY(a, fp64_view(a->fwd, &a->view), "state view");
-        ADJ_CUDA(a, cudaMemcpyAsync(c, a->view.f, 15 * fbytes, cudaMemcpyDeviceToDevice, st));
-        ADJ_CUDA(a, cudaMemcpyAsync(slot(c, a->n, 15), a->view.gpop, 15 * fbytes, cudaMemcpyDeviceToDevice, st));
-        for (int i = 0; i < 6; ++i)
-            ADJ_CUDA(a, cudaMemcpyAsync(slot(c, a->n, 30 + i), a->view.macro[i], fbytes, cudaMemcpyDeviceToDevice,
-                                        st));
+        ADJ_TRY(a, box_save_state(a->fwd, a->bslot[k]), "checkpoint save");
         ADJ_CUDA(a, cudaStreamSynchronize(st));
         *out = k;
         return LBM_OK;
@@ -475,10 +452,7 @@ lbm_status restore_state(lbm_adjoint* a, int base)
                 "reload of the initial fields");
         return LBM_OK;
     }
-    double* ck = a->bslot[base];
-    const double* m[6];
-    for (int i = 0; i < 6; ++i) m[i] = slot(ck, n, 30 + i);
-    ADJ_TRY(a, fp64_restore(a->fwd, ck, slot(ck, n, 15), m), "checkpoint restore");
+    ADJ_TRY(a, box_restore_state(a->fwd, a->bslot[base]), "checkpoint restore");
     return LBM_OK;
 }
 
@@ -513,6 +487,7 @@ lbm_status lbm_adjoint_create(const lbm_params* p, int device, const lbm_adjoint
         return LBM_ERR_BAD_ARG;
     }
     if ((cfg->binomial_checkpoints == 0 && cfg->checkpoint_interval < 1) || cfg->binomial_checkpoints < 0 ||
+        (cfg->precision != 0 && cfg->precision != 1) ||
         cfg->check_interval < 1 || !(cfg->tolerance > 0.0) ||
         (cfg->max_sweeps && cfg->max_sweeps % static_cast<uint64_t>(cfg->check_interval) != 0)) {
         g_adj_create_error = "adjoint settings: checkpoint_interval >= 1 (or binomial_checkpoints > 0), "
@@ -523,19 +498,21 @@ lbm_status lbm_adjoint_create(const lbm_params* p, int device, const lbm_adjoint
     a->prm = *p;
     a->cfg = *cfg;
     a->device = device;
-    lbm_status s = lbm_create(p, LBM_PRECISION_FP64, device, &a->fwd);
+    const lbm_precision prec = cfg->precision == 1 ? LBM_PRECISION_MIXED : LBM_PRECISION_FP64;
+    lbm_status s = lbm_create(p, prec, device, &a->fwd);
     if (s != LBM_OK) {
         g_adj_create_error = std::string("forward box: ") + lbm_last_error(nullptr);
         delete a;
         return s;
     }
-    s = fp64_view(a->fwd, &a->view);
+    s = box_info(a->fwd, &a->view);
     if (s != LBM_OK) {
-        g_adj_create_error = "forward box is not FP64";
+        g_adj_create_error = "forward box info";
         free_all(a);
         delete a;
         return s;
     }
+    a->state_bytes = box_state_bytes(a->fwd);
     const long long n = a->view.geom.n;
     a->n = n;
     const size_t K = cfg->binomial_checkpoints > 0 ? 1 : static_cast<size_t>(cfg->checkpoint_interval);
@@ -619,7 +596,7 @@ lbm_status lbm_adjoint_forward(lbm_adjoint* a, const double* phi, const double* 
     const int n_ckpt = (n_steps - 1) / K;
     cudaError_t e = cudaSuccess;
     for (int k = 0; k < n_ckpt; ++k) {
-        double* c = dalloc(36 * static_cast<size_t>(n), &e);
+        double* c = dalloc(a->state_bytes / sizeof(double), &e);
         if (e != cudaSuccess) return afail(a, LBM_ERR_OOM, "checkpoint allocation failed");
         a->ckpt.push_back(c);
     }
@@ -634,20 +611,11 @@ lbm_status lbm_adjoint_forward(lbm_adjoint* a, const double* phi, const double* 
         else ADJ_TRY(a, lbm_step(a->fwd, 1, &stt), "forward step");
         a->sweeps[k] = stt.iterations;
         a->forward_sweeps += stt.iterations;
-        ADJ_TRY(a, fp64_view(a->fwd, &a->view), "state view");
         const int done = k + 1;
-        double* dst = nullptr;
-        if (done < n_steps && done % K == 0) {
-            double* c = a->ckpt[done / K - 1];
-            ADJ_CUDA(a, cudaMemcpyAsync(c, a->view.f, 15 * fbytes, cudaMemcpyDeviceToDevice, st));
-            ADJ_CUDA(a, cudaMemcpyAsync(slot(c, n, 15), a->view.gpop, 15 * fbytes, cudaMemcpyDeviceToDevice, st));
-            dst = slot(c, n, 30);
-        } else if (done == n_steps) {
-            dst = a->final_state;
-        }
-        if (dst)
-            for (int i = 0; i < 6; ++i)
-                ADJ_CUDA(a, cudaMemcpyAsync(slot(dst, n, i), a->view.macro[i], fbytes, cudaMemcpyDeviceToDevice, st));
+        if (done < n_steps && done % K == 0)
+            ADJ_TRY(a, box_save_state(a->fwd, a->ckpt[done / K - 1]), "checkpoint save");
+        else if (done == n_steps)
+            ADJ_TRY(a, box_export(a->fwd, a->final_state, nullptr), "state export");
     }
     ADJ_CUDA(a, cudaStreamSynchronize(st));
     a->n_steps = n_steps;

@@ -491,6 +491,80 @@ void mixed_correct(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geo
     correct_kernel<<<L.grid, L.block, 0, st>>>(g, mb.u, mb.v, mb.w, mb.p, mb.rho);
 }
 
+// Layout of a saved state: f (15 n floats), g (15 n floats), phi, rho, u,
+// v, w (5 n floats), f0 (n doubles), p (n doubles); 8-byte aligned pieces.
+size_t mixed_state_bytes(const Geom& g)
+{
+    const size_t n = static_cast<size_t>(g.n);
+    return (35 * n * sizeof(float) + 7) / 8 * 8 + 2 * n * sizeof(double);
+}
+
+namespace {
+struct StatePieces {
+    float* pop[2];
+    float* macro[5];
+    double* f0;
+    double* p;
+};
+StatePieces state_pieces(void* base, const Geom& g)
+{
+    const size_t n = static_cast<size_t>(g.n);
+    float* f = static_cast<float*>(base);
+    StatePieces s;
+    s.pop[0] = f;
+    s.pop[1] = f + 15 * n;
+    for (int i = 0; i < 5; ++i) s.macro[i] = f + 30 * n + i * n;
+    char* d = static_cast<char*>(base) + (35 * n * sizeof(float) + 7) / 8 * 8;
+    s.f0 = reinterpret_cast<double*>(d);
+    s.p = s.f0 + n;
+    return s;
+}
+}  // namespace
+
+lbm_status mixed_save_state(cudaStream_t st, const MixedBuffers& mb, const Geom& g, int fcur, void* dst)
+{
+    const size_t n = static_cast<size_t>(g.n);
+    const StatePieces s = state_pieces(dst, g);
+    const float* src[5] = {mb.phi, mb.rho, mb.u, mb.v, mb.w};
+    bool ok = cudaMemcpyAsync(s.pop[0], mb.f[fcur], 15 * n * sizeof(float), cudaMemcpyDeviceToDevice, st) ==
+                  cudaSuccess &&
+              cudaMemcpyAsync(s.pop[1], mb.g[fcur], 15 * n * sizeof(float), cudaMemcpyDeviceToDevice, st) ==
+                  cudaSuccess &&
+              cudaMemcpyAsync(s.f0, mb.f0, n * sizeof(double), cudaMemcpyDeviceToDevice, st) == cudaSuccess &&
+              cudaMemcpyAsync(s.p, mb.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st) == cudaSuccess;
+    for (int i = 0; i < 5 && ok; ++i)
+        ok = cudaMemcpyAsync(s.macro[i], src[i], n * sizeof(float), cudaMemcpyDeviceToDevice, st) == cudaSuccess;
+    return ok ? LBM_OK : LBM_ERR_CUDA;
+}
+
+lbm_status mixed_restore_state(cudaStream_t st, MixedBuffers& mb, const Geom& g, int fcur, const void* src)
+{
+    const size_t n = static_cast<size_t>(g.n);
+    const StatePieces s = state_pieces(const_cast<void*>(src), g);
+    float* dst[5] = {mb.phi, mb.rho, mb.u, mb.v, mb.w};
+    bool ok = cudaMemcpyAsync(mb.f[fcur], s.pop[0], 15 * n * sizeof(float), cudaMemcpyDeviceToDevice, st) ==
+                  cudaSuccess &&
+              cudaMemcpyAsync(mb.g[fcur], s.pop[1], 15 * n * sizeof(float), cudaMemcpyDeviceToDevice, st) ==
+                  cudaSuccess &&
+              cudaMemcpyAsync(mb.f0, s.f0, n * sizeof(double), cudaMemcpyDeviceToDevice, st) == cudaSuccess &&
+              cudaMemcpyAsync(mb.p, s.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st) == cudaSuccess;
+    for (int i = 0; i < 5 && ok; ++i)
+        ok = cudaMemcpyAsync(dst[i], s.macro[i], n * sizeof(float), cudaMemcpyDeviceToDevice, st) == cudaSuccess;
+    return ok ? LBM_OK : LBM_ERR_CUDA;
+}
+
+lbm_status mixed_export(cudaStream_t st, const MixedBuffers& mb, const Geom& g, int hbuf, double* macro6,
+                        double* h15)
+{
+    const size_t n = static_cast<size_t>(g.n);
+    const float* src[5] = {mb.phi, mb.rho, mb.u, mb.v, mb.w};
+    for (int i = 0; i < 5; ++i) to_double_kernel<<<1184, 256, 0, st>>>(src[i], macro6 + i * n, g.n);
+    if (cudaMemcpyAsync(macro6 + 5 * n, mb.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        return LBM_ERR_CUDA;
+    if (h15) to_double_kernel<<<1184, 256, 0, st>>>(mb.h[hbuf], h15, 15 * g.n);
+    return cudaGetLastError() == cudaSuccess ? LBM_OK : LBM_ERR_CUDA;
+}
+
 const void* mixed_field_ptr(const MixedBuffers& mb, int which)
 {
     switch (which) {

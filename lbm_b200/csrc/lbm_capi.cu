@@ -806,6 +806,77 @@ lbm_status fp64_restore(lbm_handle* h, const double* f, const double* gpop, cons
     return LBM_OK;
 }
 
+lbm_status box_info(lbm_handle* h, BoxInfo* out)
+{
+    if (check_handle(h) != LBM_OK || !out) return LBM_ERR_BAD_ARG;
+    out->geom = h->geom;
+    out->phys = h->phys;
+    out->L = h->L;
+    out->stream = h->stream;
+    out->precision = h->precision;
+    return LBM_OK;
+}
+
+size_t box_state_bytes(const lbm_handle* h)
+{
+    if (h->precision == LBM_PRECISION_FP64) return 36 * static_cast<size_t>(h->geom.n) * sizeof(double);
+    return mixed_state_bytes(h->geom);
+}
+
+lbm_status box_save_state(lbm_handle* h, void* dst)
+{
+    if (check_handle(h) != LBM_OK || !dst) return LBM_ERR_BAD_ARG;
+    cudaStream_t st = h->stream;
+    if (h->precision != LBM_PRECISION_FP64) {
+        const lbm_status s = mixed_save_state(st, h->mb, h->geom, h->fcur, dst);
+        return s == LBM_OK ? LBM_OK : fail(h, s, "state save failed");
+    }
+    const size_t n = static_cast<size_t>(h->geom.n);
+    const size_t bytes = n * sizeof(double);
+    double* d = static_cast<double*>(dst);
+    LBM_CUDA(h, cudaMemcpyAsync(d, h->b.f[h->fcur], 15 * bytes, cudaMemcpyDeviceToDevice, st));
+    LBM_CUDA(h, cudaMemcpyAsync(d + 15 * n, h->b.g[h->fcur], 15 * bytes, cudaMemcpyDeviceToDevice, st));
+    double* m[6] = {h->b.phi, h->b.rho, h->b.u, h->b.v, h->b.w, h->b.p};
+    for (int i = 0; i < 6; ++i)
+        LBM_CUDA(h, cudaMemcpyAsync(d + (30 + i) * n, m[i], bytes, cudaMemcpyDeviceToDevice, st));
+    return LBM_OK;
+}
+
+lbm_status box_restore_state(lbm_handle* h, const void* src)
+{
+    if (check_handle(h) != LBM_OK || !src) return LBM_ERR_BAD_ARG;
+    if (h->precision == LBM_PRECISION_FP64) {
+        const size_t n = static_cast<size_t>(h->geom.n);
+        const double* d = static_cast<const double*>(src);
+        const double* m[6];
+        for (int i = 0; i < 6; ++i) m[i] = d + (30 + i) * n;
+        return fp64_restore(h, d, d + 15 * n, m);
+    }
+    const lbm_status s = mixed_restore_state(h->stream, h->mb, h->geom, h->fcur, src);
+    if (s != LBM_OK) return fail(h, s, "state restore failed");
+    LBM_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->first_step = false;
+    h->h_loaded = false;
+    return LBM_OK;
+}
+
+lbm_status box_export(lbm_handle* h, double* macro6, double* h15)
+{
+    if (check_handle(h) != LBM_OK || !macro6) return LBM_ERR_BAD_ARG;
+    cudaStream_t st = h->stream;
+    const size_t n = static_cast<size_t>(h->geom.n);
+    if (h->precision != LBM_PRECISION_FP64) {
+        const lbm_status s = mixed_export(st, h->mb, h->geom, h->h_last, macro6, h15);
+        return s == LBM_OK ? LBM_OK : fail(h, s, "state export failed");
+    }
+    double* m[6] = {h->b.phi, h->b.rho, h->b.u, h->b.v, h->b.w, h->b.p};
+    for (int i = 0; i < 6; ++i)
+        LBM_CUDA(h, cudaMemcpyAsync(macro6 + i * n, m[i], n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (h15)
+        LBM_CUDA(h, cudaMemcpyAsync(h15, h->b.h[h->h_last], 15 * n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    return LBM_OK;
+}
+
 }  // namespace lbm
 
 extern "C" {

@@ -44,6 +44,15 @@ lbm_status mixed_prologue(cudaStream_t st, MixedBuffers& mb, const Launch& L, co
 int mixed_segment(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom& g,
                   int start_parity, int n_normal, bool dual, DevState* ds);
 void mixed_correct(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom& g);
+// Saved state of a mixed box (the post-collision populations of buffer fcur,
+// the rest population, the five FP32 macro fields and p): its size in bytes,
+// and the copies in each direction.  Enqueued on st.
+size_t mixed_state_bytes(const Geom& g);
+lbm_status mixed_save_state(cudaStream_t st, const MixedBuffers& mb, const Geom& g, int fcur, void* dst);
+lbm_status mixed_restore_state(cudaStream_t st, MixedBuffers& mb, const Geom& g, int fcur, const void* src);
+// FP64 copies of the six macro fields and (h15 not null) of h buffer hbuf.
+lbm_status mixed_export(cudaStream_t st, const MixedBuffers& mb, const Geom& g, int hbuf, double* macro6,
+                        double* h15);
 // Device pointer of a field: float for phi..w, double for p.
 const void* mixed_field_ptr(const MixedBuffers& mb, int which);
 

@@ -25,7 +25,7 @@ def test_nm_lists_exports_as_c_symbols():
 
 def test_status_strings_and_version():
     lib = L.load_library()
-    assert lib.lbm_abi_version() == L.ABI_VERSION == 5
+    assert lib.lbm_abi_version() == L.ABI_VERSION == 6
     for s in range(9):
         assert lib.lbm_status_string(s)
 

@@ -208,3 +208,28 @@ def test_nonfinite_adjoint_rhs_is_an_error(krylov):
         a.backward({"p": lam_p})
     assert e.value.status == 2, str(e.value)
     a.close()
+
+
+def test_mixed_forward_adjoint_against_fp64_fd(run):
+    """The adjoint run over the mixed box (FP32 populations; the reverse pass
+    differentiates the FP64 step at the mixed forward's states): dJ/dk_f and
+    dJ/dphi_0 along a seeded direction against centred finite differences of
+    the FP64 forward (replayed sweep counts).  The gradient carries the mixed
+    forward's error, so the bar is 1e-4 relative instead of the FP64 run's
+    1e-6; the measured errors are printed."""
+    p, f, obj, y, sweeps, grads, stats, a = run
+    m = L.Adjoint(p, checkpoint_interval=KINT, check_interval=50, tolerance=1e-13, max_sweeps=2000000,
+                  precision="mixed")
+    poisson(m)
+    m.forward(f, STEPS, sweeps)
+    assert m.sweeps() == sweeps
+    ym = {k: m.download(k) for k in L.FIELDS}
+    gm, sm = m.backward(obj.adjoint(ym))
+    m.close()
+    fd_kf = fd(p, f, obj, sweeps, kf=True)
+    d = np.random.default_rng(1).standard_normal(f["phi"].shape)
+    fd_phi = fd(p, f, obj, sweeps, field="phi", d=d)
+    e_kf = abs(sm["grad_kappa_f"] - fd_kf) / abs(fd_kf)
+    e_phi = abs(float(np.sum(gm["phi"] * d)) - fd_phi) / abs(fd_phi)
+    print(f"\nmixed-forward adjoint vs FP64 FD: k_f {e_kf:.3e}, phi_0 {e_phi:.3e}")
+    assert e_kf <= 1e-4 and e_phi <= 1e-4, (e_kf, e_phi)
