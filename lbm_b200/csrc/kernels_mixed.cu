@@ -179,7 +179,8 @@ sweep_kernel64(Geom g, const float* __restrict__ hin, float* __restrict__ hout,
     float hv[Q];
     pull_regs(hv, hin, g, x, y, z);
     bounce_regs(hv, g, x);
-    collide_h_store(hv, (double)sum_q32(hv), __ldg(omega + c), __ldg(s + c), hout, g.n, c);
+    const P32 ps = sum_q32(hv);
+    collide_h_store(hv, (double)ps.hi + (double)ps.lo, __ldg(omega + c), __ldg(s + c), hout, g.n, c);
 }
 
 // Two sweeps in one pass (temporal blocking, sweep2_run in mixed_cells.cuh):

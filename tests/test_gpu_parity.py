@@ -258,7 +258,7 @@ def test_fp64_two_sweep_pass_is_bitwise(zlen, periodic, monkeypatch):
     """The FP64 temporally blocked pass (two sweeps per launch) keeps every
     cell's arithmetic, so it reproduces single-sweep launches bit for bit
     (slip walls and periodic x)."""
-    p, f = laplace_case((64, 12, 20), DD=8.0, noise=1e-4)
+    p, f = laplace_case((64, 16, 20), DD=8.0, noise=1e-4)
     p.periodic_x = periodic
     f["w"] = 0.01 * np.sin(2 * np.pi * np.arange(20) / 20)[:, None, None] * np.ones_like(f["w"])
     monkeypatch.setenv("LBM_SWEEP2_ZLEN", "0")
