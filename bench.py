@@ -928,8 +928,10 @@ def run_ours(args):
             line["mixed"] = {k: m[k] for k in ("value", "ms_per_step", "sweeps_per_step", "converged_steps",
                                                "roofline", "clocks", "phase_ms_per_step")}
             line["mixed"]["dtype"] = "f32 populations + f64 pressure sums/reductions"
-            line["mixed"]["stated_error"] = ("<= 1e-5 norm-wise relative error in phi, rho, u, v, w vs the "
-                                             "FP64 oracle on equal sweep counts (tests/test_gpu_mixed.py)")
+            line["mixed"]["stated_error"] = ("<= 1e-5 norm-wise relative error in phi, rho, u, v, w and p vs "
+                                             "the FP64 oracle on equal sweep counts, sum(phi) conserved to "
+                                             "1e-12 on periodic boxes (tests/test_gpu_mixed.py, "
+                                             "tests/test_gpu_parity_large.py)")
             line["speedup_mixed_vs_fp64"] = m["value"] / head["value"]
             if world == 1 and not args.no_accuracy:
                 try:
