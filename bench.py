@@ -208,6 +208,46 @@ def coalescence_workload(n=256, R=28.0, side=60.0, speed=0.01, ratio=1000.0, kf=
     return p, {"phi": phi, "rho": rho, "u": u, "v": v, "w": np.zeros_like(phi), "p": np.zeros_like(phi)}
 
 
+def coalescence_workload(n=256, R=28.0, side=60.0, speed=0.01, ratio=1000.0, kf=0.06, seed=4242, noise=1e-4):
+    """Three-droplet coalescence: an n^3 periodic box, three drops of radius R
+    centred on an equilateral triangle of side `side` in the plane z = n/2
+    (centroid at the box centre), each moving towards the centroid at
+    `speed`; rho_L/rho_G = ratio (rho_G = 1), mu = 0.1 rho, kappa_f = kf,
+    otherwise the Laplace-test physics (a = 1, b = 6.7, T = 0.035,
+    kappa_g = 6e-6, tau = 1, tanh interfaces W = 4, seeded phi noise).  Each
+    drop's profile is phi = phi_min + (phi_max - phi_min) * 0.5 (1 - tanh(2 (r
+    - R) / W)); where profiles overlap the largest is kept, and the velocity is
+    that of the drop whose profile is kept, scaled by it.  Built here: the
+    reference's initializer makes one or two drops on the z axis.  Returns
+    (params, fields)."""
+    import lbm_b200 as L
+    p = L.make_params(lx=n, ly=n, lz=n, rho_L=ratio, rho_G=1.0, mu_L=0.1 * ratio, mu_G=0.1, tauf=1.0, taug=1.0,
+                      k_f=kf, k_g=6e-6, T=0.035, a=1.0, b=6.7, DD=2.0 * R, init_single_droplet=1, init_tanh=1,
+                      interface_width=2.0, init_velocity=0.0, periodic_x=1)
+    c = (n - 1) / 2.0
+    rc = side / np.sqrt(3.0)             # centroid-to-vertex distance
+    centres = [(c + rc * np.cos(a), c + rc * np.sin(a), c) for a in (np.pi / 2, np.pi / 2 + 2 * np.pi / 3,
+                                                                        np.pi / 2 + 4 * np.pi / 3)]
+    frac = np.zeros((n, n, n))
+    u = np.zeros((n, n, n))
+    v = np.zeros((n, n, n))
+    x = np.arange(n, dtype=np.float64)
+    for cx_, cy_, cz_ in centres:
+        r = np.sqrt((x[None, None, :] - cx_) ** 2 + (x[None, :, None] - cy_) ** 2 + (x[:, None, None] - cz_) ** 2)
+        fr = 0.5 * (1.0 - np.tanh(2.0 * (r - R) / 4.0))
+        take = fr > frac
+        dx, dy = c - cx_, c - cy_
+        norm = np.hypot(dx, dy)
+        u = np.where(take, speed * dx / norm * fr, u)
+        v = np.where(take, speed * dy / norm * fr, v)
+        frac = np.maximum(frac, fr)
+        del r, fr, take
+    rng = np.random.default_rng(seed)
+    phi = p.fei_min + frac * (p.fei_max - p.fei_min) + rng.uniform(-noise, noise, size=frac.shape)
+    rho = p.rho_G + frac * (p.rho_L - p.rho_G)
+    return p, {"phi": phi, "rho": rho, "u": u, "v": v, "w": np.zeros_like(phi), "p": np.zeros_like(phi)}
+
+
 def adjoint_workload(n=64, e=0.0, kf_scale=1.0, seed=31, noise=1e-4):
     """Adjoint calibration box: n^3 periodic, one drop R = n/4 at the centre
     (semi-axes R(1+e), R, R/(1+e); e = 0 a sphere), tanh interface W = 4,
@@ -791,6 +831,99 @@ def adjoint_measure(args):
     return line
 
 
+def run_coalescence_adjoint(args):
+    """Bounded sample of the large adjoint configuration: the three-drop
+    coalescence (coalescence_workload, rho_L/rho_G = 1000) on an n^3 periodic
+    box, a forward run of K steps over the mixed box (FP32 populations, FP64
+    rest population, pressure and reductions; lbm_adjoint_cfg.precision = 1)
+    with binomial checkpointing, and its reverse pass (BiCGSTAB adjoint
+    Poisson solves), for each of --coalescence-samples kappa_f values drawn
+    uniformly from [0.04, 0.08].  Objective J = 0.5 sum (phi_T - phi_target)^2,
+    phi_target the final phi of the first sample's forward run with kappa_f
+    + 5 %.  Reported: MLUPS (sweeps counted) of forward and reverse, the
+    reverse/forward time ratio, the device memory in use after the reverse
+    pass (its checkpoint slots are still held), the binomial schedule's
+    recomputation, and for the first sample dJ/dk_f against a centred finite
+    difference of the FP64 forward (replayed sweep counts)."""
+    import torch
+    import lbm_b200 as L
+    n, K = args.size, args.steps
+    rng = np.random.default_rng(77)
+    kfs = [float(k) for k in rng.uniform(0.04, 0.08, size=args.coalescence_samples)]
+    slots = args.binomial_slots
+    tol_f = args.adjoint_forward_tol
+    free0, total = torch.cuda.mem_get_info()
+    out = {"metric": "MLUPS (sweeps counted) of the coalescence adjoint sample (forward + reverse)", "unit": "MLUPS",
+           "n_gpus": 1, "steps": K, "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32 populations + f64 pressure/reductions (forward); f64 adjoint",
+           "data": "synthetic (three seeded tanh drops, rho ratio 1000, phi noise 1e-4)",
+           "config": {"workload": f"three-drop coalescence {n}^3 periodic, R=28, triangle side 60 in z=n/2, "
+                                  f"approach 0.01, rho_L/rho_G=1000; {K} of 5000 steps (bounded sample)",
+                      "kappa_f": kfs, "binomial_checkpoints": slots,
+                      "poisson": {"forward_tolerance": tol_f, "adjoint_solver": "BiCGSTAB",
+                                  "adjoint_krylov_tolerance": args.adjoint_krylov_tol}},
+           "samples": []}
+    target = None
+    for i, kf in enumerate(kfs):
+        p, f = coalescence_workload(n, kf=kf)
+        if target is None:
+            pt, ft = coalescence_workload(n, kf=kf * 1.05)
+            a = L.Adjoint(pt, binomial_checkpoints=slots, check_interval=100, tolerance=1e-13, krylov=True,
+                          krylov_tolerance=args.adjoint_krylov_tol, precision="mixed")
+            a.set_poisson(check_interval=100, tolerance=tol_f, max_sweeps=args.max_sweeps, fail_on_limit=1)
+            a.forward(ft, K)
+            target = a.download("phi")
+            a.close()
+            del pt, ft
+        a = L.Adjoint(p, binomial_checkpoints=slots, check_interval=100, tolerance=1e-13, krylov=True,
+                      krylov_tolerance=args.adjoint_krylov_tol, precision="mixed")
+        a.set_poisson(check_interval=100, tolerance=tol_f, max_sweeps=args.max_sweeps, fail_on_limit=1)
+        a.forward(f, K)
+        phi_T = a.download("phi")
+        grads, st = a.backward({"phi": phi_T - target})
+        free1, _ = torch.cuda.mem_get_info()
+        sweeps = a.sweeps()
+        a.close()
+        cells = float(n) ** 3
+        fwd_s, bwd_s = st["forward_ms"] / 1e3, st["backward_ms"] / 1e3
+        fwd_updates = cells * (K + st["forward_sweeps"])
+        bwd_updates = cells * (2 * st["recompute_steps"] + st["forward_sweeps"] + st["adjoint_sweeps"])
+        rec = {"kappa_f": kf, "forward_mlups": fwd_updates / fwd_s / 1e6, "reverse_mlups": bwd_updates / bwd_s / 1e6,
+               "adjoint_forward_time_ratio": bwd_s / fwd_s, "forward_ms": st["forward_ms"],
+               "backward_ms": st["backward_ms"], "forward_sweeps_per_step": st["forward_sweeps"] / K,
+               "adjoint_matvecs_per_step": st["adjoint_sweeps"] / K, "recompute_steps": st["recompute_steps"],
+               "device_gb_in_use_after_reverse": (total - free1) / 1e9, "grad_kappa_f": st["grad_kappa_f"],
+               "objective": 0.5 * float(np.sum((phi_T - target) ** 2))}
+        if i == 0 and args.coalescence_fd:
+            h = 1e-6 * kf
+            vals = []
+            for sgn in (1.0, -1.0):
+                pp, ff = coalescence_workload(n, kf=kf + sgn * h)
+                b = L.InamuroCUDA(pp, ff, precision="fp64")
+                b.set_poisson(check_interval=100, tolerance=tol_f, max_sweeps=args.max_sweeps)
+                b.step_replay(sweeps)
+                vals.append(0.5 * float(np.sum((b.download("phi") - target) ** 2)))
+                b.close()
+                del pp, ff
+            fd = (vals[0] - vals[1]) / (2 * h)
+            rec["fd_kappa_f_fp64"] = fd
+            rec["rel_err_vs_fp64_fd"] = abs(st["grad_kappa_f"] - fd) / abs(fd)
+        out["samples"].append(rec)
+        print(json.dumps({"sample": i, **rec}), flush=True)
+        del p, f, grads
+    tot_f = sum(s["forward_ms"] for s in out["samples"])
+    tot_b = sum(s["backward_ms"] for s in out["samples"])
+    cells = float(n) ** 3
+    upd = sum(cells * (K + s["forward_sweeps_per_step"] * K) for s in out["samples"])
+    out["value"] = None
+    out["forward_mlups_mean"] = float(np.mean([s["forward_mlups"] for s in out["samples"]]))
+    out["adjoint_forward_time_ratio"] = tot_b / tot_f
+    out["ms_per_step"] = (tot_f + tot_b) / K / len(kfs)
+    out["device_gb_before"] = (total - free0) / 1e9
+    print(json.dumps(out))
+    return 0
+
+
 def run_poisson_forms(args):
     """The head-on workload in FP64 with each Poisson form (kinetic: the
     production solve; scalar: the reference's scalar Jacobi form; scalar-rb:
@@ -1031,7 +1164,8 @@ def main(argv=None):
                     help="time the non-Poisson kernels per step with --phase-sweeps sweeps per step")
     ap.add_argument("--phase-sweeps", type=int, default=100)
     ap.add_argument("--krylov-tol", type=float, default=1e-10, help="tolerance of the krylov workload")
-    ap.add_argument("--workload", choices=("headon", "batch", "adjoint", "poisson-forms", "krylov"), default="headon",
+    ap.add_argument("--workload", choices=("headon", "batch", "adjoint", "poisson-forms", "krylov",
+                                           "coalescence-adjoint"), default="headon",
                     help="batch: the batched droplet oscillation (64 uneven boxes, mixed precision); "
                          "adjoint: the adjoint calibration run (FP64, 64^3), --steps forward steps")
     ap.add_argument("--adjoint-size", type=int, default=64)
@@ -1043,6 +1177,12 @@ def main(argv=None):
     ap.add_argument("--adjoint-krylov-tol", type=float, default=1e-11)
     ap.add_argument("--adjoint-directions", type=int, default=2,
                     help="seeded random phi_0 directions checked by finite differences")
+    ap.add_argument("--coalescence-samples", type=int, default=8,
+                    help="coalescence-adjoint workload: kappa_f samples (uniform in [0.04, 0.08])")
+    ap.add_argument("--binomial-slots", type=int, default=25,
+                    help="coalescence-adjoint workload: binomial checkpoint slots")
+    ap.add_argument("--coalescence-fd", action="store_true",
+                    help="coalescence-adjoint workload: finite-difference check of dJ/dk_f (FP64 forward)")
     ap.add_argument("--batch-instances", type=int, default=64)
     ap.add_argument("--batch-seed", type=int, default=2024)
     args = ap.parse_args(argv)
@@ -1054,6 +1194,8 @@ def main(argv=None):
         return run_batch(args)
     if args.workload == "adjoint":
         return run_adjoint(args)
+    if args.workload == "coalescence-adjoint":
+        return run_coalescence_adjoint(args)
     if args.workload == "poisson-forms":
         return run_poisson_forms(args)
     if args.workload == "krylov":
