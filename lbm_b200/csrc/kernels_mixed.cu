@@ -190,10 +190,7 @@ sweep_kernel64(Geom g, const float* __restrict__ hin, float* __restrict__ hout,
 // Requires lx % 32 == 0, ly % 8 == 0 and 15 n < 2^31 (the launcher checks).
 constexpr int S2_TX = 32, S2_TY = 8;
 constexpr int S2_THREADS = sweep2_threads(S2_TX, S2_TY);   // 352: one thread per region cell
-#ifndef LBM_SWEEP2_ASYNC
-#define LBM_SWEEP2_ASYNC 0
-#endif
-constexpr int S2_SMEM = LBM_SWEEP2_ASYNC ? sweep2_async_smem<S2_TX, S2_TY>() : sweep2_smem(S2_TX, S2_TY);
+constexpr int S2_SMEM = sweep2_smem(S2_TX, S2_TY);
 
 __global__ void __launch_bounds__(S2_THREADS, 2)
 sweep2_kernel(Geom g, int zlen, const float* __restrict__ hin, float* __restrict__ hout,
@@ -201,13 +198,8 @@ sweep2_kernel(Geom g, int zlen, const float* __restrict__ hin, float* __restrict
 {
     extern __shared__ float ring[];
     const int z0 = blockIdx.z * zlen;
-#if LBM_SWEEP2_ASYNC
-    sweep2_run_async<S2_TX, S2_TY>(g, blockIdx.x * S2_TX, blockIdx.y * S2_TY, z0, min(z0 + zlen, g.lz), hin, hout,
-                                   omega, s, ring);
-#else
     sweep2_run<S2_TX, S2_TY>(g, blockIdx.x * S2_TX, blockIdx.y * S2_TY, z0, min(z0 + zlen, g.lz), hin, hout, omega,
                              s, ring);
-#endif
 }
 
 __global__ void __launch_bounds__(256)

@@ -560,102 +560,6 @@ __device__ __forceinline__ void sweep2_run(const Geom& g, int x0, int y0, int z0
     }
 }
 
-// The same two sweeps with sweep k's pulls brought in by cp.async two planes
-// ahead, into a per-thread staging area behind the ring (17 floats per region
-// cell and plane: 15 populations, omega, s; two plane slots), instead of
-// registers: more loads in flight per thread, fewer live registers.  Each
-// thread reads back only what it copied itself, after its own wait, so the
-// staging needs no barrier.
-template <int TX, int TY>
-__host__ __device__ constexpr int sweep2_async_smem()
-{
-    return (ring_planes() + 2 * 17) * (TX + 2) * (TY + 2) * static_cast<int>(sizeof(float));
-}
-
-template <int N>
-__device__ __forceinline__ void cp_async_wait_group()
-{
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
-template <int TX, int TY>
-__device__ __forceinline__ void sweep2_run_async(const Geom& g, int x0, int y0, int z0, int z1,
-                                                 const float* __restrict__ hin, float* __restrict__ hout,
-                                                 const float* __restrict__ omega, const float* __restrict__ s,
-                                                 float* __restrict__ ring)
-{
-    constexpr int RX = TX + 2, RC = RX * (TY + 2);
-    float* stage = ring + ring_planes() * RC;   // [2][17][RC]
-    const int t = threadIdx.x;
-    const int n = (int)g.n;
-    const bool owner = t < RC;
-    const int xw = (x0 - 1 + t % RX + g.lx) % g.lx;
-    const int yw = (y0 - 1 + t / RX + g.ly) % g.ly;
-    const Wrap wr(g, xw, yw, 0);
-
-    auto prefetch = [&](int zz) {        // sweep k's pulls for plane zz into its staging slot
-        if (owner) {
-            const int zw = zz < 0 ? zz + g.lz : (zz >= g.lz ? zz - g.lz : zz);
-            const int zm = zw == 0 ? g.lz - 1 : zw - 1, zp = zw == g.lz - 1 ? 0 : zw + 1;
-            float* st = stage + (zz & 1) * (17 * RC) + t;
-            static_for<0, Q>([&](auto qc) {
-                constexpr int q = decltype(qc)::value;
-                const int idx = (pick<-cz(q)>(zm, zw, zp) * g.ly + pick<-cy(q)>(wr.ym, yw, wr.yp)) * g.lx +
-                                pick<-cx(q)>(wr.xm, xw, wr.xp);
-                cp_async_elem(st + q * RC, hin + static_cast<unsigned>(q * n + idx));
-            });
-            const int c = (zw * g.ly + yw) * g.lx + xw;
-            cp_async_elem(st + 15 * RC, omega + c);
-            cp_async_elem(st + 16 * RC, s + c);
-        }
-        cp_async_commit();   // one group per plane on every thread, empty or not
-    };
-    auto finish = [&](int zz) {          // complete sweep k on plane zz into the ring
-        if (!owner) return;
-        const float* st = stage + (zz & 1) * (17 * RC) + t;
-        float a[Q];
-        static_for<0, Q>([&](auto qc) { a[decltype(qc)::value] = st[decltype(qc)::value * RC]; });
-        const float a_om = st[15 * RC], a_s = st[16 * RC];
-        bounce_regs(a, g, xw);
-        const P32 p32 = sum_q32(a);
-        static_for<0, Q>([&](auto qc) {
-            constexpr int q = decltype(qc)::value;
-            ring[ring_plane<q>(zz) * RC + t] = collide_h<q>(a[q], p32, a_om, a_s);
-        });
-    };
-
-    prefetch(z0 - 1);
-    prefetch(z0);
-    cp_async_wait_group<1>();
-    finish(z0 - 1);
-    prefetch(z0 + 1);
-    cp_async_wait_group<1>();
-    finish(z0);
-    prefetch(z0 + 2);
-    const int tx = t % TX, ty = t / TX;
-    const int x = x0 + tx, y = y0 + ty;
-    const int rc = (ty + 1) * RX + (tx + 1);
-    const bool inner = t < TX * TY && x < g.lx && y < g.ly;
-    for (int z = z0; z < z1; ++z) {
-        cp_async_wait_group<1>();        // plane z+1 has landed (z+2 may still be in flight)
-        finish(z + 1);
-        if (z + 3 <= z1) prefetch(z + 3);
-        else cp_async_commit();
-        __syncthreads();
-        if (inner) {
-            float hv[Q];
-            static_for<0, Q>([&](auto qc) {
-                constexpr int q = decltype(qc)::value;
-                hv[q] = ring[ring_plane<q>(z - cz(q)) * RC + rc - cy(q) * RX - cx(q)];
-            });
-            bounce_regs(hv, g, x);
-            const int c = (z * g.ly + y) * g.lx + x;
-            collide_h_store32(hv, sum_q32(hv), __ldg(omega + c), __ldg(s + c), hout, n, c);
-        }
-    }
-    cp_async_wait_group<0>();
-}
-
 MixPhys mix_phys(const Phys& P)
 {
     MixPhys M;

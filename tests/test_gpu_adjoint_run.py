@@ -215,8 +215,9 @@ def test_mixed_forward_adjoint_against_fp64_fd(run):
     differentiates the FP64 step at the mixed forward's states): dJ/dk_f and
     dJ/dphi_0 along a seeded direction against centred finite differences of
     the FP64 forward (replayed sweep counts).  The gradient carries the mixed
-    forward's error, so the bar is 1e-4 relative instead of the FP64 run's
-    1e-6; the measured errors are printed."""
+    forward's error, so the bar is 1e-5 relative instead of the FP64 run's
+    1e-6 (measured: 6.8e-7 along k_f, 3.2e-8 along phi_0); the errors are
+    printed."""
     p, f, obj, y, sweeps, grads, stats, a = run
     m = L.Adjoint(p, checkpoint_interval=KINT, check_interval=50, tolerance=1e-13, max_sweeps=2000000,
                   precision="mixed")
@@ -232,4 +233,4 @@ def test_mixed_forward_adjoint_against_fp64_fd(run):
     e_kf = abs(sm["grad_kappa_f"] - fd_kf) / abs(fd_kf)
     e_phi = abs(float(np.sum(gm["phi"] * d)) - fd_phi) / abs(fd_phi)
     print(f"\nmixed-forward adjoint vs FP64 FD: k_f {e_kf:.3e}, phi_0 {e_phi:.3e}")
-    assert e_kf <= 1e-4 and e_phi <= 1e-4, (e_kf, e_phi)
+    assert e_kf <= 1e-5 and e_phi <= 1e-5, (e_kf, e_phi)
