@@ -30,6 +30,7 @@
 
 #include "Inamuro.hpp"
 #include "lbm_b200.h"
+#include "lbm_b200_diagnostics.hpp"
 
 class InamuroCUDA
 {
@@ -136,7 +137,7 @@ public:
             onepass_ = o.onepass_;
             acc_ = o.acc_;
             diag_ = o.diag_;
-            csv_path_ = o.csv_path_;
+            csv_ = o.csv_;
             if (h_) lbm_set_check_callback(h_, &InamuroCUDA::onCheck, this);
         }
         return *this;
@@ -322,19 +323,7 @@ public:
         applyPoissonConfig();
     }
     // Per-check CSV, same header and columns as GPU/InamuroCUDA.cu:2610-2682.
-    void setPoissonDiagnosticsPath(const std::string& path)
-    {
-        csv_path_ = path;
-        if (path.empty()) return;
-        std::ofstream out(path);
-        if (!out) throw std::runtime_error("failed to open Poisson diagnostics CSV: " + path);
-        out << "step,iteration,pressure_l1_delta,pressure_l1_norm,relative_error,"
-            << "fixed_point_h_l1,fixed_point_h_scale,fixed_point_h_relative,"
-            << "fixed_point_p_l1,fixed_point_p_scale,fixed_point_p_relative,"
-            << "fixed_point_relative,fixed_point_evaluated,pressure_converged,fixed_point_converged,"
-            << "dual_residual_enabled,converged,block_low_frequency_fraction,"
-            << "block_size,block_count\n";
-    }
+    void setPoissonDiagnosticsPath(const std::string& path) { csv_.open(path); }
 
     void printPerformanceMetrics() const
     {
@@ -401,7 +390,7 @@ private:
     bool onepass_ = false;
     lbm_poisson_accel acc_{1.0, 1.0, 0, 1.0, 0, 0.5, 0, 1.0, 0};
     PoissonStepDiagnostics diag_;
-    std::string csv_path_;
+    lbm_b200::PoissonCsv csv_;   // per-check CSV (setPoissonDiagnosticsPath)
 
     void release()
     {
@@ -449,22 +438,6 @@ private:
 
     static void onCheck(void* user, const lbm_check_record* r)
     {
-        const InamuroCUDA* self = static_cast<const InamuroCUDA*>(user);
-        if (self->csv_path_.empty()) return;
-        std::ofstream out(self->csv_path_, std::ios::app);
-        if (!out) return;
-        out << r->step << ',' << r->iteration << ',' << std::setprecision(17) << r->pressure_l1_delta << ','
-            << r->pressure_l1_norm << ',' << r->relative_error << ',';
-        const double opt[7] = {r->fixed_point_h_l1, r->fixed_point_h_scale, r->fixed_point_h_relative,
-                               r->fixed_point_p_l1, r->fixed_point_p_scale, r->fixed_point_p_relative,
-                               r->fixed_point_relative};
-        for (double v : opt) {
-            if (std::isfinite(v)) out << v;
-            out << ',';
-        }
-        out << r->fixed_point_evaluated << ',' << r->pressure_converged << ',' << r->fixed_point_converged << ','
-            << r->dual_residual_enabled << ',' << r->converged << ',';
-        if (std::isfinite(r->block_low_frequency_fraction)) out << r->block_low_frequency_fraction;
-        out << ',' << r->spatial_block_size << ',' << r->spatial_block_count << '\n';
+        lbm_b200::PoissonCsv::on_check(&static_cast<InamuroCUDA*>(user)->csv_, r);
     }
 };

@@ -9,6 +9,7 @@
 // CPU/Inamuro.cpp:412-507), computed on the device.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 #include <fstream>
 #include <iomanip>
@@ -70,6 +71,66 @@ public:
 
 private:
     std::ofstream out_;
+};
+
+// The per-check Poisson CSV of the reference's GPU program
+// (setPoissonDiagnosticsPath, GPU/InamuroCUDA.cu:2610-2682): its header and
+// one row per convergence check, fed by lbm_set_check_callback.  Usable with
+// any handle of the C ABI:
+//   lbm_b200::PoissonCsv csv("poisson.csv");
+//   lbm_set_check_callback(h, &lbm_b200::PoissonCsv::on_check, &csv);
+// Columns that a check did not evaluate (NaN in the record) are left empty,
+// as the reference leaves them.
+class PoissonCsv {
+public:
+    PoissonCsv() = default;
+    explicit PoissonCsv(const std::string& path) { open(path); }
+
+    // Creates (truncates) the file and writes the header; "" disables.
+    void open(const std::string& path)
+    {
+        path_ = path;
+        if (path.empty()) return;
+        std::ofstream out(path);
+        if (!out) throw std::runtime_error("failed to open Poisson diagnostics CSV: " + path);
+        out << "step,iteration,pressure_l1_delta,pressure_l1_norm,relative_error,"
+            << "fixed_point_h_l1,fixed_point_h_scale,fixed_point_h_relative,"
+            << "fixed_point_p_l1,fixed_point_p_scale,fixed_point_p_relative,"
+            << "fixed_point_relative,fixed_point_evaluated,pressure_converged,fixed_point_converged,"
+            << "dual_residual_enabled,converged,block_low_frequency_fraction,"
+            << "block_size,block_count\n";
+    }
+    const std::string& path() const { return path_; }
+
+    // Appends one check row.
+    void append(const lbm_check_record& r) const
+    {
+        if (path_.empty()) return;
+        std::ofstream out(path_, std::ios::app);
+        if (!out) return;
+        out << r.step << ',' << r.iteration << ',' << std::setprecision(17) << r.pressure_l1_delta << ','
+            << r.pressure_l1_norm << ',' << r.relative_error << ',';
+        const double opt[7] = {r.fixed_point_h_l1, r.fixed_point_h_scale, r.fixed_point_h_relative,
+                               r.fixed_point_p_l1, r.fixed_point_p_scale, r.fixed_point_p_relative,
+                               r.fixed_point_relative};
+        for (double v : opt) {
+            if (std::isfinite(v)) out << v;
+            out << ',';
+        }
+        out << r.fixed_point_evaluated << ',' << r.pressure_converged << ',' << r.fixed_point_converged << ','
+            << r.dual_residual_enabled << ',' << r.converged << ',';
+        if (std::isfinite(r.block_low_frequency_fraction)) out << r.block_low_frequency_fraction;
+        out << ',' << r.spatial_block_size << ',' << r.spatial_block_count << '\n';
+    }
+
+    // lbm_check_callback adaptor: user is the PoissonCsv.
+    static void on_check(void* user, const lbm_check_record* r)
+    {
+        if (user && r) static_cast<const PoissonCsv*>(user)->append(*r);
+    }
+
+private:
+    std::string path_;
 };
 
 }  // namespace lbm_b200

@@ -14,6 +14,9 @@
 //           Writes DIR/init.bin, DIR/step%04d.bin (phi rho u v w p, N doubles
 //           each, x fastest, no ghost layers) and DIR/summary.txt
 //           ("step sweeps ms" per line).
+//   tecplot: --params F --tecplot DIR --init FIELDS.bin
+//           Writes the reference's own Tecplot binary file of the loaded
+//           fields (Inamuro::writeTecplotBinary, step 0) into DIR.
 //   sample: --params F --sample-sweeps K --out DIR [--init FIELDS.bin] [--sample-reps R]
 //           [--nonpoisson-reps M]
 //           R times (default 1): times one non-Poisson step part (collision,
@@ -85,6 +88,14 @@ public:
         writeRaw(path, buf);
     }
 
+    void writeTecplot(const std::string& dir)
+    {
+        OutputConfig oc = getOutputConfig();
+        oc.output_dir = dir + "/";
+        setOutputConfig(oc);
+        writeTecplotBinary(0);
+    }
+
     std::uint64_t lastSweeps() const { return getLastPressureSolveDiagnostics().iteration_count; }
 
     // One non-Poisson part of performTimeStep (CPU/Inamuro.cpp:350-355).
@@ -135,6 +146,7 @@ int main(int argc, char** argv)
     long sample_sweeps = -1;
     int sample_reps = 1;
     int nonpoisson_reps = -1;
+    std::string tecplot_dir;
     bool dump_h = false;
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
@@ -149,11 +161,23 @@ int main(int argc, char** argv)
         else if (a == "--sample-sweeps") sample_sweeps = std::stol(val());
         else if (a == "--sample-reps") sample_reps = std::stoi(val());
         else if (a == "--nonpoisson-reps") nonpoisson_reps = std::stoi(val());
+        else if (a == "--tecplot") tecplot_dir = val();
         else if (a == "--dump-h") dump_h = true;
         else {
             std::cerr << "unknown argument " << a << "\n";
             return 2;
         }
+    }
+    if (!params.empty() && !tecplot_dir.empty()) {
+        try {
+            Harness h(params);
+            if (!init.empty()) h.loadFields(readRaw(init, 6 * h.cells()));
+            h.writeTecplot(tecplot_dir);
+        } catch (const std::exception& e) {
+            std::cerr << "ref_cpu_harness error: " << e.what() << "\n";
+            return 1;
+        }
+        return 0;
     }
     if (params.empty() || out.empty()) {
         std::cerr << "usage: ref_cpu_harness --params F --out DIR (--steps S | --sample-sweeps K) [--init B]\n";
