@@ -388,14 +388,13 @@ def cpu_baseline_entry(n, reps_out, cells, wall, sweeps_per_step, sample_sweeps,
 
 
 # ---------------------------------------------------------------- reference GPU
-def _program_run(exe, d, pf, steps, limit, timeout):
+def _program_run(exe, d, pf, steps, timeout):
     """One run of a GPU/main.cpp front end (the reference's own program or the
     same main.cpp over this library): wall ms of its step loop (its
     wall_total_ms) and the sweeps of each step (its Poisson CSV)."""
     os.makedirs(d)
     cmd = [exe, "--mode", "gpu", "--params", pf, "--steps", str(steps), "--poisson", "split",
-           "--poisson-check-interval", "100", "--poisson-tolerance", "1e-3",
-           "--poisson-iteration-limit", str(limit), "--poisson-diagnostics", "diag.csv", "--no-roofline"]
+           "--poisson-diagnostics", "diag.csv", "--no-roofline"]
     r = subprocess.run(cmd, cwd=d, capture_output=True, text=True, timeout=timeout)
     if r.returncode != 0:
         raise RuntimeError(f"{os.path.basename(exe)} exited {r.returncode}: {(r.stdout + r.stderr)[-300:]}")
@@ -413,17 +412,15 @@ def _program_run(exe, d, pf, steps, limit, timeout):
     return ms, [sweeps[s] for s in sorted(sweeps)]
 
 
-def reference_gpu_leg(n=N_SIDE, steps=3, limit=3000, timeout=900):
+def reference_gpu_leg(n=N_SIDE, steps=1, timeout=900):
     """The reference's own FP64 GPU step (GPU/InamuroCUDA.cu, compiled from its
     unmodified sources for sm_100a: oracle/_ref/lbm_gpu_ref) beside this
     library behind the same front end (the reference's GPU/main.cpp over
     include/InamuroCUDA.hpp: oracle/_ref/lbm_gpu_dropin), on the same
     noise-free head-on params.in (the reference's own initial condition), the
-    split kinetic Poisson form, check 100, tolerance 1e-3.  The first steps of
-    this workload need ~40-50 thousand sweeps; both programs run `steps` steps
-    with the reference's poisson_iteration_limit at `limit` sweeps (the same
-    sweeps in both, the step finished unconverged at the limit), so the
-    comparison is bounded.  Host wall clock of each program's step loop.
+    reference CLI's strict production settings (split kinetic form, check 100,
+    tolerance 1e-3, unbounded), `steps` steps; the per-step sweep counts must
+    agree.  Host wall clock of each program's step loop (its wall_total_ms).
     MLUPS with sweeps counted = cells (steps + sweeps) / wall."""
     ref = os.path.join(ROOT, "oracle", "_ref", "lbm_gpu_ref")
     ours = os.path.join(ROOT, "oracle", "_ref", "lbm_gpu_dropin")
@@ -431,14 +428,14 @@ def reference_gpu_leg(n=N_SIDE, steps=3, limit=3000, timeout=900):
     if missing:
         return {"unavailable": "not built: " + ", ".join(missing)}
     cells = float(n) ** 3
-    out = {"box": [n, n, n], "steps": steps, "poisson_iteration_limit": limit,
-           "config": "head-on 256^3 params.in without noise, --poisson split, check 100, tolerance 1e-3"}
+    out = {"box": [n, n, n], "steps": steps,
+           "config": f"head-on {n}^3 params.in without noise, --poisson split, check 100, tolerance 1e-3"}
     with tempfile.TemporaryDirectory() as tmp:
         pf = os.path.join(tmp, "params.in")
         with open(pf, "w") as fh:
             fh.write(workload_params_text(n, init_keys=True))
         for name, exe in (("reference", ref), ("ours", ours)):
-            ms, sw = _program_run(exe, os.path.join(tmp, name), pf, steps, limit, timeout)
+            ms, sw = _program_run(exe, os.path.join(tmp, name), pf, steps, timeout)
             out[name] = {"wall_ms": ms, "sweeps_per_step": sw,
                          "mlups": cells * (steps + sum(sw)) / (ms / 1e3) / 1e6,
                          "mlups_reference_definition": cells * steps / (ms / 1e3) / 1e6}
@@ -1055,7 +1052,7 @@ def run_ours(args):
                 "gpu_launches": sum(r["gpu_launches"] for r in res.values()),
                 "clocks": head["clocks"], "roofline": head["roofline"],
                 "phase_ms_per_step": head["phase_ms_per_step"], "wall_s": head["wall_s"],
-                "e2e": head.get("e2e"), "cpu_baseline": cpu}
+                "e2e": head.get("e2e"), "cpu_baseline": cpu, "roofline_collide": head.get("roofline_collide")}
         if "mixed" in res and legs[0] != "mixed":
             m = res["mixed"]
             line["mixed"] = {k: m[k] for k in ("value", "ms_per_step", "sweeps_per_step", "converged_steps",
