@@ -1084,9 +1084,7 @@ def extra_legs(args, line):
     checks (adjoint), and the batched droplet oscillation (batch)."""
     import copy
     try:
-        # 128^3, one step: the reference program needs ~20 ms per sweep at
-        # 256^3 (a 256^3 step of 20 000 sweeps takes it 408 s)
-        line["reference_gpu"] = reference_gpu_leg(min(args.size, 128), 1)
+        line["reference_gpu"] = reference_gpu_leg(args.size)
     except Exception as e:
         line["reference_gpu"] = {"unavailable": str(e)[:300]}
     try:

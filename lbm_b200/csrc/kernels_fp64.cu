@@ -40,7 +40,6 @@
 #include "exact_div.cuh"
 #include "finalize.cuh"
 #include "lbm_solver.cuh"
-#include "pipeline.cuh"
 
 namespace lbm {
 namespace {
@@ -567,113 +566,6 @@ sweep2_kernel(Geom g, int zlen, const double* __restrict__ hin, double* __restri
                 constexpr int q = decltype(qc)::value;
                 hv[q] = ring2[ring_plane<q>(z - cz(q)) * F2_RC + rc - cy(q) * F2_RX - cx(q)];
             });
-            bounce_regs(hv, g, x);
-            const int c = (z * g.ly + y) * g.lx + x;
-            const double pv = sum_q(hv);
-            const double tauh = 1.0 / __ldg(rho + c) + 0.5;
-            collide_h_store(hv, pv, tauh, __ldg(s + c), hout, n, c);
-        }
-    }
-}
-
-// The same two sweeps per launch in warp-specialized form: producer warps (one
-// thread per halo-region cell of the 16 x 8 tile) collide sweep k of plane P
-// into a ring of F2W_SLOTS whole planes and arrive on full[P % F2W_SLOTS];
-// consumer warps (one thread per tile cell) wait for plane z+1, pull sweep k+1
-// of plane z from the ring, store it and arrive on empty[(z-1) % F2W_SLOTS]
-// after plane z-1's last read.  Producers reuse a slot only after its empty
-// phase completed (up to F2W_SLOTS - 2 planes ahead) and keep two planes of
-// global pulls in flight in registers.  Waits are bounded (pipeline.cuh).
-// Cell arithmetic: collide_h_store's, so the result is bitwise that of two
-// sweep_kernel launches.
-constexpr int F2W_PROD = F2_THREADS;              // 192 producer threads (180 region cells)
-constexpr int F2W_CONS = F2_TX * F2_TY;           // 128 consumer threads
-constexpr int F2W_THREADS = F2W_PROD + F2W_CONS;  // 320
-constexpr int F2W_SLOTS = 6;
-constexpr int F2W_SMEM = F2W_SLOTS * Q * F2_RC * (int)sizeof(double) + 2 * F2W_SLOTS * 8;
-
-__device__ __forceinline__ int f2w_slot(int zz) { return ((zz % F2W_SLOTS) + F2W_SLOTS) % F2W_SLOTS; }
-
-__global__ void __launch_bounds__(F2W_THREADS, 1)
-sweep2_ws_kernel(Geom g, int zlen, const double* __restrict__ hin, double* __restrict__ hout,
-                 const double* __restrict__ rho, const double* __restrict__ s, DevState* ds)
-{
-    extern __shared__ __align__(16) unsigned char f2w_raw[];
-    double* ring = reinterpret_cast<double*>(f2w_raw);                          // [F2W_SLOTS][Q][F2_RC]
-    unsigned long long* full = reinterpret_cast<unsigned long long*>(ring + F2W_SLOTS * Q * F2_RC);
-    unsigned long long* empty = full + F2W_SLOTS;
-    const int t = threadIdx.x;
-    const int n = (int)g.n;
-    const int x0 = blockIdx.x * F2_TX, y0 = blockIdx.y * F2_TY;
-    const int z0 = blockIdx.z * zlen;
-    const int z1 = min(z0 + zlen, g.lz);
-    if (t == 0) {
-        for (int i = 0; i < F2W_SLOTS; ++i) {
-            mbar_init(full + i, F2W_PROD);
-            mbar_init(empty + i, F2W_CONS);
-        }
-    }
-    __syncthreads();
-    if (t < F2W_PROD) {
-        const bool owner = t < F2_RC;
-        const int xw = (x0 - 1 + t % F2_RX + g.lx) % g.lx;
-        const int yw = (y0 - 1 + t / F2_RX + g.ly) % g.ly;
-        double a0[Q], a1[Q];
-        double r0 = 1.0, r1 = 1.0, s0 = 0.0, s1 = 0.0;
-        auto pull = [&](int zz, double (&a)[Q], double& rv, double& sv) {
-            if (!owner) return;
-            const int zw = zz < 0 ? zz + g.lz : (zz >= g.lz ? zz - g.lz : zz);
-            pull_regs32(a, hin, n, g, xw, yw, zw);
-            const int c = (zw * g.ly + yw) * g.lx + xw;
-            rv = __ldg(rho + c);
-            sv = __ldg(s + c);
-        };
-        unsigned epar = 0;
-        auto produce = [&](int zz, double (&a)[Q], double rv, double sv) -> bool {
-            const int sl = f2w_slot(zz);
-            if (zz - F2W_SLOTS >= z0 - 1) {
-                if (!mbar_wait(empty + sl, (epar >> sl) & 1u)) return false;
-                epar ^= 1u << sl;
-            }
-            if (owner) {
-                bounce_regs(a, g, xw);
-                const double pv = sum_q(a);
-                const double tauh = 1.0 / rv + 0.5;
-                collide_h_store(a, pv, tauh, sv, ring + sl * (Q * F2_RC), F2_RC, t);
-            }
-            mbar_arrive(full + sl);
-            return true;
-        };
-        pull(z0 - 1, a0, r0, s0);
-        pull(z0, a1, r1, s1);
-        for (int zz = z0 - 1; zz <= z1; zz += 2) {
-            if (!produce(zz, a0, r0, s0)) { pipeline_fail(ds); return; }
-            if (zz + 2 <= z1) pull(zz + 2, a0, r0, s0);
-            if (zz + 1 > z1) break;
-            if (!produce(zz + 1, a1, r1, s1)) { pipeline_fail(ds); return; }
-            if (zz + 3 <= z1) pull(zz + 3, a1, r1, s1);
-        }
-    } else {
-        const int ct = t - F2W_PROD;
-        const int tx = ct % F2_TX, ty = ct / F2_TX;
-        const int x = x0 + tx, y = y0 + ty;
-        const int rc = (ty + 1) * F2_RX + (tx + 1);
-        unsigned fpar = 0;
-        auto wait_full = [&](int zz) -> bool {
-            const int sl = f2w_slot(zz);
-            if (!mbar_wait(full + sl, (fpar >> sl) & 1u)) return false;
-            fpar ^= 1u << sl;
-            return true;
-        };
-        if (!wait_full(z0 - 1) || !wait_full(z0)) { pipeline_fail(ds); return; }
-        for (int z = z0; z < z1; ++z) {
-            if (!wait_full(z + 1)) { pipeline_fail(ds); return; }
-            double hv[Q];
-            static_for<0, Q>([&](auto qc) {
-                constexpr int q = decltype(qc)::value;
-                hv[q] = ring[(f2w_slot(z - cz(q)) * Q + q) * F2_RC + rc - cy(q) * F2_RX - cx(q)];
-            });
-            mbar_arrive(empty + f2w_slot(z - 1));
             bounce_regs(hv, g, x);
             const int c = (z * g.ly + y) * g.lx + x;
             const double pv = sum_q(hv);
@@ -1269,22 +1161,19 @@ void sweep(cudaStream_t st, const Launch& L, const Geom& g, const double* hin, d
         sweep_kernel<false><<<L.grid, L.block, 0, st>>>(g, hin, hout, rho, s);
 }
 
-int sweep2_prepare(const Geom& g, bool ws)
+int sweep2_prepare(const Geom& g)
 {
     if (g.lx % F2_TX != 0 || g.ly % F2_TY != 0 || g.lz < 3 || 15 * g.n >= 0x7fffffffLL) return 0;
-    if (ws) return cudaFuncSetAttribute(sweep2_ws_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, F2W_SMEM) ==
-                   cudaSuccess ? 2 : 0;
     if (cudaFuncSetAttribute(sweep2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, F2_SMEM) != cudaSuccess)
         return 0;
     return 1;
 }
 
-void sweep2(cudaStream_t st, const Geom& g, int zlen, bool ws, const double* hin, double* hout,
-            const double* rho, const double* s, DevState* ds)
+void sweep2(cudaStream_t st, const Geom& g, int zlen, const double* hin, double* hout,
+            const double* rho, const double* s)
 {
     const dim3 grid(g.lx / F2_TX, g.ly / F2_TY, (g.lz + zlen - 1) / zlen);
-    if (ws) sweep2_ws_kernel<<<grid, F2W_THREADS, F2W_SMEM, st>>>(g, zlen, hin, hout, rho, s, ds);
-    else sweep2_kernel<<<grid, F2_THREADS, F2_SMEM, st>>>(g, zlen, hin, hout, rho, s);
+    sweep2_kernel<<<grid, F2_THREADS, F2_SMEM, st>>>(g, zlen, hin, hout, rho, s);
 }
 
 void sweep_check_a(cudaStream_t st, const Launch& L, const Geom& g, const double* hin,

@@ -22,7 +22,6 @@
 #include "collide_zm.cuh"
 #include "lbm_mixed.cuh"
 #include "mixed_cells.cuh"
-#include "pipeline.cuh"
 
 namespace lbm {
 namespace {
@@ -215,7 +214,7 @@ sweep2_kernel(Geom g, int zlen, const float* __restrict__ hin, float* __restrict
 // to WS_SLOTS - 2 planes ahead of the consumers, and it keeps two planes of
 // global pulls in flight in registers.  Cell arithmetic: that of sweep2_run.
 //
-// Every wait is bounded (pipeline.cuh): after kPipeSpin polls (seconds) the thread records
+// Every wait is bounded: after kWsSpin polls (seconds) the thread records
 // SITE_PIPELINE in the box's DevState and returns, so a broken pipeline ends
 // the launch with an error the host reads at the segment's end instead of a
 // hang.  Requires lx % 32 == 0, ly % 8 == 0 and 15 n < 2^31 (as sweep2_kernel).
@@ -225,7 +224,33 @@ constexpr int WS_CONS = WS_TX * WS_TY;             // 256 consumer threads
 constexpr int WS_THREADS = WS_PROD + WS_CONS;      // 608
 constexpr int WS_SLOTS = 6;
 constexpr int WS_SMEM = WS_SLOTS * Q * WS_RC * (int)sizeof(float) + 2 * WS_SLOTS * 8;
+constexpr long long kWsSpin = 1LL << 24;
 
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return static_cast<unsigned>(__cvta_generic_to_shared(p)); }
+__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long* b)
+{
+    asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}\n" ::"r"(smem_u32(b)) : "memory");
+}
+// Waits for the phase of the given parity to complete; false after kWsSpin polls.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity)
+{
+    for (long long i = 0; i < kWsSpin; ++i) {
+        unsigned done;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                     " selp.u32 %0, 1, 0, p;\n}\n"
+                     : "=r"(done) : "r"(smem_u32(b)), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void ws_fail(DevState* ds)
+{
+    if (atomicCAS(&ds->error, 0, static_cast<int>(LBM_ERR_CUDA)) == 0) ds->error_site = SITE_PIPELINE;
+}
 __device__ __forceinline__ int ws_slot(int zz) { return ((zz % WS_SLOTS) + WS_SLOTS) % WS_SLOTS; }
 
 __global__ void __launch_bounds__(WS_THREADS, 1)
@@ -286,10 +311,10 @@ sweep2_ws_kernel(Geom g, int zlen, const float* __restrict__ hin, float* __restr
         pull(z0 - 1, a0, om0, s0);
         pull(z0, a1, om1, s1);
         for (int zz = z0 - 1; zz <= z1; zz += 2) {
-            if (!produce(zz, a0, om0, s0)) { pipeline_fail(ds); return; }
+            if (!produce(zz, a0, om0, s0)) { ws_fail(ds); return; }
             if (zz + 2 <= z1) pull(zz + 2, a0, om0, s0);
             if (zz + 1 > z1) break;
-            if (!produce(zz + 1, a1, om1, s1)) { pipeline_fail(ds); return; }
+            if (!produce(zz + 1, a1, om1, s1)) { ws_fail(ds); return; }
             if (zz + 3 <= z1) pull(zz + 3, a1, om1, s1);
         }
     } else {
@@ -305,9 +330,9 @@ sweep2_ws_kernel(Geom g, int zlen, const float* __restrict__ hin, float* __restr
             fpar ^= 1u << sl;
             return true;
         };
-        if (!wait_full(z0 - 1) || !wait_full(z0)) { pipeline_fail(ds); return; }
+        if (!wait_full(z0 - 1) || !wait_full(z0)) { ws_fail(ds); return; }
         for (int z = z0; z < z1; ++z) {
-            if (!wait_full(z + 1)) { pipeline_fail(ds); return; }
+            if (!wait_full(z + 1)) { ws_fail(ds); return; }
             float hv[Q];
             static_for<0, Q>([&](auto qc) {
                 constexpr int q = decltype(qc)::value;

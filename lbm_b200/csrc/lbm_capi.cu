@@ -81,7 +81,6 @@ struct lbm_handle {
     lbm_check_callback check_cb = nullptr;
     void* check_user = nullptr;
     int fuse_zlen = 0;                   // FP64: >0 runs plain sweeps two per launch
-    bool fuse_ws = false;                // FP64: the two-sweep pass in its warp-specialized form
     int collide_zlen = 0;                // FP64: >0 runs the z-marching collide
     double* stats_part = nullptr;        // field-statistics partials
     lbm_field_stats* stats_dev = nullptr;   // 7 results (lbm_diagnostics)
@@ -257,7 +256,7 @@ lbm_status build_segment(lbm_handle* h, const SegKey& key, cudaGraphExec_t* out,
         int n_single = key.n_normal;
         if (h->fuse_zlen > 0) {
             for (int i = 0; i + 1 < key.n_normal; i += 2) {
-                fp64::sweep2(st, g, h->fuse_zlen, h->fuse_ws, b.h[cur], b.h[1 - cur], b.rho, b.s, h->ds);
+                fp64::sweep2(st, g, h->fuse_zlen, b.h[cur], b.h[1 - cur], b.rho, b.s);
                 cur = 1 - cur;
             }
             n_single = key.n_normal & 1;
@@ -968,9 +967,7 @@ lbm_status lbm_create(const lbm_params* prm, lbm_precision precision, int device
         // run length can be tuned (0 disables) through LBM_SWEEP2_ZLEN.
         const char* env = std::getenv("LBM_SWEEP2_ZLEN");
         const int zlen = env ? std::atoi(env) : 0;
-        const char* wenv = std::getenv("LBM_SWEEP2_WS");
-        h->fuse_ws = wenv && std::atoi(wenv) == 1;
-        h->fuse_zlen = (zlen > 0 && fp64::sweep2_prepare(h->geom, h->fuse_ws)) ? zlen : 0;
+        h->fuse_zlen = (zlen > 0 && fp64::sweep2_prepare(h->geom)) ? zlen : 0;
         // z-marching collide where its tile divides the box (LBM_COLLIDE_ZLEN,
         // 0 disables).
         const char* cenv = std::getenv("LBM_COLLIDE_ZLEN");

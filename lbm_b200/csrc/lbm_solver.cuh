@@ -127,12 +127,11 @@ void poisson_init(cudaStream_t st, const Launch& L, const Geom& g, bool h_loaded
                   double sa_scale = 1.0);
 void sweep(cudaStream_t st, const Launch& L, const Geom& g, const double* hin, double* hout,
            const double* rho, const double* s);
-// Two sweeps per launch (temporal blocking).  sweep2_prepare returns nonzero
-// when the box admits it (lx % 16 == 0, ly % 8 == 0) and the kernel is set up
-// (ws: the warp-specialized form, which records a pipeline time-out in ds).
-int sweep2_prepare(const Geom& g, bool ws);
-void sweep2(cudaStream_t st, const Geom& g, int zlen, bool ws, const double* hin, double* hout,
-            const double* rho, const double* s, DevState* ds);
+// Two sweeps per launch (temporal blocking).  sweep2_prepare returns 1 when
+// the box admits it (lx % 32 == 0, ly % 4 == 0) and the kernel is set up.
+int sweep2_prepare(const Geom& g);
+void sweep2(cudaStream_t st, const Geom& g, int zlen, const double* hin, double* hout,
+            const double* rho, const double* s);
 void sweep_check_a(cudaStream_t st, const Launch& L, const Geom& g, const double* hin,
                    double* hout, double* p_chk, double* part);
 void sweep_check_b(cudaStream_t st, const Launch& L, const Geom& g, bool dual, const double* hin, double* hout,
