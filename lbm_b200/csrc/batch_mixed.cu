@@ -340,7 +340,6 @@ const char* site_message(int site)
     case SITE_GAUGE_TARGET: return "pressure mean is NaN/Inf";
     case SITE_GAUGE_SHIFT: return "pressure gauge shift is NaN/Inf";
     case SITE_RESIDUAL: return "Poisson pressure/residual contains NaN/Inf";
-    case SITE_PIPELINE: return "a sweep kernel's wait on its shared-memory pipeline timed out";
     default: return "non-finite value";
     }
 }

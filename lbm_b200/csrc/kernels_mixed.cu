@@ -202,150 +202,6 @@ sweep2_kernel(Geom g, int zlen, const float* __restrict__ hin, float* __restrict
                              s, ring);
 }
 
-// ---- warp-specialized two-sweep pass ----------------------------------------
-// The same two sweeps per launch as sweep2_kernel, with the halo region's
-// sweep k and the tile's sweep k+1 done by different warps that run decoupled
-// instead of in lockstep: 11 producer warps (one thread per region cell of the
-// 32 x 8 tile plus halo) pull plane P, collide it into a ring of WS_SLOTS whole
-// planes and arrive on full[P % WS_SLOTS]; 8 consumer warps wait for plane z+1
-// there, pull sweep k+1 of plane z from the ring, store it, and arrive on
-// empty[(z-1) % WS_SLOTS] once plane z-1 has had its last read.  A producer
-// reuses a slot only after its empty barrier has completed, so it can run up
-// to WS_SLOTS - 2 planes ahead of the consumers, and it keeps two planes of
-// global pulls in flight in registers.  Cell arithmetic: that of sweep2_run.
-//
-// Every wait is bounded: after kWsSpin polls (seconds) the thread records
-// SITE_PIPELINE in the box's DevState and returns, so a broken pipeline ends
-// the launch with an error the host reads at the segment's end instead of a
-// hang.  Requires lx % 32 == 0, ly % 8 == 0 and 15 n < 2^31 (as sweep2_kernel).
-constexpr int WS_TX = 32, WS_TY = 8, WS_RX = WS_TX + 2, WS_RC = WS_RX * (WS_TY + 2);
-constexpr int WS_PROD = (WS_RC + 31) / 32 * 32;    // 352 producer threads
-constexpr int WS_CONS = WS_TX * WS_TY;             // 256 consumer threads
-constexpr int WS_THREADS = WS_PROD + WS_CONS;      // 608
-constexpr int WS_SLOTS = 6;
-constexpr int WS_SMEM = WS_SLOTS * Q * WS_RC * (int)sizeof(float) + 2 * WS_SLOTS * 8;
-constexpr long long kWsSpin = 1LL << 24;
-
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return static_cast<unsigned>(__cvta_generic_to_shared(p)); }
-__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(b)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(unsigned long long* b)
-{
-    asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}\n" ::"r"(smem_u32(b)) : "memory");
-}
-// Waits for the phase of the given parity to complete; false after kWsSpin polls.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity)
-{
-    for (long long i = 0; i < kWsSpin; ++i) {
-        unsigned done;
-        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-                     " selp.u32 %0, 1, 0, p;\n}\n"
-                     : "=r"(done) : "r"(smem_u32(b)), "r"(parity) : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-__device__ __forceinline__ void ws_fail(DevState* ds)
-{
-    if (atomicCAS(&ds->error, 0, static_cast<int>(LBM_ERR_CUDA)) == 0) ds->error_site = SITE_PIPELINE;
-}
-__device__ __forceinline__ int ws_slot(int zz) { return ((zz % WS_SLOTS) + WS_SLOTS) % WS_SLOTS; }
-
-__global__ void __launch_bounds__(WS_THREADS, 1)
-sweep2_ws_kernel(Geom g, int zlen, const float* __restrict__ hin, float* __restrict__ hout,
-                 const float* __restrict__ omega, const float* __restrict__ s, DevState* ds)
-{
-    extern __shared__ __align__(16) unsigned char ws_raw[];
-    float* ring = reinterpret_cast<float*>(ws_raw);                       // [WS_SLOTS][Q][WS_RC]
-    unsigned long long* full = reinterpret_cast<unsigned long long*>(ring + WS_SLOTS * Q * WS_RC);
-    unsigned long long* empty = full + WS_SLOTS;
-    const int t = threadIdx.x;
-    const int n = (int)g.n;
-    const int x0 = blockIdx.x * WS_TX, y0 = blockIdx.y * WS_TY;
-    const int z0 = blockIdx.z * zlen;
-    const int z1 = min(z0 + zlen, g.lz);
-    if (t == 0) {
-        for (int i = 0; i < WS_SLOTS; ++i) {
-            mbar_init(full + i, WS_PROD);
-            mbar_init(empty + i, WS_CONS);
-        }
-    }
-    __syncthreads();
-    if (t < WS_PROD) {
-        // ---- producer: sweep k on the halo region, planes z0-1 .. z1 ----
-        const bool owner = t < WS_RC;
-        const int xw = (x0 - 1 + t % WS_RX + g.lx) % g.lx;
-        const int yw = (y0 - 1 + t / WS_RX + g.ly) % g.ly;
-        float a0[Q], a1[Q];
-        float om0 = 0.f, om1 = 0.f, s0 = 0.f, s1 = 0.f;
-        auto pull = [&](int zz, float (&a)[Q], float& om, float& sv) {
-            if (!owner) return;
-            const int zw = zz < 0 ? zz + g.lz : (zz >= g.lz ? zz - g.lz : zz);
-            pull_regs32(a, hin, n, g, xw, yw, zw);
-            const int c = (zw * g.ly + yw) * g.lx + xw;
-            om = __ldg(omega + c);
-            sv = __ldg(s + c);
-        };
-        unsigned epar = 0;   // parity bit per slot of the next empty-barrier wait
-        // collide plane zz from (a, om, sv) into its slot; false if a wait gave up
-        auto produce = [&](int zz, float (&a)[Q], float om, float sv) -> bool {
-            const int sl = ws_slot(zz);
-            if (zz - WS_SLOTS >= z0 - 1) {   // the slot held plane zz - WS_SLOTS
-                if (!mbar_wait(empty + sl, (epar >> sl) & 1u)) return false;
-                epar ^= 1u << sl;
-            }
-            if (owner) {
-                bounce_regs(a, g, xw);
-                const P32 p32 = sum_q32(a);
-                float* slot = ring + sl * (Q * WS_RC) + t;
-                static_for<0, Q>([&](auto qc) {
-                    constexpr int q = decltype(qc)::value;
-                    slot[q * WS_RC] = collide_h<q>(a[q], p32, om, sv);
-                });
-            }
-            mbar_arrive(full + sl);
-            return true;
-        };
-        pull(z0 - 1, a0, om0, s0);
-        pull(z0, a1, om1, s1);
-        for (int zz = z0 - 1; zz <= z1; zz += 2) {
-            if (!produce(zz, a0, om0, s0)) { ws_fail(ds); return; }
-            if (zz + 2 <= z1) pull(zz + 2, a0, om0, s0);
-            if (zz + 1 > z1) break;
-            if (!produce(zz + 1, a1, om1, s1)) { ws_fail(ds); return; }
-            if (zz + 3 <= z1) pull(zz + 3, a1, om1, s1);
-        }
-    } else {
-        // ---- consumer: sweep k+1 on the tile, planes z0 .. z1-1 ----
-        const int ct = t - WS_PROD;
-        const int tx = ct % WS_TX, ty = ct / WS_TX;
-        const int x = x0 + tx, y = y0 + ty;
-        const int rc = (ty + 1) * WS_RX + (tx + 1);
-        unsigned fpar = 0;
-        auto wait_full = [&](int zz) -> bool {
-            const int sl = ws_slot(zz);
-            if (!mbar_wait(full + sl, (fpar >> sl) & 1u)) return false;
-            fpar ^= 1u << sl;
-            return true;
-        };
-        if (!wait_full(z0 - 1) || !wait_full(z0)) { ws_fail(ds); return; }
-        for (int z = z0; z < z1; ++z) {
-            if (!wait_full(z + 1)) { ws_fail(ds); return; }
-            float hv[Q];
-            static_for<0, Q>([&](auto qc) {
-                constexpr int q = decltype(qc)::value;
-                hv[q] = ring[(ws_slot(z - cz(q)) * Q + q) * WS_RC + rc - cy(q) * WS_RX - cx(q)];
-            });
-            mbar_arrive(empty + ws_slot(z - 1));   // plane z-1 has had its last read
-            bounce_regs(hv, g, x);
-            const int c = (z * g.ly + y) * g.lx + x;
-            collide_h_store32(hv, sum_q32(hv), __ldg(omega + c), __ldg(s + c), hout, n, c);
-        }
-    }
-}
-
 __global__ void __launch_bounds__(256)
 sweep_check_a_kernel(Geom g, int zrun, const float* __restrict__ hin, float* __restrict__ hout,
                      double* __restrict__ p_chk, double* __restrict__ part, long long nblocks)
@@ -476,11 +332,6 @@ lbm_status mixed_alloc(MixedBuffers& mb, const Geom& g, const Launch& L)
     if (zlen > 0 && g.lx % S2_TX == 0 && g.ly % S2_TY == 0 && g.lz >= 3 && 15 * g.n < 0x7fffffffLL &&
         cudaFuncSetAttribute(sweep2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, S2_SMEM) == cudaSuccess)
         mb.fuse_zlen = zlen;
-    // The warp-specialized form of the pass (same tile; LBM_SWEEP2_WS=1).
-    const char* wenv = std::getenv("LBM_SWEEP2_WS");
-    mb.fuse_ws = mb.fuse_zlen > 0 && wenv && std::atoi(wenv) == 1 &&
-                 cudaFuncSetAttribute(sweep2_ws_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, WS_SMEM) ==
-                     cudaSuccess;
     // z-marching collide where its tile divides the box.
     const char* cenv = std::getenv("LBM_COLLIDE_ZLEN");
     const int czlen = cenv ? std::atoi(cenv) : 16;
@@ -600,12 +451,8 @@ int mixed_segment(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom
     if (mb.fuse_zlen > 0) {
         const dim3 grid(g.lx / S2_TX, g.ly / S2_TY, (g.lz + mb.fuse_zlen - 1) / mb.fuse_zlen);
         for (int i = 0; i + 1 < n_normal; i += 2) {
-            if (mb.fuse_ws)
-                sweep2_ws_kernel<<<grid, WS_THREADS, WS_SMEM, st>>>(g, mb.fuse_zlen, mb.h[cur], mb.h[1 - cur], omega,
-                                                                    mb.s, ds);
-            else
-                sweep2_kernel<<<grid, S2_THREADS, S2_SMEM, st>>>(g, mb.fuse_zlen, mb.h[cur], mb.h[1 - cur], omega,
-                                                                 mb.s);
+            sweep2_kernel<<<grid, S2_THREADS, S2_SMEM, st>>>(g, mb.fuse_zlen, mb.h[cur], mb.h[1 - cur],
+                                                                     omega, mb.s);
             cur = 1 - cur;
         }
         n_normal &= 1;

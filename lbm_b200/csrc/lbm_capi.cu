@@ -327,7 +327,6 @@ const char* site_text(int site)
     case SITE_GAUGE_SHIFT: return "pressure gauge shift is NaN/Inf";
     case SITE_FIXED_POINT: return "kinetic fixed-point residual contains NaN/Inf";
     case SITE_RESIDUAL: return "Poisson pressure/residual contains NaN/Inf";
-    case SITE_PIPELINE: return "a sweep kernel's wait on its shared-memory pipeline timed out";
     default: return "non-finite value";
     }
 }

@@ -24,7 +24,6 @@ struct MixedBuffers {
            *part_c = nullptr, *part_mass = nullptr;
     double* scratch = nullptr;   // FP64 staging for loads/downloads (n doubles)
     int fuse_zlen = 0;           // >0: plain sweeps run two per pass, z runs of this length
-    bool fuse_ws = false;        // the two-sweep pass in its warp-specialized form
     int collide_zlen = 0;        // >0: z-marching collide, z runs of this length
     bool allocated = false;
 };

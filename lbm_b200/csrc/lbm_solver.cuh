@@ -63,8 +63,7 @@ enum ErrorSite {
     SITE_GAUGE_TARGET = 3,  // "pressure mean is NaN/Inf"
     SITE_GAUGE_SHIFT = 4,   // "pressure gauge shift is NaN/Inf"
     SITE_FIXED_POINT = 5,   // "kinetic fixed-point residual contains NaN/Inf"
-    SITE_RESIDUAL = 6,      // "Poisson pressure/residual contains NaN/Inf"
-    SITE_PIPELINE = 7       // a kernel's bounded wait on its own pipeline gave up (LBM_ERR_CUDA)
+    SITE_RESIDUAL = 6       // "Poisson pressure/residual contains NaN/Inf"
 };
 
 // Launch shape: 2-D tiles of (bx, by) cells in an xy plane, one grid z-slice

@@ -172,26 +172,3 @@ def test_mixed_periodic_x_against_periodic_oracle():
         assert float(np.max(np.abs(gf[k] - of[k]))) <= 1e-5 * vscale, k
     m0 = float(np.sum(f["phi"]))
     assert max(abs(m - m0) for m in masses) <= 1e-12 * abs(m0)
-
-
-@pytest.mark.parametrize("zlen,periodic", [("32", 0), ("5", 0), ("1", 1), ("32", 1)])
-def test_warp_specialized_two_sweep_pass_is_bitwise(zlen, periodic, monkeypatch):
-    """The warp-specialized two-sweep pass (producer and consumer warps
-    decoupled through mbarriers) evaluates every cell as the lockstep pass
-    does: bitwise equal fields and sweep counts; z runs that do not divide
-    the box (5) and single-plane runs (1) included; no pipeline error."""
-    p, f = laplace_case((64, 40, 24), DD=12.0, noise=1e-4)
-    p.periodic_x = periodic
-    f["w"] = 0.01 * np.sin(2 * np.pi * np.arange(24) / 24)[:, None, None] * np.ones_like(f["w"])
-    monkeypatch.setenv("LBM_SWEEP2_ZLEN", zlen)
-    monkeypatch.setenv("LBM_SWEEP2_WS", "0")
-    a = L.InamuroCUDA(p, f, precision="mixed")
-    monkeypatch.setenv("LBM_SWEEP2_WS", "1")
-    b = L.InamuroCUDA(p, f, precision="mixed")
-    for g in (a, b):
-        g.set_poisson(max_sweeps=CAP, fail_on_limit=True)
-    for _ in range(3):
-        assert a.step(1)[0]["iterations"] == b.step(1)[0]["iterations"]
-    fa, fb = a.download_fields(), b.download_fields()
-    for k in L.FIELDS:
-        assert np.array_equal(fa[k], fb[k]), k
