@@ -833,8 +833,9 @@ def run_coalescence_adjoint(args):
     coalescence (coalescence_workload, rho_L/rho_G = 1000) on an n^3 periodic
     box, a forward run of K steps over the mixed box (FP32 populations, FP64
     rest population, pressure and reductions; lbm_adjoint_cfg.precision = 1)
-    with binomial checkpointing, and its reverse pass (BiCGSTAB adjoint
-    Poisson solves), for each of --coalescence-samples kappa_f values drawn
+    with binomial checkpointing, and its reverse pass (adjoint Poisson solves
+    by transposed sweeps, or BiCGSTAB with --adjoint-krylov), for each of
+    --coalescence-samples kappa_f values drawn
     uniformly from [0.04, 0.08].  Objective J = 0.5 sum (phi_T - phi_target)^2,
     phi_target the final phi of the first sample's forward run with kappa_f
     + 5 %.  Reported: MLUPS (sweeps counted) of forward and reverse, the
@@ -863,26 +864,28 @@ def run_coalescence_adjoint(args):
            "dtype": "f32 populations + f64 pressure/reductions (forward); f64 adjoint",
            "data": "synthetic (three seeded tanh drops, rho ratio 1000, phi noise 1e-4)",
            "config": {"workload": f"three-drop coalescence {n}^3 periodic, R=28, triangle side 60 in z=n/2, "
-                                  f"approach 0.01, rho_L/rho_G=1000; {K} of 5000 steps (bounded sample)",
+                                  f"approach 0.01, rho_L/rho_G={args.coalescence_ratio:g}; {K} of 5000 steps "
+                                  f"(bounded sample)",
                       "kappa_f": kfs, "binomial_checkpoints": slots,
                       "poisson": {"forward_tolerance": tol_f, "forward_sweep_cap": args.coalescence_cap or None,
-                                  "adjoint_solver": "BiCGSTAB",
+                                  "adjoint_solver": "BiCGSTAB" if args.adjoint_krylov else "transposed sweeps",
+                                  "adjoint_tolerance": args.adjoint_tol,
                                   "adjoint_krylov_tolerance": args.adjoint_krylov_tol}},
            "samples": []}
     target = None
     for i, kf in enumerate(kfs):
-        p, f = coalescence_workload(n, kf=kf)
+        p, f = coalescence_workload(n, kf=kf, ratio=args.coalescence_ratio)
         if target is None:
-            pt, ft = coalescence_workload(n, kf=kf * 1.05)
-            a = L.Adjoint(pt, binomial_checkpoints=slots, check_interval=100, tolerance=1e-13, krylov=True,
-                          krylov_tolerance=args.adjoint_krylov_tol, precision="mixed")
+            pt, ft = coalescence_workload(n, kf=kf * 1.05, ratio=args.coalescence_ratio)
+            a = L.Adjoint(pt, binomial_checkpoints=slots, check_interval=100, tolerance=args.adjoint_tol,
+                          krylov=args.adjoint_krylov, krylov_tolerance=args.adjoint_krylov_tol, precision="mixed")
             a.set_poisson(check_interval=100, tolerance=tol_f, max_sweeps=args.max_sweeps, fail_on_limit=fail)
             a.forward(ft, K)
             target = a.download("phi")
             a.close()
             del pt, ft
-        a = L.Adjoint(p, binomial_checkpoints=slots, check_interval=100, tolerance=1e-13, krylov=True,
-                      krylov_tolerance=args.adjoint_krylov_tol, precision="mixed")
+        a = L.Adjoint(p, binomial_checkpoints=slots, check_interval=100, tolerance=args.adjoint_tol,
+                      krylov=args.adjoint_krylov, krylov_tolerance=args.adjoint_krylov_tol, precision="mixed")
         a.set_poisson(check_interval=100, tolerance=tol_f, max_sweeps=args.max_sweeps, fail_on_limit=fail)
         a.forward(f, K)
         phi_T = a.download("phi")
@@ -899,12 +902,12 @@ def run_coalescence_adjoint(args):
                "backward_ms": st["backward_ms"], "forward_sweeps_per_step": st["forward_sweeps"] / K,
                "adjoint_matvecs_per_step": st["adjoint_sweeps"] / K, "recompute_steps": st["recompute_steps"],
                "device_gb_in_use_after_reverse": (total - free1) / 1e9, "grad_kappa_f": st["grad_kappa_f"],
-               "objective": 0.5 * float(np.sum((phi_T - target) ** 2))}
+               "objective": 0.5 * float(np.sum((phi_T - target) ** 2)), "updates": fwd_updates + bwd_updates}
         if i == 0 and args.coalescence_fd:
             h = 1e-6 * kf
             vals = []
             for sgn in (1.0, -1.0):
-                pp, ff = coalescence_workload(n, kf=kf + sgn * h)
+                pp, ff = coalescence_workload(n, kf=kf + sgn * h, ratio=args.coalescence_ratio)
                 b = L.InamuroCUDA(pp, ff, precision="fp64")
                 b.set_poisson(check_interval=100, tolerance=tol_f, max_sweeps=args.max_sweeps)
                 b.step_replay(sweeps)
@@ -919,9 +922,8 @@ def run_coalescence_adjoint(args):
         del p, f, grads
     tot_f = sum(s["forward_ms"] for s in out["samples"])
     tot_b = sum(s["backward_ms"] for s in out["samples"])
-    cells = float(n) ** 3
-    upd = sum(cells * (K + s["forward_sweeps_per_step"] * K) for s in out["samples"])
-    out["value"] = None
+    upd = sum(s["updates"] for s in out["samples"])
+    out["value"] = upd / ((tot_f + tot_b) / 1e3) / 1e6
     out["forward_mlups_mean"] = float(np.mean([s["forward_mlups"] for s in out["samples"]]))
     out["adjoint_forward_time_ratio"] = tot_b / tot_f
     out["ms_per_step"] = (tot_f + tot_b) / K / len(kfs)
@@ -1189,6 +1191,8 @@ def main(argv=None):
                     help="coalescence-adjoint workload: kappa_f samples (uniform in [0.04, 0.08])")
     ap.add_argument("--binomial-slots", type=int, default=25,
                     help="coalescence-adjoint workload: binomial checkpoint slots")
+    ap.add_argument("--coalescence-ratio", type=float, default=1000.0,
+                    help="coalescence-adjoint workload: rho_L / rho_G")
     ap.add_argument("--coalescence-cap", type=int, default=0,
                     help="coalescence-adjoint workload: sweep cap per forward step (0: converge or fail)")
     ap.add_argument("--coalescence-fd", action="store_true",
