@@ -1003,10 +1003,13 @@ def run_krylov(args):
     f = workload_fields(p)
     tol = args.krylov_tol
     out, fields = {}, {}
-    for form in ("kinetic", "krylov"):
+    degrees = [int(d) for d in args.krylov_degrees.split(",")]
+    for form in ["kinetic"] + [f"krylov_d{d}" for d in degrees]:
         g = L.InamuroCUDA(p, f, precision="fp64")
         g.set_poisson(check_interval=100, tolerance=tol, max_sweeps=args.max_sweeps, fail_on_limit=True)
-        g.set_poisson_form(form)
+        g.set_poisson_form("kinetic" if form == "kinetic" else "krylov")
+        if form != "kinetic":
+            g.set_poisson_accel(krylov_degree=int(form.split("_d")[1]))
         g.step(args.warmup)
         g.reset_timing()
         clk = ClockSampler(0)
@@ -1020,10 +1023,15 @@ def run_krylov(args):
                      "final_relative": stats[-1]["relative_error"], "clocks": clocks}
         fields[form] = g.download_fields()
         g.close()
-    diff = {k: float(np.max(np.abs(fields["krylov"][k] - fields["kinetic"][k])) /
-                     max(float(np.max(np.abs(fields["kinetic"][k]))), 1e-300)) for k in L.FIELDS}
+    diff = {form: {k: float(np.max(np.abs(fields[form][k] - fields["kinetic"][k])) /
+                       max(float(np.max(np.abs(fields["kinetic"][k]))), 1e-300)) for k in L.FIELDS}
+            for form in fields if form != "kinetic"}
+    best = min((form for form in out if form != "kinetic"), key=lambda k: out[k]["poisson_ms_per_step"])
+    for form in out:
+        if form != "kinetic":
+            out[form]["speedup_vs_kinetic"] = out["kinetic"]["poisson_ms_per_step"] / out[form]["poisson_ms_per_step"]
     line = {"metric": "Poisson time per step to the kinetic fixed point, kinetic sweeps vs BiCGSTAB",
-            "value": out["kinetic"]["poisson_ms_per_step"] / out["krylov"]["poisson_ms_per_step"],
+            "value": out["kinetic"]["poisson_ms_per_step"] / out[best]["poisson_ms_per_step"], "best": best,
             "unit": "speed-up (x)", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(config_dict(n, "fp64"), tolerance=tol), "forms": out, "rel_diff_krylov_vs_kinetic": diff}
@@ -1174,6 +1182,8 @@ def main(argv=None):
                     help="time the non-Poisson kernels per step with --phase-sweeps sweeps per step")
     ap.add_argument("--phase-sweeps", type=int, default=100)
     ap.add_argument("--krylov-tol", type=float, default=1e-10, help="tolerance of the krylov workload")
+    ap.add_argument("--krylov-degrees", default="1,4,8",
+                    help="krylov workload: polynomial preconditioner degrees to time (1: plain BiCGSTAB)")
     ap.add_argument("--workload", choices=("headon", "batch", "adjoint", "poisson-forms", "krylov",
                                            "coalescence-adjoint"), default="headon",
                     help="batch: the batched droplet oscillation (64 uneven boxes, mixed precision); "

@@ -303,7 +303,7 @@ lbm_status lbm_get_poisson_form(const lbm_handle* h, lbm_poisson_form* form, dou
  * form (LBM_ERR_BAD_ARG at the next step otherwise); two-grid correction,
  * source-aware h init and spatial diagnostics apply to the kinetic and
  * one-pass forms.  None combines with the dual residual (the reference
- * refuses that too).  Defaults: 1, 1, off, 1, off, 0.5, off, 1, off. */
+ * refuses that too).  Defaults: 1, 1, off, 1, off, 0.5, off, 1, off, 0. */
 typedef struct {
     double pressure_relax_scale;   /* --pressure-relax-scale: scales (h - E p) / tau_h */
     double fixed_point_relax;      /* --poisson-fixed-point-relax: h = h_old + omega (T(h) - h_old) */
@@ -315,6 +315,12 @@ typedef struct {
     double source_aware_scale;     /* --source-aware-hh-scale */
     int spatial_diagnostics;       /* --poisson-spatial-diagnostics: block_low_frequency_fraction of
                                       every check record */
+    int krylov_degree;             /* not a reference setting: LBM_POISSON_KRYLOV's polynomial
+                                      preconditioner, BiCGSTAB on (I - K^m) h =
+                                      (I + K + ... + K^(m-1)) b with m = krylov_degree (0 or 1: the
+                                      plain system; at most 16).  Same solution, fewer iterations
+                                      for m applications of K each; the tolerance then applies to
+                                      the preconditioned residual */
 } lbm_poisson_accel;
 lbm_status lbm_set_poisson_accel(lbm_handle* h, const lbm_poisson_accel* a);
 lbm_status lbm_get_poisson_accel(const lbm_handle* h, lbm_poisson_accel* out);

@@ -116,7 +116,7 @@ class PoissonAccel(C.Structure):
     _fields_ = [("pressure_relax_scale", C.c_double), ("fixed_point_relax", C.c_double),
                 ("anderson_m1", C.c_int), ("anderson_beta_max", C.c_double), ("two_grid", C.c_int),
                 ("two_grid_strength", C.c_double), ("source_aware_init", C.c_int),
-                ("source_aware_scale", C.c_double), ("spatial_diagnostics", C.c_int)]
+                ("source_aware_scale", C.c_double), ("spatial_diagnostics", C.c_int), ("krylov_degree", C.c_int)]
 
 
 class AdjointCfg(C.Structure):

@@ -15,6 +15,8 @@
 // added on the host.  The exit: ||b - (I - K) h||_2 < tolerance ||b||_2.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "../../include/lbm_b200.h"
 #include "lbm_solver.cuh"
 
@@ -49,17 +51,19 @@ __device__ __forceinline__ void kbounce(double (&v)[Q], const Geom& g, int x)
     }
 }
 
-// out = in - K in (kinds 0, 2), or out = b - (in - K in) with b = -(E/3) s
-// (kind 1, a true residual).  Partial sums: kind 0 dot(w, out) and
-// dot(out, out); kind 1 dot(out, out); kind 2 dot(w, out) and dot(out, out).
-// kAdj: the adjoint solve's operator B = M^T o (pull from x + c_q) instead of
-// K (M^T m = (1 - 1/tau) m + (sum_k E_k m_k) / tau per cell; periodic
-// boxes), and b_q = s (the adjoint of p, the same for every q).
+// out = in - K src (kinds 0, 2), or out = b - (in - K src) (kind 1, a true
+// residual), with b = bvec when given, else b_q = -(E/3) s; src = in for the
+// plain operator I - K, src = K^(m-1) in for the polynomial form I - K^m.
+// Kind 3: out = K src alone (no partial sums).  Partial sums: kind 0
+// dot(w, out) and dot(out, out); kind 1 dot(out, out); kind 2 dot(w, out)
+// and dot(out, out).  kAdj: the adjoint solve's operator B = M^T o (pull from
+// x + c_q) instead of K (M^T m = (1 - 1/tau) m + (sum_k E_k m_k) / tau per
+// cell; periodic boxes), and b_q = s (the adjoint of p, the same for every q).
 template <int kKind, bool kAdj>
 __global__ void __launch_bounds__(256)
-apply_kernel(Geom g, const double* __restrict__ in, double* __restrict__ out, const double* __restrict__ rho,
-             const double* __restrict__ s, const double* __restrict__ w, double* __restrict__ part,
-             long long nblocks)
+apply_kernel(Geom g, const double* __restrict__ in, const double* __restrict__ src, double* __restrict__ out,
+             const double* __restrict__ rho, const double* __restrict__ s, const double* __restrict__ bvec,
+             const double* __restrict__ w, double* __restrict__ part, long long nblocks)
 {
     int x, y, z;
     const bool active = kcell(g, x, y, z);
@@ -72,11 +76,11 @@ apply_kernel(Geom g, const double* __restrict__ in, double* __restrict__ out, co
         static_for<0, Q>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
             if constexpr (kAdj)
-                hv[q] = __ldg(in + (long long)q * n + cell_of(g, pick<cx(q)>(wr.xm, x, wr.xp),
-                                                              pick<cy(q)>(wr.ym, y, wr.yp),
-                                                              pick<cz(q)>(wr.zm, z, wr.zp)));
+                hv[q] = __ldg(src + (long long)q * n + cell_of(g, pick<cx(q)>(wr.xm, x, wr.xp),
+                                                               pick<cy(q)>(wr.ym, y, wr.yp),
+                                                               pick<cz(q)>(wr.zm, z, wr.zp)));
             else
-                hv[q] = __ldg(in + (long long)q * n + pull_src<q>(g, wr, x, y, z));
+                hv[q] = __ldg(src + (long long)q * n + pull_src<q>(g, wr, x, y, z));
         });
         if constexpr (!kAdj) kbounce(hv, g, x);
         double p = 0.0;
@@ -85,14 +89,18 @@ apply_kernel(Geom g, const double* __restrict__ in, double* __restrict__ out, co
             p += kAdj ? wE(q) * hv[q] : hv[q];
         });
         const double inv_tau = 1.0 / (1.0 / __ldg(rho + c) + 0.5);
-        const double sv = (kKind == 1) ? __ldg(s + c) : 0.0;
+        const double sv = (kKind == 1 && !bvec) ? __ldg(s + c) : 0.0;
         static_for<0, Q>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
             constexpr double E = wE(q);
             const long long i = (long long)q * n + c;
             const double kh = kAdj ? hv[q] - (hv[q] - p) * inv_tau : hv[q] - (hv[q] - E * p) * inv_tau;
+            if constexpr (kKind == 3) {
+                out[i] = kh;
+                return;
+            }
             double v = __ldg(in + i) - kh;
-            if constexpr (kKind == 1) v = (kAdj ? sv : -(E / 3.0) * sv) - v;
+            if constexpr (kKind == 1) v = (bvec ? __ldg(bvec + i) : (kAdj ? sv : -(E / 3.0) * sv)) - v;
             out[i] = v;
             if constexpr (kKind == 0) {
                 red[0] += __ldg(w + i) * v;
@@ -105,7 +113,7 @@ apply_kernel(Geom g, const double* __restrict__ in, double* __restrict__ out, co
             if constexpr (kKind == 1) red[0] += v * v;
         });
     }
-    block_sum_store<2>(red, part, nblocks, block_linear());
+    if constexpr (kKind != 3) block_sum_store<2>(red, part, nblocks, block_linear());
 }
 
 // Grid-stride vector updates over the 15 n populations.
@@ -113,6 +121,7 @@ apply_kernel(Geom g, const double* __restrict__ in, double* __restrict__ out, co
 // op 1: s = r - alpha v
 // op 2: x += alpha p + omega s; r = s - omega t; partials of r.r and r0.r
 // op 3: copy (r0 = r, p = r)
+// op 4: y0 += x0 (the polynomial right-hand side's sum)
 template <int kOp>
 __global__ void __launch_bounds__(256)
 vec_kernel(long long count, double a0, double a1, double* __restrict__ y0, double* __restrict__ y1,
@@ -132,9 +141,11 @@ vec_kernel(long long count, double a0, double a1, double* __restrict__ y0, doubl
             y1[i] = r;
             red[0] += r * r;
             red[1] += x3[i] * r;
-        } else {
+        } else if constexpr (kOp == 3) {
             y0[i] = x0[i];
             y1[i] = x0[i];
+        } else {
+            y0[i] += x0[i];
         }
     }
     if constexpr (kOp == 2) block_sum_store<2>(red, part, gridDim.x, blockIdx.x);
@@ -182,13 +193,37 @@ namespace krylov {
 namespace {
 
 // BiCGSTAB iterations on (I - A_op) h = b from the initial guess in h; the
-// operator and source as apply_kernel<., kAdj>.  *budget: stopped at the cap.
+// operator and source as apply_kernel<., kAdj>.  degree m > 1: the same
+// solution from the polynomially preconditioned system
+// (I - A_op^m) h = (I + A_op + ... + A_op^(m-1)) b (Neumann series of
+// (I - A_op)^-1 truncated after m terms as left preconditioner), which takes
+// fewer iterations -- so fewer of the memory-bound vector updates and host
+// round trips -- for m applications of A_op per operator.  *budget: stopped
+// at the cap.
 template <bool kAdj>
 lbm_status bicgstab(cudaStream_t st, const Launch& L, const Geom& g, const KrylovBuffers& kb, double* h,
-                    const double* rho, const double* s, double tol, uint64_t max_matvecs, KrylovResult* res,
-                    bool* budget_out)
+                    const double* rho, const double* s, double tol, uint64_t max_matvecs, int degree,
+                    KrylovResult* res, bool* budget_out)
 {
     const long long cnt = 15 * g.n;
+    const int m = degree > 1 ? degree : 1;
+    // out = in - A^m in (kinds 0, 2) or b_m - (in - A^m in) (kind 1), with the
+    // kind's partial sums; A^(m-1) in goes through kb.w1 / kb.w2.
+    auto apply = [&](auto kindc, const double* in, double* out, const double* w) {
+        constexpr int kKind = decltype(kindc)::value;
+        const double* src = in;
+        for (int j = 1; j < m; ++j) {
+            double* dst = (j & 1) ? kb.w1 : kb.w2;
+            apply_kernel<3, kAdj><<<L.grid, L.block, 0, st>>>(g, nullptr, src, dst, rho, nullptr, nullptr, nullptr,
+                                                               nullptr, 0);
+            src = dst;
+        }
+        apply_kernel<kKind, kAdj><<<L.grid, L.block, 0, st>>>(g, in, src, out, rho, s, m > 1 ? kb.bm : nullptr, w,
+                                                              kb.part, L.nblocks);
+    };
+    using K0 = std::integral_constant<int, 0>;
+    using K1 = std::integral_constant<int, 1>;
+    using K2 = std::integral_constant<int, 2>;
     auto host_sum = [&](long long blocks, int cols, double* out) -> bool {
         if (cudaMemcpyAsync(kb.host, kb.part, static_cast<size_t>(cols) * blocks * sizeof(double),
                             cudaMemcpyDeviceToHost, st) != cudaSuccess)
@@ -203,9 +238,26 @@ lbm_status bicgstab(cudaStream_t st, const Launch& L, const Geom& g, const Krylo
     };
     double d2[2];
     *res = KrylovResult{};
-    // ||b||: the residual of x = 0 (v is zero, and stays the v_0 = 0 of the method)
     if (cudaMemsetAsync(kb.v, 0, static_cast<size_t>(cnt) * sizeof(double), st) != cudaSuccess) return LBM_ERR_CUDA;
-    apply_kernel<1, kAdj><<<L.grid, L.block, 0, st>>>(g, kb.v, kb.t, rho, s, nullptr, kb.part, L.nblocks);
+    if (m > 1) {
+        // b_m = b + A b + ... + A^(m-1) b (b: the kind-1 residual of x = 0)
+        apply_kernel<1, kAdj><<<L.grid, L.block, 0, st>>>(g, kb.v, kb.v, kb.bm, rho, s, nullptr, nullptr, kb.part,
+                                                          L.nblocks);
+        vec_kernel<3><<<kDotBlocks, 256, 0, st>>>(cnt, 0.0, 0.0, kb.w1, kb.w2, kb.bm, nullptr, nullptr, nullptr,
+                                                   nullptr);
+        const double* cur = kb.w1;
+        for (int j = 1; j < m; ++j) {
+            double* dst = (j & 1) ? kb.w2 : kb.w1;
+            apply_kernel<3, kAdj><<<L.grid, L.block, 0, st>>>(g, nullptr, cur, dst, rho, nullptr, nullptr, nullptr,
+                                                               nullptr, 0);
+            vec_kernel<4><<<kDotBlocks, 256, 0, st>>>(cnt, 0.0, 0.0, kb.bm, nullptr, dst, nullptr, nullptr, nullptr,
+                                                       nullptr);
+            cur = dst;
+        }
+        res->matvecs += static_cast<uint64_t>(m - 1);
+    }
+    // ||b_m||: the residual of x = 0 (v is zero, and stays the v_0 = 0 of the method)
+    apply(K1{}, kb.v, kb.t, nullptr);
     if (!host_sum(L.nblocks, 1, d2)) return LBM_ERR_CUDA;
     // a NaN/Inf source or right-hand side: NaN norms would skip the loop below
     if (!isfinite(d2[0])) return LBM_ERR_NONFINITE;
@@ -213,12 +265,12 @@ lbm_status bicgstab(cudaStream_t st, const Launch& L, const Geom& g, const Krylo
     // iterate to the null-space representative nearest the start
     const double bnorm = d2[0] > 0.0 ? sqrt(d2[0]) : 1.0;
     // r = b - A x0, r0 = p = r
-    apply_kernel<1, kAdj><<<L.grid, L.block, 0, st>>>(g, h, kb.r, rho, s, nullptr, kb.part, L.nblocks);
+    apply(K1{}, h, kb.r, nullptr);
     if (!host_sum(L.nblocks, 1, d2)) return LBM_ERR_CUDA;
     double rr = d2[0];
     if (!isfinite(rr)) return LBM_ERR_NONFINITE;   // a NaN/Inf start iterate
     vec_kernel<3><<<kDotBlocks, 256, 0, st>>>(cnt, 0.0, 0.0, kb.r0, kb.p, kb.r, nullptr, nullptr, nullptr, nullptr);
-    res->matvecs = 1;
+    res->matvecs += static_cast<uint64_t>(m);
     double rho_old = 1.0, alpha = 1.0, omega = 1.0, rho_new = rr, r0r0 = rr;
     bool first = true, budget = false;
     int since = 0;
@@ -233,9 +285,9 @@ lbm_status bicgstab(cudaStream_t st, const Launch& L, const Geom& g, const Krylo
     // Restart from the true residual of the current iterate: r = b - A h,
     // r0 = p = r.
     auto restart = [&]() -> lbm_status {
-        apply_kernel<1, kAdj><<<L.grid, L.block, 0, st>>>(g, h, kb.r, rho, s, nullptr, kb.part, L.nblocks);
+        apply(K1{}, h, kb.r, nullptr);
         if (!host_sum(L.nblocks, 1, d2)) return LBM_ERR_CUDA;
-        ++res->matvecs;
+        res->matvecs += static_cast<uint64_t>(m);
         rr = d2[0];
         if (!isfinite(rr)) return LBM_ERR_NONFINITE;
         vec_kernel<3><<<kDotBlocks, 256, 0, st>>>(cnt, 0.0, 0.0, kb.r0, kb.p, kb.r, nullptr, nullptr, nullptr,
@@ -256,7 +308,7 @@ lbm_status bicgstab(cudaStream_t st, const Launch& L, const Geom& g, const Krylo
     };
     res->rel_residual = sqrt(rr) / bnorm;
     while (res->rel_residual >= tol) {
-        if (max_matvecs && res->matvecs + 3 > max_matvecs) {
+        if (max_matvecs && res->matvecs + 3 * static_cast<uint64_t>(m) > max_matvecs) {
             budget = true;
             break;
         }
@@ -275,9 +327,9 @@ lbm_status bicgstab(cudaStream_t st, const Launch& L, const Geom& g, const Krylo
         }
         const bool fresh = first;
         first = false;
-        apply_kernel<0, kAdj><<<L.grid, L.block, 0, st>>>(g, kb.p, kb.v, rho, nullptr, kb.r0, kb.part, L.nblocks);
+        apply(K0{}, kb.p, kb.v, kb.r0);
         if (!host_sum(L.nblocks, 2, d2)) return LBM_ERR_CUDA;
-        ++res->matvecs;
+        res->matvecs += static_cast<uint64_t>(m);
         if (!isfinite(d2[0]) || !isfinite(d2[1])) return LBM_ERR_NONFINITE;
         // near-breakdown: r0 . v ~ 0 against |r0| |v| (as at the rounding floor)
         if (fabs(d2[0]) <= 1e-12 * sqrt(r0r0 * d2[1])) {
@@ -289,7 +341,7 @@ lbm_status bicgstab(cudaStream_t st, const Launch& L, const Geom& g, const Krylo
         }
         alpha = rho_new / d2[0];
         vec_kernel<1><<<kDotBlocks, 256, 0, st>>>(cnt, alpha, 0.0, kb.s, nullptr, kb.r, kb.v, nullptr, nullptr, nullptr);
-        apply_kernel<2, kAdj><<<L.grid, L.block, 0, st>>>(g, kb.s, kb.t, rho, nullptr, kb.s, kb.part, L.nblocks);
+        apply(K2{}, kb.s, kb.t, kb.s);
         if (!host_sum(L.nblocks, 2, d2)) return LBM_ERR_CUDA;
         omega = d2[1] > 0.0 ? d2[0] / d2[1] : 0.0;
         vec_kernel<2><<<kDotBlocks, 256, 0, st>>>(cnt, alpha, omega, h, kb.r, kb.p, kb.s, kb.t, kb.r0, kb.part);
@@ -297,7 +349,7 @@ lbm_status bicgstab(cudaStream_t st, const Launch& L, const Geom& g, const Krylo
         rr = d2[0];
         rho_old = rho_new;
         rho_new = d2[1];
-        ++res->matvecs;
+        res->matvecs += static_cast<uint64_t>(m);
         ++res->iterations;
         ++since;
         if (!isfinite(rr)) return LBM_ERR_NONFINITE;
@@ -311,10 +363,10 @@ lbm_status bicgstab(cudaStream_t st, const Launch& L, const Geom& g, const Krylo
 
 lbm_status solve(cudaStream_t st, const Launch& L, const Geom& g, const KrylovBuffers& kb, double* h, const double* rho,
                  const double* s, double* p, double* p_prev, double target, double tol, uint64_t max_matvecs,
-                 KrylovResult* res)
+                 int degree, KrylovResult* res)
 {
     bool budget = false;
-    const lbm_status it = bicgstab<false>(st, L, g, kb, h, rho, s, tol, max_matvecs, res, &budget);
+    const lbm_status it = bicgstab<false>(st, L, g, kb, h, rho, s, tol, max_matvecs, degree, res, &budget);
     if (it != LBM_OK) return it;
     // p of the solution, gauged to the target mean (p_prev follows, as after a check)
     pressure_kernel<<<L.grid, L.block, 0, st>>>(g, h, p, kb.part, L.nblocks);
@@ -335,7 +387,7 @@ lbm_status solve_adjoint(cudaStream_t st, const Launch& L, const Geom& g, const 
                          const double* rho, const double* lp, double tol, uint64_t max_matvecs, KrylovResult* res)
 {
     bool budget = false;
-    const lbm_status it = bicgstab<true>(st, L, g, kb, y, rho, lp, tol, max_matvecs, res, &budget);
+    const lbm_status it = bicgstab<true>(st, L, g, kb, y, rho, lp, tol, max_matvecs, 1, res, &budget);
     if (it != LBM_OK) return it;
     return budget ? LBM_ERR_POISSON_BUDGET : LBM_OK;
 }

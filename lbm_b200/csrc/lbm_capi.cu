@@ -88,7 +88,7 @@ struct lbm_handle {
     int pform = LBM_POISSON_KINETIC;     // lbm_poisson_form
     double scalar_scale = 2.0;           // scalar forms: source scale (reference default 2.0)
     double sor_omega = 0.0;              // red-black form: relaxation (0: from the box size)
-    lbm_poisson_accel paccel{1.0, 1.0, 0, 1.0, 0, 0.5, 0, 1.0, 0};   // the reference's accelerator settings
+    lbm_poisson_accel paccel{1.0, 1.0, 0, 1.0, 0, 0.5, 0, 1.0, 0, 0};   // the reference's accelerator settings
     double* and_r = nullptr;             // Anderson-m1 history: previous residual, previous image (15 n each)
     double* and_i = nullptr;
     double* and_part = nullptr;          // 2 x kAndersonBlocks dot partials, and their pinned copy
@@ -148,7 +148,8 @@ void free_all(lbm_handle* h)
     }
     if (h->and_host) cudaFreeHost(h->and_host);
     h->and_host = nullptr;
-    double** kv[] = {&h->kb.r, &h->kb.r0, &h->kb.p, &h->kb.v, &h->kb.s, &h->kb.t, &h->kb.part};
+    double** kv[] = {&h->kb.r, &h->kb.r0, &h->kb.p, &h->kb.v, &h->kb.s, &h->kb.t, &h->kb.part,
+                     &h->kb.w1, &h->kb.w2, &h->kb.bm};
     for (double** p : kv) {
         if (*p) cudaFree(*p);
         *p = nullptr;
@@ -503,6 +504,14 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
         const lbm_status s = alloc_buffers(h, set, 8, "Krylov work vectors: device allocation failed");
         if (s != LBM_OK) return s;
     }
+    if (form == LBM_POISSON_KRYLOV && h->paccel.krylov_degree > 1 && !h->kb.w1) {
+        const size_t pop = 15 * static_cast<size_t>(g.n) * sizeof(double);
+        const AllocSlot set[] = {{reinterpret_cast<void**>(&h->kb.w2), pop, 0},
+                                 {reinterpret_cast<void**>(&h->kb.bm), pop, 0},
+                                 {reinterpret_cast<void**>(&h->kb.w1), pop, 0}};
+        const lbm_status s = alloc_buffers(h, set, 3, "Krylov polynomial buffers: device allocation failed");
+        if (s != LBM_OK) return s;
+    }
     if (dual) {
         const lbm_status s = ensure_dual_buffer(h);
         if (s != LBM_OK) return s;
@@ -571,7 +580,7 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
         KrylovResult kr;
         Fp64Buffers& b = h->b;
         const lbm_status ks = krylov::solve(st, L, g, h->kb, b.h[0], b.rho, b.s, b.p, b.p_prev, dh.target,
-                                            h->pcfg.tolerance, h->pcfg.max_sweeps, &kr);
+                                            h->pcfg.tolerance, h->pcfg.max_sweeps, h->paccel.krylov_degree, &kr);
         if (ks != LBM_OK && ks != LBM_ERR_POISSON_BUDGET)
             return fail(h, ks, ks == LBM_ERR_NONFINITE ? "Krylov Poisson solve broke down or diverged"
                                                        : "Krylov Poisson solve failed");
@@ -1108,6 +1117,8 @@ lbm_status lbm_set_poisson_accel(lbm_handle* h, const lbm_poisson_accel* a)
     if (!(a->two_grid_strength >= 0.0))
         return fail(h, LBM_ERR_BAD_ARG, "Poisson two-grid strength must be non-negative");
     if (!std::isfinite(a->source_aware_scale)) return fail(h, LBM_ERR_BAD_ARG, "source-aware scale must be finite");
+    if (a->krylov_degree < 0 || a->krylov_degree > 16)
+        return fail(h, LBM_ERR_BAD_ARG, "Krylov polynomial degree must be in [0, 16]");
     if ((a->pressure_relax_scale != 1.0 || a->fixed_point_relax != 1.0 || a->anderson_m1 || a->two_grid ||
          a->source_aware_init || a->spatial_diagnostics) && h->precision != LBM_PRECISION_FP64)
         return fail(h, LBM_ERR_BAD_ARG, "the Poisson accelerators run in FP64 precision only");

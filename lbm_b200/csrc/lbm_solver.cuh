@@ -195,6 +195,7 @@ struct KrylovBuffers {
     double *r, *r0, *p, *v, *s, *t;
     double* part;
     double* host;
+    double *w1, *w2, *bm;   // polynomial form (degree > 1): powers of the operator, right-hand side
 };
 struct KrylovResult {
     uint64_t matvecs = 0;      // applications of (I - K): two per iteration plus the initial residual
@@ -208,9 +209,11 @@ namespace krylov {
 // the solution's p gauged to `target`.  Stops at ||r|| < tol ||b||;
 // LBM_ERR_POISSON_BUDGET past max_matvecs applications (0: no cap),
 // LBM_ERR_NONFINITE on a breakdown or a non-finite residual.
+// degree > 1: BiCGSTAB on the polynomially preconditioned system
+// (I - K^m) h = (I + K + ... + K^(m-1)) b, m = degree (kb.w1, w2, bm needed).
 lbm_status solve(cudaStream_t st, const Launch& L, const Geom& g, const KrylovBuffers& kb, double* h, const double* rho,
                  const double* s, double* p, double* p_prev, double target, double tol, uint64_t max_matvecs,
-                 KrylovResult* res);
+                 int degree, KrylovResult* res);
 // The adjoint Poisson problem y = M^T (pull from x + c_q of y) + lam_p
 // (periodic boxes) by the same method: y initial guess in, solution out.
 lbm_status solve_adjoint(cudaStream_t st, const Launch& L, const Geom& g, const KrylovBuffers& kb, double* y,

@@ -158,6 +158,27 @@ def test_krylov_reaches_the_kinetic_fixed_point():
     assert e.value.status == 4 and "replay" in str(e.value)
 
 
+@pytest.mark.parametrize("degree", [4, 8])
+def test_krylov_polynomial_form_reaches_the_same_fixed_point(degree):
+    """BiCGSTAB on the polynomially preconditioned system (I - K^m) h =
+    (I + ... + K^(m-1)) b (lbm_poisson_accel.krylov_degree = m) reaches the
+    kinetic form's fixed point as the plain system does (fields within 1e-8
+    of the kinetic form run to 1e-12)."""
+    p, f = case(True)
+    a = gpu_box(p, f, "kinetic", 1e-12, cap=2000000)
+    b = gpu_box(p, f, "krylov", 1e-10, cap=2000000)
+    b.set_poisson_accel(krylov_degree=degree)
+    a.step(2)
+    sb = b.step(2)
+    assert all(s["converged"] == 1 for s in sb)
+    fa, fb = a.download_fields(), b.download_fields()
+    for k in L.FIELDS:
+        assert rel_err(fb[k], fa[k]) <= 1e-8, k
+    with pytest.raises(L.LBMError) as e:
+        b.set_poisson_accel(krylov_degree=17)
+    assert e.value.status == 4
+
+
 def test_accelerators_through_python():
     """lbm_set_poisson_accel from Python: the one-pass form with every
     accelerator converges; the kinetic form refuses the one-pass-only
