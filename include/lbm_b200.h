@@ -276,7 +276,7 @@ typedef enum {
                                     system is inconsistent), no dual residual, no two-grid or
                                     spatial diagnostics, no lbm_step_replay (it has no sweep count
                                     to replay).  A NaN/Inf source or start iterate returns
-                                    LBM_ERR_NONFINITE; five restarts in a row that do not lower
+                                    LBM_ERR_NONFINITE; twenty restarts in a row that do not lower
                                     the true residual (a tolerance below the rounding floor)
                                     stop the solve with LBM_ERR_POISSON_BUDGET */
     LBM_POISSON_VARCOEF_RB = 5   /* not a reference form: div((1/rho) grad p) = s, the continuum

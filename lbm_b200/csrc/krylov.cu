@@ -279,7 +279,7 @@ lbm_status bicgstab(cudaStream_t st, const Launch& L, const Geom& g, const Krylo
     // the attainable rounding floor would otherwise restart forever when no
     // matvec budget is set.  After kStalledRestarts of them the solve stops
     // with LBM_ERR_POISSON_BUDGET (the iterate is the last one).
-    constexpr int kStalledRestarts = 5;
+    constexpr int kStalledRestarts = 20;
     double best = rr;
     int stalled = 0;
     // Restart from the true residual of the current iterate: r = b - A h,

@@ -515,22 +515,11 @@ __device__ __forceinline__ void sweep2_run(const Geom& g, int x0, int y0, int z0
 
     float a[Q];
     float a_om = 0.f, a_s = 0.f;
-    // The in-plane source offsets of this thread's region cell (x - c_x, y -
-    // c_y wrapped) are fixed for the whole march: only the plane changes.
-    const int plane = g.lx * g.ly;
-    const int xo[3] = {xw == g.lx - 1 ? 0 : xw + 1, xw, xw == 0 ? g.lx - 1 : xw - 1};   // by c_x = -1, 0, +1
-    const int yo[3] = {(yw == g.ly - 1 ? 0 : yw + 1) * g.lx, yw * g.lx, (yw == 0 ? g.ly - 1 : yw - 1) * g.lx};
     auto prefetch = [&](int zz) {        // issue sweep k's pulls for plane zz
         if (!owner) return;
         const int zw = zz < 0 ? zz + g.lz : (zz >= g.lz ? zz - g.lz : zz);
-        const int zo[3] = {(zw == g.lz - 1 ? 0 : zw + 1) * plane, zw * plane,
-                           (zw == 0 ? g.lz - 1 : zw - 1) * plane};
-        static_for<0, Q>([&](auto qc) {
-            constexpr int q = decltype(qc)::value;
-            const unsigned idx = static_cast<unsigned>(zo[cz(q) + 1] + yo[cy(q) + 1] + xo[cx(q) + 1]);
-            a[q] = __ldg(hin + static_cast<unsigned>(q * n) + idx);
-        });
-        const int c = zo[1] + yo[1] + xo[1];
+        pull_regs32(a, hin, n, g, xw, yw, zw);
+        const int c = (zw * g.ly + yw) * g.lx + xw;
         a_om = __ldg(omega + c);
         a_s = __ldg(s + c);
     };
