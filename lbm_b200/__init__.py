@@ -436,8 +436,9 @@ class InamuroCUDA:
     def set_poisson_accel(self, **kw):
         """lbm_set_poisson_accel: the reference's accelerators (pressure_relax_scale,
         fixed_point_relax, anderson_m1, anderson_beta_max, two_grid,
-        two_grid_strength, source_aware_init, source_aware_scale); unnamed
-        settings keep their current values."""
+        two_grid_strength, source_aware_init, source_aware_scale), plus
+        krylov_degree (the Neumann polynomial degree of the BiCGSTAB form, 0/1
+        = plain, at most 16); unnamed settings keep their current values."""
         a = PoissonAccel()
         self._check(self._lib.lbm_get_poisson_accel(self._h, C.byref(a)), "get_poisson_accel")
         for k, v in kw.items():
