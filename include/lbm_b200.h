@@ -489,8 +489,10 @@ const char* lbm_batch_last_error(const lbm_batch* b);
  * FP64 kernel of the solver (bitwise the same values); the matching backward
  * call takes the adjoint (dJ/d output) of every output and returns the adjoint
  * of every input at the same state, i.e. the transposed Jacobian applied to
- * it.  Backward calls need lbm_params.periodic_x = 1 (LBM_ERR_BAD_ARG
- * otherwise): the slip walls are not differentiated.
+ * it.  Both x boundaries are differentiated: with the reference's slip walls
+ * (lbm_params.periodic_x = 0) the backward calls transpose the walls'
+ * overwrite of the pulled populations and the mirrored x neighbours of the
+ * stencils and of the correction.
  *
  * Collide (CPU/Inamuro.cpp:134-250): pull of the previous post-collision
  * populations fin/gin, then the f and g collisions with the stencils of phi,
@@ -521,9 +523,10 @@ lbm_status lbm_correct_backward(const lbm_params* p, const double* press, const 
                                 const double* lam_v, const double* lam_w, double* lam_p, double* lam_rho);
 
 /* ---- adjoint runs: gradients through whole FP64 time steps ------------------
- * A forward run of n steps of one periodic FP64 box (lbm_params.periodic_x =
- * 1) from loaded macro fields, then its reverse pass: given the adjoint of the
- * final fields (dJ/d phi_T, ... for an objective J of them), the gradient of J
+ * A forward run of n steps of one FP64 box (slip walls or periodic x, as
+ * lbm_params.periodic_x says) from loaded macro fields, then its reverse
+ * pass: given the adjoint of the final fields (dJ/d phi_T, ... for an
+ * objective J of them), the gradient of J
  * with respect to the loaded fields and to k_f (kappa_f).  The Poisson solve
  * is differentiated implicitly: each step's reverse pass solves one adjoint
  * problem of the solve's fixed point (the transposed kinetic sweep, iterated

@@ -671,7 +671,8 @@ def correct_backward(p, press, rho, lam_u, lam_v, lam_w, lam_p, lam_rho) -> None
 
 
 class Adjoint:
-    """Gradients through whole FP64 steps of one periodic box (lbm_adjoint_*):
+    """Gradients through whole FP64 steps of one box, slip walls or periodic x
+    (lbm_adjoint_*):
     forward(fields, n_steps) runs and checkpoints, backward(lam) returns
     dJ/d(loaded fields) and dJ/dk_f for the adjoint lam of the final fields."""
 

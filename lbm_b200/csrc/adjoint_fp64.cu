@@ -12,11 +12,14 @@
 //   moments  (f*, g*) -> (phi, rho, u*, v*, w*)     CPU/Inamuro.cpp:294-346
 //   correct  (u*, v*, w*, p, rho) -> (u, v, w)     CPU/Inamuro.cpp:794-823
 // The pull stream is a permutation, so its transpose is a push; the stencils'
-// transposes gather the per-cell stencil adjoints from x - c_k.  Periodic x
-// only (lbm_params.periodic_x = 1): the slip walls' overwrite and mirrored
-// stencils are not differentiated.  Derivatives are exact for the real-number
-// map; they match centred finite differences of the FP64 forward kernels
-// (tests/test_gpu_adjoint.py).
+// transposes gather the per-cell stencil adjoints from x - c_k.  With the
+// reference's x slip walls (CPU/Inamuro.cpp:589-623) the overwrite after the
+// pull is transposed too (slip_T: a discarded incoming population gets 0, its
+// mirror gains its adjoint), and so are the stencils' and the correction's
+// mirrored x neighbours (x - 1 -> 1 at x = 0, x + 1 -> lx - 2 at x = lx - 1,
+// CPU/Inamuro.hpp:230-248).  Derivatives are exact for the real-number map;
+// they match centred finite differences of the FP64 forward kernels on both
+// x boundaries (tests/test_gpu_adjoint.py).
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
@@ -127,7 +130,9 @@ collide_adjoint_local(Geom g, Phys P, const double* __restrict__ phi, const doub
         const long long src = pull_src<q>(g, wr, x, y, z);
         // ---- f: out = fv (1 - 1/tau_f) + feq / tau_f ----
         const double lF = lf[(long long)q * n + c];
-        if (lfin) lfin[(long long)q * n + src] = kFirst ? 0.0 : lF * kf1;
+        if (lfin)
+            lfin[(long long)q * n + src] =
+                kFirst ? 0.0 : slip_T<q>(g, x, [&](auto k) { return lf[decltype(k)::value * n + c]; }) * kf1;
         const double le = kFirst ? lF : lF * kf2;   // adjoint of f_eq
         if constexpr (q == 0) {
             a_fei += le;
@@ -150,7 +155,9 @@ collide_adjoint_local(Geom g, Phys P, const double* __restrict__ phi, const doub
         }
         // ---- g: out = gv (1 - 1/tau_g) + geq / tau_g + 3 E mu lapdot / rho ----
         const double lG = lg[(long long)q * n + c];
-        if (lgin) lgin[(long long)q * n + src] = kFirst ? 0.0 : lG * kg1;
+        if (lgin)
+            lgin[(long long)q * n + src] =
+                kFirst ? 0.0 : slip_T<q>(g, x, [&](auto k) { return lg[decltype(k)::value * n + c]; }) * kg1;
         const double lq = kFirst ? lG : lG * kg2;   // adjoint of g_eq
         const double Cq = -2.0 / 3.0 * F * P.k_g;   // (2/3 F k_g / rho) sum_rho term coefficient
         a_sumrho += Cq / lr * lq;
@@ -222,7 +229,9 @@ collide_adjoint_local(Geom g, Phys P, const double* __restrict__ phi, const doub
 }
 
 // Transpose of one field's stencils at cell t: the cells c = t - c_k read t as
-// their neighbour k.
+// their neighbour k.  With the slip walls x does not wrap, and the wall cells
+// read the mirrored neighbour: x = 0 reads x = 1 for c_x = -1, x = lx - 1
+// reads x = lx - 2 for c_x = +1.
 __device__ __forceinline__ double stencil_T(const Geom& g, int x, int y, int z, long long t,
                                             const double* __restrict__ agx, const double* __restrict__ agy,
                                             const double* __restrict__ agz, const double* __restrict__ alap)
@@ -230,9 +239,21 @@ __device__ __forceinline__ double stencil_T(const Geom& g, int x, int y, int z, 
     double s = 0.0, l = 0.0;
     static_for<1, Q>([&](auto kc) {
         constexpr int k = decltype(kc)::value;
-        const long long c = nb(g, x, y, z, -cx(k), -cy(k), -cz(k));
-        s += cx(k) * agx[c] + cy(k) * agy[c] + cz(k) * agz[c];
-        if (alap) l += alap[c];
+        auto add = [&](long long c) {
+            s += cx(k) * agx[c] + cy(k) * agy[c] + cz(k) * agz[c];
+            if (alap) l += alap[c];
+        };
+        if (g.periodic_x) {
+            add(nb(g, x, y, z, -cx(k), -cy(k), -cz(k)));
+        } else {
+            const int xc = x - cx(k);
+            if (xc >= 0 && xc < g.lx) add(nb(g, xc, y, z, 0, -cy(k), -cz(k)));
+            if constexpr (cx(k) == -1) {
+                if (x == 1) add(nb(g, 0, y, z, 0, -cy(k), -cz(k)));
+            } else if constexpr (cx(k) == 1) {
+                if (x == g.lx - 2) add(nb(g, g.lx - 1, y, z, 0, -cy(k), -cz(k)));
+            }
+        }
     });
     double out = s / 10.0;
     if (alap) out += (l - 14.0 * alap[t]) / 5.0;
@@ -258,7 +279,8 @@ collide_adjoint_gather(Geom g, const double* __restrict__ scratch, double* __res
 }
 
 // Moments backward: phi = sum_q f*(x - c_q), rho = rho(phi) (the sine
-// interpolation, CPU/Inamuro.cpp:315-327), u* = sum_q c_q g*(x - c_q).
+// interpolation, CPU/Inamuro.cpp:315-327), u* = sum_q c_q g*(x - c_q), the
+// pulled populations overwritten at the slip walls (slip_T).
 // kAdd: add to lf, lg instead of overwriting them.
 template <bool kAdd>
 __global__ void __launch_bounds__(256)
@@ -282,7 +304,11 @@ moments_adjoint(Geom g, Phys P, const double* __restrict__ phi, const double* __
     static_for<0, Q>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
         const long long src = pull_src<q>(g, wr, x, y, z);
-        const double vf = a_phi, vg = cx(q) * au + cy(q) * av + cz(q) * aw;
+        const double vf = slip_T<q>(g, x, [&](auto) { return a_phi; });
+        const double vg = slip_T<q>(g, x, [&](auto k) {
+            constexpr int j = decltype(k)::value;
+            return cx(j) * au + cy(j) * av + cz(j) * aw;
+        });
         if constexpr (kAdd) {
             lf[(long long)q * n + src] += vf;
             lg[(long long)q * n + src] += vg;
@@ -295,7 +321,10 @@ moments_adjoint(Geom g, Phys P, const double* __restrict__ phi, const double* __
 
 // Correction backward: u = u* - (p(x+1) - p(x-1)) / (2 rho), likewise v, w.
 // lu, lv, lw: adjoints of u, v, w (= those of u*, v*, w*); outputs the
-// adjoints of p and rho (kAdd: added to lp, lrho).
+// adjoints of p and rho (kAdd: added to lp, lrho).  With the slip walls the
+// x neighbours are mirrored (CPU/Inamuro.cpp:794-823): a wall cell reads the
+// same cell as both neighbours, so its x difference is identically zero and
+// it contributes nothing, and x does not wrap.
 template <bool kAdd>
 __global__ void __launch_bounds__(256)
 correct_adjoint(Geom g, const double* __restrict__ p, const double* __restrict__ rho,
@@ -307,11 +336,21 @@ correct_adjoint(Geom g, const double* __restrict__ p, const double* __restrict__
     const long long t = cell_of(g, x, y, z);
     const double* la[3] = {lu, lv, lw};
     const int d[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    const Mirror mr(g, x, y, z);
     double ap = 0.0, ar = 0.0;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const long long cm = nb(g, x, y, z, -d[a][0], -d[a][1], -d[a][2]);   // reads t as its + neighbour
         const long long cp = nb(g, x, y, z, d[a][0], d[a][1], d[a][2]);      // reads t as its - neighbour
+        if (a == 0 && !g.periodic_x) {
+            // x: interior cells only (x = 1 .. lx-2), no wrap
+            const double am = (x - 1 >= 1) ? -la[a][cm] / (2.0 * rho[cm]) : 0.0;
+            const double bp = (x + 1 <= g.lx - 2) ? la[a][cp] / (2.0 * rho[cp]) : 0.0;
+            ap += am + bp;
+            const double grad = p[cell_of(g, mr.xp, y, z)] - p[cell_of(g, mr.xm, y, z)];
+            ar += la[a][t] * grad / (2.0 * rho[t] * rho[t]);
+            continue;
+        }
         ap += -la[a][cm] / (2.0 * rho[cm]) + la[a][cp] / (2.0 * rho[cp]);
         const double grad = p[cp] - p[cm];
         ar += la[a][t] * grad / (2.0 * rho[t] * rho[t]);
@@ -340,6 +379,20 @@ correct_adjoint(Geom g, const double* __restrict__ p, const double* __restrict__
 //   dJ/drho = -sum_q mu_q (hv_q - E_q p) / (tau^2 rho^2)   (hv = R h*).
 // The constant mode (K^T 1 = 1) only shifts dJ/ds by a constant, which the
 // source's mean projection and the periodic stencils' transposes remove.
+//
+// Slip walls: R becomes W R, W the overwrite of the incoming populations at
+// x = 0 and lx-1 (not a permutation), and the pull from x + c_q becomes the
+// transposed pull tpull (W^T, then the push).  K no longer conserves
+// sum(h): (I - K) keeps the right null vector E (uniform p), but its left
+// null vector l is not uniform, so the forward system is inconsistent and the
+// sweeps drift along E by delta per sweep, which the gauge removes at each
+// check.  The converged, gauged state solves the bordered system
+//   (I - K) h + delta E = b,   mean(P h) = target,
+// whose adjoint is (I - K)^T mu + nu P^T 1/N = P^T lam_p with E . mu = 0:
+// nu = sum(lam_p) (the gauge's share, as above), and the transposed
+// iteration keeps E . mu fixed (E^T K^T = E^T because K E = E) at its start
+// value 0 (the start y = lam_p - mean has E . y = 0), so it converges to that
+// solution without l itself.
 
 // y_q(x) = lp(x) for every q.
 __global__ void __launch_bounds__(256)
@@ -369,8 +422,8 @@ padj_pi(Geom g, const double* __restrict__ y, double* __restrict__ pi)
 // One transposed sweep.  kCheck: also the relative change of
 // pi = sum_q y_q against the copy kept from the previous check (block
 // partials of sum |pi - pi_prev| and sum |pi|), and the new copy.  The pull
-// from x + c_q uses the forward sweep's wrap table with the directions
-// reversed; kOff32: 32-bit offsets (15 n < 2^31).
+// from x + c_q (tpull) uses the forward sweep's wrap table with the
+// directions reversed; kOff32: 32-bit offsets (15 n < 2^31).
 template <bool kCheck, bool kOff32>
 __global__ void __launch_bounds__(256)
 padj_sweep(Geom g, const double* __restrict__ yin, double* __restrict__ yout, const double* __restrict__ rho,
@@ -389,10 +442,7 @@ padj_sweep(Geom g, const double* __restrict__ yin, double* __restrict__ yout, co
         double S = 0.0;
         static_for<0, Q>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
-            const I src = (static_cast<I>(pick<cz(q)>(w.zm, z, w.zp)) * static_cast<I>(g.ly) +
-                           static_cast<I>(pick<cy(q)>(w.ym, yy, w.yp))) * static_cast<I>(g.lx) +
-                          static_cast<I>(pick<cx(q)>(w.xm, x, w.xp));
-            m[q] = __ldg(yin + static_cast<I>(q) * n + src);
+            m[q] = tpull<q>(yin, n, g, w, x, yy, z);
             S += wE(q) * m[q];
         });
         const double tau = 1.0 / __ldg(rho + c) + 0.5;
@@ -425,13 +475,15 @@ padj_final(Geom g, const double* __restrict__ y, const double* __restrict__ h, c
     const long long c = cell_of(g, x, yy, z);
     double mu[Q], hv[Q];
     double p = 0.0, smu = 0.0;
+    const Wrap w(g, x, yy, z);
     static_for<0, Q>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
-        mu[q] = y[(long long)q * n + nb(g, x, yy, z, cx(q), cy(q), cz(q))];
+        mu[q] = tpull<q>(y, n, g, w, x, yy, z);
         hv[q] = h[(long long)q * n + nb(g, x, yy, z, -cx(q), -cy(q), -cz(q))];
-        p += hv[q];
         smu += wE(q) * mu[q];
     });
+    bounce_regs(hv, g, x);
+    static_for<0, Q>([&](auto qc) { p += hv[decltype(qc)::value]; });
     double t = 0.0;
     static_for<0, Q>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
@@ -563,10 +615,9 @@ struct Box {
     Launch L;
 };
 
-lbm_status make_box(const lbm_params* prm, bool need_periodic, Box& b)
+lbm_status make_box(const lbm_params* prm, Box& b)
 {
     if (!prm || prm->lx < 2 || prm->ly < 1 || prm->lz < 1 || prm->lz > 65535) return LBM_ERR_BAD_ARG;
-    if (need_periodic && !prm->periodic_x) return LBM_ERR_BAD_ARG;
     b.g.lx = prm->lx;
     b.g.ly = prm->ly;
     b.g.lz = prm->lz;
@@ -594,7 +645,7 @@ lbm_status lbm_collide_forward(const lbm_params* prm, const double* fin, const d
                                double* gout, double* dux, double* dvy, double* dwz)
 {
     Box b;
-    const lbm_status s = make_box(prm, false, b);
+    const lbm_status s = make_box(prm, b);
     if (s != LBM_OK) return s;
     if (!fin || !gin || !phi || !rho || !u || !v || !w || !fout || !gout || !dux || !dvy || !dwz) return LBM_ERR_BAD_ARG;
     double* part = nullptr;
@@ -612,7 +663,7 @@ lbm_status lbm_collide_backward(const lbm_params* prm, const double* fin, const 
                                 double* lam_phi, double* lam_rho, double* lam_u, double* lam_v, double* lam_w)
 {
     Box b;
-    const lbm_status s = make_box(prm, true, b);
+    const lbm_status s = make_box(prm, b);
     if (s != LBM_OK) return s;
     if (!phi || !rho || !u || !v || !w || !lam_fout || !lam_gout || !lam_dux || !lam_dvy || !lam_dwz || !lam_fin ||
         !lam_gin || !lam_phi || !lam_rho || !lam_u || !lam_v || !lam_w)
@@ -634,7 +685,7 @@ lbm_status lbm_moments_forward(const lbm_params* prm, const double* f, const dou
                                double* u, double* v, double* w)
 {
     Box b;
-    const lbm_status s = make_box(prm, false, b);
+    const lbm_status s = make_box(prm, b);
     if (s != LBM_OK) return s;
     if (!f || !g || !phi || !rho || !u || !v || !w) return LBM_ERR_BAD_ARG;
     double* part = nullptr;
@@ -650,7 +701,7 @@ lbm_status lbm_moments_backward(const lbm_params* prm, const double* phi, const 
                                 double* lam_f, double* lam_g)
 {
     Box b;
-    const lbm_status s = make_box(prm, true, b);
+    const lbm_status s = make_box(prm, b);
     if (s != LBM_OK) return s;
     if (!phi || !lam_phi || !lam_rho || !lam_u || !lam_v || !lam_w || !lam_f || !lam_g) return LBM_ERR_BAD_ARG;
     moments_adjoint<false><<<b.L.grid, b.L.block>>>(b.g, b.P, phi, lam_phi, lam_rho, lam_u, lam_v, lam_w, lam_f, lam_g);
@@ -661,7 +712,7 @@ lbm_status lbm_correct_forward(const lbm_params* prm, double* u, double* v, doub
                                const double* rho)
 {
     Box b;
-    const lbm_status s = make_box(prm, false, b);
+    const lbm_status s = make_box(prm, b);
     if (s != LBM_OK) return s;
     if (!u || !v || !w || !p || !rho) return LBM_ERR_BAD_ARG;
     fp64::correct(0, b.L, b.g, u, v, w, p, rho);
@@ -672,7 +723,7 @@ lbm_status lbm_correct_backward(const lbm_params* prm, const double* p, const do
                                 const double* lam_v, const double* lam_w, double* lam_p, double* lam_rho)
 {
     Box b;
-    const lbm_status s = make_box(prm, true, b);
+    const lbm_status s = make_box(prm, b);
     if (s != LBM_OK) return s;
     if (!p || !rho || !lam_u || !lam_v || !lam_w || !lam_p || !lam_rho) return LBM_ERR_BAD_ARG;
     correct_adjoint<false><<<b.L.grid, b.L.block>>>(b.g, p, rho, lam_u, lam_v, lam_w, lam_p, lam_rho);

@@ -482,10 +482,6 @@ lbm_status lbm_adjoint_create(const lbm_params* p, int device, const lbm_adjoint
         return LBM_ERR_BAD_ARG;
     }
     *out = nullptr;
-    if (!p->periodic_x) {
-        g_adj_create_error = "adjoint runs need periodic_x = 1 (the slip walls are not differentiated)";
-        return LBM_ERR_BAD_ARG;
-    }
     if ((cfg->binomial_checkpoints == 0 && cfg->checkpoint_interval < 1) || cfg->binomial_checkpoints < 0 ||
         (cfg->precision != 0 && cfg->precision != 1) ||
         cfg->check_interval < 1 || !(cfg->tolerance > 0.0) ||

@@ -33,32 +33,16 @@ __device__ __forceinline__ bool kcell(const Geom& g, int& x, int& y, int& z)
     return x < g.lx && y < g.ly;
 }
 
-// x slip overwrite of pulled populations (CPU/Inamuro.cpp:589-623).
-__device__ __forceinline__ void kbounce(double (&v)[Q], const Geom& g, int x)
-{
-    if (g.periodic_x) return;
-    if (x == 0) {
-        static_for<0, Q>([&](auto qc) {
-            constexpr int q = decltype(qc)::value;
-            if constexpr (bounce_left(q) != q) v[q] = v[bounce_left(q)];
-        });
-    }
-    if (x == g.lx - 1) {
-        static_for<0, Q>([&](auto qc) {
-            constexpr int q = decltype(qc)::value;
-            if constexpr (bounce_right(q) != q) v[q] = v[bounce_right(q)];
-        });
-    }
-}
-
 // out = in - K src (kinds 0, 2), or out = b - (in - K src) (kind 1, a true
 // residual), with b = bvec when given, else b_q = -(E/3) s; src = in for the
 // plain operator I - K, src = K^(m-1) in for the polynomial form I - K^m.
 // Kind 3: out = K src alone (no partial sums).  Partial sums: kind 0
 // dot(w, out) and dot(out, out); kind 1 dot(out, out); kind 2 dot(w, out)
-// and dot(out, out).  kAdj: the adjoint solve's operator B = M^T o (pull from
+// and dot(out, out).  kAdj: the adjoint solve's operator B = M^T o (the
+// transposed pull tpull: the slip overwrite's transpose, then the pull from
 // x + c_q) instead of K (M^T m = (1 - 1/tau) m + (sum_k E_k m_k) / tau per
-// cell; periodic boxes), and b_q = s (the adjoint of p, the same for every q).
+// cell), and b_q = s (the adjoint of p, the same for every q).  Its system is
+// consistent on both x boundaries: E^T B = E^T and s has zero sum.
 template <int kKind, bool kAdj>
 __global__ void __launch_bounds__(256)
 apply_kernel(Geom g, const double* __restrict__ in, const double* __restrict__ src, double* __restrict__ out,
@@ -76,13 +60,11 @@ apply_kernel(Geom g, const double* __restrict__ in, const double* __restrict__ s
         static_for<0, Q>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
             if constexpr (kAdj)
-                hv[q] = __ldg(src + (long long)q * n + cell_of(g, pick<cx(q)>(wr.xm, x, wr.xp),
-                                                               pick<cy(q)>(wr.ym, y, wr.yp),
-                                                               pick<cz(q)>(wr.zm, z, wr.zp)));
+                hv[q] = tpull<q>(src, n, g, wr, x, y, z);
             else
                 hv[q] = __ldg(src + (long long)q * n + pull_src<q>(g, wr, x, y, z));
         });
-        if constexpr (!kAdj) kbounce(hv, g, x);
+        if constexpr (!kAdj) bounce_regs(hv, g, x);
         double p = 0.0;
         static_for<0, Q>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
@@ -167,7 +149,7 @@ pressure_kernel(Geom g, const double* __restrict__ h, double* __restrict__ p, do
             constexpr int q = decltype(qc)::value;
             hv[q] = __ldg(h + (long long)q * g.n + pull_src<q>(g, wr, x, y, z));
         });
-        kbounce(hv, g, x);
+        bounce_regs(hv, g, x);
         double pv = 0.0;
 #pragma unroll
         for (int q = 0; q < Q; ++q) pv += hv[q];

@@ -9,6 +9,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 #include <utility>
 
 namespace lbm {
@@ -217,6 +218,59 @@ __device__ __forceinline__ int ring_plane(int zz)
     constexpr int S = ring_group_slots(gq);
     const int slot = ((zz % S) + S) % S;
     return ring_group_base(gq) + slot * 5 + ring_rank(q);
+}
+
+// x slip overwrite of pulled populations (CPU/Inamuro.cpp:589-623).
+template <class T>
+__device__ __forceinline__ void bounce_regs(T (&v)[Q], const Geom& g, int x)
+{
+    if (g.periodic_x) return;
+    if (x == 0) {
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            if constexpr (bounce_left(q) != q) v[q] = v[bounce_left(q)];
+        });
+    }
+    if (x == g.lx - 1) {
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            if constexpr (bounce_right(q) != q) v[q] = v[bounce_right(q)];
+        });
+    }
+}
+
+// Transpose of the overwrite for population q at cell x: the adjoint of the
+// pulled (not yet overwritten) q, given a(q') = the adjoint of overwritten
+// population q' at the same cell.  A population the overwrite discards (the
+// incoming ones: c_x = +1 at x = 0, c_x = -1 at x = lx-1) gets 0; the one it
+// copies from gains the adjoint of its copy.
+template <int q, class A>
+__device__ __forceinline__ auto slip_T(const Geom& g, int x, A&& a) -> decltype(a(std::integral_constant<int, q>{}))
+{
+    using T = decltype(a(std::integral_constant<int, q>{}));
+    T v = a(std::integral_constant<int, q>{});
+    if (g.periodic_x) return v;
+    if constexpr (cx(q) == 1) {
+        if (x == 0) return T(0);
+        if (x == g.lx - 1) v += a(std::integral_constant<int, bounce_left(q)>{});
+    } else if constexpr (cx(q) == -1) {
+        if (x == g.lx - 1) return T(0);
+        if (x == 0) v += a(std::integral_constant<int, bounce_right(q)>{});
+    }
+    return v;
+}
+
+// Transposed pull: the value the transpose of "pull from x - c_q, then the
+// slip overwrite" (the sweeps' stream) sends to population q of cell
+// (x, y, z), i.e. slip_T at the neighbour x + c_q of y's populations there.
+// I: the offset type (32-bit when 15 n < 2^31).
+template <int q, class I, class T>
+__device__ __forceinline__ T tpull(const T* __restrict__ y, I n, const Geom& g, const Wrap& w, int x, int yy, int z)
+{
+    const int xs = pick<cx(q)>(w.xm, x, w.xp);
+    const I src = (static_cast<I>(pick<cz(q)>(w.zm, z, w.zp)) * static_cast<I>(g.ly) +
+                   static_cast<I>(pick<cy(q)>(w.ym, yy, w.yp))) * static_cast<I>(g.lx) + static_cast<I>(xs);
+    return slip_T<q>(g, xs, [&](auto qq) { return __ldg(y + static_cast<I>(decltype(qq)::value) * n + src); });
 }
 
 // Stencil neighbour x + c_k.

@@ -13,24 +13,6 @@
 namespace lbm {
 namespace {
 
-template <class T>
-__device__ __forceinline__ void bounce_regs(T (&v)[Q], const Geom& g, int x)
-{
-    if (g.periodic_x) return;
-    if (x == 0) {
-        static_for<0, Q>([&](auto qc) {
-            constexpr int q = decltype(qc)::value;
-            if constexpr (bounce_left(q) != q) v[q] = v[bounce_left(q)];
-        });
-    }
-    if (x == g.lx - 1) {
-        static_for<0, Q>([&](auto qc) {
-            constexpr int q = decltype(qc)::value;
-            if constexpr (bounce_right(q) != q) v[q] = v[bounce_right(q)];
-        });
-    }
-}
-
 template <int Q0 = 0>
 __device__ __forceinline__ void pull_regs(float (&v)[Q], const float* __restrict__ src, const Geom& g,
                                           int x, int y, int z)

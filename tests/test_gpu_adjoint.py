@@ -7,8 +7,11 @@ random direction d of one input and random output adjoints lam,
 With e = 1e-6 of each field's scale the truncation error is O(e^2) and the
 rounding error O(1e-16 / e), so both sides agree to ~1e-10 of the sum of the
 terms' magnitudes; the tolerance is 1e-7 of that sum.  Forward calls are also
-checked against numpy restatements (moments, correction) on the periodic box,
-and a chained collide -> moments gradient against finite differences."""
+checked against numpy restatements (moments, correction), and a chained
+collide -> moments gradient against finite differences.  Every test runs on
+both x boundaries: periodic, and the reference's slip walls (the overwrite of
+the incoming populations at x = 0 and lx-1 after the pull, and the mirrored
+x neighbours of the stencils and the correction)."""
 import numpy as np
 import pytest
 
@@ -34,11 +37,16 @@ def ptr(t):
     return t.data_ptr()
 
 
-def state(seed=3):
-    """A periodic droplet box with an interface (the sine branch of rho(phi)
-    is active), a random small velocity and random populations."""
+BCS = pytest.mark.parametrize("periodic", [1, 0], ids=["periodic_x", "slip_x"])
+BOUNCE_LEFT = {1: 4, 7: 8, 9: 14, 10: 13, 12: 11}     # incoming at x = 0 <- its mirror
+BOUNCE_RIGHT = {v: k for k, v in BOUNCE_LEFT.items()}  # incoming at x = lx-1 <- its mirror
+
+
+def state(seed=3, periodic=1):
+    """A droplet box with an interface (the sine branch of rho(phi) is
+    active), a random small velocity and random populations."""
     p, f = laplace_case(SHAPE, DD=8.0, noise=1e-3, seed=seed)
-    p.periodic_x = 1
+    p.periodic_x = periodic
     rng = np.random.default_rng(seed)
     shp = f["phi"].shape
     n = f["phi"].size
@@ -106,8 +114,9 @@ def collide_bwd(p, x, lam):
     return gr
 
 
-def test_collide_backward_is_the_transposed_jacobian():
-    p, x = state()
+@BCS
+def test_collide_backward_is_the_transposed_jacobian(periodic):
+    p, x = state(periodic=periodic)
     set_taus(p)
     y = collide_fwd(p, x)
     lam = {k: rand_like(y[k], 7 + i) for i, k in enumerate(COLLIDE_OUT)}
@@ -120,11 +129,12 @@ DEPS = {"fout": ("fin", "phi", "u", "v", "w"), "gout": ("gin", "rho", "u", "v", 
         "dux": ("u",), "dvy": ("v",), "dwz": ("w",)}
 
 
-def test_collide_backward_per_output():
+@BCS
+def test_collide_backward_per_output(periodic):
     """One output adjoint at a time (the others zero), so that a wrong term
     cannot hide behind another output's; inputs the output does not depend on
     get exactly zero."""
-    p, x = state(seed=5)
+    p, x = state(seed=5, periodic=periodic)
     set_taus(p)
     y = collide_fwd(p, x)
     for j, o in enumerate(COLLIDE_OUT):
@@ -146,21 +156,33 @@ def moments_fwd(p, x):
     return y
 
 
+def pulled(a, shape, periodic):
+    """The pull stream x - c_q of every population, then (slip walls) the
+    overwrite of the incoming ones by their mirrors (CPU/Inamuro.cpp:589-623)."""
+    v = [np.roll(a[q].reshape(shape), (CZ[q], CY[q], CX[q]), axis=(0, 1, 2)) for q in range(15)]
+    if not periodic:
+        for q, m in BOUNCE_LEFT.items():
+            v[q][:, :, 0] = v[m][:, :, 0]
+        for q, m in BOUNCE_RIGHT.items():
+            v[q][:, :, -1] = v[m][:, :, -1]
+    return v
+
+
 def moments_numpy(p, f, g, shape):
-    lz, ly, lx = shape
-    pull = lambda a, q: np.roll(a[q].reshape(shape), (CZ[q], CY[q], CX[q]), axis=(0, 1, 2))
-    phi = sum(pull(f, q) for q in range(15))
-    u = sum(CX[q] * pull(g, q) for q in range(15))
-    v = sum(CY[q] * pull(g, q) for q in range(15))
-    w = sum(CZ[q] * pull(g, q) for q in range(15))
+    fv, gv = pulled(f, shape, p.periodic_x), pulled(g, shape, p.periodic_x)
+    phi = sum(fv[q] for q in range(15))
+    u = sum(CX[q] * gv[q] for q in range(15))
+    v = sum(CY[q] * gv[q] for q in range(15))
+    w = sum(CZ[q] * gv[q] for q in range(15))
     arg = (phi - (p.fei_L + p.fei_G) / 2) / (p.fei_L - p.fei_G) * np.pi
     rho = (p.rho_L - p.rho_G) / 2 * (np.sin(arg) + 1) + p.rho_G
     rho = np.where(phi <= p.fei_G, p.rho_G, np.where(phi >= p.fei_L, p.rho_L, rho))
     return {"phi": phi, "rho": rho, "u": u, "v": v, "w": w}
 
 
-def test_moments_forward_and_backward():
-    p, s = state(seed=9)
+@BCS
+def test_moments_forward_and_backward(periodic):
+    p, s = state(seed=9, periodic=periodic)
     x = {"f": s["fin"], "g": s["gin"]}
     y = moments_fwd(p, x)
     want = moments_numpy(p, x["f"].cpu().numpy(), x["g"].cpu().numpy(), s["phi"].shape)
@@ -182,13 +204,17 @@ def correct_fwd(p, x):
     return y
 
 
-def test_correct_forward_and_backward():
-    p, x = state(seed=11)
+@BCS
+def test_correct_forward_and_backward(periodic):
+    p, x = state(seed=11, periodic=periodic)
     x["p"] = x["p"] + dev(1e-3 * np.random.default_rng(4).standard_normal(tuple(x["p"].shape)))
     y = correct_fwd(p, x)
     pn, rn = x["p"].cpu().numpy(), x["rho"].cpu().numpy()
     for k, ax in (("u", 2), ("v", 1), ("w", 0)):
         grad = np.roll(pn, -1, axis=ax) - np.roll(pn, 1, axis=ax)
+        if ax == 2 and not periodic:
+            grad[:, :, 0] = 0.0     # mirrored neighbours: x = 0 reads x = 1 on both sides
+            grad[:, :, -1] = 0.0
         want = x[k].cpu().numpy() - grad * (1.0 / (2.0 * rn))
         assert np.max(np.abs(y[k].cpu().numpy() - want)) <= 1e-15 * max(np.max(np.abs(want)), 1e-300), k
     lam = {k: rand_like(y[k], 50 + i) for i, k in enumerate(("u", "v", "w"))}
@@ -200,11 +226,12 @@ def test_correct_forward_and_backward():
 
 
 # ---- chained: collide then moments (the explicit part of a step) -------------
-def test_collide_then_moments_gradient():
+@BCS
+def test_collide_then_moments_gradient(periodic):
     """J = <c, phi' + rho' + u' + v' + w'> after collide -> moments; the
     gradient by moments_backward then collide_backward against finite
     differences of the chained forward calls."""
-    p, x = state(seed=13)
+    p, x = state(seed=13, periodic=periodic)
     set_taus(p)
     y = collide_fwd(p, x)
     m = moments_fwd(p, {"f": y["fout"], "g": y["gout"]})
@@ -223,11 +250,20 @@ def test_collide_then_moments_gradient():
     dot_check(chain, x, lam_m, gr, COLLIDE_IN, seed=300)
 
 
-def test_backward_needs_periodic_x():
-    p, x = state()
-    p.periodic_x = 0
-    y = correct_fwd(p, x)   # forward calls accept the slip walls
-    out = zeros_like(x["p"])
-    with pytest.raises(L.LBMError) as e:
-        L.correct_backward(p, ptr(x["p"]), ptr(x["rho"]), ptr(y["u"]), ptr(y["v"]), ptr(y["w"]), ptr(out), ptr(out))
-    assert e.value.status == 4
+def test_slip_wall_adjoint_differs_from_periodic():
+    """The walls change the transposes: the same state and output adjoints give
+    different input adjoints next to the walls and the same ones in the
+    interior (x = 3 .. lx-4, out of reach of the wall cells' reads)."""
+    grads = []
+    for periodic in (1, 0):
+        p, x = state(seed=17, periodic=periodic)
+        set_taus(p)
+        y = collide_fwd(p, x)
+        lam = {k: rand_like(y[k], 70 + i) for i, k in enumerate(COLLIDE_OUT)}
+        grads.append(collide_bwd(p, x, lam))
+    lz, ly, lx = state()[1]["phi"].shape
+    for k in ("phi", "u"):
+        a = grads[0][k].reshape(lz, ly, lx).cpu().numpy()
+        b = grads[1][k].reshape(lz, ly, lx).cpu().numpy()
+        assert np.array_equal(a[:, :, 3:lx - 3], b[:, :, 3:lx - 3]), k
+        assert not np.allclose(a[:, :, 0], b[:, :, 0]), k

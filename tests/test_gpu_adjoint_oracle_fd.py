@@ -1,10 +1,9 @@
 """Gradients of the GPU adjoint against centred finite differences of the
 reference CPU solver's arithmetic: the FP64 oracle (oracle/lbm_oracle.c, the
-bit-exact restatement of CPU/Inamuro.cpp, with x periodic), not this
-library's own forward.
+bit-exact restatement of CPU/Inamuro.cpp), not this library's own forward.
 
-Box 16^3 periodic, one tanh drop (rho_L/rho_G = 50, seeded phi noise), three
-steps.  J = 0.5 sum (phi_T - phi_target)^2, phi_target the oracle's final phi
+Box 16^3, one tanh drop (rho_L/rho_G = 50, seeded phi noise), three steps,
+on both x boundaries: periodic, and the reference's own slip walls.  J = 0.5 sum (phi_T - phi_target)^2, phi_target the oracle's final phi
 with k_f raised by 5 %.  The oracle's natural exits (relative change 1e-11,
 check 100) fix the sweep counts; the GPU forward and every oracle run of a
 finite difference replay them, so J is a smooth function of the inputs.
@@ -29,7 +28,7 @@ def oracle_final_phi(p, f, sweeps=None, kf=None):
     prm = oracle_params(p)
     if kf is not None:
         prm["k_f"] = kf
-    o = pyoracle.Oracle(p.shape, prm, f, tol=1e-11, max_sweeps=2_000_000, periodic_x=True)
+    o = pyoracle.Oracle(p.shape, prm, f, tol=1e-11, max_sweeps=2_000_000, periodic_x=bool(p.periodic_x))
     counts = []
     for s in range(STEPS):
         info = o.step(0 if sweeps is None else sweeps[s])
@@ -39,10 +38,10 @@ def oracle_final_phi(p, f, sweeps=None, kf=None):
     return phi, counts
 
 
-@pytest.fixture(scope="module")
-def case():
+@pytest.fixture(scope="module", params=[1, 0], ids=["periodic_x", "slip_x"])
+def case(request):
     p, f = laplace_case(SHAPE, DD=8.0, noise=1e-4, seed=41)
-    p.periodic_x = 1
+    p.periodic_x = request.param
     target, _ = oracle_final_phi(p, f, kf=p.k_f * 1.05)
     _, sweeps = oracle_final_phi(p, f)
     a = L.Adjoint(p, checkpoint_interval=2, check_interval=100, tolerance=1e-13, max_sweeps=2_000_000)

@@ -19,7 +19,9 @@ J is a smooth function of the inputs; the base run's Poisson exit (relative
 change 1e-11 between checks) and the adjoint solve's (1e-13) make the
 implicit derivative and that of the replayed run agree far below 1e-6.
 Seven steps with checkpoints every three: two recomputed intervals and a
-partial one."""
+partial one.  The same checks run on the reference's x slip walls (the
+transposed overwrite and mirrored stencils, and the adjoint of the gauged
+solve whose sweeps drift along the constant mode)."""
 import numpy as np
 import pytest
 
@@ -34,9 +36,9 @@ FD_STEP = 1e-6
 TOL = 1e-6
 
 
-def setup_case():
+def setup_case(periodic=1):
     p, f = laplace_case(SHAPE, DD=7.0, noise=1e-4, seed=21)
-    p.periodic_x = 1
+    p.periodic_x = periodic
     rng = np.random.default_rng(5)
     shp = f["phi"].shape
     f["u"] = 0.005 * np.sin(2 * np.pi * np.arange(SHAPE[0]) / SHAPE[0])[None, None, :] * np.ones(shp)
@@ -77,9 +79,8 @@ class Objective:
         return {"phi": y["phi"] - self.target, "rho": self.w_rho, "u": self.w_u, "p": self.w_p}
 
 
-@pytest.fixture(scope="module")
-def run():
-    p, f = setup_case()
+def make_run(periodic):
+    p, f = setup_case(periodic)
     obj = Objective(p, f)
     a = L.Adjoint(p, checkpoint_interval=KINT, check_interval=50, tolerance=1e-13, max_sweeps=2000000)
     poisson(a)
@@ -88,6 +89,16 @@ def run():
     sweeps = a.sweeps()
     grads, stats = a.backward(obj.adjoint(y))
     return p, f, obj, y, sweeps, grads, stats, a
+
+
+@pytest.fixture(scope="module")
+def run():
+    return make_run(1)
+
+
+@pytest.fixture(scope="module")
+def run_walls():
+    return make_run(0)
 
 
 def fd(p, f, obj, sweeps, field=None, d=None, kf=False, step=FD_STEP):
@@ -149,12 +160,52 @@ def test_reverse_pass_bookkeeping(run):
     assert s2["grad_kappa_f"] == stats["grad_kappa_f"]
 
 
-def test_adjoint_needs_periodic_x():
-    p, f = setup_case()
-    p.periodic_x = 0
-    with pytest.raises(L.LBMError) as e:
-        L.Adjoint(p)
-    assert e.value.status == 4 and "periodic" in str(e.value)
+def test_slip_walls_forward_matches_the_solver(run_walls):
+    p, f, obj, y, sweeps, grads, stats, a = run_walls
+    assert p.periodic_x == 0
+    g = L.InamuroCUDA(p, f, precision="fp64")
+    g.set_poisson(check_interval=100, tolerance=1e-11, max_sweeps=400000, fail_on_limit=True)
+    st = g.step(STEPS)
+    assert [int(s["iterations"]) for s in st] == sweeps
+    for k in L.FIELDS:
+        assert np.array_equal(g.download(k), y[k]), k
+
+
+@pytest.mark.parametrize("field,seed,step", [("phi", 1, FD_STEP), ("phi", 2, FD_STEP), ("u", 4, FD_STEP),
+                                             ("p", 5, FD_STEP)])
+def test_slip_walls_gradient_matches_finite_differences(run_walls, field, seed, step):
+    p, f, obj, y, sweeps, grads, stats, a = run_walls
+    rng = np.random.default_rng(seed)
+    scale = max(float(np.max(np.abs(f[field]))), 1e-2)
+    d = scale * rng.standard_normal(f[field].shape)
+    want = fd(p, f, obj, sweeps, field, d, step=step)
+    got = float(np.sum(grads[field] * d))
+    assert abs(got - want) <= TOL * abs(want), (field, got, want)
+
+
+def test_slip_walls_kappa_f_gradient_matches_finite_differences(run_walls):
+    p, f, obj, y, sweeps, grads, stats, a = run_walls
+    want = fd(p, f, obj, sweeps, kf=True)
+    got = stats["grad_kappa_f"]
+    assert abs(got - want) <= TOL * abs(want), (got, want)
+    gp = grads["p"]
+    assert np.ptp(gp) <= 1e-12 * max(np.max(np.abs(gp)), 1e-300)
+
+
+def test_slip_walls_krylov_adjoint_matches_the_sweeps(run_walls):
+    """BiCGSTAB on the walls' adjoint system (consistent: E^T B = E^T and the
+    right-hand side has zero sum) reaches the transposed sweeps' solution."""
+    p, f, obj, y, sweeps, grads, stats, a = run_walls
+    b = L.Adjoint(p, checkpoint_interval=KINT, check_interval=50, tolerance=1e-13, max_sweeps=2000000,
+                  krylov=True, krylov_tolerance=1e-11)
+    poisson(b)
+    b.forward(f, STEPS)
+    g2, s2 = b.backward(obj.adjoint(y))
+    for k in L.FIELDS:
+        scale = float(np.max(np.abs(grads[k])))
+        assert float(np.max(np.abs(g2[k] - grads[k]))) <= 1e-7 * scale, k
+    assert abs(s2["grad_kappa_f"] - stats["grad_kappa_f"]) <= 1e-7 * abs(stats["grad_kappa_f"])
+    b.close()
 
 
 @pytest.mark.parametrize("slots", [1, 2])
