@@ -54,14 +54,16 @@ __device__ __forceinline__ long long nb(const Geom& g, int x, int y, int z, int 
     return cell_of(g, x, y, z);
 }
 
-// Gradient (/10) and laplacian (/5) stencils of one field at a cell.
+// Gradient (/10) and laplacian (/5) stencils of one field at a cell, x
+// neighbours mirrored at the slip walls as in the forward collision.
 __device__ __forceinline__ void grad_lap(const double* __restrict__ f, const Geom& g, int x, int y, int z,
                                          long long c, double& gx, double& gy, double& gz, double& lap)
 {
     double ax = 0.0, ay = 0.0, az = 0.0, al = 0.0;
+    const Mirror m(g, x, y, z);
     static_for<1, Q>([&](auto kc) {
         constexpr int k = decltype(kc)::value;
-        const double val = f[nb(g, x, y, z, cx(k), cy(k), cz(k))];
+        const double val = f[stencil_nb<k>(g, m, x, y, z)];
         ax += cx(k) * val;
         ay += cy(k) * val;
         az += cz(k) * val;
