@@ -989,27 +989,37 @@ def run_poisson_forms(args):
 
 
 def run_krylov(args):
-    """The kinetic Poisson fixed point to a tight tolerance, by the kinetic
-    sweeps (relative change < tol between checks 100 sweeps apart) and by
-    BiCGSTAB (residual < tol), FP64, the head-on workload at --size with x
-    periodic: W warm-up
-    steps, K timed steps each, device time from the handle's CUDA events;
-    reports sweeps (kinetic-map applications) per step, the Poisson time per
-    step and the two forms' difference after the run."""
+    """The kinetic Poisson fixed point by the kinetic sweeps (relative change
+    < --kinetic-tol between checks 100 sweeps apart, default --krylov-tol)
+    and by BiCGSTAB (residual < --krylov-tol) at each polynomial degree, FP64,
+    the head-on workload at --size with the x boundary of --krylov-boundary
+    (the reference's slip walls by default): W warm-up steps, K timed steps
+    each, device time from the handle's CUDA events; reports sweeps
+    (kinetic-map applications) per step, the Poisson time per step and the
+    forms' difference after the run.  --krylov-truth-tol t > 0 also runs the
+    highest degree to residual t and reports every form's error against it
+    (how far each stop leaves p and u from the fixed point)."""
     import lbm_b200 as L
     n = args.size
     p = workload_params(n)
-    p.periodic_x = 1   # the Krylov form needs periodic x
+    p.periodic_x = 1 if args.krylov_boundary == "periodic" else 0
     f = workload_fields(p)
     tol = args.krylov_tol
+    ktol = args.kinetic_tol if args.kinetic_tol > 0 else tol
     out, fields = {}, {}
     degrees = [int(d) for d in args.krylov_degrees.split(",")]
-    for form in ["kinetic"] + [f"krylov_d{d}" for d in degrees]:
+    forms = ["kinetic"] + [f"krylov_d{d}" for d in degrees]
+    if args.krylov_truth_tol > 0:
+        forms.append("truth")
+    for form in forms:
         g = L.InamuroCUDA(p, f, precision="fp64")
-        g.set_poisson(check_interval=100, tolerance=tol, max_sweeps=args.max_sweeps, fail_on_limit=True)
+        ftol = ktol if form == "kinetic" else (args.krylov_truth_tol if form == "truth" else tol)
+        g.set_poisson(check_interval=100, tolerance=ftol, max_sweeps=args.max_sweeps, fail_on_limit=True)
+        if form == "truth":
+            form = f"krylov_d{max(degrees)}_truth"
         g.set_poisson_form("kinetic" if form == "kinetic" else "krylov")
         if form != "kinetic":
-            g.set_poisson_accel(krylov_degree=int(form.split("_d")[1]))
+            g.set_poisson_accel(krylov_degree=int(form.split("_d")[1].split("_")[0]))
         g.step(args.warmup)
         g.reset_timing()
         clk = ClockSampler(0)
@@ -1023,18 +1033,27 @@ def run_krylov(args):
                      "final_relative": stats[-1]["relative_error"], "clocks": clocks}
         fields[form] = g.download_fields()
         g.close()
-    diff = {form: {k: float(np.max(np.abs(fields[form][k] - fields["kinetic"][k])) /
-                       max(float(np.max(np.abs(fields["kinetic"][k]))), 1e-300)) for k in L.FIELDS}
-            for form in fields if form != "kinetic"}
-    best = min((form for form in out if form != "kinetic"), key=lambda k: out[k]["poisson_ms_per_step"])
-    for form in out:
-        if form != "kinetic":
-            out[form]["speedup_vs_kinetic"] = out["kinetic"]["poisson_ms_per_step"] / out[form]["poisson_ms_per_step"]
+
+    def rel(a, b):
+        return {k: float(np.max(np.abs(a[k] - b[k])) / max(float(np.max(np.abs(b[k]))), 1e-300)) for k in L.FIELDS}
+
+    truth = next((form for form in fields if form.endswith("_truth")), None)
+    diff = {form: rel(fields[form], fields["kinetic"]) for form in fields if form not in ("kinetic", truth)}
+    timed = [form for form in out if form not in ("kinetic", truth)]
+    best = min(timed, key=lambda k: out[k]["poisson_ms_per_step"])
+    for form in timed:
+        out[form]["speedup_vs_kinetic"] = out["kinetic"]["poisson_ms_per_step"] / out[form]["poisson_ms_per_step"]
+    if truth:
+        for form in out:
+            if form != truth:
+                out[form]["error_vs_truth"] = rel(fields[form], fields[truth])
     line = {"metric": "Poisson time per step to the kinetic fixed point, kinetic sweeps vs BiCGSTAB",
             "value": out["kinetic"]["poisson_ms_per_step"] / out[best]["poisson_ms_per_step"], "best": best,
             "unit": "speed-up (x)", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(config_dict(n, "fp64"), tolerance=tol), "forms": out, "rel_diff_krylov_vs_kinetic": diff}
+            "config": dict(config_dict(n, "fp64"), boundary_x=args.krylov_boundary, tolerance=tol,
+                           kinetic_tolerance=ktol, truth_tolerance=args.krylov_truth_tol or None),
+            "forms": out, "rel_diff_krylov_vs_kinetic": diff}
     print(json.dumps(line))
     return 0
 
@@ -1182,6 +1201,12 @@ def main(argv=None):
                     help="time the non-Poisson kernels per step with --phase-sweeps sweeps per step")
     ap.add_argument("--phase-sweeps", type=int, default=100)
     ap.add_argument("--krylov-tol", type=float, default=1e-10, help="tolerance of the krylov workload")
+    ap.add_argument("--kinetic-tol", type=float, default=0.0,
+                    help="krylov workload: the kinetic sweeps' relative-change tolerance (0: --krylov-tol)")
+    ap.add_argument("--krylov-truth-tol", type=float, default=0.0,
+                    help="krylov workload: also solve to this residual and report each form's error against it")
+    ap.add_argument("--krylov-boundary", choices=("slip", "periodic"), default="slip",
+                    help="krylov workload: x boundary (slip: the reference's walls)")
     ap.add_argument("--krylov-degrees", default="1,4,8",
                     help="krylov workload: polynomial preconditioner degrees to time (1: plain BiCGSTAB)")
     ap.add_argument("--workload", choices=("headon", "batch", "adjoint", "poisson-forms", "krylov",

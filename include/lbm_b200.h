@@ -271,9 +271,11 @@ typedef enum {
     LBM_POISSON_KRYLOV = 4,      /* not a reference form: the kinetic form's fixed point solved by
                                     BiCGSTAB, stopping at ||b - (I - K) h|| < tolerance ||b|| (the
                                     lbm_poisson_cfg tolerance; max_sweeps caps the applications of
-                                    the kinetic map).  Same fixed point as the kinetic form; FP64,
-                                    periodic x only (with the slip walls' overwrite the singular
-                                    system is inconsistent), no dual residual, no two-grid or
+                                    the kinetic map).  Same fixed point as the kinetic form (with
+                                    the slip walls, the gauged one: the walls' overwrite makes
+                                    the system inconsistent, and the solve runs on the bordered
+                                    system with the sweeps' drift and the gauge); FP64,
+                                    no dual residual, no two-grid or
                                     spatial diagnostics, no lbm_step_replay (it has no sweep count
                                     to replay).  A NaN/Inf source or start iterate returns
                                     LBM_ERR_NONFINITE; twenty restarts in a row that do not lower

@@ -513,7 +513,7 @@ lbm_status lbm_adjoint_create(const lbm_params* p, int device, const lbm_adjoint
     a->n = n;
     const size_t K = cfg->binomial_checkpoints > 0 ? 1 : static_cast<size_t>(cfg->checkpoint_interval);
     if (cfg->krylov) {
-        const size_t parts = 2 * static_cast<size_t>(std::max<long long>(a->view.L.nblocks, kKrylovBlocks));
+        const size_t parts = 3 * static_cast<size_t>(std::max<long long>(a->view.L.nblocks, kKrylovBlocks));
         double** kv[] = {&a->kb.r, &a->kb.r0, &a->kb.p, &a->kb.v, &a->kb.s, &a->kb.t};
         cudaError_t ke = cudaSuccess;
         for (double** p : kv)

@@ -490,7 +490,7 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
     }
     if (form == LBM_POISSON_KRYLOV && !h->kb.r) {
         const size_t pop = 15 * static_cast<size_t>(g.n) * sizeof(double);
-        const size_t parts = 2 * static_cast<size_t>(std::max<long long>(L.nblocks, kKrylovBlocks)) * sizeof(double);
+        const size_t parts = 3 * static_cast<size_t>(std::max<long long>(L.nblocks, kKrylovBlocks)) * sizeof(double);
         // kb.r doubles as the set's "allocated" flag: alloc_set stores it
         // only with all the others
         const AllocSlot set[] = {{reinterpret_cast<void**>(&h->kb.r0), pop, 0},
@@ -1078,10 +1078,6 @@ lbm_status lbm_set_poisson_form(lbm_handle* h, lbm_poisson_form form, double sou
     if (!(omega == 0.0 || (omega > 0.0 && omega < 2.0)))
         return fail(h, LBM_ERR_BAD_ARG, "SOR relaxation must be 0 (automatic) or in (0, 2)");
     const Geom& g = h->geom;
-    if (form == LBM_POISSON_KRYLOV && !g.periodic_x)
-        return fail(h, LBM_ERR_BAD_ARG,
-                    "the Krylov form needs periodic x: the slip walls' overwrite makes the singular system "
-                    "inconsistent, and the sweeps' gauge absorbs what a Krylov solve cannot");
     const bool rb = form == LBM_POISSON_SCALAR_RB || form == LBM_POISSON_VARCOEF_RB;
     if (rb && (g.ly % 2 || g.lz % 2 || (g.periodic_x && g.lx % 2)))
         return fail(h, LBM_ERR_BAD_ARG, "the red-black forms need even extents along the periodic axes");

@@ -188,7 +188,7 @@ void block_abs_sum(cudaStream_t st, const Geom& g, const double* bsum, double* p
 }  // namespace fp64
 
 // BiCGSTAB on the kinetic fixed point (krylov.cu).  Work vectors of 15 n
-// doubles; part/host: at least 2 * max(L.nblocks, kKrylovBlocks) doubles
+// doubles; part/host: at least 3 * max(L.nblocks, kKrylovBlocks) doubles
 // (host pinned).  kKrylovBlocks: grid of the vector updates (8 per SM).
 constexpr int kKrylovBlocks = 1184;
 struct KrylovBuffers {
