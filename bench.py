@@ -188,46 +188,6 @@ def coalescence_workload(n=256, R=28.0, side=60.0, speed=0.01, ratio=1000.0, kf=
     rc = side / np.sqrt(3.0)             # centroid-to-vertex distance
     centres = [(c + rc * np.cos(a), c + rc * np.sin(a), c) for a in (np.pi / 2, np.pi / 2 + 2 * np.pi / 3,
                                                                         np.pi / 2 + 4 * np.pi / 3)]
-    z, y, x = np.meshgrid(np.arange(n, dtype=np.float64), np.arange(n, dtype=np.float64),
-                          np.arange(n, dtype=np.float64), indexing="ij")
-    frac = np.zeros((n, n, n))
-    u = np.zeros((n, n, n))
-    v = np.zeros((n, n, n))
-    for cx_, cy_, cz_ in centres:
-        r = np.sqrt((x - cx_) ** 2 + (y - cy_) ** 2 + (z - cz_) ** 2)
-        fr = 0.5 * (1.0 - np.tanh(2.0 * (r - R) / 4.0))
-        take = fr > frac
-        dx, dy = c - cx_, c - cy_
-        norm = np.hypot(dx, dy)
-        u = np.where(take, speed * dx / norm * fr, u)
-        v = np.where(take, speed * dy / norm * fr, v)
-        frac = np.maximum(frac, fr)
-    rng = np.random.default_rng(seed)
-    phi = p.fei_min + frac * (p.fei_max - p.fei_min) + rng.uniform(-noise, noise, size=frac.shape)
-    rho = p.rho_G + frac * (p.rho_L - p.rho_G)
-    return p, {"phi": phi, "rho": rho, "u": u, "v": v, "w": np.zeros_like(phi), "p": np.zeros_like(phi)}
-
-
-def coalescence_workload(n=256, R=28.0, side=60.0, speed=0.01, ratio=1000.0, kf=0.06, seed=4242, noise=1e-4):
-    """Three-droplet coalescence: an n^3 periodic box, three drops of radius R
-    centred on an equilateral triangle of side `side` in the plane z = n/2
-    (centroid at the box centre), each moving towards the centroid at
-    `speed`; rho_L/rho_G = ratio (rho_G = 1), mu = 0.1 rho, kappa_f = kf,
-    otherwise the Laplace-test physics (a = 1, b = 6.7, T = 0.035,
-    kappa_g = 6e-6, tau = 1, tanh interfaces W = 4, seeded phi noise).  Each
-    drop's profile is phi = phi_min + (phi_max - phi_min) * 0.5 (1 - tanh(2 (r
-    - R) / W)); where profiles overlap the largest is kept, and the velocity is
-    that of the drop whose profile is kept, scaled by it.  Built here: the
-    reference's initializer makes one or two drops on the z axis.  Returns
-    (params, fields)."""
-    import lbm_b200 as L
-    p = L.make_params(lx=n, ly=n, lz=n, rho_L=ratio, rho_G=1.0, mu_L=0.1 * ratio, mu_G=0.1, tauf=1.0, taug=1.0,
-                      k_f=kf, k_g=6e-6, T=0.035, a=1.0, b=6.7, DD=2.0 * R, init_single_droplet=1, init_tanh=1,
-                      interface_width=2.0, init_velocity=0.0, periodic_x=1)
-    c = (n - 1) / 2.0
-    rc = side / np.sqrt(3.0)             # centroid-to-vertex distance
-    centres = [(c + rc * np.cos(a), c + rc * np.sin(a), c) for a in (np.pi / 2, np.pi / 2 + 2 * np.pi / 3,
-                                                                        np.pi / 2 + 4 * np.pi / 3)]
     frac = np.zeros((n, n, n))
     u = np.zeros((n, n, n))
     v = np.zeros((n, n, n))
