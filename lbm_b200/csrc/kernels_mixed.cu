@@ -325,10 +325,31 @@ lbm_status mixed_alloc(MixedBuffers& mb, const Geom& g, const Launch& L)
     }
     cudaMemset(mb.part_c, 0, 3 * nb * sizeof(double));
     mb.dwz = nullptr;
-    // Two-sweep temporal blocking where the tile divides the box.
+    // Two-sweep temporal blocking where the tile divides the box, on z runs
+    // of the longest length in {32, 16, 8} whose grid still gives every SM
+    // 1.5 CTAs (shorter runs recompute more halo planes; a grid of fewer CTAs
+    // leaves SMs idle): measured on B200 (us per sweep, mixed), 128^3: 32.4
+    // at runs of 32 (256 CTAs); 96^3: 15.7 at 8 (432) against 22.2 at 32;
+    // 64^3 and 32^3: single sweeps 4.9 and 2.1 against 5.4 and 3.5 at the
+    // best run length, so no two-sweep pass below 1.5 CTAs per SM at runs of
+    // 8.  LBM_SWEEP2_ZLEN overrides (0 disables).
     mb.fuse_zlen = 0;
-    const char* env = std::getenv("LBM_SWEEP2_ZLEN");
-    const int zlen = env ? std::atoi(env) : 32;
+    int zlen = 0;
+    if (const char* env = std::getenv("LBM_SWEEP2_ZLEN")) {
+        zlen = std::atoi(env);
+    } else if (g.lx % S2_TX == 0 && g.ly % S2_TY == 0) {
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            sms = 148;
+        const long long tiles = static_cast<long long>(g.lx / S2_TX) * (g.ly / S2_TY);
+        for (int zl : {32, 16, 8}) {
+            if (2 * tiles * ((g.lz + zl - 1) / zl) >= 3LL * sms) {
+                zlen = zl;
+                break;
+            }
+        }
+    }
     if (zlen > 0 && g.lx % S2_TX == 0 && g.ly % S2_TY == 0 && g.lz >= 3 && 15 * g.n < 0x7fffffffLL &&
         cudaFuncSetAttribute(sweep2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, S2_SMEM) == cudaSuccess)
         mb.fuse_zlen = zlen;

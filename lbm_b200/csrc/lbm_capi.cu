@@ -7,15 +7,19 @@
 //             post-collision populations) -> f*, g*, u_x, v_y, w_z, sum(div)
 //   moments   pull f*, g* + x slip -> phi, rho, u*, sum(phi)
 //   prep      source projection s = (u_x - mean) + v_y + w_z, sum(p)
-//   Poisson   h* = C(h0, p); then segments of check_interval sweeps, each a
-//             captured CUDA graph ending in the device-side convergence test
-//             and one 200-byte device->host copy of the solver state
+//   Poisson   h* = C(h0, p); then segments of check_interval sweeps, each
+//             ending in the device-side convergence test, run by a CUDA
+//             graph whose conditional WHILE node repeats them until a
+//             one-thread decide kernel stops it (exit, replayed count, sweep
+//             cap, error, or 64 segments per launch), then one device->host
+//             copy of the solver state
 //   correct   u -= grad p / (2 rho)
 //
 // All scalars that the reference brings to the host between kernels (source
 // mean, gauge target, gauge shift, residual norms) are reduced and used on the
-// device; the host reads the state once per segment to decide whether to
-// launch the next one.
+// device, and so is the decision to run the next segment; the host reads the
+// state once per loop launch.  With a per-check callback (and for the one-pass
+// and Krylov forms) the host launches one segment graph at a time instead.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -42,15 +46,53 @@ struct SegKey {
     int start_parity, n_normal, dual;
     int form = 0;   // lbm_poisson_form
     int accel = 0;  // 1: two-grid correction, 2: spatial diagnostics
+    int loop = 0;   // 1: the device-side loop of such segments (build_loop)
     bool operator<(const SegKey& o) const
     {
         if (start_parity != o.start_parity) return start_parity < o.start_parity;
         if (n_normal != o.n_normal) return n_normal < o.n_normal;
         if (dual != o.dual) return dual < o.dual;
         if (form != o.form) return form < o.form;
-        return accel < o.accel;
+        if (accel != o.accel) return accel < o.accel;
+        return loop < o.loop;
     }
 };
+
+// Control block of the device-side Poisson loop.  The host writes replay,
+// max_sweeps and segs = 0 before each launch; the decide kernel counts the
+// segments and stops the loop.
+struct LoopCtl {
+    unsigned long long replay;       // 0: natural exit; else stop once this many sweeps ran
+    unsigned long long max_sweeps;   // 0: no cap
+    unsigned int segs;               // segments run in this launch
+    unsigned int pad;
+};
+
+// Segments one launch of the loop runs at most before the host looks at the
+// state again (a bounded launch; at 256^3 FP64 about 4 s of sweeps).
+constexpr unsigned kLoopSegments = 64;
+
+// After a segment's convergence test: stop on an error, at the natural exit
+// (or the replayed count), at the sweep cap or at the launch's segment cap;
+// mode 1 (the first of two parity-alternating segments) drives the IF node of
+// the second segment and ends the WHILE loop only when it stops.
+__global__ void poisson_loop_decide(const DevState* __restrict__ ds, LoopCtl* __restrict__ ctl,
+                                    cudaGraphConditionalHandle w, cudaGraphConditionalHandle second, int mode)
+{
+    const unsigned long long it = ds->iterations;
+    const unsigned segs = ++ctl->segs;
+    bool stop = ds->error != 0;
+    if (ctl->replay) stop = stop || it >= ctl->replay;
+    else stop = stop || ds->converged != 0;
+    if (ctl->max_sweeps && it >= ctl->max_sweeps) stop = true;
+    if (segs >= kLoopSegments) stop = true;
+    if (mode == 1) {
+        cudaGraphSetConditional(second, stop ? 0u : 1u);
+        if (stop) cudaGraphSetConditional(w, 0u);
+    } else {
+        cudaGraphSetConditional(w, stop ? 0u : 1u);
+    }
+}
 
 }  // namespace
 
@@ -96,6 +138,9 @@ struct lbm_handle {
     double* tg_sum = nullptr;            // two-grid / spatial diagnostics: 4^3 block sums of the change
     double* blk_part = nullptr;          // spatial diagnostics: partials of sum |block sum|
     KrylovBuffers kb{};                  // BiCGSTAB work vectors (LBM_POISSON_KRYLOV)
+    LoopCtl* loopctl = nullptr;          // device-side Poisson loop: control block, its pinned copy
+    LoopCtl* loopctl_host = nullptr;
+    bool loop_ok = true;                 // false once a loop graph failed to build (host loop then)
 };
 
 namespace {
@@ -162,6 +207,10 @@ void free_all(lbm_handle* h)
     h->stats_dev = nullptr;
     if (h->ds) cudaFree(h->ds);
     if (h->ds_host) cudaFreeHost(h->ds_host);
+    if (h->loopctl) cudaFree(h->loopctl);
+    if (h->loopctl_host) cudaFreeHost(h->loopctl_host);
+    h->loopctl = nullptr;
+    h->loopctl_host = nullptr;
     h->ds = nullptr;
     h->ds_host = nullptr;
     for (auto& e : h->ev)
@@ -219,14 +268,13 @@ void upload_state_config(lbm_handle* h)
     h->ds_host->n_cells = static_cast<double>(h->geom.lx) * h->geom.ly * h->geom.lz;
 }
 
-// Captures one Poisson segment as a CUDA graph: n_normal plain sweeps, the
-// check pair (A: stream/bounce/sum at the check sweep, B: gauge + relative
-// change + R_p terms + collision of the next sweep), in dual mode the shadow
-// sweep C (R_h terms), the convergence test, and the state copy to the host.
-lbm_status build_segment(lbm_handle* h, const SegKey& key, cudaGraphExec_t* out, int* end_parity)
+// Enqueues one Poisson segment's kernels on st (a capturing stream): n_normal
+// plain sweeps, the check pair (A: stream/bounce/sum at the check sweep, B:
+// gauge + relative change + R_p terms + collision of the next sweep), in dual
+// mode the shadow sweep C (R_h terms), and the convergence test.  Returns
+// the h buffer parity the segment ends on.
+int enqueue_segment(lbm_handle* h, const SegKey& key, cudaStream_t st)
 {
-    cudaStream_t st = h->stream;
-    LBM_CUDA(h, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     int cur = key.start_parity;
     const Geom& g = h->geom;
     const Launch& L = h->L;
@@ -291,6 +339,15 @@ lbm_status build_segment(lbm_handle* h, const SegKey& key, cudaGraphExec_t* out,
     } else {
         cur = mixed_segment(st, h->mb, L, g, key.start_parity, key.n_normal, key.dual != 0, h->ds);
     }
+    return cur;
+}
+
+// Captures one segment as a CUDA graph, ending in the state copy to the host.
+lbm_status build_segment(lbm_handle* h, const SegKey& key, cudaGraphExec_t* out, int* end_parity)
+{
+    cudaStream_t st = h->stream;
+    LBM_CUDA(h, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const int cur = enqueue_segment(h, key, st);
     cudaMemcpyAsync(h->ds_host, h->ds, sizeof(DevState), cudaMemcpyDeviceToHost, st);
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamEndCapture(st, &graph);
@@ -317,6 +374,132 @@ lbm_status get_segment(lbm_handle* h, const SegKey& key, cudaGraphExec_t* out, i
     h->graphs[key] = {ex, *end_parity};
     *out = ex;
     return LBM_OK;
+}
+
+// Captures the device-side loop of the segments `key` describes: a WHILE
+// node whose body runs one segment and poisson_loop_decide; when a segment
+// ends on the other h buffer, a nested IF node runs the segment from that
+// buffer and its decide, so that every body iteration returns to the start
+// parity.  After the loop the state and the control block go to the host.
+// Returns cudaSuccess or the first error (the caller then keeps the host
+// loop); *end_parity: where one segment ends.
+cudaError_t build_loop(lbm_handle* h, const SegKey& key, cudaGraphExec_t* out, int* end_parity)
+{
+    cudaStream_t st = h->stream;
+    SegKey k1 = key;
+    k1.loop = 0;
+    cudaGraphExec_t seg = nullptr;
+    int end1 = key.start_parity;
+    if (get_segment(h, k1, &seg, &end1) != LBM_OK) return cudaErrorUnknown;
+    const bool flip = end1 != key.start_parity;
+    cudaGraph_t top = nullptr;
+    cudaError_t e = cudaGraphCreate(&top, 0);
+    if (e != cudaSuccess) return e;
+    auto done = [&](cudaError_t err) {
+        cudaGraphDestroy(top);
+        return err;
+    };
+    cudaGraphConditionalHandle hw = 0, hi = 0;
+    e = cudaGraphConditionalHandleCreate(&hw, top, 1, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) return done(e);
+    cudaGraphNodeParams wp{};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = hw;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t wnode = nullptr;
+    e = cudaGraphAddNode(&wnode, top, nullptr, 0, &wp);
+    if (e != cudaSuccess) return done(e);
+    cudaGraph_t body = wp.conditional.phGraph_out[0];
+    if (flip) {
+        e = cudaGraphConditionalHandleCreate(&hi, body, 0, 0);
+        if (e != cudaSuccess) return done(e);
+    }
+    // body: segment + decide
+    e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return done(e);
+    enqueue_segment(h, k1, st);
+    poisson_loop_decide<<<1, 1, 0, st>>>(h->ds, h->loopctl, hw, hi, flip ? 1 : 0);
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    e = cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &ndeps);
+    std::vector<cudaGraphNode_t> last;
+    if (e == cudaSuccess && deps) last.assign(deps, deps + ndeps);
+    cudaGraph_t captured = nullptr;
+    cudaError_t ec = cudaStreamEndCapture(st, &captured);
+    if (e == cudaSuccess) e = ec;
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) return done(e);
+    if (flip) {
+        if (last.empty()) return done(cudaErrorInvalidValue);
+        cudaGraphNodeParams ip{};
+        ip.type = cudaGraphNodeTypeConditional;
+        ip.conditional.handle = hi;
+        ip.conditional.type = cudaGraphCondTypeIf;
+        ip.conditional.size = 1;
+        cudaGraphNode_t inode = nullptr;
+        e = cudaGraphAddNode(&inode, body, last.data(), last.size(), &ip);
+        if (e != cudaSuccess) return done(e);
+        cudaGraph_t ibody = ip.conditional.phGraph_out[0];
+        e = cudaStreamBeginCaptureToGraph(st, ibody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return done(e);
+        SegKey k2 = k1;
+        k2.start_parity = end1;
+        const int end2 = enqueue_segment(h, k2, st);
+        poisson_loop_decide<<<1, 1, 0, st>>>(h->ds, h->loopctl, hw, hi, 0);
+        ec = cudaStreamEndCapture(st, &captured);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = ec;
+        if (e == cudaSuccess && end2 != key.start_parity) e = cudaErrorInvalidValue;
+        if (e != cudaSuccess) return done(e);
+    }
+    cudaGraphNode_t c1 = nullptr, c2 = nullptr;
+    e = cudaGraphAddMemcpyNode1D(&c1, top, &wnode, 1, h->ds_host, h->ds, sizeof(DevState), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaGraphAddMemcpyNode1D(&c2, top, &c1, 1, h->loopctl_host, h->loopctl, sizeof(LoopCtl),
+                                     cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(out, top, 0);
+    *end_parity = end1;
+    return done(e);
+}
+
+// Cached loop graph for `key` (build_loop); false when it cannot be built.
+bool get_loop(lbm_handle* h, const SegKey& key, cudaGraphExec_t* out, int* end_parity)
+{
+    auto it = h->graphs.find(key);
+    if (it != h->graphs.end()) {
+        *out = it->second.first;
+        *end_parity = it->second.second;
+        return true;
+    }
+    if (!h->loopctl) {
+        if (cudaMalloc(&h->loopctl, sizeof(LoopCtl)) != cudaSuccess) {
+            h->loopctl = nullptr;
+            return false;
+        }
+        if (cudaMallocHost(&h->loopctl_host, sizeof(LoopCtl)) != cudaSuccess) {
+            cudaFree(h->loopctl);
+            h->loopctl = nullptr;
+            h->loopctl_host = nullptr;
+            return false;
+        }
+    }
+    cudaGraphExec_t ex = nullptr;
+    if (build_loop(h, key, &ex, end_parity) != cudaSuccess) {
+        // leave the stream usable and report nothing: the host loop takes over
+        cudaStreamCaptureStatus cs;
+        if (cudaStreamIsCapturing(h->stream, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(h->stream, &g);
+            if (g) cudaGraphDestroy(g);
+        }
+        cudaGetLastError();
+        return false;
+    }
+    h->graphs[key] = {ex, *end_parity};
+    *out = ex;
+    return true;
 }
 
 const char* site_text(int site)
@@ -610,6 +793,8 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
         }
     }
     for (; form != LBM_POISSON_KRYLOV;) {
+        uint64_t nseg = 1;   // segments run by this pass (the device-side loop runs several)
+        bool looped = false;
         const int n_normal =
             form != LBM_POISSON_KINETIC ? ci : (dual ? (first_seg ? ci - 1 : ci - 2) : ci - 1);
         if (form == LBM_POISSON_ONEPASS) {
@@ -621,38 +806,62 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
             SegKey key{hcur, n_normal, dual, form, accel};
             cudaGraphExec_t ex = nullptr;
             int end_parity = hcur;
-            const lbm_status gs = get_segment(h, key, &ex, &end_parity);
-            if (gs != LBM_OK) return gs;
-            LBM_CUDA(h, cudaGraphLaunch(ex, st));
-            LBM_CUDA(h, cudaStreamSynchronize(st));
-            hcur = end_parity;
+            // The device-side loop (no host round trip between segments), except
+            // with a per-check callback and for the dual form's shorter first
+            // segment; LBM_POISSON_LOOP=0 keeps the host loop.
+            const char* lenv = std::getenv("LBM_POISSON_LOOP");
+            const bool try_loop = h->loop_ok && !h->check_cb && !(lenv && lenv[0] == '0') &&
+                                  !(form == LBM_POISSON_KINETIC && dual && first_seg);
+            SegKey lk = key;
+            lk.loop = 1;
+            if (try_loop && get_loop(h, lk, &ex, &end_parity)) {
+                h->loopctl_host->replay = replay;
+                h->loopctl_host->max_sweeps = h->pcfg.max_sweeps;
+                h->loopctl_host->segs = 0;
+                LBM_CUDA(h, cudaMemcpyAsync(h->loopctl, h->loopctl_host, sizeof(LoopCtl), cudaMemcpyHostToDevice, st));
+                LBM_CUDA(h, cudaGraphLaunch(ex, st));
+                LBM_CUDA(h, cudaStreamSynchronize(st));
+                nseg = h->loopctl_host->segs;
+                looped = true;
+                if (nseg < 1) return fail(h, LBM_ERR_CUDA, "device Poisson loop ran no segment");
+                if (end_parity != hcur && (nseg & 1)) hcur = end_parity;
+            } else {
+                if (try_loop) h->loop_ok = false;
+                const lbm_status gs = get_segment(h, key, &ex, &end_parity);
+                if (gs != LBM_OK) return gs;
+                LBM_CUDA(h, cudaGraphLaunch(ex, st));
+                LBM_CUDA(h, cudaStreamSynchronize(st));
+                hcur = end_parity;
+            }
         }
         h->h_last = hcur;
         // sweep-equivalents executed (plain, A, B, C) and actual launches
         // (two plain sweeps per launch where the mixed box fuses them)
+        if (looped) launches += nseg;   // the device-side loop's decide kernels
         if (form == LBM_POISSON_ONEPASS) {
             kernels += static_cast<uint64_t>(n_normal);   // launches counted by onepass_segment
         } else if (form != LBM_POISSON_KINETIC) {
             // scalar sweeps (red-black: two launches each), p sum, check, 2 finalize
             // (+ the operator residual of the variable-coefficient form)
             const bool rb = form == LBM_POISSON_SCALAR_RB || form == LBM_POISSON_VARCOEF_RB;
-            kernels += static_cast<uint64_t>(n_normal);
-            launches += static_cast<uint64_t>(n_normal) * (rb ? 2 : 1) + 4 + (form == LBM_POISSON_VARCOEF_RB ? 1 : 0);
+            kernels += static_cast<uint64_t>(n_normal) * nseg;
+            launches += (static_cast<uint64_t>(n_normal) * (rb ? 2 : 1) + 4 +
+                         (form == LBM_POISSON_VARCOEF_RB ? 1 : 0)) * nseg;
         } else {
-            kernels += static_cast<uint64_t>(n_normal) + 2 + (dual ? 1 : 0);
+            kernels += (static_cast<uint64_t>(n_normal) + 2 + (dual ? 1 : 0)) * nseg;
             const bool fused = h->precision == LBM_PRECISION_MIXED ? h->mb.fuse_zlen > 0 : h->fuse_zlen > 0;
             const uint64_t plain_launches = fused ? static_cast<uint64_t>(n_normal / 2 + n_normal % 2)
                                                   : static_cast<uint64_t>(n_normal);
-            launches += plain_launches + 4 + (dual ? 1 : 0);
-            if (fused) fused_sweeps += static_cast<uint64_t>(n_normal / 2) * 2;
+            launches += (plain_launches + 4 + (dual ? 1 : 0)) * nseg;
+            if (fused) fused_sweeps += static_cast<uint64_t>(n_normal / 2) * 2 * nseg;
         }
         first_seg = false;
         if (dh.error) {
             return fail(h, static_cast<lbm_status>(dh.error), site_text(dh.error_site));
         }
-        if (iters > UINT64_MAX - static_cast<uint64_t>(ci))
+        if (iters > UINT64_MAX - static_cast<uint64_t>(ci) * nseg)
             return fail(h, LBM_ERR_OVERFLOW, "Poisson iteration counter overflow");
-        iters += static_cast<uint64_t>(ci);
+        iters += static_cast<uint64_t>(ci) * nseg;
         if (h->check_cb) {
             lbm_step_stats tmp;
             fill_stats(h, dh, &tmp);
