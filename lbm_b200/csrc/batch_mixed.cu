@@ -16,8 +16,10 @@
 // sweeps, check kernels A and B, the per-instance finalisations) is one
 // captured CUDA graph for the whole batch; items of instances that have left
 // the loop are skipped, and each instance's h parity advances only while it is
-// active.  The host reads the control words once per segment and stops when
-// no instance is active.
+// active.  The segments repeat on the device (a conditional WHILE graph node
+// and b_loop_decide) until no instance is active, at most 64 per launch; the
+// host reads the control words once per launch and relaunches while any
+// instance is still active.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -344,6 +346,23 @@ const char* site_message(int site)
     }
 }
 
+constexpr int kLoopKey = 1 << 20;           // graph-map key offset of the device-side loop
+constexpr unsigned kBatchLoopSegments = 64;   // segments per launch of the device-side loop
+
+// After a segment: continue while any instance is still in its Poisson loop,
+// for at most kBatchLoopSegments segments per launch.
+__global__ void __launch_bounds__(256)
+b_loop_decide(const BCtl* __restrict__ ctl, int n, unsigned* __restrict__ segs, cudaGraphConditionalHandle w)
+{
+    int any = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) any |= ctl[i].active;
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) {
+        const unsigned s = ++*segs;
+        cudaGraphSetConditional(w, (any && s < kBatchLoopSegments) ? 1u : 0u);
+    }
+}
+
 }  // namespace
 }  // namespace lbm
 
@@ -376,7 +395,10 @@ struct lbm_batch {
     lbm_batch_tuning tune{32, 8, 4, 4, 0, 0, 0.0};
     int fcur = 0;
     bool first_step = true;
-    std::map<int, cudaGraphExec_t> graphs;    // key: plain sweeps per segment
+    std::map<int, cudaGraphExec_t> graphs;    // key: plain sweeps per segment (+ kLoopKey: the loop)
+    unsigned* loop_segs = nullptr;            // device-side loop: segments run by a launch, pinned copy
+    unsigned* loop_segs_host = nullptr;
+    bool loop_ok = true;                      // false once the loop graph failed to build
     cudaEvent_t ev[6]{};
     lbm_timing acc{};
     std::string err;
@@ -488,6 +510,10 @@ void free_batch(lbm_batch* b)
     if (b->ctl) cudaFree(b->ctl);
     if (b->ds_host) cudaFreeHost(b->ds_host);
     if (b->ctl_host) cudaFreeHost(b->ctl_host);
+    if (b->loop_segs) cudaFree(b->loop_segs);
+    if (b->loop_segs_host) cudaFreeHost(b->loop_segs_host);
+    b->loop_segs = nullptr;
+    b->loop_segs_host = nullptr;
     b->inst_d = nullptr;
     b->items_d = nullptr;
     b->ds = nullptr;
@@ -530,19 +556,12 @@ lbm_status load_instance(lbm_batch* b, int i, const double* const src[6])
     return LBM_OK;
 }
 
-// One segment graph: n_normal plain sweeps, check A, FIN_SIGMA, check B,
-// FIN_CHECK, and the copy of the control words to the host.
-lbm_status get_segment(lbm_batch* b, int n_normal, cudaGraphExec_t* out)
+// One segment's kernels on st (a capturing stream): n_normal plain sweeps,
+// check A, FIN_SIGMA, check B, FIN_CHECK.
+void enqueue_segment(lbm_batch* b, int n_normal, cudaStream_t st)
 {
-    auto it = b->graphs.find(n_normal);
-    if (it != b->graphs.end()) {
-        *out = it->second;
-        return LBM_OK;
-    }
-    cudaStream_t st = b->stream;
     const int grid = grid_of(b);
     const int tx = b->tune.tile_x;
-    BCUDA(b, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     // j counts buffer swaps: a two-sweep launch swaps once, a single sweep once
     int j = 0;
     int singles = n_normal;
@@ -558,6 +577,20 @@ lbm_status get_segment(lbm_batch* b, int n_normal, cudaGraphExec_t* out)
     b_finalize<<<b->n, 256, 0, st>>>(FIN_SIGMA, b->ds, b->ctl, b->inst_d, b->part_a, b->n_items, 0);
     b_check_b<<<grid, 256, 0, st>>>(b->items_d, b->n_items, b->inst_d, tx, b->ctl, b->ds, j++, b->pool, b->part_b);
     b_finalize<<<b->n, 256, 0, st>>>(FIN_CHECK, b->ds, b->ctl, b->inst_d, b->part_b, b->n_items, j);
+}
+
+// One segment graph: the segment's kernels and the copy of the control words
+// to the host.
+lbm_status get_segment(lbm_batch* b, int n_normal, cudaGraphExec_t* out)
+{
+    auto it = b->graphs.find(n_normal);
+    if (it != b->graphs.end()) {
+        *out = it->second;
+        return LBM_OK;
+    }
+    cudaStream_t st = b->stream;
+    BCUDA(b, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    enqueue_segment(b, n_normal, st);
     cudaMemcpyAsync(b->ctl_host, b->ctl, b->n * sizeof(BCtl), cudaMemcpyDeviceToHost, st);
     cudaGraph_t graph = nullptr;
     const cudaError_t e = cudaStreamEndCapture(st, &graph);
@@ -597,6 +630,79 @@ void fill_batch_stats(const DevState& d, lbm_step_stats* s)
 }
 
 // One step of every instance.  replay: per-instance sweep counts, or null.
+// The device-side loop of segments: a graph whose conditional WHILE node runs
+// the segment's kernels and b_loop_decide until no instance is active (or
+// kBatchLoopSegments ran), then copies the control words and the segment
+// count to the host.  False (and nothing reported) when it cannot be built:
+// the host then launches one segment graph at a time.
+bool get_loop(lbm_batch* b, int n_normal, cudaGraphExec_t* out)
+{
+    auto it = b->graphs.find(kLoopKey + n_normal);
+    if (it != b->graphs.end()) {
+        *out = it->second;
+        return true;
+    }
+    if (!b->loop_segs) {
+        if (cudaMalloc(&b->loop_segs, sizeof(unsigned)) != cudaSuccess) {
+            b->loop_segs = nullptr;
+            return false;
+        }
+        if (cudaMallocHost(&b->loop_segs_host, sizeof(unsigned)) != cudaSuccess) {
+            cudaFree(b->loop_segs);
+            b->loop_segs = nullptr;
+            b->loop_segs_host = nullptr;
+            return false;
+        }
+    }
+    cudaStream_t st = b->stream;
+    cudaGraph_t top = nullptr;
+    if (cudaGraphCreate(&top, 0) != cudaSuccess) return false;
+    cudaGraphExec_t ex = nullptr;
+    cudaError_t e = cudaSuccess;
+    cudaGraphConditionalHandle hw = 0;
+    cudaGraphNode_t wnode = nullptr, c1 = nullptr, c2 = nullptr;
+    cudaGraphNodeParams wp{};
+    e = cudaGraphConditionalHandleCreate(&hw, top, 1, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) {
+        wp.type = cudaGraphNodeTypeConditional;
+        wp.conditional.handle = hw;
+        wp.conditional.type = cudaGraphCondTypeWhile;
+        wp.conditional.size = 1;
+        e = cudaGraphAddNode(&wnode, top, nullptr, 0, &wp);
+    }
+    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(st, wp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                            cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        enqueue_segment(b, n_normal, st);
+        b_loop_decide<<<1, 256, 0, st>>>(b->ctl, b->n, b->loop_segs, hw);
+        cudaGraph_t captured = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(st, &captured);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = ec;
+    }
+    if (e == cudaSuccess)
+        e = cudaGraphAddMemcpyNode1D(&c1, top, &wnode, 1, b->ctl_host, b->ctl, b->n * sizeof(BCtl),
+                                     cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaGraphAddMemcpyNode1D(&c2, top, &c1, 1, b->loop_segs_host, b->loop_segs, sizeof(unsigned),
+                                     cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&ex, top, 0);
+    cudaGraphDestroy(top);
+    if (e != cudaSuccess) {
+        cudaStreamCaptureStatus cs;
+        if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(st, &g);
+            if (g) cudaGraphDestroy(g);
+        }
+        cudaGetLastError();
+        return false;
+    }
+    b->graphs[kLoopKey + n_normal] = ex;
+    *out = ex;
+    return true;
+}
+
 lbm_status batch_step_once(lbm_batch* b, const uint64_t* replay, lbm_step_stats* stats)
 {
     cudaStream_t st = b->stream;
@@ -646,11 +752,25 @@ lbm_status batch_step_once(lbm_batch* b, const uint64_t* replay, lbm_step_stats*
     cudaGraphExec_t seg = nullptr;
     const lbm_status gs = get_segment(b, ci - 1, &seg);
     if (gs != LBM_OK) return gs;
-    uint64_t segments = 0;
+    uint64_t segments = 0, decides = 0;
+    const char* lenv = std::getenv("LBM_POISSON_LOOP");
+    cudaGraphExec_t loop = nullptr;
+    const bool use_loop = b->loop_ok && !(lenv && lenv[0] == '0') && (b->loop_ok = get_loop(b, ci - 1, &loop));
     for (;;) {
-        BCUDA(b, cudaGraphLaunch(seg, st));
-        BCUDA(b, cudaStreamSynchronize(st));
-        ++segments;
+        if (use_loop) {
+            *b->loop_segs_host = 0;
+            BCUDA(b, cudaMemcpyAsync(b->loop_segs, b->loop_segs_host, sizeof(unsigned), cudaMemcpyHostToDevice, st));
+            BCUDA(b, cudaGraphLaunch(loop, st));
+            BCUDA(b, cudaStreamSynchronize(st));
+            const unsigned ran = *b->loop_segs_host;
+            if (ran < 1) return bfail(b, LBM_ERR_CUDA, "device Poisson loop ran no segment");
+            segments += ran;
+            decides += ran;
+        } else {
+            BCUDA(b, cudaGraphLaunch(seg, st));
+            BCUDA(b, cudaStreamSynchronize(st));
+            ++segments;
+        }
         bool any = false;
         for (int i = 0; i < b->n; ++i) any = any || b->ctl_host[i].active;
         if (!any) break;
@@ -675,7 +795,7 @@ lbm_status batch_step_once(lbm_batch* b, const uint64_t* replay, lbm_step_stats*
     // 7 prologue launches and the correction
     b->acc.sweep_kernels += segments * static_cast<uint64_t>(ci + 1);
     const uint64_t plain = b->n_items2 > 0 ? static_cast<uint64_t>((ci - 1) / 2 + (ci - 1) % 2) : ci - 1;
-    b->acc.kernel_launches += 8 + segments * (plain + 4);
+    b->acc.kernel_launches += 8 + segments * (plain + 4) + decides;
     if (b->n_items2 > 0) b->acc.fused_sweeps += segments * static_cast<uint64_t>((ci - 1) / 2 * 2);
     lbm_status status = LBM_OK;
     for (int i = 0; i < b->n; ++i) {

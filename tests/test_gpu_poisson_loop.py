@@ -90,3 +90,31 @@ def test_device_loop_sweep_cap():
     with pytest.raises(L.LBMError) as e:
         run(True, 0, tol=1e-14, cap=500, fail=True)
     assert e.value.status == 3
+
+
+def batch_run(loop, replay=None, steps=2):
+    from tests.test_gpu_batch import CAP, uneven_cases
+    os.environ["LBM_POISSON_LOOP"] = "1" if loop else "0"
+    try:
+        cases = uneven_cases()
+        b = L.Batch([p for p, _ in cases], [f for _, f in cases])
+        b.set_poisson(max_sweeps=CAP, fail_on_limit=True)
+        st = b.step_replay(replay) if replay else b.step(steps)
+        counts = [[int(s["iterations"]) for s in row] for row in st]
+        fields = [b.download_fields(i) for i in range(len(cases))]
+        return counts, fields
+    finally:
+        os.environ.pop("LBM_POISSON_LOOP", None)
+
+
+@pytest.mark.parametrize("replay", [None, [[300, 200, 7000, 100, 300]]], ids=["natural", "replay"])
+def test_batch_device_loop_is_the_host_loop(replay):
+    """The batch's device-side loop (segments until no instance is active,
+    64 per launch) against one segment graph per host round trip: the same
+    per-instance sweep counts and bitwise equal fields."""
+    ca, fa = batch_run(False, replay)
+    cb, fb = batch_run(True, replay)
+    assert ca == cb, (ca, cb)
+    for i, (x, y) in enumerate(zip(fa, fb)):
+        for k in L.FIELDS:
+            assert np.array_equal(x[k], y[k]), (i, k)
