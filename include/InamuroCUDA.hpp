@@ -111,7 +111,7 @@ public:
         check(lbm_load_fields_ghosted(h_, buf[0].data(), buf[1].data(), buf[2].data(), buf[3].data(),
                                       buf[4].data(), buf[5].data()),
               "InamuroCUDA: upload");
-        lbm_set_check_callback(h_, &InamuroCUDA::onCheck, this);
+        syncCheckCallback();
         applyPoissonConfig();
     }
 
@@ -138,7 +138,7 @@ public:
             acc_ = o.acc_;
             diag_ = o.diag_;
             csv_ = o.csv_;
-            if (h_) lbm_set_check_callback(h_, &InamuroCUDA::onCheck, this);
+            syncCheckCallback();
         }
         return *this;
     }
@@ -323,7 +323,11 @@ public:
         applyPoissonConfig();
     }
     // Per-check CSV, same header and columns as GPU/InamuroCUDA.cu:2610-2682.
-    void setPoissonDiagnosticsPath(const std::string& path) { csv_.open(path); }
+    void setPoissonDiagnosticsPath(const std::string& path)
+    {
+        csv_.open(path);
+        syncCheckCallback();
+    }
 
     void printPerformanceMetrics() const
     {
@@ -434,6 +438,13 @@ private:
         cfg.max_sweeps = iteration_limit_;
         cfg.fail_on_limit = 0;
         check(lbm_set_poisson(h_, &cfg), "Poisson configuration");
+    }
+
+    // The per-check callback only while a CSV is written: without one the
+    // library runs the Poisson segments in its device-side loop.
+    void syncCheckCallback()
+    {
+        if (h_) lbm_set_check_callback(h_, csv_.path().empty() ? nullptr : &InamuroCUDA::onCheck, this);
     }
 
     static void onCheck(void* user, const lbm_check_record* r)
