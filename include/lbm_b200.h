@@ -340,7 +340,11 @@ lbm_status lbm_step_replay(lbm_handle* h, int n_steps, const uint64_t* sweeps,
 
 /* Calls cb(user, record) on the host after every Poisson convergence check
  * (NULL cb disables).  Replaces InamuroCUDA::setPoissonDiagnosticsPath's
- * per-check CSV rows (GPU/InamuroCUDA.cu:2610-2682): the caller formats them. */
+ * per-check CSV rows (GPU/InamuroCUDA.cu:2610-2682): the caller formats them.
+ * While a callback is set the Poisson loop returns to the host after every
+ * check; without one the checks run back to back on the device (a CUDA graph
+ * with a conditional WHILE node, at most 64 checks per launch), with the same
+ * results and sweep counts. */
 lbm_status lbm_set_check_callback(lbm_handle* h, lbm_check_callback cb, void* user);
 
 /* Device -> host download of one field (physical layout). */
