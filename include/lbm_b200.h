@@ -281,7 +281,7 @@ typedef enum {
                                     LBM_ERR_NONFINITE; twenty restarts in a row that do not lower
                                     the true residual (a tolerance below the rounding floor)
                                     stop the solve with LBM_ERR_POISSON_BUDGET */
-    LBM_POISSON_VARCOEF_RB = 5   /* not a reference form: div((1/rho) grad p) = s, the continuum
+    LBM_POISSON_VARCOEF_RB = 5,  /* not a reference form: div((1/rho) grad p) = s, the continuum
                                     limit of the kinetic form (diffusivity 1/(3 rho), source
                                     -s/3), on the D3Q15 neighbours with arithmetic face means
                                     of 1/rho (x mirrored at the slip walls), solved by red-black
@@ -293,6 +293,16 @@ typedef enum {
                                     kinetic form's: its p differs at the interface.  FP64, even
                                     ly, lz (and lx with periodic_x), no lbm_poisson_cfg dual
                                     residual, no accelerators */
+    LBM_POISSON_REFINE = 6       /* not a reference form: the kinetic form on the mixed box by
+                                    iterative refinement.  The post-collision h is kept in FP64
+                                    (a further 300 B/cell); each check interval runs as one FP64
+                                    residual r = K h + b - h, check_interval - 2 FP32 correction
+                                    sweeps e <- K e + r and the FP64 check (gauge, relative
+                                    change) on h + e: in exact arithmetic the kinetic form's
+                                    sweeps and exit, but the FP32 rounding falls on the
+                                    correction only, so tight tolerances converge to the FP64
+                                    fixed point (the plain mixed sweeps stall near 1e-7).
+                                    Mixed precision only; no dual residual, no accelerators */
 } lbm_poisson_form;
 lbm_status lbm_set_poisson_form(lbm_handle* h, lbm_poisson_form form, double source_scale, double omega);
 /* Current form, source scale and the relaxation in use (the computed optimum

@@ -421,15 +421,16 @@ class InamuroCUDA:
         cfg = PoissonCfg(check_interval, tolerance, int(dual), max_sweeps, int(fail_on_limit))
         self._check(self._lib.lbm_set_poisson(self._h, C.byref(cfg)), "set_poisson")
 
-    POISSON_FORMS = {"kinetic": 0, "scalar": 1, "scalar-rb": 2, "onepass": 3, "krylov": 4, "varcoef-rb": 5}
+    POISSON_FORMS = {"kinetic": 0, "scalar": 1, "scalar-rb": 2, "onepass": 3, "krylov": 4, "varcoef-rb": 5, "refine": 6}
 
     def set_poisson_form(self, form: str = "kinetic", source_scale: float = 2.0, omega: float = 0.0):
         """lbm_set_poisson_form: "kinetic" (the production solve), "scalar"
         (the reference's scalar Jacobi form), "scalar-rb" (red-black SOR of
         the same scalar equation; omega 0 = the optimum for the box),
         "onepass" (the reference's one-pass form), "krylov" (BiCGSTAB on the
-        kinetic fixed point) or "varcoef-rb" (red-black SOR of
-        div((1/rho) grad p) = s)."""
+        kinetic fixed point), "varcoef-rb" (red-black SOR of
+        div((1/rho) grad p) = s) or, on the mixed box, "refine" (the kinetic
+        form by iterative refinement: FP64 residual, FP32 correction sweeps)."""
         self._check(self._lib.lbm_set_poisson_form(self._h, self.POISSON_FORMS[form], source_scale, omega),
                     "set_poisson_form")
 

@@ -260,6 +260,158 @@ sweep_check_c_kernel(Geom g, int zrun, const float* __restrict__ hin, float* __r
     block_sum_store<3>(red, part, nblocks, block_linear());
 }
 
+// ---- iterative refinement of the Poisson solve (LBM_POISSON_REFINE) ------
+// The FP32 sweeps alone stall at a relative change of ~1e-7: every sweep
+// rounds h to FP32, and the kinetic map's slow modes (relaxation over ~1e5
+// sweeps at 64^3) amplify that noise, so the FP32 iteration's limit sits
+// ~1e-4 of max|p| away from the FP64 fixed point.  Refinement keeps the
+// post-collision state H in FP64 and computes each segment's sweeps as a
+// correction: r = K H + b - H in FP64 (b = -(E/3) s), then e_1 = r and
+// e_(k+1) = K e_k + r in FP32, so that H + e_k is, in exact arithmetic, the
+// state after k sweeps from H; the FP32 rounding now applies to the
+// correction, which shrinks as the solve converges.  Checks A and B run in
+// FP64 on H + e, as the FP64 box's do.  K uses the box's FP32 omega and s as
+// data in both precisions, so the fixed point is the mixed box's own.
+
+// FP64 Poisson start: H = collide(E p) (or of the loaded FP32 h).
+__global__ void __launch_bounds__(256)
+refine_init_kernel(Geom g, int h_loaded, const float* __restrict__ hload, double* __restrict__ hd,
+                   const double* __restrict__ p, const float* __restrict__ omega, const float* __restrict__ s)
+{
+    int x, y, z;
+    if (!tile_coords(g, x, y, z)) return;
+    const long long c = cell_of(g, x, y, z);
+    const double pv = p[c];
+    double hv[Q];
+    double sum = 0.0;
+    static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        hv[q] = h_loaded ? (double)hload[(long long)q * g.n + c] : pv * wE(q);
+        sum += hv[q];
+    });
+    const double om = omega[c], sv = s[c];
+    static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        hd[(long long)q * g.n + c] = hv[q] - om * (hv[q] - wE(q) * sum) - wE(q) / 3.0 * sv;
+    });
+}
+
+// r = K H + b - H (FP64 arithmetic, stored in FP32).
+__global__ void __launch_bounds__(256)
+refine_residual_kernel(Geom g, const double* __restrict__ hd, float* __restrict__ r,
+                       const float* __restrict__ omega, const float* __restrict__ s)
+{
+    int x, y, z;
+    if (!tile_coords(g, x, y, z)) return;
+    const long long c = cell_of(g, x, y, z);
+    const Wrap w(g, x, y, z);
+    double hv[Q];
+    double pv = 0.0;
+    static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        hv[q] = __ldg(hd + (long long)q * g.n + pull_src<q>(g, w, x, y, z));
+    });
+    bounce_regs(hv, g, x);
+    static_for<0, Q>([&](auto qc) { pv += hv[decltype(qc)::value]; });
+    const double om = __ldg(omega + c), sv = __ldg(s + c);
+    static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        const long long i = (long long)q * g.n + c;
+        const double kh = hv[q] - om * (hv[q] - wE(q) * pv) - wE(q) / 3.0 * sv;
+        r[i] = (float)(kh - __ldg(hd + i));
+    });
+}
+
+// One correction sweep in FP32: e' = K e + r.
+__global__ void __launch_bounds__(256)
+refine_sweep_kernel(Geom g, const float* __restrict__ ein, float* __restrict__ eout, const float* __restrict__ r,
+                    const float* __restrict__ omega)
+{
+    int x, y, z;
+    if (!tile_coords(g, x, y, z)) return;
+    const long long c = cell_of(g, x, y, z);
+    float ev[Q];
+    pull_regs(ev, ein, g, x, y, z);
+    bounce_regs(ev, g, x);
+    float pe = 0.f;
+    static_for<0, Q>([&](auto qc) { pe += ev[decltype(qc)::value]; });
+    const float om = __ldg(omega + c);
+    static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        const long long i = (long long)q * g.n + c;
+        eout[i] = fmaf(-om, ev[q] - float(wE(q)) * pe, ev[q]) + __ldg(r + i);
+    });
+}
+
+// Check A in FP64: pull H + e, slip, p = sum (FP64); the uncollided values
+// go to hpre, red[0] += p.
+__global__ void __launch_bounds__(256)
+refine_check_a_kernel(Geom g, int zrun, const double* __restrict__ hd, const float* __restrict__ e,
+                      double* __restrict__ hpre, double* __restrict__ p_chk, double* __restrict__ part,
+                      long long nblocks)
+{
+    int x, y, z0, z1;
+    const bool active = tile_zrun(g, zrun, x, y, z0, z1);
+    double red[1] = {0.0};
+    for (int z = z0; active && z < z1; ++z) {
+        const long long c = cell_of(g, x, y, z);
+        const Wrap w(g, x, y, z);
+        double hv[Q];
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            const long long src = (long long)q * g.n + pull_src<q>(g, w, x, y, z);
+            hv[q] = __ldg(hd + src) + (double)__ldg(e + src);
+        });
+        bounce_regs(hv, g, x);
+        double pv = 0.0;
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            pv += hv[q];
+            hpre[(long long)q * g.n + c] = hv[q];
+        });
+        p_chk[c] = pv;
+        red[0] += pv;
+    }
+    block_sum_store<1>(red, part, nblocks, block_linear());
+}
+
+// Check B in FP64: gauge (p -= shift, h -= E shift), relative-change terms,
+// p and p_prev, then the collision of the next sweep, in place.
+__global__ void __launch_bounds__(256)
+refine_check_b_kernel(Geom g, int zrun, double* __restrict__ hd, const double* __restrict__ p_chk,
+                      double* __restrict__ p_prev, double* __restrict__ p, const float* __restrict__ omega,
+                      const float* __restrict__ s, const DevState* __restrict__ ds, double* __restrict__ part,
+                      long long nblocks)
+{
+    int x, y, z0, z1;
+    const bool active = tile_zrun(g, zrun, x, y, z0, z1);
+    double red[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const double shift = ds->sigma;
+    for (int z = z0; active && z < z1; ++z) {
+        const long long c = cell_of(g, x, y, z);
+        const double pv = p_chk[c] - shift;
+        red[0] += fabs(pv - p_prev[c]);
+        red[1] += fabs(pv);
+        p_prev[c] = pv;
+        p[c] = pv;
+        const double om = __ldg(omega + c), sv = __ldg(s + c);
+        static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            const long long i = (long long)q * g.n + c;
+            const double hv = hd[i] - wE(q) * shift;
+            hd[i] = hv - om * (hv - wE(q) * pv) - wE(q) / 3.0 * sv;
+        });
+    }
+    block_sum_store<5>(red, part, nblocks, block_linear());
+}
+
+__global__ void __launch_bounds__(256)
+refine_to_float_kernel(const double* __restrict__ src, float* __restrict__ dst, long long count)
+{
+    for (long long i = blockIdx.x * 256LL + threadIdx.x; i < count; i += (long long)gridDim.x * 256)
+        dst[i] = (float)src[i];
+}
+
 __global__ void __launch_bounds__(256)
 correct_kernel(Geom g, float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
                const double* __restrict__ p, const float* __restrict__ rho)
@@ -377,11 +529,13 @@ void mixed_free(MixedBuffers& mb)
         *p = nullptr;
     }
     double** db[] = {&mb.p, &mb.p_prev, &mb.p_chk, &mb.scratch, &mb.f0, &mb.part_src, &mb.part_prep, &mb.part_a,
-                     &mb.part_b, &mb.part_c, &mb.part_mass};
+                     &mb.part_b, &mb.part_c, &mb.part_mass, &mb.hd[0], &mb.hd[1]};
     for (double** p : db) {
         if (*p) cudaFree(*p);
         *p = nullptr;
     }
+    if (mb.rr) cudaFree(mb.rr);
+    mb.rr = nullptr;
     mb.allocated = false;
 }
 
@@ -511,6 +665,61 @@ int mixed_segment(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom
 void mixed_correct(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom& g)
 {
     correct_kernel<<<L.grid, L.block, 0, st>>>(g, mb.u, mb.v, mb.w, mb.p, mb.rho);
+}
+
+lbm_status mixed_alloc_refine(MixedBuffers& mb, const Geom& g)
+{
+    if (mb.rr) return LBM_OK;
+    const size_t n15 = 15 * static_cast<size_t>(g.n);
+    double* hd[2] = {nullptr, nullptr};
+    float* rr = nullptr;
+    if (cudaMalloc(&hd[0], n15 * sizeof(double)) != cudaSuccess || cudaMalloc(&hd[1], n15 * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&rr, n15 * sizeof(float)) != cudaSuccess) {
+        if (hd[0]) cudaFree(hd[0]);
+        if (hd[1]) cudaFree(hd[1]);
+        if (rr) cudaFree(rr);
+        cudaGetLastError();
+        return LBM_ERR_OOM;
+    }
+    mb.hd[0] = hd[0];
+    mb.hd[1] = hd[1];
+    mb.rr = rr;
+    return LBM_OK;
+}
+
+void mixed_refine_init(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom& g, bool h_loaded)
+{
+    refine_init_kernel<<<L.grid, L.block, 0, st>>>(g, h_loaded ? 1 : 0, mb.h[1], mb.hd[0], mb.p, mb.dvy, mb.s);
+}
+
+int mixed_refine_segment(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom& g, int start_parity,
+                         int n_normal, DevState* ds)
+{
+    const float* omega = mb.dvy;
+    double* H = mb.hd[start_parity];
+    double* Hn = mb.hd[1 - start_parity];
+    // sweep 1 as the residual: e_1 = r = K H + b - H
+    refine_residual_kernel<<<L.grid, L.block, 0, st>>>(g, H, mb.rr, omega, mb.s);
+    // sweeps 2 .. n_normal as FP32 corrections e_(k+1) = K e_k + r
+    const float* e = mb.rr;
+    int cur = 0;
+    for (int i = 1; i < n_normal; ++i) {
+        refine_sweep_kernel<<<L.grid, L.block, 0, st>>>(g, e, mb.h[cur], mb.rr, omega);
+        e = mb.h[cur];
+        cur = 1 - cur;
+    }
+    // the check sweep in FP64 on H + e
+    refine_check_a_kernel<<<L.cgrid, L.block, 0, st>>>(g, L.zrun, H, e, Hn, mb.p_chk, mb.part_a, L.cnblocks);
+    finalize(st, FIN_SIGMA, ds, mb.part_a, L.cnblocks, nullptr, 0, nullptr, 0);
+    refine_check_b_kernel<<<L.cgrid, L.block, 0, st>>>(g, L.zrun, Hn, mb.p_chk, mb.p_prev, mb.p, omega, mb.s, ds,
+                                                       mb.part_b, L.cnblocks);
+    finalize(st, FIN_CHECK, ds, mb.part_b, L.cnblocks, nullptr, 0, nullptr, 0);
+    return 1 - start_parity;
+}
+
+void mixed_refine_finish(cudaStream_t st, MixedBuffers& mb, const Geom& g, int parity)
+{
+    refine_to_float_kernel<<<1184, 256, 0, st>>>(mb.hd[parity], mb.h[parity], 15 * g.n);
 }
 
 // Layout of a saved state: f (15 n floats), g (15 n floats), phi, rho, u,

@@ -278,7 +278,9 @@ int enqueue_segment(lbm_handle* h, const SegKey& key, cudaStream_t st)
     int cur = key.start_parity;
     const Geom& g = h->geom;
     const Launch& L = h->L;
-    if (key.form != LBM_POISSON_KINETIC) {
+    if (key.form == LBM_POISSON_REFINE) {
+        cur = mixed_refine_segment(st, h->mb, L, g, key.start_parity, key.n_normal, h->ds);
+    } else if (key.form != LBM_POISSON_KINETIC) {
         // Scalar forms: n_normal sweeps, the gauge mean, the check; p ends in b.p.
         Fp64Buffers& b = h->b;
         double* P[2] = {b.p, b.p_chk};
@@ -699,6 +701,10 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
         const lbm_status s = ensure_dual_buffer(h);
         if (s != LBM_OK) return s;
     }
+    if (form == LBM_POISSON_REFINE && !h->mb.rr) {
+        const lbm_status s = mixed_alloc_refine(h->mb, g);
+        if (s != LBM_OK) return fail(h, s, "refinement buffers: device allocation failed");
+    }
     // Reset per-solve flags, keep config.
     DevState& dh = *h->ds_host;
     std::memset(&dh, 0, sizeof(DevState));
@@ -738,6 +744,7 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
                                              h->h_loaded, h->ds, h->timing ? h->ev : nullptr);
         if (s2 != LBM_OK) return fail(h, s2, "mixed prologue launch failed");
         h->fcur = 1 - h->fcur;
+        if (form == LBM_POISSON_REFINE) mixed_refine_init(st, h->mb, L, g, h->h_loaded);
     }
     LBM_CUDA(h, cudaGetLastError());
     h->first_step = false;
@@ -795,8 +802,9 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
     for (; form != LBM_POISSON_KRYLOV;) {
         uint64_t nseg = 1;   // segments run by this pass (the device-side loop runs several)
         bool looped = false;
-        const int n_normal =
-            form != LBM_POISSON_KINETIC ? ci : (dual ? (first_seg ? ci - 1 : ci - 2) : ci - 1);
+        const int n_normal = form == LBM_POISSON_REFINE ? ci - 1
+                             : form != LBM_POISSON_KINETIC ? ci
+                                                           : (dual ? (first_seg ? ci - 1 : ci - 2) : ci - 1);
         if (form == LBM_POISSON_ONEPASS) {
             const lbm_status os = onepass_segment(h, &anderson_history, &launches);
             if (os != LBM_OK) return os;
@@ -840,6 +848,10 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
         if (looped) launches += nseg;   // the device-side loop's decide kernels
         if (form == LBM_POISSON_ONEPASS) {
             kernels += static_cast<uint64_t>(n_normal);   // launches counted by onepass_segment
+        } else if (form == LBM_POISSON_REFINE) {
+            // residual + corrections (n_normal), checks A and B, two finalisations
+            kernels += (static_cast<uint64_t>(n_normal) + 2) * nseg;
+            launches += (static_cast<uint64_t>(n_normal) + 4) * nseg;
         } else if (form != LBM_POISSON_KINETIC) {
             // scalar sweeps (red-black: two launches each), p sum, check, 2 finalize
             // (+ the operator residual of the variable-coefficient form)
@@ -901,6 +913,10 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
                 return fail(h, LBM_ERR_POISSON_BUDGET, "Poisson sweep limit reached without convergence");
             break;
         }
+    }
+    if (form == LBM_POISSON_REFINE) {
+        mixed_refine_finish(st, h->mb, g, hcur);   // the FP32 h the rest of the box reads
+        ++launches;
     }
     if (h->timing) LBM_CUDA(h, cudaEventRecord(h->ev[4], st));
     if (h->precision == LBM_PRECISION_FP64) {
@@ -1279,9 +1295,12 @@ lbm_status lbm_set_poisson_form(lbm_handle* h, lbm_poisson_form form, double sou
 {
     if (check_handle(h) != LBM_OK) return LBM_ERR_BAD_ARG;
     if (form != LBM_POISSON_KINETIC && form != LBM_POISSON_SCALAR_JACOBI && form != LBM_POISSON_SCALAR_RB &&
-        form != LBM_POISSON_ONEPASS && form != LBM_POISSON_KRYLOV && form != LBM_POISSON_VARCOEF_RB)
+        form != LBM_POISSON_ONEPASS && form != LBM_POISSON_KRYLOV && form != LBM_POISSON_VARCOEF_RB &&
+        form != LBM_POISSON_REFINE)
         return fail(h, LBM_ERR_BAD_ARG, "unknown Poisson form");
-    if (form != LBM_POISSON_KINETIC && h->precision != LBM_PRECISION_FP64)
+    if (form == LBM_POISSON_REFINE && h->precision != LBM_PRECISION_MIXED)
+        return fail(h, LBM_ERR_BAD_ARG, "the refinement form runs on the mixed-precision box only");
+    if (form != LBM_POISSON_KINETIC && form != LBM_POISSON_REFINE && h->precision != LBM_PRECISION_FP64)
         return fail(h, LBM_ERR_BAD_ARG, "the scalar, one-pass and Krylov Poisson forms run in FP64 precision only");
     if (!std::isfinite(source_scale)) return fail(h, LBM_ERR_BAD_ARG, "scalar source scale must be finite");
     if (!(omega == 0.0 || (omega > 0.0 && omega < 2.0)))

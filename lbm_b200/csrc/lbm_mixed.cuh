@@ -23,6 +23,10 @@ struct MixedBuffers {
     double *part_src = nullptr, *part_prep = nullptr, *part_a = nullptr, *part_b = nullptr,
            *part_c = nullptr, *part_mass = nullptr;
     double* scratch = nullptr;   // FP64 staging for loads/downloads (n doubles)
+    // Iterative refinement of the Poisson solve (LBM_POISSON_REFINE): the FP64
+    // post-collision populations (two buffers) and the FP32 residual.
+    double* hd[2] = {nullptr, nullptr};
+    float* rr = nullptr;
     int fuse_zlen = 0;           // >0: plain sweeps run two per pass, z runs of this length
     int collide_zlen = 0;        // >0: z-marching collide, z runs of this length
     bool allocated = false;
@@ -44,6 +48,16 @@ lbm_status mixed_prologue(cudaStream_t st, MixedBuffers& mb, const Launch& L, co
 int mixed_segment(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom& g,
                   int start_parity, int n_normal, bool dual, DevState* ds);
 void mixed_correct(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom& g);
+// Iterative refinement of the kinetic Poisson solve: allocates hd and rr (all
+// or nothing); refine_init starts hd[0] from the prologue's p (or the loaded
+// h); refine_segment enqueues one segment (an FP64 residual, n_normal - 1 FP32
+// correction sweeps, FP64 checks A and B) and returns the hd buffer it ends
+// in; refine_finish copies hd[parity] into the FP32 h[parity].
+lbm_status mixed_alloc_refine(MixedBuffers& mb, const Geom& g);
+void mixed_refine_init(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom& g, bool h_loaded);
+int mixed_refine_segment(cudaStream_t st, MixedBuffers& mb, const Launch& L, const Geom& g, int start_parity,
+                         int n_normal, DevState* ds);
+void mixed_refine_finish(cudaStream_t st, MixedBuffers& mb, const Geom& g, int parity);
 // Saved state of a mixed box (the post-collision populations of buffer fcur,
 // the rest population, the five FP32 macro fields and p): its size in bytes,
 // and the copies in each direction.  Enqueued on st.
