@@ -202,6 +202,17 @@ sweep2_kernel(Geom g, int zlen, const float* __restrict__ hin, float* __restrict
                              s, ring);
 }
 
+// The refinement form's correction sweeps two per pass (sweep2_run<., ., true>).
+__global__ void __maxnreg__(88)
+sweep2_refine_kernel(Geom g, int zlen, const float* __restrict__ ein, float* __restrict__ eout,
+                     const float* __restrict__ omega, const float* __restrict__ r)
+{
+    extern __shared__ float ring[];
+    const int z0 = blockIdx.z * zlen;
+    sweep2_run<S2_TX, S2_TY, true>(g, blockIdx.x * S2_TX, blockIdx.y * S2_TY, z0, min(z0 + zlen, g.lz), ein, eout,
+                                   omega, r, ring);
+}
+
 __global__ void __launch_bounds__(256)
 sweep_check_a_kernel(Geom g, int zrun, const float* __restrict__ hin, float* __restrict__ hout,
                      double* __restrict__ p_chk, double* __restrict__ part, long long nblocks)
@@ -333,13 +344,12 @@ refine_sweep_kernel(Geom g, const float* __restrict__ ein, float* __restrict__ e
     float ev[Q];
     pull_regs(ev, ein, g, x, y, z);
     bounce_regs(ev, g, x);
-    float pe = 0.f;
-    static_for<0, Q>([&](auto qc) { pe += ev[decltype(qc)::value]; });
+    const float pe = refine_sum(ev);
     const float om = __ldg(omega + c);
     static_for<0, Q>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
         const long long i = (long long)q * g.n + c;
-        eout[i] = fmaf(-om, ev[q] - float(wE(q)) * pe, ev[q]) + __ldg(r + i);
+        eout[i] = refine_cell<q>(ev[q], pe, om, __ldg(r + i));
     });
 }
 
@@ -503,7 +513,9 @@ lbm_status mixed_alloc(MixedBuffers& mb, const Geom& g, const Launch& L)
         }
     }
     if (zlen > 0 && g.lx % S2_TX == 0 && g.ly % S2_TY == 0 && g.lz >= 3 && 15 * g.n < 0x7fffffffLL &&
-        cudaFuncSetAttribute(sweep2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, S2_SMEM) == cudaSuccess)
+        cudaFuncSetAttribute(sweep2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, S2_SMEM) == cudaSuccess &&
+        cudaFuncSetAttribute(sweep2_refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, S2_SMEM) ==
+            cudaSuccess)
         mb.fuse_zlen = zlen;
     // z-marching collide where its tile divides the box.
     const char* cenv = std::getenv("LBM_COLLIDE_ZLEN");
@@ -700,10 +712,20 @@ int mixed_refine_segment(cudaStream_t st, MixedBuffers& mb, const Launch& L, con
     double* Hn = mb.hd[1 - start_parity];
     // sweep 1 as the residual: e_1 = r = K H + b - H
     refine_residual_kernel<<<L.grid, L.block, 0, st>>>(g, H, mb.rr, omega, mb.s);
-    // sweeps 2 .. n_normal as FP32 corrections e_(k+1) = K e_k + r
+    // sweeps 2 .. n_normal as FP32 corrections e_(k+1) = K e_k + r, two per
+    // pass where the box runs two-sweep passes
     const float* e = mb.rr;
     int cur = 0;
-    for (int i = 1; i < n_normal; ++i) {
+    int i = 1;
+    if (mb.fuse_zlen > 0) {
+        const dim3 grid(g.lx / S2_TX, g.ly / S2_TY, (g.lz + mb.fuse_zlen - 1) / mb.fuse_zlen);
+        for (; i + 1 < n_normal; i += 2) {
+            sweep2_refine_kernel<<<grid, S2_THREADS, S2_SMEM, st>>>(g, mb.fuse_zlen, e, mb.h[cur], omega, mb.rr);
+            e = mb.h[cur];
+            cur = 1 - cur;
+        }
+    }
+    for (; i < n_normal; ++i) {
         refine_sweep_kernel<<<L.grid, L.block, 0, st>>>(g, e, mb.h[cur], mb.rr, omega);
         e = mb.h[cur];
         cur = 1 - cur;

@@ -849,9 +849,13 @@ lbm_status step_once(lbm_handle* h, uint64_t replay, lbm_step_stats* stats)
         if (form == LBM_POISSON_ONEPASS) {
             kernels += static_cast<uint64_t>(n_normal);   // launches counted by onepass_segment
         } else if (form == LBM_POISSON_REFINE) {
-            // residual + corrections (n_normal), checks A and B, two finalisations
+            // residual + n_normal - 1 corrections (in pairs where the box runs
+            // two-sweep passes), checks A and B, two finalisations
+            const uint64_t nc = static_cast<uint64_t>(n_normal) - 1;
+            const uint64_t pairs = h->mb.fuse_zlen > 0 ? nc / 2 : 0;
             kernels += (static_cast<uint64_t>(n_normal) + 2) * nseg;
-            launches += (static_cast<uint64_t>(n_normal) + 4) * nseg;
+            launches += (1 + (nc - 2 * pairs) + pairs + 4) * nseg;
+            fused_sweeps += 2 * pairs * nseg;
         } else if (form != LBM_POISSON_KINETIC) {
             // scalar sweeps (red-black: two launches each), p sum, check, 2 finalize
             // (+ the operator residual of the variable-coefficient form)

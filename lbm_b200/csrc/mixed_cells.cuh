@@ -474,14 +474,29 @@ __device__ __forceinline__ void mixc_correct(const Geom& g, float* __restrict__ 
 // two single sweeps; tile cells outside the box (partial tiles) store
 // nothing.  Cell arithmetic: mixc_sweep32's (collide_h, sum_q32).  The ring
 // is the z-direction-grouped one of lbm_device.cuh (ring_plane, 45 population
-// planes).
+// planes).  kRefine: the refinement form's correction sweeps instead,
+// e' = K e + r with r a per-population source (src = r, 15 n floats), the
+// arithmetic of refine_sweep_kernel.
 __host__ __device__ constexpr int sweep2_threads(int tx, int ty) { return ((tx + 2) * (ty + 2) + 31) / 32 * 32; }
 __host__ __device__ constexpr int sweep2_smem(int tx, int ty)
 {
     return ring_planes() * (tx + 2) * (ty + 2) * static_cast<int>(sizeof(float));
 }
 
-template <int TX, int TY>
+// Correction-sweep update of the refinement form: K e + r in FP32.
+__device__ __forceinline__ float refine_sum(const float (&ev)[Q])
+{
+    float pe = 0.f;
+    static_for<0, Q>([&](auto qc) { pe += ev[decltype(qc)::value]; });
+    return pe;
+}
+template <int q>
+__device__ __forceinline__ float refine_cell(float ev, float pe, float om, float r)
+{
+    return fmaf(-om, ev - float(wE(q)) * pe, ev) + r;
+}
+
+template <int TX, int TY, bool kRefine = false>
 __device__ __forceinline__ void sweep2_run(const Geom& g, int x0, int y0, int z0, int z1,
                                            const float* __restrict__ hin, float* __restrict__ hout,
                                            const float* __restrict__ omega, const float* __restrict__ s,
@@ -497,22 +512,35 @@ __device__ __forceinline__ void sweep2_run(const Geom& g, int x0, int y0, int z0
 
     float a[Q];
     float a_om = 0.f, a_s = 0.f;
+    float ar[kRefine ? Q : 1];           // kRefine: the source r of the cell's plane
     auto prefetch = [&](int zz) {        // issue sweep k's pulls for plane zz
         if (!owner) return;
         const int zw = zz < 0 ? zz + g.lz : (zz >= g.lz ? zz - g.lz : zz);
         pull_regs32(a, hin, n, g, xw, yw, zw);
         const int c = (zw * g.ly + yw) * g.lx + xw;
         a_om = __ldg(omega + c);
-        a_s = __ldg(s + c);
+        if constexpr (kRefine) {
+            static_for<0, Q>([&](auto qc) { ar[decltype(qc)::value] = __ldg(s + decltype(qc)::value * n + c); });
+        } else {
+            a_s = __ldg(s + c);
+        }
     };
     auto finish = [&](int zz) {          // complete sweep k on plane zz into the ring
         if (!owner) return;
         bounce_regs(a, g, xw);
-        const P32 p32 = sum_q32(a);
-        static_for<0, Q>([&](auto qc) {
-            constexpr int q = decltype(qc)::value;
-            ring[ring_plane<q>(zz) * RC + t] = collide_h<q>(a[q], p32, a_om, a_s);
-        });
+        if constexpr (kRefine) {
+            const float pe = refine_sum(a);
+            static_for<0, Q>([&](auto qc) {
+                constexpr int q = decltype(qc)::value;
+                ring[ring_plane<q>(zz) * RC + t] = refine_cell<q>(a[q], pe, a_om, ar[q]);
+            });
+        } else {
+            const P32 p32 = sum_q32(a);
+            static_for<0, Q>([&](auto qc) {
+                constexpr int q = decltype(qc)::value;
+                ring[ring_plane<q>(zz) * RC + t] = collide_h<q>(a[q], p32, a_om, a_s);
+            });
+        }
     };
 
     prefetch(z0 - 1);
@@ -537,7 +565,16 @@ __device__ __forceinline__ void sweep2_run(const Geom& g, int x0, int y0, int z0
             });
             bounce_regs(hv, g, x);
             const int c = (z * g.ly + y) * g.lx + x;
-            collide_h_store32(hv, sum_q32(hv), __ldg(omega + c), __ldg(s + c), hout, n, c);
+            if constexpr (kRefine) {
+                const float pe = refine_sum(hv);
+                const float om = __ldg(omega + c);
+                static_for<0, Q>([&](auto qc) {
+                    constexpr int q = decltype(qc)::value;
+                    hout[q * n + c] = refine_cell<q>(hv[q], pe, om, __ldg(s + q * n + c));
+                });
+            } else {
+                collide_h_store32(hv, sum_q32(hv), __ldg(omega + c), __ldg(s + c), hout, n, c);
+            }
         }
     }
 }

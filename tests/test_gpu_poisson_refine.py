@@ -104,3 +104,27 @@ def test_refinement_form_is_refused_where_it_does_not_apply():
     with pytest.raises(L.LBMError) as e:
         m.step(1)
     assert e.value.status == 4
+
+
+def test_two_sweep_corrections_are_single_sweeps(monkeypatch):
+    """The correction sweeps in two-sweep passes (the plane-ring pass with r
+    as a per-population source) compute every cell as the single correction
+    sweeps do: bitwise equal fields and sweep counts (a 64 x 32 x 24 box,
+    z runs of 8 forced, the slip walls)."""
+    out = []
+    for zlen in ("0", "8"):
+        monkeypatch.setenv("LBM_SWEEP2_ZLEN", zlen)
+        p = bench.workload_params(64)
+        p.ly, p.lz = 32, 24
+        p.DD, p.init_separation = 10.0, 24.0
+        f = bench.workload_fields(p)
+        g = L.InamuroCUDA(p, f, precision="mixed")
+        g.set_poisson(check_interval=100, tolerance=1e-8, max_sweeps=2_000_000, fail_on_limit=True)
+        g.set_poisson_form("refine")
+        st = [int(s["iterations"]) for s in g.step(2)]
+        out.append((st, g.download_fields(), g.timing()["fused_sweeps"]))
+    (sa, fa, na), (sb, fb, nb) = out
+    assert sa == sb, (sa, sb)
+    assert na == 0 and nb > 0, (na, nb)
+    for k in L.FIELDS:
+        assert np.array_equal(fa[k], fb[k]), k
