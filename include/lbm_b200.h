@@ -46,7 +46,11 @@ typedef enum {
 
 typedef enum {
     LBM_PRECISION_FP64 = 0,      /* plain FP64, reference operation order: the drop-in */
-    LBM_PRECISION_MIXED = 1      /* FP32 populations as deviations + FP64 reductions */
+    LBM_PRECISION_MIXED = 1      /* FP32 populations as deviations + FP64 reductions.  Its
+                                    plain Poisson sweeps stall at a relative change near 1e-7:
+                                    for tighter tolerances select LBM_POISSON_REFINE, or the
+                                    loop runs to max_sweeps (forever with no cap, as the
+                                    reference's loop would) */
 } lbm_precision;
 
 typedef enum {
