@@ -1075,11 +1075,57 @@ def run_ours(args):
     return 0
 
 
+def refine_measure(n=64, steps=2, tol=1e-10):
+    """The mixed box at a tight Poisson stop (relative change `tol`, check
+    100) on the head-on workload at n^3 with the reference's slip walls: the
+    FP64 box to 1e-12 as the fixed point, then the FP64 box, the mixed box by
+    iterative refinement (LBM_POISSON_REFINE) and the plain mixed box (capped
+    at 4x the FP64 box's sweeps; its relative change stalls near 1e-7) to
+    `tol`.  Reports sweeps and Poisson ms per step, and each run's max-norm
+    relative error in p, u and phi against the fixed point."""
+    import lbm_b200 as L
+    p = workload_params(n)
+    p.DD, p.init_separation = n / 4.0, n / 2.0
+    p.periodic_x = 0
+    f = workload_fields(p)
+    runs = {}
+    fields = {}
+    cap = 0
+    for name, prec, form, t in (("fp64_fixed_point", "fp64", "kinetic", 1e-12), ("fp64", "fp64", "kinetic", tol),
+                                ("mixed_refine", "mixed", "refine", tol), ("mixed_plain", "mixed", "kinetic", tol)):
+        g = L.InamuroCUDA(p, f, precision=prec)
+        limit = cap if name == "mixed_plain" else 10_000_000
+        g.set_poisson(check_interval=100, tolerance=t, max_sweeps=limit, fail_on_limit=False)
+        if form != "kinetic":
+            g.set_poisson_form(form)
+        st = g.step(steps)
+        tm = g.timing()
+        sw = [int(s["iterations"]) for s in st]
+        runs[name] = {"sweeps_per_step": sw, "converged": [int(s["converged"]) for s in st],
+                      "poisson_ms_per_step": tm["poisson_ms"] / steps,
+                      "ms_per_sweep": tm["poisson_ms"] / max(1, sum(sw))}
+        fields[name] = g.download_fields()
+        g.close()
+        if name == "fp64":
+            cap = 4 * (max(sw) // 100 + 1) * 100
+    ref = fields["fp64_fixed_point"]
+    for name in ("fp64", "mixed_refine", "mixed_plain"):
+        runs[name]["rel_err_vs_fixed_point"] = {
+            k: float(np.max(np.abs(fields[name][k] - ref[k])) / max(float(np.max(np.abs(ref[k]))), 1e-300))
+            for k in ("p", "u", "phi")}
+    runs["speedup_refine_vs_fp64"] = runs["fp64"]["poisson_ms_per_step"] / runs["mixed_refine"]["poisson_ms_per_step"]
+    runs["config"] = {"workload": f"head-on droplet pair {n}^3 (R={n / 8:g}, {n / 2:g} apart, +-0.02, "
+                                  f"rho_L/rho_G=100), slip walls", "steps": steps, "tolerance": tol,
+                      "check_interval": 100}
+    return runs
+
+
 def extra_legs(args, line):
     """Bounded samples of the other measurements, in the default line: the
     reference's own GPU step beside this library's (reference_gpu), the
     adjoint calibration run with its adjoint/forward cost and finite-difference
-    checks (adjoint), and the batched droplet oscillation (batch)."""
+    checks (adjoint), the batched droplet oscillation (batch), and the mixed
+    box at a tight Poisson stop by iterative refinement (refine)."""
     import copy
     try:
         # 128^3, one step: the reference program needs ~20 ms per sweep at
@@ -1105,6 +1151,10 @@ def extra_legs(args, line):
                                            "roofline", "tuning", "gpu_launches", "converged", "config")}
     except Exception as e:
         line["batch"] = {"unavailable": str(e)[:300]}
+    try:
+        line["refine"] = refine_measure()
+    except Exception as e:
+        line["refine"] = {"unavailable": str(e)[:300]}
 
 
 def run_phase_timing(args):
