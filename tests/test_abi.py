@@ -87,3 +87,14 @@ def test_python_structs_match_the_header_layout(tmp_path):
         assert int(got[cname]) == ctypes.sizeof(cls), cname
         for f, _ in cls._fields_:
             assert int(got[f"{cname}.{f}"]) == getattr(cls, f).offset, (cname, f)
+
+
+def test_python_poisson_form_names_match_the_header_enum():
+    """Every lbm_poisson_form value the header declares has its Python name
+    with the same value (and no Python name has a value the header lacks)."""
+    import re
+    hdr = open(os.path.join(os.path.dirname(L.LIB_PATH), "..", "include", "lbm_b200.h")).read()
+    body = hdr[hdr.index("LBM_POISSON_KINETIC"):hdr.index("} lbm_poisson_form;")]
+    values = {int(v) for v in re.findall(r"LBM_POISSON_[A-Z_]+\s*=\s*(\d+)", body)}
+    assert values == set(L.InamuroCUDA.POISSON_FORMS.values()), (values, L.InamuroCUDA.POISSON_FORMS)
+    assert L.InamuroCUDA.POISSON_FORMS["refine"] == 6
